@@ -1,0 +1,195 @@
+"""Problem setups that call the LGF-FMM path: domain configurations, refinement
+predicates and source / exact fields, in the roles the reference's setups and
+tests play (tests/poisson/vortexrings.hpp, tests/conv_test/ffmTest.cpp).
+
+Everything here is host-side numpy that produces inputs for the solver; the
+solver itself lives in the CUDA library. Fields are numpy arrays of shape
+(n_octants, Nb, Nb, Nb) indexed [octant][z][y][x] (x fastest in memory), i.e.
+the reference's column-major Nb^3 blocks with their one-cell buffers.
+"""
+import numpy as np
+
+
+# --------------------------------------------------------------------------
+# Vortex-ring manufactured solution (tests/poisson/vortexrings.hpp:50-145)
+def vortex_ring_psi_lap(x, y, z, R, c1, c2):
+    """psi = c1 exp(-c2 / (1 - t^2)), t = dist(ring)/R, and its analytic
+    Laplacian (chain rule in s = t^2), zero outside the torus t >= 1."""
+    r = np.sqrt(x * x + y * y)
+    s = ((r - R) ** 2 + z * z) / R ** 2
+    inside = s < 1.0
+    sc = np.where(inside, s, 0.0)
+    om = 1.0 - sc
+    psi = np.where(inside, c1 * np.exp(-c2 / om), 0.0)
+    ps = psi * (-c2 / om ** 2)
+    pss = psi * (c2 * c2 / om ** 4 - 2.0 * c2 / om ** 3)
+    rr = np.where(r > 0, r, 1.0)
+    lap = ps * (6.0 / R ** 2 - 2.0 / (rr * R)) + pss * 4.0 * sc / R ** 2
+    return psi, np.where(inside, lap, 0.0)
+
+
+class VortexRingPoisson:
+    """tests/poisson/configs/config_1_lv_{0,1}: 192^3 bounding box, 96^3 block
+    region of 6^3 blocks, Lx = 2.5, one ring R = 0.125, c1 = 1e6, c2 = 15,
+    refinement_factor 0.125, EXP_LInf 0.0116450 (nLevels 0) / 1e-2 (nLevels 1).
+    """
+
+    def __init__(self, n_levels=0, block_extent=6):
+        self.bd_base = (-96, -96, -96)
+        self.bd_extent = (192, 192, 192)
+        self.block_extent = block_extent
+        self.dx_base = 2.5 / 192.0
+        self.blocks = [((-48, -48, -48), (96, 96, 96))]
+        self.n_levels = n_levels
+        self.R, self.c1, self.c2 = 0.125, 1.0e6, 15.0
+        self.refinement_factor = 0.125
+        self.exp_linf = 0.0116450 if n_levels == 0 else 1e-2
+        # bounding box centre in base cells, (max - min) / 2 + min
+        self.center = (self.bd_base[0] + self.bd_extent[0] - 1 - self.bd_base[0]) / 2.0 + self.bd_base[0]
+        _, lap = vortex_ring_psi_lap(np.array([self.R]), np.array([0.0]), np.array([0.0]),
+                                     self.R, self.c1, self.c2)
+        self.source_max = abs(float(lap[0]))
+
+    def _xyz(self, base, n, rl, lo=0):
+        sc = 2 ** rl
+        dxl = self.dx_base / sc
+        i = np.arange(n) + lo
+        c = self.center * sc
+        return ((base[0] + i - c + 0.5) * dxl, (base[1] + i - c + 0.5) * dxl,
+                (base[2] + i - c + 0.5) * dxl)
+
+    def predicate(self, base, extent, rl, diff_level):
+        """vortexrings.hpp:481-517: refine if |source| exceeds
+        source_max * refinement_factor^diff_level on the block grown by 2."""
+        e = extent[0]
+        X, Y, Z = self._xyz(base, e + 4, rl, lo=-2)
+        _, lap = vortex_ring_psi_lap(X[:, None, None], Y[None, :, None], Z[None, None, :],
+                                     self.R, self.c1, self.c2)
+        return bool((np.abs(lap) > self.source_max * self.refinement_factor ** diff_level).any())
+
+    def fields(self, octs):
+        """Source on every leaf and the exact solution, interior nodes only."""
+        Nb, e = self.block_extent + 2, self.block_extent
+        src = np.zeros((octs.n, Nb, Nb, Nb))
+        ex = np.zeros_like(src)
+        for o in range(octs.n):
+            if not octs.leaf[o]:
+                continue
+            rl = int(octs.levels[o]) - octs.base_level
+            X, Y, Z = self._xyz(octs.bbase[o], e, rl)
+            p, lap = vortex_ring_psi_lap(X[None, None, :], Y[None, :, None], Z[:, None, None],
+                                         self.R, self.c1, self.c2)
+            src[o, 1:-1, 1:-1, 1:-1] = lap
+            ex[o, 1:-1, 1:-1, 1:-1] = p
+        return src, ex
+
+    def finest_linf(self, octs, num, ex):
+        L = octs.depth - 1
+        err = 0.0
+        for o in range(octs.n):
+            if octs.levels[o] != L or not octs.leaf[o] or octs.correction[o]:
+                continue
+            err = max(err, float(np.abs(num[o, 1:-1, 1:-1, 1:-1] - ex[o, 1:-1, 1:-1, 1:-1]).max()))
+        return err
+
+
+# --------------------------------------------------------------------------
+# Gaussian-source Poisson problems (the LGF-FMM benchmark workloads)
+class GaussianPoisson:
+    """Unbounded 3-D Poisson problem with a sum-of-Gaussians source sampled at
+    cell centres, x = (i + 0.5) dx_level in level cell units, origin at the
+    centre of the block region.
+
+    uniform_64:  4x4x4 blocks of 16^3 cells (64^3 cells), dx = 1, one level;
+                 source = +exp(-|x-c+|^2/32) - exp(-|x-c-|^2/32), c = (+-12,0,0).
+    amr_3level:  8x8x8 base blocks of 16^3 cells, two refinement levels where
+                 |f| > 1e-3 max|f| (base -> 1) and > 1e-2 max|f| (1 -> 2) on
+                 the block grown by 2 cells; source = the uniform_64 pair plus
+                 16 Gaussians, sigma ~ U[2, 6] cells, amplitude ~ U[-1, 1],
+                 centres uniform in the inner 50% of the block region
+                 (numpy PCG64, seed 20261203).
+    """
+
+    def __init__(self, name="uniform_64", block_extent=16, seed=20261203):
+        self.name = name
+        self.block_extent = block_extent
+        self.dx_base = 1.0
+        g = [(1.0, 4.0, (12.0, 0.0, 0.0)), (-1.0, 4.0, (-12.0, 0.0, 0.0))]
+        if name == "uniform_64":
+            half = 32
+            self.n_levels = 0
+        elif name == "amr_3level":
+            half = 64
+            self.n_levels = 2
+            rng = np.random.Generator(np.random.PCG64(seed))
+            for _ in range(16):
+                sig = rng.uniform(2.0, 6.0)
+                amp = rng.uniform(-1.0, 1.0)
+                c = rng.uniform(-half / 2.0, half / 2.0, size=3)
+                g.append((amp, sig, tuple(c)))
+        else:
+            raise ValueError(name)
+        self.gaussians = g
+        self.bd_base = (-2 * half,) * 3
+        self.bd_extent = (4 * half,) * 3
+        self.blocks = [((-half,) * 3, (2 * half,) * 3)]
+        self.fmax = self._fmax()
+
+    def f(self, X, Y, Z):
+        out = np.zeros(np.broadcast(X, Y, Z).shape)
+        for a, s, c in self.gaussians:
+            out += a * np.exp(-((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) / (2.0 * s * s))
+        return out
+
+    def _fmax(self):
+        x = np.arange(-self.blocks[0][1][0] // 2, self.blocks[0][1][0] // 2) + 0.5
+        return float(np.abs(self.f(x[:, None, None], x[None, :, None], x[None, None, :])).max())
+
+    def _xyz(self, base, n, rl, lo=0):
+        dxl = self.dx_base / 2 ** rl
+        i = np.arange(n) + lo
+        return ((base[0] + i + 0.5) * dxl, (base[1] + i + 0.5) * dxl, (base[2] + i + 0.5) * dxl)
+
+    def predicate(self, base, extent, rl, diff_level):
+        e = extent[0]
+        X, Y, Z = self._xyz(base, e + 4, rl, lo=-2)
+        thresh = self.fmax * (1e-3 if rl == 0 else 1e-2)
+        return bool((np.abs(self.f(X[:, None, None], Y[None, :, None], Z[None, None, :])) > thresh).any())
+
+    def fields(self, octs):
+        Nb, e = self.block_extent + 2, self.block_extent
+        src = np.zeros((octs.n, Nb, Nb, Nb))
+        for o in range(octs.n):
+            if not octs.leaf[o]:
+                continue
+            rl = int(octs.levels[o]) - octs.base_level
+            X, Y, Z = self._xyz(octs.bbase[o], e, rl)
+            src[o, 1:-1, 1:-1, 1:-1] = self.f(X[None, None, :], Y[None, :, None], Z[:, None, None])
+        return src
+
+    def n_cells(self, octs):
+        """Cells per solve: leaf blocks (correction leaves included) x e^3,
+        the reference's get_nPoints (domain.hpp:1218-1248)."""
+        return int(np.count_nonzero(octs.leaf)) * self.block_extent ** 3
+
+
+class ImpulseFmm:
+    """tests/conv_test/configs/configFFMTest: 48^3 domain, block_extent 6,
+    nLevels 0; unit impulse at local (1,1,1) of the first non-correction leaf
+    in key order; the base-level FMM must reproduce LGF_GL::get."""
+
+    def __init__(self, dx_base=1.0):
+        self.bd_base = (-24, -24, -24)
+        self.bd_extent = (48, 48, 48)
+        self.block_extent = 6
+        self.dx_base = dx_base
+        self.blocks = [((-24, -24, -24), (48, 48, 48))]
+        self.n_levels = 0
+
+    def source(self, octs):
+        Nb = self.block_extent + 2
+        src = np.zeros((octs.n, Nb, Nb, Nb))
+        order = np.argsort(octs.keys, kind="stable")
+        i0 = next(int(i) for i in order if octs.leaf[i] and not octs.correction[i])
+        src[i0, 1, 1, 1] = 1.0
+        return src, i0, np.array(octs.bbase[i0])

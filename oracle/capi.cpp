@@ -1,0 +1,204 @@
+// ORACLE (test infrastructure): plain C entry points used by tests/ (ctypes),
+// __graft_entry__.smoke() and bench.py's cpu_baseline leg.
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+
+#include "orc.hpp"
+
+using namespace orc;
+
+namespace
+{
+thread_local std::string g_err;
+struct Handle
+{
+    std::unique_ptr<Domain> d;
+    std::unique_ptr<Solver> s;
+};
+template<class F>
+int guard(F&& f)
+{
+    try
+    {
+        f();
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 1;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+double orc_lgf_get(int x, int y, int z) { return lgf_get(x, y, z); }
+
+int orc_lgf_table_size() { return lgf_table_size(); }
+
+void orc_lgf_table(double* out) { std::memcpy(out, lgf_table().data(), sizeof(double) * lgf_table().size()); }
+
+void orc_bessel_ie(double x, int nmax, double* out) { bessel_ie_all(x, nmax, out); }
+
+void orc_nli_matrix(int Nb, int pts_cap, double* out) { nli_matrix(Nb, pts_cap, out); }
+
+void orc_cc_matrix(int Nb, int pts_cap, int relpos, double* out) { cc_matrix(Nb, pts_cap, relpos, out); }
+
+void* orc_domain_create(const int* bd_base, const int* bd_extent, int block_extent, double dx_base,
+                        int n_blocks, const int* block_base, const int* block_ext)
+{
+    auto* h = new Handle;
+    if (guard([&] {
+            h->d = domain_create(bd_base, bd_extent, block_extent, dx_base, n_blocks, block_base,
+                                 block_ext);
+        }))
+    {
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+void orc_domain_destroy(void* h) { delete static_cast<Handle*>(h); }
+
+int orc_domain_init_refine(void* hp, int nRef, int global_refinement, RefinePred pred, void* user)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] { h->d->init_refine(nRef, global_refinement, pred, user); });
+}
+
+// canonical order, masks (AMR2AMR for every refinement level, STREAM)
+int orc_domain_finalize(void* hp, int subtract_non_leaf)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        h->d->construct_level_maps();
+        h->d->construct_lists();
+        h->d->finalize();
+        fmm_lgf_mask_build(*h->d, subtract_non_leaf != 0);
+        fmm_stream_mask_build(*h->d);
+    });
+}
+
+int orc_domain_info(void* hp, int* base_level, int* depth, int* n_octants)
+{
+    auto* h = static_cast<Handle*>(hp);
+    *base_level = h->d->base_level;
+    *depth = h->d->depth;
+    *n_octants = (int)h->d->octs.size();
+    return 0;
+}
+
+// flags: bit0 leaf, bit1 correction
+int orc_domain_octants(void* hp, unsigned long long* keys, int* levels, int* flags, int* bbase)
+{
+    auto* h = static_cast<Handle*>(hp);
+    for (size_t i = 0; i < h->d->octs.size(); ++i)
+    {
+        Octant* o = h->d->octs[i];
+        keys[i] = o->key;
+        levels[i] = o->level;
+        flags[i] = (o->leaf ? 1 : 0) | (o->correction ? 2 : 0);
+        for (int d = 0; d < 3; ++d) bbase[3 * i + d] = o->bbase[d];
+    }
+    return 0;
+}
+
+// neighbour (27 per octant) and influence (189 per octant) lists as canonical
+// indices, -1 for absent
+int orc_domain_lists(void* hp, int* nbr, int* infl, int* n_infl)
+{
+    auto* h = static_cast<Handle*>(hp);
+    for (size_t i = 0; i < h->d->octs.size(); ++i)
+    {
+        Octant* o = h->d->octs[i];
+        for (int j = 0; j < 27; ++j) nbr[27 * i + j] = o->neighbor[j] ? o->neighbor[j]->idx : -1;
+        for (int j = 0; j < 189; ++j)
+            infl[189 * i + j] = (j < o->n_infl && o->influence[j]) ? o->influence[j]->idx : -1;
+        n_infl[i] = o->n_infl;
+    }
+    return 0;
+}
+
+int orc_domain_masks(void* hp, int mask_idx, unsigned char* out)
+{
+    auto* h = static_cast<Handle*>(hp);
+    for (size_t i = 0; i < h->d->octs.size(); ++i)
+    {
+        out[2 * i] = h->d->octs[i]->mask[mask_idx][0];
+        out[2 * i + 1] = h->d->octs[i]->mask[mask_idx][1];
+    }
+    return 0;
+}
+
+int orc_solver_create(void* hp, int intrp_order)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] { h->s = std::make_unique<Solver>(h->d.get(), intrp_order); });
+}
+
+int orc_fmm_apply(void* hp, const double* src, double* tgt, int level, int nlas, double scale,
+                  int fmm_type)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Field s(src, src + n), t(tgt, tgt + n);
+        h->s->fmm_apply(s, t, level, nlas != 0, scale, fmm_type);
+        std::memcpy(tgt, t.data(), n * sizeof(double));
+    });
+}
+
+int orc_apply_lgf(void* hp, const double* src, double* tgt, int use_correction, int subtract_non_leaf)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Field s(src, src + n), t(tgt, tgt + n);
+        h->s->apply_lgf(s, t, AMR2AMR, use_correction != 0, subtract_non_leaf != 0);
+        std::memcpy(tgt, t.data(), n * sizeof(double));
+    });
+}
+
+// Single-block linear convolution with the reference's Convolution contract
+// (convolution.hpp:225-304): kernel holds P^3 values (P = 2Nb-1, x fastest),
+// out (Nb^3) += scale * window[Nb-1, 2Nb-2]^3 of (kernel (*) zero-padded src).
+int orc_block_conv(int Nb, const double* src, const double* kernel, double* out, double scale)
+{
+    return guard([&] {
+        const int P = 2 * Nb - 1;
+        Fft1d f(P);
+        std::vector<cplx> a((size_t)P * P * P, 0.0), b((size_t)P * P * P);
+        for (int k = 0; k < Nb; ++k)
+            for (int j = 0; j < Nb; ++j)
+                for (int i = 0; i < Nb; ++i)
+                    a[i + (size_t)P * (j + (size_t)P * k)] = src[i + (size_t)Nb * (j + (size_t)Nb * k)];
+        for (size_t i = 0; i < b.size(); ++i) b[i] = kernel[i];
+        std::vector<cplx> w(3 * P);
+        auto f3 = [&](std::vector<cplx>& x, bool fw) {
+            for (int k = 0; k < P; ++k)
+                for (int j = 0; j < P; ++j) f.run(&x[(size_t)P * (j + (size_t)P * k)], 1, fw, w.data());
+            for (int k = 0; k < P; ++k)
+                for (int i = 0; i < P; ++i) f.run(&x[i + (size_t)P * P * k], P, fw, w.data());
+            for (int j = 0; j < P; ++j)
+                for (int i = 0; i < P; ++i) f.run(&x[i + (size_t)P * j], P * P, fw, w.data());
+        };
+        f3(a, true);
+        f3(b, true);
+        const double s = scale / ((double)P * P * P);
+        for (size_t i = 0; i < a.size(); ++i) a[i] = a[i] * b[i] * s;
+        f3(a, false);
+        for (int k = 0; k < Nb; ++k)
+            for (int j = 0; j < Nb; ++j)
+                for (int i = 0; i < Nb; ++i)
+                    out[i + (size_t)Nb * (j + (size_t)Nb * k)] +=
+                        a[(i + Nb - 1) + (size_t)P * ((j + Nb - 1) + (size_t)P * (k + Nb - 1))].real();
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle_iblgf.so).
+
+Test infrastructure: used by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py only.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(ROOT, "oracle", "liboracle_iblgf.so")
+
+PRED_T = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                          ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_lgf_get.restype = cd
+        L.orc_lgf_get.argtypes = [ci, ci, ci]
+        L.orc_lgf_table_size.restype = ci
+        L.orc_lgf_table.argtypes = [vp]
+        L.orc_bessel_ie.argtypes = [cd, ci, vp]
+        L.orc_nli_matrix.argtypes = [ci, ci, vp]
+        L.orc_cc_matrix.argtypes = [ci, ci, ci, vp]
+        L.orc_domain_create.restype = vp
+        L.orc_domain_create.argtypes = [vp, vp, ci, cd, ci, vp, vp]
+        L.orc_domain_destroy.argtypes = [vp]
+        L.orc_domain_init_refine.argtypes = [vp, ci, ci, PRED_T, vp]
+        L.orc_domain_finalize.argtypes = [vp, ci]
+        L.orc_domain_info.argtypes = [vp, vp, vp, vp]
+        L.orc_domain_octants.argtypes = [vp, vp, vp, vp, vp]
+        L.orc_domain_lists.argtypes = [vp, vp, vp, vp]
+        L.orc_domain_masks.argtypes = [vp, ci, vp]
+        L.orc_solver_create.argtypes = [vp, ci]
+        L.orc_fmm_apply.argtypes = [vp, vp, vp, ci, ci, cd, ci]
+        L.orc_apply_lgf.argtypes = [vp, vp, vp, ci, ci]
+        L.orc_block_conv.argtypes = [ci, vp, vp, vp, cd]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+
+
+def lgf_get(x, y, z):
+    return lib().orc_lgf_get(int(x), int(y), int(z))
+
+
+def block_conv(src, kernel, scale=1.0):
+    """Single-block convolution (reference Convolution contract)."""
+    Nb = src.shape[0]
+    out = np.zeros(Nb ** 3)
+    _check(lib().orc_block_conv(Nb, _p(np.ascontiguousarray(src.ravel(order="F"))),
+                                _p(np.ascontiguousarray(kernel.ravel(order="F"))), _p(out), scale))
+    return out.reshape((Nb,) * 3, order="F")
+
+
+class Domain:
+    """Oracle domain: base mesh, refinement, correction marking, masks."""
+
+    def __init__(self, bd_base, bd_extent, block_extent, dx_base, blocks, n_levels=0,
+                 global_refinement=0, predicate=None, subtract_non_leaf=False, intrp_order=5):
+        L = lib()
+        bb = np.array([b[0] for b in blocks], dtype=np.int32).ravel()
+        be = np.array([b[1] for b in blocks], dtype=np.int32).ravel()
+        self.h = L.orc_domain_create(_p(np.array(bd_base, np.int32)), _p(np.array(bd_extent, np.int32)),
+                                     int(block_extent), float(dx_base), len(blocks), _p(bb), _p(be))
+        if not self.h:
+            raise RuntimeError("oracle: " + L.orc_last_error().decode())
+        self.block_extent = block_extent
+        self.Nb = block_extent + 2
+        self._cb = None
+        if n_levels > 0 or global_refinement > 0:
+            if predicate is not None:
+                def cb(user, base, ext, rl, diff):
+                    return 1 if predicate((base[0], base[1], base[2]), (ext[0], ext[1], ext[2]),
+                                          rl, diff) else 0
+                self._cb = PRED_T(cb)
+            else:
+                self._cb = PRED_T(lambda *a: 0)
+            _check(L.orc_domain_init_refine(self.h, n_levels, global_refinement, self._cb, None))
+        else:
+            # init_refine with nothing to refine still marks corrections
+            self._cb = PRED_T(lambda *a: 0)
+            _check(L.orc_domain_init_refine(self.h, 0, 0, self._cb, None))
+        _check(L.orc_domain_finalize(self.h, 1 if subtract_non_leaf else 0))
+        bl, dp, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.orc_domain_info(self.h, ctypes.byref(bl), ctypes.byref(dp), ctypes.byref(n))
+        self.base_level, self.depth, self.n = bl.value, dp.value, n.value
+        self.keys = np.zeros(self.n, np.uint64)
+        self.levels = np.zeros(self.n, np.int32)
+        self.flags = np.zeros(self.n, np.int32)
+        self.bbase = np.zeros((self.n, 3), np.int32)
+        L.orc_domain_octants(self.h, _p(self.keys), _p(self.levels), _p(self.flags), _p(self.bbase))
+        _check(L.orc_solver_create(self.h, intrp_order))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_domain_destroy(self.h)
+            self.h = None
+
+    @property
+    def leaf(self):
+        return (self.flags & 1) != 0
+
+    @property
+    def correction(self):
+        return (self.flags & 2) != 0
+
+    def lists(self):
+        nbr = np.zeros((self.n, 27), np.int32)
+        infl = np.zeros((self.n, 189), np.int32)
+        ni = np.zeros(self.n, np.int32)
+        lib().orc_domain_lists(self.h, _p(nbr), _p(infl), _p(ni))
+        return nbr, infl, ni
+
+    def masks(self, mask_idx):
+        out = np.zeros((self.n, 2), np.uint8)
+        lib().orc_domain_masks(self.h, int(mask_idx), _p(out))
+        return out
+
+    def zeros(self):
+        return np.zeros((self.n, self.Nb, self.Nb, self.Nb))  # [oct][z][y][x]
+
+    def fmm_apply(self, src, tgt, level, non_leaf_as_source, scale=1.0, fmm_type=1):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        out = np.ascontiguousarray(tgt, dtype=np.float64).copy()
+        _check(lib().orc_fmm_apply(self.h, _p(src), _p(out), int(level), int(non_leaf_as_source),
+                                   float(scale), int(fmm_type)))
+        return out
+
+    def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        out = self.zeros() if tgt is None else np.ascontiguousarray(tgt, dtype=np.float64).copy()
+        _check(lib().orc_apply_lgf(self.h, _p(src), _p(out), int(use_correction),
+                                   int(subtract_non_leaf)))
+        return out
