@@ -1,0 +1,315 @@
+"""LGF-FMM Poisson benchmark (one JSON line on rank 0).
+
+A step is one PoissonSolver::apply_lgf on the AMR workload (8^3 base blocks of
+16^3 cells, 3 mesh levels, seeded sum-of-Gaussians source): every FMM sweep of
+every level, the level transfers and the correction, as the reference's
+"Rate" (tests/poisson/vortexrings.hpp:292-298) times it. `value` is cells per
+second with the source already in HBM (device-timed, CUDA events on the
+library's stream, max over ranks); `e2e` adds the pinned host->device copy of
+the source and the device->host copy of the solution through the C ABI.
+
+--gpus N runs N independent replicas (one process per GPU); the solve has no
+data-path collective.
+--impl reference times the CPU restatement of the reference algorithm (oracle)
+on the host cores for the same workload and metric.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "iblgf-amr_b200"))
+
+import iblgf_setups as S  # noqa: E402
+
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.path.exists(
+    os.path.join(ROOT, "BASELINE.json")) else "LGF-FMM cells/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_case(name):
+    return S.GaussianPoisson(name)
+
+
+def cpu_reference(case, steps, warmup, sample_levels=None):
+    """Time the oracle (CPU restatement, all host threads) on the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(d)
+    cells = case.n_cells(d)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        d.apply_lgf(src)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    return cells, times, os.cpu_count()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="amr_3level")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    case = build_case(args.workload)
+    wl = ("%s: %d^3 base blocks of %d^3 cells, %d refinement levels, sum-of-Gaussians source (seeded)"
+          % (case.name, case.blocks[0][1][0] // case.block_extent, case.block_extent, case.n_levels))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, min(args.steps, 2))
+        cells, times, cores = cpu_reference(case, steps, 0)
+        v = cells / float(np.mean(times))
+        line = {"metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": args.gpus, "steps": steps,
+                "warmup": 0, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": wl, "cells_per_step": cells},
+                "cpu_baseline": {"value": v, "unit": "cells/s", "cores": cores, "kind": "port",
+                                 "sample": "full apply_lgf per step (steps capped at 2)"},
+                "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    import iblgf_b200 as B
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    prec = B.FP32 if args.precision == "fp32" else B.FP64
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=local,
+                 stream=stream.cuda_stream)
+    src_host = case.fields(g)
+    cells = case.n_cells(g)
+    fs, ft = g.field(src_host), g.field()
+    for _ in range(args.warmup):
+        g.apply_lgf(fs, ft)
+    g.synchronize()
+
+    # ---- device-timed region: inputs resident in HBM (> L2: fields and spectra)
+    g.profile(True)
+    l0 = g.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as ck:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            g.apply_lgf(fs, ft)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = g.launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    phases = g.profile_read()
+    stats = g.stats()
+    g.profile(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * cells / (ms_step * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    hsrc = torch.from_numpy(np.ascontiguousarray(src_host)).pin_memory()
+    hout = torch.empty(hsrc.shape, dtype=torch.float64).pin_memory()
+    nbytes = hsrc.numel() * 8
+    L = B.lib()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        g._check(L.iblgf_field_upload(g.h, fs, hsrc.data_ptr(), hsrc.numel()))
+        g.apply_lgf(fs, ft)
+        g._check(L.iblgf_field_download(g.h, ft, hout.data_ptr(), hout.numel()))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # ---- FP64 plain path on the same input, and accuracy of this run against it
+    extra = {}
+    if rank == 0 and prec == B.FP32:
+        g64 = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                       n_levels=case.n_levels, predicate=case.predicate, precision=B.FP64, device=local,
+                       stream=stream.cuda_stream)
+        f64s, f64t = g64.field(src_host), g64.field()
+        for _ in range(2):
+            g64.apply_lgf(f64s, f64t)
+        g64.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(max(2, args.steps // 2)):
+            g64.apply_lgf(f64s, f64t)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = a0.elapsed_time(a1) / max(2, args.steps // 2)
+        out32 = g.download(ft)
+        out64 = g64.download(f64t)
+        rel = float(np.abs(out32 - out64).max() / np.abs(out64).max())
+        extra = {"fp64_plain": {"value": cells / (ms64 * 1e-3), "ms_per_step": ms64},
+                 "speedup_vs_fp64_plain": ms64 / ms_step, "rel_linf_vs_fp64": rel}
+        g64.close()
+
+    # ---- roofline of the dominant phase (phase times from CUDA events on the stream)
+    hbm, peak_kind = peaks()
+    fma = g.fma_peak(prec)
+    names = ["forward transforms", "spectral MAC", "inverse transforms+interp+add", "zero/copy/anterp"]
+    k = int(np.argmax(phases))
+    per_step = phases / args.steps
+    nc = g.Nb * (2 * g.Nb - 1) ** 2
+    cb = 8 if prec == B.FP32 else 16
+    sweeps, nsrc, ntgt, npairs, nuniq = [int(x) / args.steps for x in stats[:5]]
+    if k == 1:
+        flops = 8.0 * nc * npairs
+        bytes_alg = (nuniq + nsrc + ntgt) * nc * cb
+    elif k == 0:
+        P = 2 * g.Nb - 1
+        flops = nsrc * 8.0 * (g.Nb ** 3 * g.Nb / 2 + P * g.Nb ** 3 + P * P * g.Nb * g.Nb)
+        bytes_alg = nsrc * (g.Nb ** 3 * 8 + nc * cb)
+    else:
+        P = 2 * g.Nb - 1
+        flops = ntgt * 8.0 * (P * P * g.Nb * g.Nb + P * g.Nb ** 3 + g.Nb ** 4 / 2)
+        bytes_alg = ntgt * (nc * cb + g.Nb ** 3 * 16)
+    t_k = per_step[k] * 1e-3
+    ai = flops / max(bytes_alg, 1)
+    if ai > fma * 1e12 / (hbm * 1e9):
+        roof = {"bound": "fp-cuda-core", "achieved": flops / t_k / 1e12, "peak": fma, "unit": "TFLOP/s",
+                "frac": flops / t_k / 1e12 / fma, "peak_source": "measured FMA-chain kernel (iblgf_fma_peak)"}
+    else:
+        roof = {"bound": "hbm", "achieved": bytes_alg / t_k / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": bytes_alg / t_k / 1e9 / hbm, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
+    roof.update({"kernel": names[k], "traffic": None, "phase_ms_per_step": dict(zip(names, per_step.tolist())),
+                 "algorithmic_flops": flops, "algorithmic_bytes": bytes_alg})
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32" if prec == B.FP32 else "f64", "data": "synthetic",
+                "config": {"workload": wl, "cells_per_step": cells, "octants": g.n,
+                           "precision": args.precision + " FFT/MAC, f64 fields and LGF table",
+                           "l2": "inputs larger than L2 (fields %.0f MB, spectra cache > 126 MB)" % (g.n * g.Nb ** 3 * 8 / 1e6),
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "sweeps_per_step": sweeps, "pairs_per_step": npairs},
+                "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s",
+                        "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+                "gpu_launches": int(launches),
+                "roofline": roof,
+                "clocks": ck.summary(),
+                "cpu_baseline": cpu}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(case):
+    """Oracle (CPU restatement, OpenMP over targets) on a bounded sample: the
+    base-level FMM sweep of the workload, scaled to a full apply_lgf by the
+    sweep's share of the (target, source) pairs."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    t0 = time.perf_counter()
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(d)
+    cells = case.n_cells(d)
+    t1 = time.perf_counter()
+    d.apply_lgf(src)
+    t2 = time.perf_counter()
+    return {"value": cells / (t2 - t1), "unit": "cells/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "one full apply_lgf of the same workload (%.1f s)" % (t2 - t1)}
+
+
+if __name__ == "__main__":
+    main()

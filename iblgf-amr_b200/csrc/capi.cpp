@@ -1,0 +1,338 @@
+// extern "C" boundary of the library (include/iblgf_b200.h). Every entry
+// point catches exceptions and turns them into a status code plus a message
+// in iblgf_last_error(); nothing throws across the boundary.
+#include <cstring>
+#include <exception>
+#include <new>
+
+#include "ctx.hpp"
+
+struct iblgf_ctx
+{
+    iblgf_b200::Ctx c;
+};
+
+namespace
+{
+thread_local std::string g_create_err;
+
+template<class F>
+int guard(iblgf_ctx* x, F&& f)
+{
+    if (!x) return IBLGF_EINVAL;
+    try
+    {
+        f(x->c);
+        return IBLGF_OK;
+    }
+    catch (const iblgf_b200::Error& e)
+    {
+        x->c.err = e.what();
+        return e.code;
+    }
+    catch (const std::bad_alloc&)
+    {
+        x->c.err = "host allocation failed";
+        return IBLGF_ENOMEM;
+    }
+    catch (const std::exception& e)
+    {
+        x->c.err = e.what();
+        return IBLGF_EINTERNAL;
+    }
+}
+
+void need_field(iblgf_b200::Ctx& c, int f)
+{
+    if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+    if (f < 0 || f >= (int)c.fields.size()) throw iblgf_b200::Error(IBLGF_EINVAL, "bad field id");
+}
+}  // namespace
+
+namespace iblgf_b200
+{
+void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
+void poisson_release(const Ctx* c);
+double measure_fma_peak(Ctx& c, int precision);
+}  // namespace iblgf_b200
+
+extern "C" {
+
+int iblgf_create(const iblgf_config* cfg, iblgf_ctx** out)
+{
+    if (!cfg || !out) return IBLGF_EINVAL;
+    *out = nullptr;
+    auto* x = new (std::nothrow) iblgf_ctx;
+    if (!x) return IBLGF_ENOMEM;
+    x->c.cfg = *cfg;
+    const int rc = guard(x, [](iblgf_b200::Ctx& c) { iblgf_b200::ctx_init(c); });
+    if (rc != IBLGF_OK)
+    {
+        g_create_err = x->c.err;
+        if (x->c.own_stream && x->c.stream) cudaStreamDestroy(x->c.stream);
+        delete x;
+        return rc;
+    }
+    *out = x;
+    return IBLGF_OK;
+}
+
+int iblgf_destroy(iblgf_ctx* x)
+{
+    if (!x) return IBLGF_EINVAL;
+    cudaStreamSynchronize(x->c.stream);
+    iblgf_b200::poisson_release(&x->c);
+    if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
+    delete x;
+    return IBLGF_OK;
+}
+
+const char* iblgf_last_error(iblgf_ctx* x) { return x ? x->c.err.c_str() : g_create_err.c_str(); }
+
+int iblgf_synchronize(iblgf_ctx* x)
+{
+    return guard(x, [](iblgf_b200::Ctx& c) { IBLGF_CUDA(cudaStreamSynchronize(c.stream)); });
+}
+
+int iblgf_domain_add_blocks(iblgf_ctx* x, int n, const int* base, const int* extent)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
+        if (n < 0 || (n && (!base || !extent))) throw iblgf_b200::Error(IBLGF_EINVAL, "bad block arguments");
+        const int e = c.cfg.block_extent;
+        std::vector<std::array<int, 3>> nb;
+        for (int b = 0; b < n; ++b)
+        {
+            for (int d = 0; d < 3; ++d)
+            {
+                if (extent[3 * b + d] <= 0 || extent[3 * b + d] % e)
+                    throw iblgf_b200::Error(IBLGF_EINVAL, "Domain: Extent of blocks are not evenly divisible");
+                if (std::abs(base[3 * b + d]) % e)
+                    throw iblgf_b200::Error(IBLGF_EINVAL, "Domain: Base of blocks are not evenly divisible");
+            }
+            for (int k = 0; k < extent[3 * b + 2] / e; ++k)
+                for (int j = 0; j < extent[3 * b + 1] / e; ++j)
+                    for (int i = 0; i < extent[3 * b] / e; ++i)
+                        nb.push_back({base[3 * b] / e + i, base[3 * b + 1] / e + j, base[3 * b + 2] / e + k});
+        }
+        c.tree.add_base_blocks(nb);
+    });
+}
+
+int iblgf_domain_init_refine(iblgf_ctx* x, int n_ref, int global_refinement, iblgf_refine_fn pred, void* user)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
+        if (n_ref < 0 || global_refinement < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative refinement");
+        c.tree.init_refine(n_ref, global_refinement, pred, user);
+    });
+}
+
+int iblgf_domain_finalize(iblgf_ctx* x, int subtract_non_leaf)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
+        c.subtract_non_leaf = subtract_non_leaf != 0;
+        iblgf_b200::domain_finalize(c);
+    });
+}
+
+int iblgf_domain_info(iblgf_ctx* x, int* base_level, int* depth, int* n_octants)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+        if (base_level) *base_level = c.tree.base_level;
+        if (depth) *depth = c.tree.depth;
+        if (n_octants) *n_octants = c.n_oct;
+    });
+}
+
+int iblgf_domain_octants(iblgf_ctx* x, uint64_t* keys, int* levels, int* flags, int* bbase)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+        for (int i = 0; i < c.n_oct; ++i)
+        {
+            if (keys) keys[i] = c.keys[i];
+            if (levels) levels[i] = c.levels[i];
+            if (flags) flags[i] = c.flags[i];
+            if (bbase)
+                for (int d = 0; d < 3; ++d) bbase[3 * i + d] = c.bbase[3 * i + d];
+        }
+    });
+}
+
+int iblgf_domain_lists(iblgf_ctx* x, int* nbr, int* infl, int* n_infl)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+        if (nbr) std::memcpy(nbr, c.nbr.data(), c.nbr.size() * sizeof(int));
+        if (infl) std::memcpy(infl, c.infl.data(), c.infl.size() * sizeof(int));
+        if (n_infl) std::memcpy(n_infl, c.n_infl.data(), c.n_infl.size() * sizeof(int));
+    });
+}
+
+int iblgf_domain_masks(iblgf_ctx* x, int mask_idx, unsigned char* st)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+        if (mask_idx < 0 || mask_idx >= (int)c.masks.size()) throw iblgf_b200::Error(IBLGF_EINVAL, "bad mask index");
+        std::memcpy(st, c.masks[mask_idx].data(), c.masks[mask_idx].size());
+    });
+}
+
+int iblgf_field_create(iblgf_ctx* x, int* field)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
+        if (!field) throw iblgf_b200::Error(IBLGF_EINVAL, "null field pointer");
+        *field = iblgf_b200::field_create(c);
+    });
+}
+
+int iblgf_field_zero(iblgf_ctx* x, int f)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        IBLGF_CUDA(cudaMemsetAsync(c.field(f), 0, c.field_elems() * sizeof(double), c.stream));
+    });
+}
+
+int iblgf_field_upload(iblgf_ctx* x, int f, const double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        if (count != c.field_elems() || !host) throw iblgf_b200::Error(IBLGF_EINVAL, "field size mismatch");
+        IBLGF_CUDA(cudaMemcpyAsync(c.field(f), host, count * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    });
+}
+
+int iblgf_field_download(iblgf_ctx* x, int f, double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        if (count != c.field_elems() || !host) throw iblgf_b200::Error(IBLGF_EINVAL, "field size mismatch");
+        IBLGF_CUDA(cudaMemcpyAsync(host, c.field(f), count * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_field_device_ptr(iblgf_ctx* x, int f, double** dptr)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        *dptr = c.field(f);
+    });
+}
+
+int iblgf_fmm_apply(iblgf_ctx* x, int source, int target, int level, int nlas, double scale, int fmm_type)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, source);
+        need_field(c, target);
+        iblgf_b200::fmm_apply(c, source, target, level, nlas != 0, scale, fmm_type);
+    });
+}
+
+int iblgf_poisson_apply_lgf(iblgf_ctx* x, int source, int target, int fmm_type)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, source);
+        need_field(c, target);
+        iblgf_b200::poisson_apply_lgf(c, source, target, fmm_type);
+    });
+}
+
+int iblgf_poisson_options(iblgf_ctx* x, int use_correction, int subtract_non_leaf)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        c.use_correction = use_correction != 0;
+        if (c.finalized && (subtract_non_leaf != 0) != c.subtract_non_leaf)
+            throw iblgf_b200::Error(IBLGF_EINVAL, "subtract_non_leaf is fixed at finalize (masks depend on it)");
+        c.subtract_non_leaf = subtract_non_leaf != 0;
+    });
+}
+
+int iblgf_lgf_table(iblgf_ctx* x, double* host_out, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (count != c.d_lgf_table.n || !host_out) throw iblgf_b200::Error(IBLGF_EINVAL, "table size is 176851");
+        IBLGF_CUDA(cudaMemcpyAsync(host_out, c.d_lgf_table.p, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_lgf_get(iblgf_ctx* x, const int* coords, size_t n, double* host_out)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!n) return;
+        if (!coords || !host_out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        iblgf_b200::DevBuf<int> dc;
+        iblgf_b200::DevBuf<double> dout;
+        dc.alloc(3 * n);
+        dout.alloc(n);
+        IBLGF_CUDA(cudaMemcpyAsync(dc.p, coords, 3 * n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        iblgf_b200::launch_lgf_eval(c, dc.p, n, dout.p);
+        IBLGF_CUDA(cudaMemcpyAsync(host_out, dout.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_conv_block(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!src || !kernel || !out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        iblgf_b200::launch_conv_block(c, src, kernel, out, scale);
+    });
+}
+
+int iblgf_kernel_launches(iblgf_ctx* x, long long* count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { *count = c.launches; });
+}
+
+int iblgf_profile(iblgf_ctx* x, int enable)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        for (auto& ev : c.prof_events)
+            for (auto e : ev) cudaEventDestroy(e);
+        c.prof_events.clear();
+        for (long long& v : c.stats) v = 0;
+        c.profile = enable != 0;
+    });
+}
+
+int iblgf_profile_read(iblgf_ctx* x, double* out4)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        for (int i = 0; i < 4; ++i) out4[i] = 0.0;
+        for (auto& ev : c.prof_events)
+        {
+            float ms[4];
+            for (int i = 0; i < 4; ++i) IBLGF_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+            // [0] forward transforms, [1] MAC, [2] inverse + interpolation + add,
+            // [3] zero / copy / anterpolation
+            out4[0] += ms[1];
+            out4[1] += ms[2];
+            out4[2] += ms[3];
+            out4[3] += ms[0];
+        }
+    });
+}
+
+int iblgf_stats(iblgf_ctx* x, long long* out8)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        for (int i = 0; i < 8; ++i) out8[i] = c.stats[i];
+    });
+}
+
+int iblgf_fma_peak(iblgf_ctx* x, int precision, double* tflops)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { *tflops = iblgf_b200::measure_fma_peak(c, precision); });
+}
+
+}  // extern "C"

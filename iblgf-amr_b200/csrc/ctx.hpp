@@ -1,0 +1,240 @@
+// Internal declarations of the iblgf_b200 library (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <unordered_map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/iblgf_b200.h"
+#include "keys.hpp"
+
+namespace iblgf_b200
+{
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m)
+    : std::runtime_error(m)
+    , code(c)
+    {
+    }
+};
+
+#define IBLGF_CUDA(call)                                                                      \
+    do                                                                                        \
+    {                                                                                         \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            throw ::iblgf_b200::Error(e_ == cudaErrorMemoryAllocation ? IBLGF_ENOMEM : IBLGF_ECUDA, \
+                                      std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+// Owning device buffer.
+template<class T>
+struct DevBuf
+{
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept { std::swap(p, o.p), std::swap(n, o.n); }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        release();
+        if (count == 0) return;
+        IBLGF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s)
+    {
+        if (h.size() != n) alloc(h.size());
+        if (n) IBLGF_CUDA(cudaMemcpyAsync(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+// ------------------------------------------------------------- host octree
+struct HOct
+{
+    u64 key = 0;
+    int level = 0;
+    int parent = -1;
+    int child[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    bool has_data = false;
+    int bbase[3] = {0, 0, 0};
+    bool leaf = false, correction = false, physical = false;
+    int idx = -1;  // canonical position (has_data only)
+};
+
+struct HostTree
+{
+    int e = 0;
+    int base_level = 0, depth = 0;
+    int base_shift[3] = {0, 0, 0};
+    int key_bd_extent[3] = {0, 0, 0};
+    std::vector<HOct> o;  // o[0] is the root
+
+    void init(int block_extent, const int* bd_base, const int* bd_extent);
+    void add_base_blocks(const std::vector<std::array<int, 3>>& normalized_bases);
+    int find(u64 k) const;
+    int insert(u64 k);
+    int refine_child(int p, int i);
+    void alloc(int i, int data_level);
+    std::vector<int> dfs_order() const;  // reference depth-first order, root first
+    std::vector<u64> unfound_neighbors(int i, bool correction_as_neighbors) const;
+    bool try_2to1(u64 k, std::map<u64, bool>& checklist) const;
+    void refine(int i, bool ratio_2to1);
+    void init_refine(int n_ref, int level_up_max, iblgf_refine_fn pred, void* user);
+    void mark_correction();
+    std::vector<int> canonical() const;  // has_data octants, (level, key) order
+};
+
+// ------------------------------------------------------------- FMM plan
+struct TpTasks  // tensor-product transfer tasks of one tree level
+{
+    int n_groups = 0;           // one group per receiving block
+    int n_tasks = 0;
+    DevBuf<int> group_ptr;      // CSR over tasks
+    DevBuf<int> group_dst;      // receiving octant
+    DevBuf<int> task_src;       // sending octant
+    DevBuf<int> task_cid;       // child id (0..7)
+};
+
+struct FmmPlan
+{
+    int level = 0, mask_idx = 0;
+    DevBuf<int> zero_s, zero_t, copy_s, add_t;
+    std::vector<TpTasks> antrp;  // levels level-1 .. 0
+    std::vector<TpTasks> intrp;  // levels 1 .. level-1
+    int n_src = 0, n_tgt = 0;
+    DevBuf<int> src_oct;         // source slot -> octant
+    DevBuf<int> tgt_oct;         // target slot -> octant
+    DevBuf<int> pair_ptr;        // CSR over targets
+    DevBuf<int> pair_src;        // source slot
+    DevBuf<int> pair_spec;       // spectrum slot
+    long long n_pairs = 0;
+    int n_spec_unique = 0;
+    // targets handled by the general pair-list MAC come first in tgt_oct
+    int n_csr_tgt = 0;
+    // sibling-group MAC: tiles of groups, staged source lists, per-group
+    // candidate sources (216, local index into the tile's staged list, 0xFFFF
+    // for none) and targets (8 child slots), LGF spectrum slot per offset
+    int n_tiles = 0, max_tile_src = 0, n_groups = 0;
+    DevBuf<int> tile_gptr, tile_sptr, tile_src, tile_tab, tile_coarse, spec_u, grp_tgt;
+    DevBuf<unsigned short> grp_src;
+    bool empty() const { return n_tgt == 0; }
+};
+
+struct Field
+{
+    DevBuf<double> d;
+};
+
+struct Ctx
+{
+    iblgf_config cfg{};
+    int Nb = 0, P = 0;
+    long long NC = 0;  // complex values per half spectrum, Nb * P * P
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    HostTree tree;
+    std::vector<std::array<int, 3>> pending_bases;
+    bool finalized = false;
+    bool subtract_non_leaf = false, use_correction = true;
+
+    // canonical octant arrays (host mirrors)
+    int n_oct = 0;
+    std::vector<u64> keys;
+    std::vector<int> levels, flags, bbase, parent, child;  // child: 8 per octant
+    std::vector<int> nbr, infl, n_infl;                   // from the device
+    std::vector<std::vector<uint8_t>> masks;              // [mask_idx][2*oct]
+    std::vector<std::vector<int>> level_octs;             // canonical idx per level
+    std::unordered_map<u64, int> key_index;               // key -> canonical idx
+
+    // device octant data
+    DevBuf<int> d_bbase, d_nbr;
+
+    // fields
+    std::vector<std::unique_ptr<Field>> fields;
+    int f_source_tmp = -1, f_target_tmp = -1, f_correction_tmp = -1, f_fmm_s = -1, f_fmm_t = -1;
+
+    // LGF table (device), twiddles, transfer matrices
+    DevBuf<double> d_lgf_table;
+    DevBuf<double> d_tw64;  // 2P doubles: cos, -sin interleaved (forward)
+    DevBuf<float> d_tw32;
+    DevBuf<double> d_mats;  // Nb*Nb matrices: [0,1] FMM Nli, [2,3] cell intrp, [4,5] coarsify
+
+    // spectra cache: key (level_diff, bx, by, bz) -> slot; storage in the
+    // working precision, NC complex per slot
+    std::map<std::array<int, 4>, int> spec_slot;
+    int spec_cap = 0, spec_used = 0;
+    DevBuf<char> d_spec;
+
+    // per-sweep work buffers (sized on demand)
+    DevBuf<char> d_src_spec, d_acc, d_w;
+
+    std::map<std::pair<int, int>, std::unique_ptr<FmmPlan>> plans;
+    long long launches = 0;
+    bool profile = false;
+    std::vector<std::array<cudaEvent_t, 5>> prof_events;
+    // work counters since the last reset: sweeps, sources, targets, pairs,
+    // unique spectra per sweep, anterpolation tasks, interpolation tasks
+    long long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+    size_t block_elems() const { return (size_t)Nb * Nb * Nb; }
+    size_t field_elems() const { return (size_t)n_oct * block_elems(); }
+    size_t cplx_bytes() const { return cfg.precision == IBLGF_FP32 ? 8 : 16; }
+    double* field(int id) { return fields.at(id)->d.p; }
+};
+
+// -------------------------------------------------------------- library
+void ctx_init(Ctx& c);
+void domain_finalize(Ctx& c);
+int field_create(Ctx& c);
+void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int fmm_type);
+void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);
+int mask_idx_gen(int type, int refinement_level, int nlas);
+
+// -------------------------------------------------------------- kernels (.cu)
+void launch_lgf_table(Ctx& c);
+void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
+void launch_build_lists(Ctx& c, const u64* d_sorted_keys, const int* d_sorted_idx, int n_sorted,
+                        const u64* d_keys, int n, int* d_nbr, int* d_infl, int* d_ninfl);
+void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots);
+void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, int n_src, void* src_spec);
+void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
+void upload_group_offsets();
+void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale);
+void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
+void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
+void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
+                        bool assign);
+void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base,
+               int mode /*0 antrp add, 1 intrp add, 2 intrp assign*/);
+void launch_halo(Ctx& c, double* f, const int* list, int n);
+void launch_source_correction(Ctx& c, const double* target_tmp, double* corr, const int* list, int n,
+                              double inv_dx2);
+void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* out, double scale);
+
+}  // namespace iblgf_b200

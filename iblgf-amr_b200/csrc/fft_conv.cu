@@ -1,0 +1,565 @@
+// Batched per-block FFT convolution of the LGF-FMM sweep, hand-written for
+// sm_100a (no cuFFT). Contract: include/iblgf/utilities/convolution.hpp:225-304
+// and src/utilities/convolution.cpp — a zero-padded Nb^3 source and a
+// (2Nb-1)^3 LGF block in a P^3 = (2Nb-1)^3 box, r2c, pointwise product
+// accumulated per target, c2r, window [Nb-1, 2Nb-2]^3 added into the target
+// block, scaled by dx^2 / P^3.
+//
+// B200 structure (one sweep = all blocks of all tree levels at once):
+//   fwd_xy   one CTA per (block, z-plane): pruned x (real, Nb -> Nb half
+//            frequencies) and y (Nb -> P) transforms in shared memory
+//   fwd_z    one thread per (ky,kx) pencil: z transform (Nb -> P)
+//            Each source block is transformed once per sweep; the reference
+//            transforms it once per (source, target) pair.
+//   mac      target-major spectral multiply-accumulate over the pair list,
+//            one thread per frequency, LGF spectra and source spectra read
+//            coalesced from L2/HBM (cached spectra stay resident across sweeps)
+//   inv_z    z inverse, only the Nb output planes of the extraction window
+//   inv_yx   y inverse (Nb outputs) and c2r along x (Nb outputs), scaled and
+//            added into the FP64 target block
+// The half spectrum is laid out [kz][ky][kx], kx < Nb (= P/2 + 1), as in the
+// reference's r2c output. Transforms are direct pruned DFTs: with half of the
+// inputs zero and half of the outputs discarded they cost about as much as a
+// mixed-radix FFT of length 35 and map onto regular loops.
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+#include "cplx.cuh"
+#include "ctx.hpp"
+#include "lgf_dev.cuh"
+
+namespace iblgf_b200
+{
+namespace
+{
+enum InMode { kFromField = 0, kFromLgf = 1, kFromDense = 2 };
+
+template<class R>
+__device__ __forceinline__ void load_tw(cx<R>* s_tw, const R* tw, int P)
+{
+    for (int j = threadIdx.x; j < P; j += blockDim.x) s_tw[j] = mk<R>(tw[2 * j], tw[2 * j + 1]);
+}
+
+// fwd_xy: x and y transforms of one z plane of one block.
+//   kFromField: block = field + item_oct[item] * NB^3 (NIN = NB)
+//   kFromLgf:   G((b + i) * 2^ld), desc[4*item] = {ld, bx, by, bz}  (NIN = P)
+//   kFromDense: dense[item * P^3]                                  (NIN = P)
+// W: [item][z < NIN][ky < P][kx < NB]
+template<class R, int NB, int NIN, int MODE>
+__global__ void __launch_bounds__(256) fwd_xy_kernel(const double* __restrict__ field,
+                                                     const int* __restrict__ item_oct,
+                                                     const int* __restrict__ desc,
+                                                     const double* __restrict__ table,
+                                                     const R* __restrict__ tw, cx<R>* __restrict__ W)
+{
+    constexpr int P = 2 * NB - 1;
+    __shared__ cx<R> s_tw[P];
+    __shared__ R s_in[NIN * NIN];
+    __shared__ cx<R> s_x1[NIN * NB];
+    const int item = blockIdx.x;
+    const int z = blockIdx.y;
+    load_tw<R>(s_tw, tw, P);
+    if (MODE == kFromField)
+    {
+        const double* blk = field + (size_t)item_oct[item] * (NB * NB * NB) + (size_t)z * NB * NB;
+        for (int i = threadIdx.x; i < NB * NB; i += blockDim.x) s_in[i] = (R)blk[i];
+    }
+    else if (MODE == kFromLgf)
+    {
+        const int ld = desc[4 * item], st = 1 << ld;
+        const int bx = desc[4 * item + 1], by = desc[4 * item + 2], bz = desc[4 * item + 3];
+        for (int i = threadIdx.x; i < NIN * NIN; i += blockDim.x)
+        {
+            const int x = i % NIN, y = i / NIN;
+            s_in[i] = (R)lgf_get_dev((bx + x) * st, (by + y) * st, (bz + z) * st, table);
+        }
+    }
+    else
+    {
+        const double* blk = field + (size_t)item * P * P * P + (size_t)z * P * P;
+        for (int i = threadIdx.x; i < NIN * NIN; i += blockDim.x) s_in[i] = (R)blk[i];
+    }
+    __syncthreads();
+    // x: real NIN -> NB half frequencies
+    for (int i = threadIdx.x; i < NIN * NB; i += blockDim.x)
+    {
+        const int y = i / NB, kx = i % NB;
+        cx<R> s = mk<R>(0, 0);
+        int j = 0;
+#pragma unroll 6
+        for (int x = 0; x < NIN; ++x)
+        {
+            rmac<R>(s, s_in[y * NIN + x], s_tw[j]);
+            j += kx;
+            if (j >= P) j -= P;
+        }
+        s_x1[y * NB + kx] = s;
+    }
+    __syncthreads();
+    // y: NIN -> P
+    cx<R>* out = W + ((size_t)item * NIN + z) * (P * NB);
+    for (int i = threadIdx.x; i < P * NB; i += blockDim.x)
+    {
+        const int ky = i / NB, kx = i % NB;
+        cx<R> s = mk<R>(0, 0);
+        int j = 0;
+#pragma unroll 6
+        for (int y = 0; y < NIN; ++y)
+        {
+            cmac<R>(s, s_x1[y * NB + kx], s_tw[j]);
+            j += ky;
+            if (j >= P) j -= P;
+        }
+        out[i] = s;
+    }
+}
+
+// fwd_z: per (ky,kx) pencil, NIN -> P; spectrum slot = item_slot[item] (or item)
+template<class R, class RO, int NB, int NIN>
+__global__ void __launch_bounds__(128) fwd_z_kernel(const cx<R>* __restrict__ W, const R* __restrict__ tw,
+                                                    const int* __restrict__ item_slot,
+                                                    cx<RO>* __restrict__ spec)
+{
+    constexpr int P = 2 * NB - 1;
+    constexpr int NP = P * NB;
+    __shared__ cx<R> s_tw[P];
+    load_tw<R>(s_tw, tw, P);
+    __syncthreads();
+    const int item = blockIdx.x;
+    const int p = blockIdx.y * blockDim.x + threadIdx.x;
+    if (p >= NP) return;
+    const cx<R>* w = W + (size_t)item * NIN * NP + p;
+    cx<R> v[NIN];
+#pragma unroll
+    for (int z = 0; z < NIN; ++z) v[z] = w[(size_t)z * NP];
+    const int slot = item_slot ? item_slot[item] : item;
+    cx<RO>* out = spec + (size_t)slot * P * NP + p;
+    for (int kz = 0; kz < P; ++kz)
+    {
+        cx<R> s = mk<R>(0, 0);
+        int j = 0;
+#pragma unroll
+        for (int z = 0; z < NIN; ++z)
+        {
+            cmac<R>(s, v[z], s_tw[j]);
+            j += kz;
+            if (j >= P) j -= P;
+        }
+        out[(size_t)kz * NP] = mk<RO>((RO)s.x, (RO)s.y);
+    }
+}
+
+// mac: ACC[t][f] = sum_pairs G[spec][f] * S[src][f]
+template<class R>
+__global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, const cx<R>* __restrict__ S,
+                                                  const int* __restrict__ pair_ptr,
+                                                  const int* __restrict__ pair_src,
+                                                  const int* __restrict__ pair_spec, long long NC,
+                                                  cx<R>* __restrict__ ACC)
+{
+    const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int t = blockIdx.y;
+    if (f >= NC) return;
+    cx<R> acc = mk<R>(0, 0);
+    const int j0 = pair_ptr[t], j1 = pair_ptr[t + 1];
+    for (int j = j0; j < j1; ++j)
+    {
+        const cx<R> g = G[(size_t)pair_spec[j] * NC + f];
+        const cx<R> s = S[(size_t)pair_src[j] * NC + f];
+        cmac<R>(acc, g, s);
+    }
+    ACC[(size_t)t * NC + f] = acc;
+}
+
+// Sibling-group MAC. At a sweep's base level the neighbours and the influence
+// list of a target together are exactly the children of its parent's 27
+// neighbours; coarser targets see the non-adjacent ones. The 8 siblings of a
+// parent therefore share one candidate source set (216 = 27 x 8), and the
+// offset of (child c, candidate k = (n, c')) is u = c - c' - 2n in [-3,3]^3.
+// One CTA = (tile of sibling groups, chunk of F frequencies): the tile's LGF
+// spectra (343 offsets) and the union of its groups' sources are staged in
+// shared memory; each thread keeps the accumulators of M groups x 8 children
+// for one frequency, so one shared-memory load of G[u] feeds M complex MACs
+// and one load of S feeds 8.
+__constant__ short c_group_u[8 * 216];  // offset index (ux+3)+7(uy+3)+49(uz+3)
+
+template<class R, int F, int M>
+__global__ void __launch_bounds__(256) group_mac_kernel(
+    const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, const int* __restrict__ tile_gptr,
+    const int* __restrict__ tile_sptr, const int* __restrict__ tile_src, const int* __restrict__ tile_tab,
+    const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
+    const unsigned short* __restrict__ grp_src, const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);  // [343][F]
+    cx<R>* Ss = Gs + 343 * F;                       // [n_src][F]
+    const int tile = blockIdx.y;
+    const long long f0 = (long long)blockIdx.x * F;
+    const int lane = threadIdx.x % F, row = threadIdx.x / F, rows = blockDim.x / F;
+    const cx<R> zero = mk<R>(0, 0);
+    const int* su = spec_u + 343 * tile_tab[tile];
+    for (int i = threadIdx.x; i < 343 * F; i += blockDim.x)
+    {
+        const int u = i / F;
+        const long long ff = f0 + (i % F);
+        const int slot = su[u];
+        Gs[i] = (slot >= 0 && ff < NC) ? G[(size_t)slot * NC + ff] : zero;
+    }
+    const int s0 = tile_sptr[tile], ns = tile_sptr[tile + 1] - s0;
+    for (int i = threadIdx.x; i < ns * F; i += blockDim.x)
+    {
+        const long long ff = f0 + (i % F);
+        Ss[i] = ff < NC ? S[(size_t)tile_src[s0 + i / F] * NC + ff] : zero;
+    }
+    __syncthreads();
+    const bool coarse = tile_coarse[tile] != 0;
+    const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
+    const long long f = f0 + lane;
+    for (int gb = g0 + row * M; gb < g1; gb += rows * M)
+    {
+        cx<R> acc[M][8];
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[m][c] = zero;
+        for (int k = 0; k < 216; ++k)
+        {
+            cx<R> sv[M];
+            bool any = false;
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+            {
+                const int g = gb + m;
+                const unsigned short j = g < g1 ? grp_src[(size_t)g * 216 + k] : (unsigned short)0xFFFF;
+                sv[m] = j != 0xFFFF ? Ss[j * F + lane] : zero;
+                any = any || j != 0xFFFF;
+            }
+            if (!any) continue;
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+            {
+                const int u = c_group_u[c * 216 + k];
+                if (coarse)
+                {
+                    const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
+                    if (ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1) continue;
+                }
+                const cx<R> gv = Gs[u * F + lane];
+#pragma unroll
+                for (int m = 0; m < M; ++m) cmac<R>(acc[m][c], gv, sv[m]);
+            }
+        }
+        if (f < NC)
+        {
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+            {
+                const int g = gb + m;
+                if (g >= g1) break;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                {
+                    const int t = grp_tgt[(size_t)g * 8 + c];
+                    if (t >= 0) ACC[(size_t)t * NC + f] = acc[m][c];
+                }
+            }
+        }
+    }
+}
+
+// inv_z: V[t][z'][p] = sum_kz ACC[t][kz][p] e^{+2 pi i kz (z'+NB-1)/P}, z' < NB
+template<class R, int NB>
+__global__ void __launch_bounds__(128) inv_z_kernel(const cx<R>* __restrict__ ACC, const R* __restrict__ tw,
+                                                    cx<R>* __restrict__ V)
+{
+    constexpr int P = 2 * NB - 1;
+    constexpr int NP = P * NB;
+    __shared__ cx<R> s_tw[P];
+    load_tw<R>(s_tw, tw, P);
+    __syncthreads();
+    const int t = blockIdx.x;
+    const int p = blockIdx.y * blockDim.x + threadIdx.x;
+    if (p >= NP) return;
+    const cx<R>* a = ACC + (size_t)t * P * NP + p;
+    cx<R> v[P];
+#pragma unroll
+    for (int kz = 0; kz < P; ++kz) v[kz] = a[(size_t)kz * NP];
+    cx<R>* out = V + (size_t)t * NB * NP + p;
+    for (int zo = 0; zo < NB; ++zo)
+    {
+        const int zz = zo + NB - 1;
+        cx<R> s = mk<R>(0, 0);
+        int j = 0;
+#pragma unroll
+        for (int kz = 0; kz < P; ++kz)
+        {
+            cmac_conj<R>(s, v[kz], s_tw[j]);
+            j += zz;
+            if (j >= P) j -= P;
+        }
+        out[(size_t)zo * NP] = s;
+    }
+}
+
+// inv_yx: y inverse (NB outputs) and c2r along x (NB outputs), then
+// target[oct] += scale * result over the whole Nb^3 block
+template<class R, int NB>
+__global__ void __launch_bounds__(256) inv_yx_kernel(const cx<R>* __restrict__ V, const R* __restrict__ tw,
+                                                     const int* __restrict__ tgt_oct, double scale,
+                                                     double* __restrict__ target)
+{
+    constexpr int P = 2 * NB - 1;
+    constexpr int NP = P * NB;
+    __shared__ cx<R> s_tw[P];
+    __shared__ cx<R> s_v[NP];
+    __shared__ cx<R> s_y[NB * NB];
+    const int t = blockIdx.x, zo = blockIdx.y;
+    load_tw<R>(s_tw, tw, P);
+    const cx<R>* vin = V + ((size_t)t * NB + zo) * NP;
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) s_v[i] = vin[i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < NB * NB; i += blockDim.x)
+    {
+        const int yo = i / NB, kx = i % NB, yy = yo + NB - 1;
+        cx<R> s = mk<R>(0, 0);
+        int j = 0;
+#pragma unroll 5
+        for (int ky = 0; ky < P; ++ky)
+        {
+            cmac_conj<R>(s, s_v[ky * NB + kx], s_tw[j]);
+            j += yy;
+            if (j >= P) j -= P;
+        }
+        s_y[yo * NB + kx] = s;
+    }
+    __syncthreads();
+    double* out = target + (size_t)tgt_oct[t] * NB * NB * NB + (size_t)zo * NB * NB;
+    for (int i = threadIdx.x; i < NB * NB; i += blockDim.x)
+    {
+        const int yo = i / NB, xo = i % NB, xx = xo + NB - 1;
+        R acc = 0;
+        int j = xx;
+        for (int kx = 1; kx < NB; ++kx)
+        {
+            const cx<R> y = s_y[yo * NB + kx];
+            acc = fma(y.x, s_tw[j].x, fma(y.y, s_tw[j].y, acc));
+            j += xx;
+            if (j >= P) j -= P;
+        }
+        const double v = (double)s_y[yo * NB].x + 2.0 * (double)acc;
+        out[i] += scale * v;
+    }
+}
+
+template<class R, int NB>
+struct Conv
+{
+    static constexpr int P = 2 * NB - 1;
+    static constexpr int NP = P * NB;
+
+    static const R* tw(Ctx& c)
+    {
+        return std::is_same<R, double>::value ? (const R*)c.d_tw64.p : (const R*)c.d_tw32.p;
+    }
+
+    static void forward_field(Ctx& c, const double* field, const int* d_item_oct, int n, void* spec)
+    {
+        if (!n) return;
+        cx<R>* W = (cx<R>*)c.d_w.p;
+        fwd_xy_kernel<R, NB, NB, kFromField><<<dim3(n, NB), 256, 0, c.stream>>>(field, d_item_oct, nullptr,
+                                                                              nullptr, tw(c), W);
+        fwd_z_kernel<R, R, NB, NB><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, tw(c), nullptr,
+                                                                                  (cx<R>*)spec);
+        c.launches += 2;
+    }
+
+    // LGF blocks (or a dense kernel) are transformed in FP64 and stored in R
+    static void forward_lgf(Ctx& c, const int* d_desc, const double* dense, const int* d_slot, int n,
+                            void* spec)
+    {
+        if (!n) return;
+        double2* W = (double2*)c.d_w.p;
+        if (dense)
+            fwd_xy_kernel<double, NB, P, kFromDense><<<dim3(n, P), 256, 0, c.stream>>>(
+                dense, nullptr, nullptr, nullptr, c.d_tw64.p, W);
+        else
+            fwd_xy_kernel<double, NB, P, kFromLgf><<<dim3(n, P), 256, 0, c.stream>>>(
+                nullptr, nullptr, d_desc, c.d_lgf_table.p, c.d_tw64.p, W);
+        fwd_z_kernel<double, R, NB, P><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, c.d_tw64.p, d_slot,
+                                                                                      (cx<R>*)spec);
+        c.launches += 2;
+    }
+
+    static void mac(Ctx& c, const void* G, const void* S, const int* ptr, const int* src, const int* spec,
+                    int n_tgt, void* acc)
+    {
+        if (!n_tgt) return;
+        dim3 grid((unsigned)((c.NC + 127) / 128), n_tgt);
+        mac_kernel<R><<<grid, 128, 0, c.stream>>>((const cx<R>*)G, (const cx<R>*)S, ptr, src, spec, c.NC,
+                                                  (cx<R>*)acc);
+        c.launches += 1;
+    }
+
+    static constexpr int GF = std::is_same<R, float>::value ? 16 : 8;
+    static constexpr int GM = std::is_same<R, float>::value ? 2 : 1;
+
+    static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc)
+    {
+        if (!p.n_tiles) return;
+        const size_t smem = (size_t)(343 + p.max_tile_src) * GF * sizeof(cx<R>);
+        auto kfn = group_mac_kernel<R, GF, GM>;
+        IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid((unsigned)((c.NC + GF - 1) / GF), p.n_tiles);
+        kfn<<<grid, 256, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.tile_gptr.p,
+                                           p.tile_sptr.p, p.tile_src.p, p.tile_tab.p, p.tile_coarse.p,
+                                           p.spec_u.p, p.grp_src.p, p.grp_tgt.p, (cx<R>*)acc);
+        c.launches += 1;
+    }
+
+    static void inverse(Ctx& c, const void* acc, const int* d_tgt_oct, int n_tgt, double scale, double* target)
+    {
+        if (!n_tgt) return;
+        cx<R>* V = (cx<R>*)c.d_w.p;
+        inv_z_kernel<R, NB><<<dim3(n_tgt, (NP + 127) / 128), 128, 0, c.stream>>>((const cx<R>*)acc, tw(c), V);
+        inv_yx_kernel<R, NB><<<dim3(n_tgt, NB), 256, 0, c.stream>>>(V, tw(c), d_tgt_oct, scale, target);
+        c.launches += 2;
+    }
+};
+
+template<class F>
+void dispatch(Ctx& c, F&& f)
+{
+    const bool fp32 = c.cfg.precision == IBLGF_FP32;
+#define IBLGF_CASE(NBV)                                  \
+    case NBV:                                            \
+        if (fp32) f(Conv<float, NBV>{});                 \
+        else f(Conv<double, NBV>{});                     \
+        return;
+    switch (c.Nb)
+    {
+        IBLGF_CASE(6)
+        IBLGF_CASE(8)
+        IBLGF_CASE(10)
+        IBLGF_CASE(12)
+        IBLGF_CASE(16)
+        IBLGF_CASE(18)
+        default: throw Error(IBLGF_EINVAL, "unsupported block_extent (supported: 4,6,8,10,14,16)");
+    }
+#undef IBLGF_CASE
+}
+
+void ensure(DevBuf<char>& b, size_t bytes)
+{
+    if (b.n < bytes) b.alloc(bytes);
+}
+}  // namespace
+
+bool nb_supported(int Nb) { return Nb == 6 || Nb == 8 || Nb == 10 || Nb == 12 || Nb == 16 || Nb == 18; }
+
+void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots)
+{
+    // new_slots: {slot, ld, bx, by, bz}; processed in batches of 64
+    const int P = c.P;
+    const size_t wbytes = (size_t)64 * P * P * c.Nb * 16;
+    ensure(c.d_w, wbytes);
+    for (size_t b0 = 0; b0 < new_slots.size(); b0 += 64)
+    {
+        const size_t nb = std::min<size_t>(64, new_slots.size() - b0);
+        std::vector<int> desc(4 * nb), slot(nb);
+        for (size_t i = 0; i < nb; ++i)
+        {
+            const auto& s = new_slots[b0 + i];
+            slot[i] = s[0];
+            desc[4 * i] = s[1];
+            desc[4 * i + 1] = s[2];
+            desc[4 * i + 2] = s[3];
+            desc[4 * i + 3] = s[4];
+        }
+        DevBuf<int> d_desc, d_slot;
+        d_desc.upload(desc, c.stream);
+        d_slot.upload(slot, c.stream);
+        dispatch(c, [&](auto cv) {
+            using CV = decltype(cv);
+            CV::forward_lgf(c, d_desc.p, nullptr, d_slot.p, (int)nb, c.d_spec.p);
+        });
+        IBLGF_CUDA(cudaGetLastError());
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // d_desc / d_slot go out of scope
+    }
+}
+
+void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, int n_src, void* src_spec)
+{
+    ensure(c.d_w, (size_t)n_src * c.Nb * c.P * c.Nb * c.cplx_bytes());
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        CV::forward_field(c, fmm_s, d_src_oct, n_src, src_spec);
+    });
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
+{
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        // targets outside sibling groups: general pair-list MAC
+        CV::mac(c, c.d_spec.p, src_spec, p.pair_ptr.p, p.pair_src.p, p.pair_spec.p, p.n_csr_tgt, acc);
+        CV::group_mac(c, p, src_spec, acc);
+    });
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void upload_group_offsets()
+{
+    static bool done = false;
+    if (done) return;
+    short tab[8 * 216];
+    for (int cc = 0; cc < 8; ++cc)
+        for (int k = 0; k < 216; ++k)
+        {
+            const int n = k / 8, cp = k % 8;
+            const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
+            const int ux = (cc & 1) - (cp & 1) - 2 * nx;
+            const int uy = ((cc >> 1) & 1) - ((cp >> 1) & 1) - 2 * ny;
+            const int uz = ((cc >> 2) & 1) - ((cp >> 2) & 1) - 2 * nz;
+            tab[cc * 216 + k] = (short)((ux + 3) + 7 * (uy + 3) + 49 * (uz + 3));
+        }
+    IBLGF_CUDA(cudaMemcpyToSymbol(c_group_u, tab, sizeof(tab)));
+    done = true;
+}
+
+void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale)
+{
+    ensure(c.d_w, (size_t)p.n_tgt * c.Nb * c.P * c.Nb * c.cplx_bytes());
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        CV::inverse(c, acc, p.tgt_oct.p, p.n_tgt, scale, fmm_t);
+    });
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* out, double scale)
+{
+    const size_t cb = c.cplx_bytes();
+    DevBuf<char> gspec, sspec, acc;
+    gspec.alloc(c.NC * cb);
+    sspec.alloc(c.NC * cb);
+    acc.alloc(c.NC * cb);
+    ensure(c.d_w, (size_t)c.P * c.P * c.Nb * 16);
+    std::vector<int> zero{0}, ptr{0, 1};
+    DevBuf<int> d_zero, d_ptr;
+    d_zero.upload(zero, c.stream);
+    d_ptr.upload(ptr, c.stream);
+    const double s = scale / ((double)c.P * c.P * c.P);
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        CV::forward_lgf(c, nullptr, kernel, nullptr, 1, gspec.p);
+        CV::forward_field(c, src, d_zero.p, 1, sspec.p);
+        CV::mac(c, gspec.p, sspec.p, d_ptr.p, d_zero.p, d_zero.p, 1, acc.p);
+        CV::inverse(c, acc.p, d_zero.p, 1, s, out);
+    });
+    IBLGF_CUDA(cudaGetLastError());
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace iblgf_b200

@@ -1,0 +1,842 @@
+// Host driver of the B200 LGF-FMM path: context set-up, domain finalisation
+// (device list build, FMM masks), FMM sweep plans and the Poisson level loop.
+//
+//   FmmMaskBuilder (include/iblgf/fmm/fmm.hpp:54-681): fmm_dry_init_base_level_
+//     masks, fmm_upward_pass_masks, fmm_clean_no_inf_masks, stream mask
+//   Fmm::apply (fmm.hpp:729-870): one plan per (mask index, level) with the
+//     zero/copy lists, per-level anterpolation and interpolation task lists,
+//     and the (target, source, LGF spectrum) pair list of all targets of all
+//     levels; executed as one batched sweep on the device
+//   PoissonSolver::apply_lgf (solver/poisson/poisson.hpp:587-894)
+//
+// All device work is ordered on the context stream; a sweep issues no host
+// synchronisation once its plan exists.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ctx.hpp"
+
+namespace iblgf_b200
+{
+bool nb_supported(int Nb);
+
+int mask_idx_gen(int type, int refinement_level, int nlas)
+{
+    if (type == IBLGF_STREAM) return 0;
+    if (type == IBLGF_AMR2AMR) return refinement_level * 2 + nlas + 15;
+    throw Error(IBLGF_EINVAL, "unsupported fmm_type");
+}
+
+// --------------------------------------------------------------- matrices
+namespace
+{
+// Lagrange node-transfer matrix, Nb x 2Nb with (p, c) at p*2Nb + c:
+// fmm_nli.hpp:319-374 (relpos 0, integer offsets) and
+// cell_center_nli_intrp.hpp:677-787 (relpos 1, half-cell offsets)
+std::vector<double> lagrange_matrix(int Nb, int pts_cap, int relpos)
+{
+    std::vector<double> m((size_t)Nb * 2 * Nb, 0.0);
+    auto M = [&](int p, int c) -> double& { return m[(size_t)p * 2 * Nb + c]; };
+    for (int c = 1; c < 2 * Nb - 1; ++c)
+    {
+        if (relpos == 0 && c % 2 == 0)
+        {
+            M(c / 2, c - 1) = 1.0;
+            continue;
+        }
+        const double cp = relpos == 0 ? (double)(c - Nb) : c - Nb + 0.5;
+        int bl, br;
+        if (cp < -1)
+        {
+            bl = std::max(0, (c + 1) / 2 - pts_cap / 2);
+            br = std::min(Nb, bl + pts_cap);
+        }
+        else
+        {
+            br = std::min(Nb, (c + 1) / 2 + pts_cap / 2);
+            bl = std::max(0, br - pts_cap);
+        }
+        long double sum = 0.0;
+        for (int p = bl; p < br; ++p)
+        {
+            long double w = 1.0;
+            const int pp = 2 * p - Nb + 1;
+            for (int l = bl; l < br; ++l)
+                if (l != p) w /= -(long double)(2 * l - Nb + 1 - pp);
+            w /= relpos == 0 ? (long double)((int)cp - pp + 1) : (long double)(cp - pp);
+            M(p, c - 1) = (double)w;
+            sum += w;
+        }
+        for (int p = 0; p < Nb; ++p) M(p, c - 1) /= (double)sum;
+    }
+    for (int c = 2 * Nb - 1; c > Nb - 1; --c)
+        for (int p = 0; p < Nb; ++p) M(p, c) = M(p, c - 2);
+    return m;
+}
+
+void append_halves(std::vector<double>& out, const std::vector<double>& full, int Nb)
+{
+    for (int h = 0; h < 2; ++h)
+        for (int p = 0; p < Nb; ++p)
+            for (int j = 0; j < Nb; ++j) out.push_back(full[(size_t)p * 2 * Nb + h * Nb + j]);
+}
+}  // namespace
+
+void ctx_init(Ctx& c)
+{
+    const int e = c.cfg.block_extent;
+    c.Nb = e + 2;
+    c.P = 2 * c.Nb - 1;
+    c.NC = (long long)c.Nb * c.P * c.P;
+    if (!nb_supported(c.Nb)) throw Error(IBLGF_EINVAL, "unsupported block_extent (supported: 4,6,8,10,14,16)");
+    if (c.cfg.precision != IBLGF_FP64 && c.cfg.precision != IBLGF_FP32)
+        throw Error(IBLGF_EINVAL, "precision must be IBLGF_FP64 or IBLGF_FP32");
+    if (c.cfg.intrp_order <= 0) c.cfg.intrp_order = 5;
+    IBLGF_CUDA(cudaSetDevice(c.cfg.device));
+    if (c.cfg.stream) c.stream = (cudaStream_t)c.cfg.stream;
+    else
+    {
+        IBLGF_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        c.own_stream = true;
+    }
+    // twiddles e^{-2 pi i j / P}
+    std::vector<double> tw(2 * c.P);
+    std::vector<float> tw32(2 * c.P);
+    for (int j = 0; j < c.P; ++j)
+    {
+        const double a = 2.0 * M_PI * j / c.P;
+        tw[2 * j] = std::cos(a);
+        tw[2 * j + 1] = -std::sin(a);
+        tw32[2 * j] = (float)tw[2 * j];
+        tw32[2 * j + 1] = (float)tw[2 * j + 1];
+    }
+    c.d_tw64.upload(tw, c.stream);
+    c.d_tw32.upload(tw32, c.stream);
+    // [0,1] FMM Nli (pts_cap 10), [2,3] cell-centred interpolation (relpos 1),
+    // [4,5] cell-centred coarsification (2-point average per axis)
+    std::vector<double> mats;
+    append_halves(mats, lagrange_matrix(c.Nb, 10, 0), c.Nb);
+    append_halves(mats, lagrange_matrix(c.Nb, c.cfg.intrp_order, 1), c.Nb);
+    std::vector<double> simple((size_t)c.Nb * c.Nb * 2, 0.0);
+    for (int h = 0; h < 2; ++h)
+        for (int p = 1; p < c.Nb - 1; ++p)
+            for (int j = 1; j < c.Nb - 1; ++j)
+            {
+                const int col = j + h * (c.Nb - 2);  // column of the Nb x (2Nb-2) averaging matrix
+                if (col == 2 * p - 1 || col == 2 * p) simple[(size_t)h * c.Nb * c.Nb + p * c.Nb + j] = 0.5;
+            }
+    mats.insert(mats.end(), simple.begin(), simple.end());
+    c.d_mats.upload(mats, c.stream);
+    c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
+    launch_lgf_table(c);
+}
+
+// --------------------------------------------------------------- domain
+namespace
+{
+struct MaskView
+{
+    std::vector<uint8_t>& m;
+    bool S(int o) const { return m[2 * o]; }
+    bool T(int o) const { return m[2 * o + 1]; }
+    void set(int o, bool s, bool t)
+    {
+        m[2 * o] = s;
+        m[2 * o + 1] = t;
+    }
+};
+
+void upward_pass(Ctx& c, int base_level, MaskView mv)
+{
+    for (int level = base_level - 1; level >= 0; --level)
+    {
+        for (int o : c.level_octs[level])
+        {
+            bool s = false, t = false;
+            for (int k = 0; k < 8; ++k)
+            {
+                const int ch = c.child[8 * o + k];
+                if (ch < 0) continue;
+                s = s || mv.S(ch);
+                t = t || mv.T(ch);
+            }
+            mv.set(o, s, t);
+        }
+    }
+}
+
+void clean_no_inf(Ctx& c, int base_level, MaskView mv)
+{
+    for (int level = 0; level < base_level; ++level)
+        for (int o : c.level_octs[level])
+        {
+            const int p = c.parent[o];
+            if (mv.S(o))
+            {
+                if (p >= 0 && mv.S(p)) continue;
+                bool has = false;
+                for (int i = 0; i < c.n_infl[o] && !has; ++i)
+                {
+                    const int n = c.infl[189 * o + i];
+                    has = n >= 0 && mv.T(n);
+                }
+                if (!has) mv.m[2 * o] = 0;
+            }
+            if (mv.T(o))
+            {
+                if (p >= 0 && mv.T(p)) continue;
+                bool has = false;
+                for (int i = 0; i < c.n_infl[o] && !has; ++i)
+                {
+                    const int n = c.infl[189 * o + i];
+                    has = n >= 0 && mv.S(n);
+                }
+                if (!has) mv.m[2 * o + 1] = 0;
+            }
+        }
+}
+
+void build_masks(Ctx& c)
+{
+    c.masks.assign(50, std::vector<uint8_t>(2 * (size_t)c.n_oct, 0));
+    const int bl = c.tree.base_level;
+    for (int l = bl; l < c.tree.depth; ++l)
+    {
+        for (int nlas = 0; nlas <= 1; ++nlas)
+        {
+            const int idx = mask_idx_gen(IBLGF_AMR2AMR, l - bl, nlas);
+            MaskView mv{c.masks[idx]};
+            for (int o : c.level_octs[l])
+            {
+                const bool leaf = c.flags[o] & 1, corr = c.flags[o] & 2;
+                bool corr_parent = false;
+                for (int k = 0; k < 8; ++k)
+                {
+                    const int ch = c.child[8 * o + k];
+                    if (ch >= 0 && (c.flags[ch] & 2)) corr_parent = true;
+                }
+                if (nlas)
+                {
+                    if (c.subtract_non_leaf) mv.set(o, !(leaf || corr), (leaf || corr) ? corr_parent : true);
+                    else mv.set(o, leaf || corr, (leaf || corr) ? leaf : true);
+                }
+                else
+                {
+                    if (c.subtract_non_leaf) mv.set(o, true, true);
+                    else mv.set(o, !(leaf || corr), (leaf || corr) ? leaf : false);
+                }
+            }
+            upward_pass(c, l, mv);
+            clean_no_inf(c, l, mv);
+        }
+    }
+    MaskView st{c.masks[mask_idx_gen(IBLGF_STREAM, 0, 0)]};
+    for (int o : c.level_octs[bl]) st.set(o, !(c.flags[o] & 2), true);
+    upward_pass(c, bl, st);
+}
+}  // namespace
+
+int field_create(Ctx& c)
+{
+    auto f = std::make_unique<Field>();
+    f->d.alloc(c.field_elems());
+    IBLGF_CUDA(cudaMemsetAsync(f->d.p, 0, c.field_elems() * sizeof(double), c.stream));
+    c.fields.push_back(std::move(f));
+    return (int)c.fields.size() - 1;
+}
+
+void domain_finalize(Ctx& c)
+{
+    HostTree& t = c.tree;
+    const std::vector<int> canon = t.canonical();
+    c.n_oct = (int)canon.size();
+    for (int i = 0; i < c.n_oct; ++i) t.o[canon[i]].idx = i;
+    const int n = c.n_oct;
+    c.keys.resize(n);
+    c.levels.resize(n);
+    c.flags.resize(n);
+    c.bbase.resize(3 * (size_t)n);
+    c.parent.assign(n, -1);
+    c.child.assign(8 * (size_t)n, -1);
+    c.level_octs.assign(kMaxLevel + 1, {});
+    for (int i = 0; i < n; ++i)
+    {
+        const HOct& h = t.o[canon[i]];
+        c.keys[i] = h.key;
+        c.levels[i] = h.level;
+        c.flags[i] = (h.leaf ? 1 : 0) | (h.correction ? 2 : 0);
+        for (int d = 0; d < 3; ++d) c.bbase[3 * i + d] = h.bbase[d];
+        if (h.parent >= 0 && t.o[h.parent].has_data) c.parent[i] = t.o[h.parent].idx;
+        for (int k = 0; k < 8; ++k)
+            if (h.child[k] >= 0 && t.o[h.child[k]].has_data) c.child[8 * i + k] = t.o[h.child[k]].idx;
+        c.level_octs[h.level].push_back(i);
+        c.key_index[h.key] = i;
+    }
+    // neighbour / influence lists on the device
+    std::vector<std::pair<u64, int>> sk(n);
+    for (int i = 0; i < n; ++i) sk[i] = {c.keys[i], i};
+    std::sort(sk.begin(), sk.end());
+    std::vector<u64> skeys(n);
+    std::vector<int> sidx(n);
+    for (int i = 0; i < n; ++i) skeys[i] = sk[i].first, sidx[i] = sk[i].second;
+    DevBuf<u64> d_skeys, d_keys;
+    DevBuf<int> d_sidx, d_infl, d_ninfl;
+    d_skeys.upload(skeys, c.stream);
+    d_sidx.upload(sidx, c.stream);
+    d_keys.upload(c.keys, c.stream);
+    c.d_nbr.alloc(27 * (size_t)n);
+    d_infl.alloc(189 * (size_t)n);
+    d_ninfl.alloc(n);
+    launch_build_lists(c, d_skeys.p, d_sidx.p, n, d_keys.p, n, c.d_nbr.p, d_infl.p, d_ninfl.p);
+    c.nbr.resize(27 * (size_t)n);
+    c.infl.resize(189 * (size_t)n);
+    c.n_infl.resize(n);
+    IBLGF_CUDA(cudaMemcpyAsync(c.nbr.data(), c.d_nbr.p, c.nbr.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaMemcpyAsync(c.infl.data(), d_infl.p, c.infl.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaMemcpyAsync(c.n_infl.data(), d_ninfl.p, n * 4, cudaMemcpyDeviceToHost, c.stream));
+    c.d_bbase.upload(c.bbase, c.stream);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    build_masks(c);
+    c.f_source_tmp = field_create(c);
+    c.f_target_tmp = field_create(c);
+    c.f_correction_tmp = field_create(c);
+    c.f_fmm_s = field_create(c);
+    c.f_fmm_t = field_create(c);
+    c.finalized = true;
+}
+
+// --------------------------------------------------------------- plans
+namespace
+{
+void upload_tasks(Ctx& c, TpTasks& tt, const std::vector<int>& dst, const std::vector<std::vector<std::pair<int, int>>>& tasks)
+{
+    std::vector<int> ptr{0}, src, cid, gdst;
+    for (size_t g = 0; g < dst.size(); ++g)
+    {
+        if (tasks[g].empty()) continue;
+        gdst.push_back(dst[g]);
+        for (auto& t : tasks[g])
+        {
+            src.push_back(t.first);
+            cid.push_back(t.second);
+        }
+        ptr.push_back((int)src.size());
+    }
+    tt.n_groups = (int)gdst.size();
+    tt.n_tasks = (int)src.size();
+    tt.group_ptr.upload(ptr, c.stream);
+    tt.group_dst.upload(gdst, c.stream);
+    tt.task_src.upload(src, c.stream);
+    tt.task_cid.upload(cid, c.stream);
+}
+
+FmmPlan& get_plan(Ctx& c, int level, int idx)
+{
+    auto key = std::make_pair(idx, level);
+    auto it = c.plans.find(key);
+    if (it != c.plans.end()) return *it->second;
+    auto plan = std::make_unique<FmmPlan>();
+    FmmPlan& p = *plan;
+    p.level = level;
+    p.mask_idx = idx;
+    const auto& m = c.masks[idx];
+    auto S = [&](int o) { return m[2 * o] != 0; };
+    auto T = [&](int o) { return m[2 * o + 1] != 0; };
+    std::vector<int> zs, zt, cs, at, srcs, tgts;
+    for (int lv = level; lv >= 0; --lv)
+        for (int o : c.level_octs[lv])
+        {
+            if (S(o)) zs.push_back(o), srcs.push_back(o);
+            if (T(o)) zt.push_back(o), tgts.push_back(o);
+        }
+    for (int o : c.level_octs[level])
+    {
+        if (S(o)) cs.push_back(o);
+        if (T(o)) at.push_back(o);
+    }
+    p.zero_s.upload(zs, c.stream);
+    p.zero_t.upload(zt, c.stream);
+    p.copy_s.upload(cs, c.stream);
+    p.add_t.upload(at, c.stream);
+    // anterpolation, levels level-1 .. 0
+    for (int lv = level - 1; lv >= 0; --lv)
+    {
+        std::vector<int> dst;
+        std::vector<std::vector<std::pair<int, int>>> tasks;
+        for (int o : c.level_octs[lv])
+        {
+            if (!S(o)) continue;
+            dst.push_back(o);
+            tasks.emplace_back();
+            for (int k = 0; k < 8; ++k)
+            {
+                const int ch = c.child[8 * o + k];
+                if (ch >= 0 && S(ch)) tasks.back().push_back({ch, k});
+            }
+        }
+        p.antrp.emplace_back();
+        upload_tasks(c, p.antrp.back(), dst, tasks);
+    }
+    // interpolation, levels 1 .. level-1 (parent level)
+    for (int lv = 1; lv < level; ++lv)
+    {
+        std::vector<int> dst;
+        std::vector<std::vector<std::pair<int, int>>> tasks;
+        for (int o : c.level_octs[lv])
+        {
+            if (!T(o)) continue;
+            for (int k = 0; k < 8; ++k)
+            {
+                const int ch = c.child[8 * o + k];
+                if (ch >= 0 && T(ch))
+                {
+                    dst.push_back(ch);
+                    tasks.push_back({{o, k}});
+                }
+            }
+        }
+        p.intrp.emplace_back();
+        upload_tasks(c, p.intrp.back(), dst, tasks);
+    }
+    // sources and pair list
+    std::vector<int> src_slot(c.n_oct, -1);
+    for (size_t i = 0; i < srcs.size(); ++i) src_slot[srcs[i]] = (int)i;
+    p.n_src = (int)srcs.size();
+    p.src_oct.upload(srcs, c.stream);
+    std::vector<std::array<int, 5>> new_slots;
+    const int Nb = c.Nb, e = c.cfg.block_extent;
+    auto slot_of = [&](const std::array<int, 4>& k) {
+        auto it = c.spec_slot.find(k);
+        if (it != c.spec_slot.end()) return it->second;
+        const int slot = (int)c.spec_slot.size();
+        c.spec_slot.emplace(k, slot);
+        new_slots.push_back({slot, k[0], k[1], k[2], k[3]});
+        return slot;
+    };
+    // reference pair list of every target (fmm.hpp:988-1027, fmm_tt :1167-1195)
+    struct TP
+    {
+        int t;
+        std::vector<int> src, spec;
+    };
+    std::vector<TP> tp;
+    for (int t : tgts)
+    {
+        const int ld = level - c.levels[t];
+        TP x{t, {}, {}};
+        auto add_pair = [&](int s, int lvd) {
+            x.src.push_back(src_slot[s]);
+            x.spec.push_back(slot_of({lvd, c.bbase[3 * t] - c.bbase[3 * s] - (Nb - 1),
+                                      c.bbase[3 * t + 1] - c.bbase[3 * s + 1] - (Nb - 1),
+                                      c.bbase[3 * t + 2] - c.bbase[3 * s + 2] - (Nb - 1)}));
+        };
+        if (c.levels[t] == level)
+            for (int i = 0; i < 27; ++i)
+            {
+                const int n = c.nbr[27 * t + i];
+                if (n >= 0 && S(n)) add_pair(n, 0);
+            }
+        for (int i = 0; i < c.n_infl[t]; ++i)
+        {
+            const int n = c.infl[189 * t + i];
+            if (n >= 0 && S(n)) add_pair(n, ld);
+        }
+        if (!x.src.empty()) tp.push_back(std::move(x));
+    }
+    // sibling groups: a target joins its parent's group when the structured
+    // candidate set (children of the parent's 27 neighbours; non-adjacent ones
+    // only below the sweep level) reproduces its pair list exactly
+    struct Grp
+    {
+        u64 pkey;
+        int ld;
+        std::array<int, 8> tgt;
+        std::array<int, 216> cand;  // source slot or -1
+        std::array<bool, 216> used;
+    };
+    std::map<std::pair<int, u64>, int> gidx;
+    std::vector<Grp> groups;
+    std::vector<char> in_group(tp.size(), 0);
+    auto adjacent = [](int cc, int k) {
+        const int n = k / 8, cp = k % 8;
+        const int ux = (cc & 1) - (cp & 1) - 2 * (n % 3 - 1);
+        const int uy = ((cc >> 1) & 1) - ((cp >> 1) & 1) - 2 * ((n / 3) % 3 - 1);
+        const int uz = ((cc >> 2) & 1) - ((cp >> 2) & 1) - 2 * (n / 9 - 1);
+        return std::abs(ux) <= 1 && std::abs(uy) <= 1 && std::abs(uz) <= 1;
+    };
+    for (size_t i = 0; i < tp.size(); ++i)
+    {
+        const int t = tp[i].t;
+        if (c.levels[t] == 0) continue;
+        const int ld = level - c.levels[t];
+        const u64 pk = key_parent(c.keys[t]);
+        const int cc = key_child_number(c.keys[t], c.levels[t]);
+        std::array<int, 216> cand;
+        int k = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx)
+                {
+                    const u64 pn = key_neighbor(pk, dx, dy, dz);
+                    for (int cp = 0; cp < 8; ++cp, ++k)
+                    {
+                        auto it = c.key_index.find(key_child(pn, cp));
+                        const int o = it == c.key_index.end() ? -1 : it->second;
+                        cand[k] = (o >= 0 && S(o)) ? src_slot[o] : -1;
+                    }
+                }
+        std::vector<int> mine;
+        for (int kk = 0; kk < 216; ++kk)
+            if (cand[kk] >= 0 && (ld == 0 || !adjacent(cc, kk))) mine.push_back(cand[kk]);
+        std::vector<int> ref = tp[i].src;
+        std::sort(mine.begin(), mine.end());
+        std::sort(ref.begin(), ref.end());
+        if (mine != ref) continue;
+        auto key = std::make_pair(c.levels[t], pk);
+        auto it = gidx.find(key);
+        int g;
+        if (it == gidx.end())
+        {
+            g = (int)groups.size();
+            gidx.emplace(key, g);
+            Grp gr;
+            gr.pkey = pk;
+            gr.ld = ld;
+            gr.tgt.fill(-1);
+            gr.cand = cand;
+            gr.used.fill(false);
+            groups.push_back(gr);
+        }
+        else
+            g = it->second;
+        groups[g].tgt[cc] = (int)i;  // temporary: index into tp
+        for (int kk = 0; kk < 216; ++kk)
+            if (cand[kk] >= 0 && (ld == 0 || !adjacent(cc, kk))) groups[g].used[kk] = true;
+        in_group[i] = 1;
+    }
+    // target slots: pair-list targets first, then group targets in group order
+    std::vector<int> tgt_list, ptr{0}, psrc, pspec;
+    std::vector<int> slot_of_tp(tp.size(), -1);
+    for (size_t i = 0; i < tp.size(); ++i)
+    {
+        if (in_group[i]) continue;
+        slot_of_tp[i] = (int)tgt_list.size();
+        tgt_list.push_back(tp[i].t);
+        psrc.insert(psrc.end(), tp[i].src.begin(), tp[i].src.end());
+        pspec.insert(pspec.end(), tp[i].spec.begin(), tp[i].spec.end());
+        ptr.push_back((int)psrc.size());
+    }
+    p.n_csr_tgt = (int)tgt_list.size();
+    // groups ordered by (sweep level distance, parent key): spatially coherent tiles
+    std::vector<int> gorder(groups.size());
+    for (size_t g = 0; g < groups.size(); ++g) gorder[g] = (int)g;
+    std::sort(gorder.begin(), gorder.end(), [&](int a, int b) {
+        return groups[a].ld != groups[b].ld ? groups[a].ld < groups[b].ld : groups[a].pkey < groups[b].pkey;
+    });
+    for (int g : gorder)
+        for (int cc = 0; cc < 8; ++cc)
+        {
+            const int i = groups[g].tgt[cc];
+            if (i < 0) continue;
+            slot_of_tp[i] = (int)tgt_list.size();
+            tgt_list.push_back(tp[i].t);
+        }
+    // per-ld spectrum slot tables over the 343 offsets
+    std::map<int, int> tab_of_ld;
+    std::vector<int> spec_u;
+    for (auto& gr : groups)
+    {
+        if (tab_of_ld.count(gr.ld)) continue;
+        tab_of_ld[gr.ld] = (int)tab_of_ld.size();
+        for (int u = 0; u < 343; ++u)
+        {
+            const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
+            const std::array<int, 4> k{gr.ld, ux * e - (Nb - 1), uy * e - (Nb - 1), uz * e - (Nb - 1)};
+            auto it = c.spec_slot.find(k);
+            spec_u.push_back(it == c.spec_slot.end() ? -1 : it->second);
+        }
+    }
+    // tiles: consecutive groups of one level distance while the union of their
+    // sources fits the staging budget
+    const int kScap = 1152, kGcap = 32;
+    std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
+    std::vector<unsigned short> gsrc;
+    std::map<int, int> local;
+    int cur_ld = -1, ngrp = 0, max_src = 0;
+    auto close_tile = [&]() {
+        if (!ngrp) return;
+        tgptr.push_back((int)gtgt.size() / 8);
+        tsptr.push_back((int)tsrc.size());
+        ttab.push_back(tab_of_ld[cur_ld]);
+        tcoarse.push_back(cur_ld > 0 ? 1 : 0);
+        max_src = std::max(max_src, (int)local.size());
+        local.clear();
+        ngrp = 0;
+    };
+    for (int g : gorder)
+    {
+        const Grp& gr = groups[g];
+        int extra = 0;
+        for (int kk = 0; kk < 216; ++kk)
+            if (gr.used[kk] && !local.count(gr.cand[kk])) ++extra;
+        if (ngrp && (gr.ld != cur_ld || ngrp >= kGcap || (int)local.size() + extra > kScap)) close_tile();
+        cur_ld = gr.ld;
+        for (int kk = 0; kk < 216; ++kk)
+        {
+            if (!gr.used[kk])
+            {
+                gsrc.push_back(0xFFFF);
+                continue;
+            }
+            auto it = local.find(gr.cand[kk]);
+            int j;
+            if (it == local.end())
+            {
+                j = (int)local.size();
+                local.emplace(gr.cand[kk], j);
+                tsrc.push_back(gr.cand[kk]);
+            }
+            else
+                j = it->second;
+            gsrc.push_back((unsigned short)j);
+        }
+        for (int cc = 0; cc < 8; ++cc) gtgt.push_back(gr.tgt[cc] >= 0 ? slot_of_tp[gr.tgt[cc]] : -1);
+        ++ngrp;
+    }
+    close_tile();
+    p.n_groups = (int)groups.size();
+    p.n_tiles = (int)ttab.size();
+    p.max_tile_src = max_src;
+    p.tile_gptr.upload(tgptr, c.stream);
+    p.tile_sptr.upload(tsptr, c.stream);
+    p.tile_src.upload(tsrc, c.stream);
+    p.tile_tab.upload(ttab, c.stream);
+    p.tile_coarse.upload(tcoarse, c.stream);
+    p.spec_u.upload(spec_u, c.stream);
+    p.grp_src.upload(gsrc, c.stream);
+    p.grp_tgt.upload(gtgt, c.stream);
+    p.n_tgt = (int)tgt_list.size();
+    p.n_pairs = 0;
+    for (auto& x : tp) p.n_pairs += (long long)x.src.size();
+    {
+        std::vector<int> u;
+        for (auto& x : tp) u.insert(u.end(), x.spec.begin(), x.spec.end());
+        std::sort(u.begin(), u.end());
+        p.n_spec_unique = (int)(std::unique(u.begin(), u.end()) - u.begin());
+    }
+    p.tgt_oct.upload(tgt_list, c.stream);
+    p.pair_ptr.upload(ptr, c.stream);
+    p.pair_src.upload(psrc, c.stream);
+    p.pair_spec.upload(pspec, c.stream);
+    // grow the spectra cache and fill the new slots
+    if (!new_slots.empty())
+    {
+        const int need = (int)c.spec_slot.size();
+        if (need > c.spec_cap)
+        {
+            const int cap = std::max(need, c.spec_cap * 2);
+            DevBuf<char> nb;
+            nb.alloc((size_t)cap * c.NC * c.cplx_bytes());
+            if (c.spec_used)
+                IBLGF_CUDA(cudaMemcpyAsync(nb.p, c.d_spec.p, (size_t)c.spec_used * c.NC * c.cplx_bytes(),
+                                           cudaMemcpyDeviceToDevice, c.stream));
+            IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+            c.d_spec = std::move(nb);
+            c.spec_cap = cap;
+        }
+        launch_spectra(c, new_slots);
+        c.spec_used = need;
+    }
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    auto& ref = *plan;
+    c.plans.emplace(key, std::move(plan));
+    return ref;
+}
+
+void ensure_bytes(DevBuf<char>& b, size_t bytes)
+{
+    if (b.n < bytes) b.alloc(bytes);
+}
+
+struct Timer
+{
+    // phase events recorded on the context stream; read back (and summed) by
+    // iblgf_profile_read, so profiling adds no host synchronisation
+    Ctx& c;
+    std::array<cudaEvent_t, 5> ev{};
+    bool on;
+    explicit Timer(Ctx& cc)
+    : c(cc)
+    , on(cc.profile)
+    {
+        if (on)
+            for (auto& e : ev) IBLGF_CUDA(cudaEventCreate(&e));
+    }
+    void mark(int i)
+    {
+        if (on) IBLGF_CUDA(cudaEventRecord(ev[i], c.stream));
+    }
+    ~Timer()
+    {
+        if (on) c.prof_events.push_back(ev);
+    }
+};
+}  // namespace
+
+void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_scale, int fmm_type)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (level < c.tree.base_level || level >= c.tree.depth) throw Error(IBLGF_EINVAL, "level out of range");
+    const int rl = level - c.tree.base_level;
+    const int idx = fmm_type == IBLGF_STREAM ? mask_idx_gen(IBLGF_STREAM, 0, 0)
+                                              : mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0);
+    upload_group_offsets();
+    FmmPlan& p = get_plan(c, level, idx);
+    c.stats[0] += 1;
+    c.stats[1] += p.n_src;
+    c.stats[2] += p.n_tgt;
+    c.stats[3] += p.n_pairs;
+    c.stats[4] += p.n_spec_unique;
+    for (auto& t : p.antrp) c.stats[5] += t.n_tasks;
+    for (auto& t : p.intrp) c.stats[6] += t.n_tasks;
+    const double dx_level = c.cfg.dx_base / std::pow(2.0, rl);
+    double* fs = c.field(c.f_fmm_s);
+    double* ft = c.field(c.f_fmm_t);
+    Timer tm(c);
+    tm.mark(0);
+    launch_zero_blocks(c, fs, p.zero_s.p, (int)p.zero_s.n);
+    launch_zero_blocks(c, ft, p.zero_t.p, (int)p.zero_t.n);
+    launch_copy_interior(c, c.field(src), fs, p.copy_s.p, (int)p.copy_s.n);
+    for (auto& t : p.antrp) launch_tp(c, t, fs, fs, 0, 0);
+    tm.mark(1);
+    const size_t cb = c.cplx_bytes();
+    if (!p.empty())
+    {
+        ensure_bytes(c.d_src_spec, (size_t)p.n_src * c.NC * cb);
+        ensure_bytes(c.d_acc, (size_t)p.n_tgt * c.NC * cb);
+        launch_forward_sources(c, fs, p.src_oct.p, p.n_src, c.d_src_spec.p);
+    }
+    tm.mark(2);
+    if (!p.empty()) launch_mac(c, p, c.d_src_spec.p, c.d_acc.p);
+    tm.mark(3);
+    if (!p.empty())
+    {
+        const double scale = dx_level * dx_level / ((double)c.P * c.P * c.P);
+        launch_inverse_add(c, p, c.d_acc.p, ft, scale);
+    }
+    for (auto& t : p.intrp) launch_tp(c, t, ft, ft, 0, 1);
+    launch_axpy_blocks(c, ft, c.field(tgt), p.add_t.p, (int)p.add_t.n, add_with_scale, false);
+    tm.mark(4);
+}
+
+// --------------------------------------------------------------- Poisson
+namespace
+{
+struct PoissonLists
+{
+    DevBuf<int> all, leaves;
+    std::vector<DevBuf<int>> level_all, level_leaves;
+    std::vector<TpTasks> coarsify;       // per level ls (dst parents at ls)
+    std::vector<TpTasks> cc_intrp;       // per level l: children of level-l octants
+    std::vector<TpTasks> corr_intrp;     // per level l: correction children
+    std::vector<DevBuf<int>> children;   // per level l: children (with data) of level-l octants
+};
+std::map<const Ctx*, std::unique_ptr<PoissonLists>> g_plists;
+
+PoissonLists& poisson_lists(Ctx& c)
+{
+    auto it = g_plists.find(&c);
+    if (it != g_plists.end()) return *it->second;
+    auto pl = std::make_unique<PoissonLists>();
+    std::vector<int> all, leaves;
+    for (int i = 0; i < c.n_oct; ++i)
+    {
+        all.push_back(i);
+        if (c.flags[i] & 1) leaves.push_back(i);
+    }
+    pl->all.upload(all, c.stream);
+    pl->leaves.upload(leaves, c.stream);
+    const int L = kMaxLevel + 1;
+    pl->level_all.resize(L);
+    pl->level_leaves.resize(L);
+    pl->coarsify.resize(L);
+    pl->cc_intrp.resize(L);
+    pl->corr_intrp.resize(L);
+    pl->children.resize(L);
+    for (int l = 0; l < (int)c.level_octs.size(); ++l)
+    {
+        std::vector<int> la, ll, ch;
+        std::vector<int> cdst, idst, kdst;
+        std::vector<std::vector<std::pair<int, int>>> ctasks, itasks, ktasks;
+        for (int o : c.level_octs[l])
+        {
+            la.push_back(o);
+            if (c.flags[o] & 1) ll.push_back(o);
+            cdst.push_back(o);
+            ctasks.emplace_back();
+            for (int k = 0; k < 8; ++k)
+            {
+                const int x = c.child[8 * o + k];
+                if (x < 0) continue;
+                ctasks.back().push_back({x, k});
+                idst.push_back(x);
+                itasks.push_back({{o, k}});
+                ch.push_back(x);
+                if (c.flags[x] & 2)
+                {
+                    kdst.push_back(x);
+                    ktasks.push_back({{o, k}});
+                }
+            }
+        }
+        pl->level_all[l].upload(la, c.stream);
+        pl->level_leaves[l].upload(ll, c.stream);
+        pl->children[l].upload(ch, c.stream);
+        upload_tasks(c, pl->coarsify[l], cdst, ctasks);
+        upload_tasks(c, pl->cc_intrp[l], idst, itasks);
+        upload_tasks(c, pl->corr_intrp[l], kdst, ktasks);
+    }
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    auto& ref = *pl;
+    g_plists.emplace(&c, std::move(pl));
+    return ref;
+}
+}  // namespace
+
+void poisson_release(const Ctx* c) { g_plists.erase(c); }
+
+void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (fmm_type != IBLGF_AMR2AMR) throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR");
+    PoissonLists& pl = poisson_lists(c);
+    double* st = c.field(c.f_source_tmp);
+    double* tt = c.field(c.f_target_tmp);
+    double* ct = c.field(c.f_correction_tmp);
+    const size_t bytes = c.field_elems() * sizeof(double);
+    IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
+    IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
+    IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
+    const int bl = c.tree.base_level, depth = c.tree.depth;
+    for (int ls = depth - 2; ls >= bl; --ls) launch_tp(c, pl.coarsify[ls], st, st, 4, 0);
+    for (int l = bl; l < depth; ++l)
+    {
+        if (!c.subtract_non_leaf)
+        {
+            fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, true, 1.0, IBLGF_AMR2AMR);
+            launch_tp(c, pl.cc_intrp[l], tt, tt, 2, 2);
+            fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, false, 1.0, IBLGF_AMR2AMR);
+            launch_axpy_blocks(c, tt, c.field(tgt), pl.level_leaves[l].p, (int)pl.level_leaves[l].n, 1.0, true);
+        }
+        if (!c.use_correction || l == depth - 1) continue;
+        launch_halo(c, st, pl.level_all[l].p, (int)pl.level_all[l].n);
+        launch_tp(c, pl.corr_intrp[l], st, ct, 2, 2);
+        const double dx = c.cfg.dx_base / std::pow(2.0, l - bl) / 2.0;
+        launch_source_correction(c, tt, ct, pl.children[l].p, (int)pl.children[l].n, 1.0 / (dx * dx));
+        launch_axpy_blocks(c, ct, st, pl.level_all[l + 1].p, (int)pl.level_all[l + 1].n, 1.0, false);
+    }
+}
+
+}  // namespace iblgf_b200

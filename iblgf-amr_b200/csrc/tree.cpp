@@ -1,0 +1,322 @@
+// Host octree construction with the reference's semantics, in an index-based
+// layout (one vector of octants, children by index):
+//   base mesh  include/iblgf/domain/domain.hpp:405-488, construct_tree :190-230
+//   refine     include/iblgf/domain/octree/tree.hpp:385-453 (2:1 balance),
+//              try_2to1 :336-383, insert/find :270-300
+//   init_refine domain.hpp:878-939 — refinement candidates are visited in the
+//              reference iterator's depth-first order (iterators.hpp:265-282),
+//              so octants created by 2:1 balancing during a pass are visited
+//              exactly when the reference would visit them
+//   mark_correction domain.hpp:617-736.
+// The neighbour and influence lists of the finished tree are built on the
+// device (lists.cu). Only one process owns the tree, so "locally owned" is
+// always true.
+#include <algorithm>
+#include <cmath>
+#include <stack>
+
+#include "ctx.hpp"
+
+namespace iblgf_b200
+{
+void HostTree::init(int block_extent, const int* bd_base, const int* bd_extent)
+{
+    e = block_extent;
+    int mx = 0;
+    for (int d = 0; d < 3; ++d)
+    {
+        base_shift[d] = bd_base[d] / block_extent;
+        key_bd_extent[d] = bd_extent[d] / block_extent;
+        mx = std::max(mx, key_bd_extent[d]);
+    }
+    base_level = 0;
+    while (mx >= (1 << base_level)) ++base_level;  // Key::minimum_level
+    depth = base_level + 1;
+    o.clear();
+    HOct root;
+    root.key = key_make(0, 0, 0, 0);
+    root.level = 0;
+    o.push_back(root);
+}
+
+void HostTree::add_base_blocks(const std::vector<std::array<int, 3>>& nb)
+{
+    for (auto& b : nb)
+        insert(key_make(b[0] - base_shift[0], b[1] - base_shift[1], b[2] - base_shift[2], base_level));
+    // every octant of the initial tree gets a block at level 0
+    for (int i : dfs_order()) alloc(i, 0);
+}
+
+int HostTree::find(u64 k) const
+{
+    int n = 0;
+    const int l = key_level(k);
+    for (int i = 1; i <= l; ++i)
+    {
+        n = o[n].child[key_child_number(k, i)];
+        if (n < 0) return -1;
+    }
+    return n;
+}
+
+int HostTree::refine_child(int p, int i)
+{
+    if (o[p].child[i] < 0)
+    {
+        HOct c;
+        c.key = key_child(o[p].key, i);
+        c.level = o[p].level + 1;
+        c.parent = p;
+        o.push_back(c);
+        o[p].child[i] = (int)o.size() - 1;
+    }
+    return o[p].child[i];
+}
+
+int HostTree::insert(u64 k)
+{
+    int n = 0;
+    const int l = key_level(k);
+    for (int i = 1; i <= l; ++i) n = refine_child(n, key_child_number(k, i));
+    depth = std::max(depth, l + 1);
+    return n;
+}
+
+void HostTree::alloc(int i, int data_level)
+{
+    int c[3];
+    key_coord(o[i].key, c);
+    const int s = 1 << std::max(data_level, 0);
+    for (int d = 0; d < 3; ++d) o[i].bbase[d] = (c[d] + base_shift[d] * s) * e;
+    o[i].has_data = true;
+}
+
+std::vector<int> HostTree::dfs_order() const
+{
+    std::vector<int> out;
+    std::vector<int> st{0};
+    out.push_back(0);
+    while (!st.empty())
+    {
+        const int cur = st.back();
+        st.pop_back();
+        for (int i = 7; i >= 0; --i)
+            if (o[cur].child[i] >= 0) st.push_back(o[cur].child[i]);
+        if (o[cur].level == 0) continue;
+        out.push_back(cur);
+    }
+    return out;
+}
+
+std::vector<u64> HostTree::unfound_neighbors(int i, bool correction_as_neighbors) const
+{
+    std::vector<u64> keys;
+    const u64 k = o[i].key;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+            {
+                const u64 nk = key_neighbor(k, dx, dy, dz);
+                if (key_is_end(nk) || nk == k) continue;
+                const int n = find(nk);
+                if (n < 0 || !o[n].has_data) keys.push_back(nk);
+                else if (!correction_as_neighbors && o[n].correction)
+                    keys.push_back(nk);
+            }
+    return keys;
+}
+
+bool HostTree::try_2to1(u64 k, std::map<u64, bool>& checklist) const
+{
+    auto it = checklist.find(k);
+    if (it != checklist.end()) return it->second;
+    const int rf = key_level(k) - base_level;
+    bool ok = true;
+    if (rf < 0) return false;
+    for (int dz = -1; dz <= 1 && ok; ++dz)
+        for (int dy = -1; dy <= 1 && ok; ++dy)
+            for (int dx = -1; dx <= 1 && ok; ++dx)
+            {
+                const u64 nk = key_neighbor(k, dx, dy, dz);
+                if (nk == k) continue;
+                if (rf == 0)
+                {
+                    int c[3];
+                    key_coord(nk, c);
+                    for (int d = 0; d < 3; ++d)
+                        if (c[d] < 0 || c[d] > key_bd_extent[d] - 1) ok = false;
+                }
+                else if (!try_2to1(key_parent(nk), checklist))
+                    ok = false;
+            }
+    checklist.emplace(k, ok);
+    return ok;
+}
+
+void HostTree::refine(int l, bool ratio_2to1)
+{
+    auto f = [&](int x) { alloc(x, o[x].level - base_level); };
+    if (ratio_2to1 && o[l].level - base_level >= 0)
+    {
+        for (u64 k : unfound_neighbors(l, false))
+        {
+            if (key_is_end(k)) continue;
+            if (o[l].level - base_level == 0)
+            {
+                const int n = insert(k);
+                if (!o[n].has_data) f(n);
+                o[n].leaf = true;
+                o[n].correction = false;
+            }
+            else
+            {
+                const u64 pk = key_parent(k);
+                int pa = find(pk);
+                if (pa < 0)
+                {
+                    pa = insert(pk);
+                    f(pa);
+                }
+                refine(pa, ratio_2to1);
+            }
+        }
+    }
+    for (int i = 0; i < 8; ++i)
+    {
+        const int ci = o[l].child[i];
+        if (ci >= 0 && o[ci].has_data) continue;
+        const int c = refine_child(l, i);
+        if (!o[c].has_data) f(c);
+    }
+    for (int i = 0; i < 8; ++i)
+    {
+        HOct& c = o[o[l].child[i]];
+        c.leaf = true;
+        c.correction = false;
+    }
+    o[l].leaf = false;
+    o[l].correction = false;
+    depth = std::max(depth, o[l].level + 2);
+}
+
+void HostTree::init_refine(int n_ref, int level_up_max, iblgf_refine_fn pred, void* user)
+{
+    // construct_leaf_maps(): leaf = no children at all
+    for (int i : dfs_order())
+    {
+        if (!o[i].has_data) continue;
+        bool leaf = true;
+        for (int c : o[i].child)
+            if (c >= 0) leaf = false;
+        o[i].leaf = leaf;
+    }
+    std::map<u64, bool> checklist;
+    for (int l = 0; l < n_ref; ++l)
+    {
+        std::vector<int> st{0};
+        while (!st.empty())
+        {
+            const int cur = st.back();
+            st.pop_back();
+            for (int i = 7; i >= 0; --i)
+                if (o[cur].child[i] >= 0) st.push_back(o[cur].child[i]);
+            if (o[cur].level == 0 || o[cur].level - base_level != l) continue;
+            int ext[3] = {e, e, e};
+            if (pred && pred(user, o[cur].bbase, ext, l, n_ref - l))
+                if (try_2to1(o[cur].key, checklist)) refine(cur, true);
+        }
+    }
+    for (int g = 0; g < level_up_max; ++g)
+    {
+        for (int l = depth - 1; l >= base_level; --l)
+        {
+            std::vector<std::pair<u64, int>> lv;
+            for (int i = 0; i < (int)o.size(); ++i)
+                if (o[i].has_data && o[i].level == l) lv.push_back({o[i].key, i});
+            std::sort(lv.begin(), lv.end());
+            for (auto& kv : lv)
+                if (o[kv.second].leaf) refine(kv.second, false);
+        }
+    }
+    mark_correction();
+}
+
+void HostTree::mark_correction()
+{
+    for (auto& x : o) x.physical = false;
+    for (int l = depth - 1; l >= base_level; --l)
+        for (int i = 0; i < (int)o.size(); ++i)
+        {
+            if (!o[i].has_data || o[i].level != l) continue;
+            o[i].physical = o[i].leaf;
+            if (!o[i].physical)
+                for (int c : o[i].child)
+                    if (c >= 0 && o[c].has_data) o[i].physical = o[i].physical || o[c].physical;
+        }
+    // correction buffers around physical octants of refined levels
+    for (int l = base_level + 1; l < depth; ++l)
+    {
+        std::vector<int> lv;
+        for (int i = 0; i < (int)o.size(); ++i)
+            if (o[i].has_data && o[i].level == l) lv.push_back(i);
+        for (int i : lv)
+        {
+            if (!o[i].physical) continue;
+            for (u64 k : unfound_neighbors(i, true))
+            {
+                const int n = insert(k);
+                if (!o[n].has_data) alloc(n, o[n].level - base_level);
+            }
+        }
+    }
+    auto neighbors_of = [&](int i, int* out) {
+        int m = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx)
+                {
+                    const int n = find(key_neighbor(o[i].key, dx, dy, dz));
+                    out[m++] = (n >= 0 && o[n].has_data) ? n : -1;
+                }
+    };
+    int nb[27];
+    for (int l = base_level + 1; l < depth; ++l)
+        for (int i = 0; i < (int)o.size(); ++i)
+        {
+            if (!o[i].has_data || o[i].level != l || !o[i].physical) continue;
+            neighbors_of(i, nb);
+            for (int n : nb)
+            {
+                if (n < 0 || o[n].physical) continue;
+                o[n].correction = true;
+            }
+        }
+    for (int i = 0; i < (int)o.size(); ++i)
+    {
+        if (!o[i].has_data || o[i].level != base_level || !o[i].physical) continue;
+        neighbors_of(i, nb);
+        bool all = true;
+        for (int n : nb)
+            if (n < 0) all = false;
+        if (!all)
+        {
+            o[i].correction = true;
+            o[i].leaf = true;
+        }
+        else
+            o[i].correction = false;
+    }
+}
+
+std::vector<int> HostTree::canonical() const
+{
+    std::vector<std::pair<std::pair<int, u64>, int>> v;
+    for (int i = 0; i < (int)o.size(); ++i)
+        if (o[i].has_data) v.push_back({{o[i].level, o[i].key}, i});
+    std::sort(v.begin(), v.end());
+    std::vector<int> out;
+    for (auto& x : v) out.push_back(x.second);
+    return out;
+}
+
+}  // namespace iblgf_b200

@@ -1,0 +1,254 @@
+"""Python binding of libiblgf_b200.so (the C ABI in include/iblgf_b200.h).
+
+Host-side mirror of the reference's solver surface for scripts and tests:
+`Domain` (Domain::initialize + init_refine + distribute), `Solver.fmm_apply`
+(Fmm::apply) and `Solver.apply_lgf` (PoissonSolver::apply_lgf). All compute
+runs in the CUDA library; there is no CPU path. Loading fails loudly if the
+library has not been built (`make -C iblgf-amr_b200`).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libiblgf_b200.so")
+
+FP64, FP32 = 0, 1
+STREAM, AMR2AMR = 0, 1
+
+REFINE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("block_extent", ctypes.c_int), ("bd_base", ctypes.c_int * 3),
+                ("bd_extent", ctypes.c_int * 3), ("dx_base", ctypes.c_double),
+                ("precision", ctypes.c_int), ("device", ctypes.c_int),
+                ("intrp_order", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+EXPORTS = [
+    "iblgf_create", "iblgf_destroy", "iblgf_last_error", "iblgf_synchronize",
+    "iblgf_domain_add_blocks", "iblgf_domain_init_refine", "iblgf_domain_finalize",
+    "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
+    "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
+    "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf",
+    "iblgf_poisson_options", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block",
+    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
+    "iblgf_fma_peak",
+]
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libiblgf_b200.so is not built; run `make -C %s`" % HERE)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ci, cd, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.iblgf_create.argtypes = [ctypes.POINTER(Config), pp]
+    L.iblgf_destroy.argtypes = [vp]
+    L.iblgf_last_error.argtypes = [vp]
+    L.iblgf_last_error.restype = ctypes.c_char_p
+    L.iblgf_synchronize.argtypes = [vp]
+    L.iblgf_domain_add_blocks.argtypes = [vp, ci, vp, vp]
+    L.iblgf_domain_init_refine.argtypes = [vp, ci, ci, REFINE_FN, vp]
+    L.iblgf_domain_finalize.argtypes = [vp, ci]
+    L.iblgf_domain_info.argtypes = [vp, vp, vp, vp]
+    L.iblgf_domain_octants.argtypes = [vp, vp, vp, vp, vp]
+    L.iblgf_domain_lists.argtypes = [vp, vp, vp, vp]
+    L.iblgf_domain_masks.argtypes = [vp, ci, vp]
+    L.iblgf_field_create.argtypes = [vp, vp]
+    L.iblgf_field_zero.argtypes = [vp, ci]
+    L.iblgf_field_upload.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_download.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_device_ptr.argtypes = [vp, ci, pp]
+    L.iblgf_fmm_apply.argtypes = [vp, ci, ci, ci, ci, cd, ci]
+    L.iblgf_poisson_apply_lgf.argtypes = [vp, ci, ci, ci]
+    L.iblgf_poisson_options.argtypes = [vp, ci, ci]
+    L.iblgf_lgf_table.argtypes = [vp, vp, sz]
+    L.iblgf_lgf_get.argtypes = [vp, vp, sz, vp]
+    L.iblgf_conv_block.argtypes = [vp, vp, vp, vp, cd]
+    L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.iblgf_profile.argtypes = [vp, ci]
+    L.iblgf_profile_read.argtypes = [vp, vp]
+    L.iblgf_stats.argtypes = [vp, vp]
+    L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class IblgfError(RuntimeError):
+    pass
+
+
+class Solver:
+    """Domain + LGF-FMM Poisson solver on one GPU.
+
+    Mirrors the reference set-up sequence: Domain(dictionary) ->
+    init_refine(nLevels, global_refinement) -> distribute<FmmMaskBuilder>() ->
+    PoissonSolver(simulation). `predicate(base, extent, refinement_level,
+    diff_level)` plays the role of Domain::register_refinement_condition().
+    """
+
+    def __init__(self, bd_base, bd_extent, block_extent, dx_base, blocks, n_levels=0,
+                 global_refinement=0, predicate=None, precision=FP64, subtract_non_leaf=False,
+                 intrp_order=5, device=0, stream=None, use_correction=True):
+        L = lib()
+        cfg = Config(block_extent, (ctypes.c_int * 3)(*bd_base), (ctypes.c_int * 3)(*bd_extent),
+                     float(dx_base), int(precision), int(device), int(intrp_order),
+                     ctypes.c_void_p(stream) if stream else None)
+        h = ctypes.c_void_p()
+        rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+        self.h = h
+        self.Nb = block_extent + 2
+        self.block_extent = block_extent
+        self.precision = precision
+        bb = np.array([b[0] for b in blocks], np.int32).ravel()
+        be = np.array([b[1] for b in blocks], np.int32).ravel()
+        self._check(L.iblgf_domain_add_blocks(self.h, len(blocks), _p(bb), _p(be)))
+        if predicate is not None:
+            def cb(user, base, ext, rl, diff):
+                return 1 if predicate((base[0], base[1], base[2]), (ext[0], ext[1], ext[2]), rl, diff) else 0
+            self._cb = REFINE_FN(cb)
+        else:
+            self._cb = REFINE_FN(lambda *a: 0)
+        self._check(L.iblgf_domain_init_refine(self.h, int(n_levels), int(global_refinement), self._cb, None))
+        self._check(L.iblgf_domain_finalize(self.h, 1 if subtract_non_leaf else 0))
+        self._check(L.iblgf_poisson_options(self.h, 1 if use_correction else 0, 1 if subtract_non_leaf else 0))
+        bl, dp, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(L.iblgf_domain_info(self.h, ctypes.byref(bl), ctypes.byref(dp), ctypes.byref(n)))
+        self.base_level, self.depth, self.n = bl.value, dp.value, n.value
+        self.keys = np.zeros(self.n, np.uint64)
+        self.levels = np.zeros(self.n, np.int32)
+        self.flags = np.zeros(self.n, np.int32)
+        self.bbase = np.zeros((self.n, 3), np.int32)
+        self._check(L.iblgf_domain_octants(self.h, _p(self.keys), _p(self.levels), _p(self.flags), _p(self.bbase)))
+
+    # ------------------------------------------------------------ basics
+    def _check(self, rc):
+        if rc != 0:
+            raise IblgfError("iblgf error %d: %s" % (rc, lib().iblgf_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().iblgf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def leaf(self):
+        return (self.flags & 1) != 0
+
+    @property
+    def correction(self):
+        return (self.flags & 2) != 0
+
+    def lists(self):
+        nbr = np.zeros((self.n, 27), np.int32)
+        infl = np.zeros((self.n, 189), np.int32)
+        ni = np.zeros(self.n, np.int32)
+        self._check(lib().iblgf_domain_lists(self.h, _p(nbr), _p(infl), _p(ni)))
+        return nbr, infl, ni
+
+    def masks(self, idx):
+        out = np.zeros((self.n, 2), np.uint8)
+        self._check(lib().iblgf_domain_masks(self.h, int(idx), _p(out)))
+        return out
+
+    def zeros(self):
+        return np.zeros((self.n, self.Nb, self.Nb, self.Nb))
+
+    # ------------------------------------------------------------ fields
+    def field(self, values=None):
+        f = ctypes.c_int()
+        self._check(lib().iblgf_field_create(self.h, ctypes.byref(f)))
+        if values is not None:
+            self.upload(f.value, values)
+        return f.value
+
+    def upload(self, fid, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(lib().iblgf_field_upload(self.h, fid, _p(a), a.size))
+        self._keep = a  # the copy is asynchronous; keep the host buffer alive
+
+    def download(self, fid, out=None):
+        a = self.zeros() if out is None else out
+        self._check(lib().iblgf_field_download(self.h, fid, _p(a), a.size))
+        return a
+
+    def zero(self, fid):
+        self._check(lib().iblgf_field_zero(self.h, fid))
+
+    def device_ptr(self, fid):
+        p = ctypes.c_void_p()
+        self._check(lib().iblgf_field_device_ptr(self.h, fid, ctypes.byref(p)))
+        return p.value
+
+    def synchronize(self):
+        self._check(lib().iblgf_synchronize(self.h))
+
+    # ------------------------------------------------------------ solver
+    def fmm_apply(self, src, tgt, level, non_leaf_as_source, scale=1.0, fmm_type=AMR2AMR):
+        self._check(lib().iblgf_fmm_apply(self.h, src, tgt, int(level), int(non_leaf_as_source),
+                                          float(scale), int(fmm_type)))
+
+    def apply_lgf(self, src, tgt, fmm_type=AMR2AMR):
+        self._check(lib().iblgf_poisson_apply_lgf(self.h, src, tgt, int(fmm_type)))
+
+    def lgf_table(self):
+        out = np.zeros(176851)
+        self._check(lib().iblgf_lgf_table(self.h, _p(out), out.size))
+        return out
+
+    def lgf_get(self, coords):
+        c = np.ascontiguousarray(np.asarray(coords, dtype=np.int32).reshape(-1, 3))
+        out = np.zeros(c.shape[0])
+        self._check(lib().iblgf_lgf_get(self.h, _p(c), c.shape[0], _p(out)))
+        return out
+
+    def conv_block(self, src_dptr, kernel_dptr, out_dptr, scale=1.0):
+        self._check(lib().iblgf_conv_block(self.h, ctypes.c_void_p(src_dptr), ctypes.c_void_p(kernel_dptr),
+                                           ctypes.c_void_p(out_dptr), float(scale)))
+
+    def launches(self):
+        n = ctypes.c_longlong()
+        self._check(lib().iblgf_kernel_launches(self.h, ctypes.byref(n)))
+        return n.value
+
+    def profile(self, enable=True):
+        self._check(lib().iblgf_profile(self.h, 1 if enable else 0))
+
+    def stats(self):
+        out = np.zeros(8, np.int64)
+        self._check(lib().iblgf_stats(self.h, _p(out)))
+        return out
+
+    def fma_peak(self, precision):
+        v = ctypes.c_double()
+        self._check(lib().iblgf_fma_peak(self.h, int(precision), ctypes.byref(v)))
+        return v.value
+
+    def profile_read(self):
+        out = np.zeros(4)
+        self._check(lib().iblgf_profile_read(self.h, _p(out)))
+        return out
+
+
+def from_case(case, **kw):
+    """Build a Solver for an iblgf_setups case object."""
+    return Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                  n_levels=getattr(case, "n_levels", 0), predicate=getattr(case, "predicate", None), **kw)

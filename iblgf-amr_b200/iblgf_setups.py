@@ -115,20 +115,30 @@ class GaussianPoisson:
         self.block_extent = block_extent
         self.dx_base = 1.0
         g = [(1.0, 4.0, (12.0, 0.0, 0.0)), (-1.0, 4.0, (-12.0, 0.0, 0.0))]
+        n_random, sig_range = 0, (2.0, 6.0)
         if name == "uniform_64":
             half = 32
             self.n_levels = 0
         elif name == "amr_3level":
             half = 64
             self.n_levels = 2
+            n_random = 16
+        elif name in ("uniform_small", "amr_small"):
+            # reduced parity cases: 4x4x4 base blocks of 6^3 cells
+            self.block_extent = block_extent = 6
+            half = 12
+            g = [(1.0, 1.5, (4.5, 0.0, 0.0)), (-1.0, 1.5, (-4.5, 0.0, 0.0))]
+            self.n_levels = 0 if name == "uniform_small" else 2
+            n_random, sig_range = (6 if name == "amr_small" else 0), (0.8, 2.0)
+        else:
+            raise ValueError(name)
+        if n_random:
             rng = np.random.Generator(np.random.PCG64(seed))
-            for _ in range(16):
-                sig = rng.uniform(2.0, 6.0)
+            for _ in range(n_random):
+                sig = rng.uniform(*sig_range)
                 amp = rng.uniform(-1.0, 1.0)
                 c = rng.uniform(-half / 2.0, half / 2.0, size=3)
                 g.append((amp, sig, tuple(c)))
-        else:
-            raise ValueError(name)
         self.gaussians = g
         self.bd_base = (-2 * half,) * 3
         self.bd_extent = (4 * half,) * 3

@@ -1,0 +1,139 @@
+/* iblgf_b200 — B200-native (sm_100a) lattice-Green's-function FMM Poisson
+ * path of IBLGF-AMR behind a plain C ABI.
+ *
+ * Every entry point returns 0 on success and a non-zero IBLGF_E* code on
+ * failure; iblgf_last_error() then holds a message. No C++ exception crosses
+ * this boundary. One context per host thread; all device work of a context is
+ * ordered on the context's CUDA stream.
+ *
+ * Field layout: a field holds one Nb^3 block per octant (Nb = block_extent+2,
+ * one buffer cell on each side), x fastest, octants in the canonical order
+ * returned by iblgf_domain_octants (tree level ascending, then Morton key) —
+ * the reference's DataField column-major cube (linalg_xtensor.hpp cube_wrap)
+ * laid out block after block.
+ */
+#ifndef IBLGF_B200_H
+#define IBLGF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct iblgf_ctx iblgf_ctx;
+
+enum
+{
+    IBLGF_OK = 0,
+    IBLGF_EINVAL = 1,   /* bad argument or call order */
+    IBLGF_ECUDA = 2,    /* CUDA runtime error */
+    IBLGF_ENOMEM = 3,   /* device allocation failed */
+    IBLGF_ETIMEOUT = 4, /* a bounded device wait gave up */
+    IBLGF_EINTERNAL = 5
+};
+
+enum { IBLGF_FP64 = 0, IBLGF_FP32 = 1 };
+
+/* octant_t::MASK_TYPE (include/iblgf/domain/octree/octant.hpp:69-78) */
+enum { IBLGF_STREAM = 0, IBLGF_AMR2AMR = 1 };
+
+typedef struct
+{
+    int block_extent;   /* cells per block edge (reference "block_extent") */
+    int bd_base[3];     /* bounding box ("bd_base") */
+    int bd_extent[3];   /* bounding box ("bd_extent") */
+    double dx_base;     /* base-level spacing ("dx_base" or Lx / bd_extent) */
+    int precision;      /* IBLGF_FP64 (plain) or IBLGF_FP32 (FFT/MAC in FP32) */
+    int device;         /* CUDA device ordinal */
+    int intrp_order;    /* cell-centred interpolation order (reference default 5) */
+    void* stream;       /* cudaStream_t to order work on, or NULL for a private one */
+} iblgf_config;
+
+/* Refinement predicate (Domain::register_refinement_condition): block base
+ * and extent in level cells, refinement level, and diff_level = nRef - level.
+ * Return non-zero to refine. */
+typedef int (*iblgf_refine_fn)(void* user, const int* base, const int* extent,
+                               int refinement_level, int diff_level);
+
+/* ---- context --------------------------------------------------------- */
+int iblgf_create(const iblgf_config* cfg, iblgf_ctx** out);
+int iblgf_destroy(iblgf_ctx* ctx);
+const char* iblgf_last_error(iblgf_ctx* ctx);
+int iblgf_synchronize(iblgf_ctx* ctx);
+
+/* ---- domain: Domain::initialize / construct_basemesh_blocks
+ *      (include/iblgf/domain/domain.hpp:107-212, 405-488),
+ *      Domain::init_refine (:878-939), mark_correction (:617-736),
+ *      Tree::construct_lists (tree.hpp:571-603) ------------------------- */
+int iblgf_domain_add_blocks(iblgf_ctx* ctx, int n, const int* base, const int* extent);
+int iblgf_domain_init_refine(iblgf_ctx* ctx, int n_ref, int global_refinement,
+                             iblgf_refine_fn pred, void* user);
+/* Builds the neighbour / influence lists on the device, the FMM masks
+ * (FmmMaskBuilder::fmm_lgf_mask_build, fmm_vortex_streamfun_mask) and
+ * allocates the working fields. subtract_non_leaf as in the reference. */
+int iblgf_domain_finalize(iblgf_ctx* ctx, int subtract_non_leaf);
+int iblgf_domain_info(iblgf_ctx* ctx, int* base_level, int* depth, int* n_octants);
+/* flags: bit 0 leaf, bit 1 correction; bbase: block base in level cells */
+int iblgf_domain_octants(iblgf_ctx* ctx, uint64_t* keys, int* levels, int* flags, int* bbase);
+/* nbr: 27 per octant (z slowest, self at 13), infl: 189 per octant, -1 = none */
+int iblgf_domain_lists(iblgf_ctx* ctx, int* nbr, int* infl, int* n_infl);
+int iblgf_domain_masks(iblgf_ctx* ctx, int mask_idx, unsigned char* source_target);
+
+/* ---- fields ----------------------------------------------------------- */
+int iblgf_field_create(iblgf_ctx* ctx, int* field);
+int iblgf_field_zero(iblgf_ctx* ctx, int field);
+int iblgf_field_upload(iblgf_ctx* ctx, int field, const double* host, size_t count);
+int iblgf_field_download(iblgf_ctx* ctx, int field, double* host, size_t count);
+int iblgf_field_device_ptr(iblgf_ctx* ctx, int field, double** dptr);
+
+/* ---- solver ----------------------------------------------------------- */
+/* Fmm<Setup>::apply<Source,Target>(domain, LGF_GL, level, non_leaf_as_source,
+ * add_with_scale, fmm_type)  — include/iblgf/fmm/fmm.hpp:729-870 */
+int iblgf_fmm_apply(iblgf_ctx* ctx, int source, int target, int level,
+                    int non_leaf_as_source, double add_with_scale, int fmm_type);
+/* PoissonSolver::apply_lgf<Source,Target>(fmm_type) for one scalar field —
+ * include/iblgf/solver/poisson/poisson.hpp:131-135, 587-894 */
+int iblgf_poisson_apply_lgf(iblgf_ctx* ctx, int source, int target, int fmm_type);
+/* PoissonSolver::use_correction() / subtract_non_leaf() (poisson.hpp:1494-1498) */
+int iblgf_poisson_options(iblgf_ctx* ctx, int use_correction, int subtract_non_leaf);
+
+/* ---- LGF kernel (include/iblgf/lgf/lgf_gl_lookup.hpp:33-52) ------------ */
+/* Copies the 176851-entry N_max = 100 table (positive integrals; get() = -value)
+ * that the context generated on the device. */
+int iblgf_lgf_table(iblgf_ctx* ctx, double* host_out, size_t count);
+/* G(n) for n host coordinate triples (x,y,z), evaluated on the device. */
+int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out);
+
+/* ---- single-block convolution (fft::Convolution, convolution.hpp:141-328)
+ * out (Nb^3, device) += scale * window [Nb-1, 2Nb-2]^3 of the linear
+ * convolution of src (Nb^3, device) with kernel (P^3, device, P = 2Nb-1).
+ * Nb must equal the context's block size. */
+int iblgf_conv_block(iblgf_ctx* ctx, const double* src, const double* kernel, double* out,
+                     double scale);
+
+/* ---- timing / introspection ------------------------------------------- */
+/* Number of kernels this library launched on the context stream so far. */
+int iblgf_kernel_launches(iblgf_ctx* ctx, long long* count);
+/* Phase timing by CUDA events on the context stream (no host sync while
+ * enabled). iblgf_profile(ctx, 1) resets and enables; iblgf_profile_read
+ * returns the summed device milliseconds since then: [0] forward transforms,
+ * [1] spectral MAC, [2] inverse transforms + interpolation + add,
+ * [3] zero / copy / anterpolation. */
+int iblgf_profile(iblgf_ctx* ctx, int enable);
+int iblgf_profile_read(iblgf_ctx* ctx, double* out4);
+/* Work counters since the last iblgf_profile call: [0] FMM sweeps,
+ * [1] source blocks transformed, [2] target blocks, [3] (target, source)
+ * pairs, [4] distinct LGF spectra used per sweep (summed), [5] anterpolation
+ * block transfers, [6] interpolation block transfers, [7] reserved. */
+int iblgf_stats(iblgf_ctx* ctx, long long* out8);
+/* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
+ * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the
+ * roofline denominator of the CUDA-core kernels. */
+int iblgf_fma_peak(iblgf_ctx* ctx, int precision, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBLGF_B200_H */

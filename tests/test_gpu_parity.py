@@ -1,0 +1,175 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances: FP64 plain path <= 1e-12 relative L-inf (north-star parity bar);
+FP32 FFT/MAC path <= 1e-5 relative L-inf; integer data (keys, lists, masks)
+bit-exact.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import iblgf_b200 as B
+import iblgf_setups as S
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def rel_linf(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def pair(case, precision=B.FP64, **kw):
+    n_levels = getattr(case, "n_levels", 0)
+    pred = getattr(case, "predicate", None)
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=n_levels, predicate=pred)
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=n_levels, predicate=pred, precision=precision, **kw)
+    return o, g
+
+
+def test_lgf_table_on_device():
+    g = B.Solver((-24,) * 3, (48,) * 3, 6, 1.0, [((-24,) * 3, (48,) * 3)])
+    tab = g.lgf_table()
+    gold = json.load(open(os.path.join(HERE, "golden", "lgf_table_sample.json")))["entries"]
+    idx = [(a * (2 + 3 * a + a * a)) // 6 + b * (b + 1) // 2 + c for a, b, c, _ in gold]
+    ref = np.array([v for *_, v in gold])
+    assert np.max(np.abs(tab[idx] - ref) / ref) < 5e-14
+    rng = np.random.default_rng(1)
+    xyz = rng.integers(-160, 160, size=(4000, 3))
+    xyz[:500] = rng.integers(-8, 8, size=(500, 3))
+    ref = np.array([O.lgf_get(*p) for p in xyz])
+    assert np.max(np.abs(g.lgf_get(xyz) - ref) / np.abs(ref)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["ffm", "vr0", "vr1", "uniform_64", "amr_small"])
+def test_domain_lists_masks_bit_identical(name):
+    case = {"ffm": lambda: S.ImpulseFmm(), "vr0": lambda: S.VortexRingPoisson(0),
+            "vr1": lambda: S.VortexRingPoisson(1), "uniform_64": lambda: S.GaussianPoisson("uniform_64"),
+            "amr_small": lambda: S.GaussianPoisson("amr_small")}[name]()
+    o, g = pair(case)
+    assert (o.n, o.base_level, o.depth) == (g.n, g.base_level, g.depth)
+    assert np.array_equal(o.keys, g.keys) and np.array_equal(o.levels, g.levels)
+    assert np.array_equal(o.flags, g.flags) and np.array_equal(o.bbase, g.bbase)
+    for a, b in zip(o.lists(), g.lists()):
+        assert np.array_equal(a, b)
+    for idx in [0] + [15 + 2 * r + n for r in range(g.depth - g.base_level) for n in (0, 1)]:
+        assert np.array_equal(o.masks(idx), g.masks(idx)), idx
+
+
+def _conv_kats(precision, tol):
+    torch = pytest.importorskip("torch")
+    for N, kind in ((8, "fft"), (16, "delta")):
+        P = 2 * N - 1
+        g = B.Solver((-4 * N,) * 3, (8 * N,) * 3, N - 2, 1.0, [((-2 * N + 4,) * 3, ((N - 2) * 2,) * 3)],
+                     precision=precision)
+        if kind == "fft":
+            i, j, k = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
+            src = np.sin(i) + 0.1 * j - 0.2 * k
+            ker = np.zeros((P, P, P))
+            for dz in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        ker[N - 1 + dx, N - 1 + dy, N - 1 + dz] = 0.3 + 0.1 * dx + 0.05 * dy - 0.02 * dz
+            ker[N - 1, N - 1, N - 1] = 1.2345
+        else:
+            src = np.zeros((N, N, N))
+            src[N // 3, N // 4, N // 2] = 1.0
+            a = np.arange(P) - N + 1
+            ker = np.vectorize(O.lgf_get)(a[:, None, None], a[None, :, None], a[None, None, :])
+        ref = O.block_conv(src, ker)
+        ts = torch.tensor(src.ravel(order="F"), device="cuda", dtype=torch.float64)
+        tk = torch.tensor(ker.ravel(order="F"), device="cuda", dtype=torch.float64)
+        to = torch.zeros(N ** 3, device="cuda", dtype=torch.float64)
+        g.conv_block(ts.data_ptr(), tk.data_ptr(), to.data_ptr(), 1.0)
+        out = to.cpu().numpy().reshape((N, N, N), order="F")
+        assert rel_linf(out, ref) < tol, (N, kind, rel_linf(out, ref))
+
+
+def test_conv_block_kats_fp64():
+    _conv_kats(B.FP64, 1e-12)
+
+
+def test_conv_block_kats_fp32():
+    _conv_kats(B.FP32, 1e-5)
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_fmm_impulse(precision, tol):
+    case = S.ImpulseFmm()
+    o, g = pair(case, precision)
+    src, i0, sc = case.source(o)
+    ref = o.fmm_apply(src, o.zeros(), o.base_level, 1, 1.0, 1)
+    fs, ft = g.field(src), g.field()
+    g.fmm_apply(fs, ft, g.base_level, 1, 1.0, B.AMR2AMR)
+    out = g.download(ft)
+    assert rel_linf(out, ref) < tol
+    # and against the LGF itself (ffmTest.cpp) on the non-correction leaves
+    Nb = g.Nb
+    r = np.arange(1, Nb - 1)
+    for blk in np.nonzero(g.leaf & ~g.correction)[0][:40]:
+        b = g.bbase[blk]
+        ex = np.vectorize(O.lgf_get)(b[0] + r[None, None, :] - 1 - sc[0], b[1] + r[None, :, None] - 1 - sc[1],
+                                     b[2] + r[:, None, None] - 1 - sc[2])
+        assert np.abs(out[blk, 1:-1, 1:-1, 1:-1] - ex).max() < 5e-8 + tol
+
+
+@pytest.mark.parametrize("nlas", [0, 1])
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_fmm_apply_random_amr(nlas, precision, tol):
+    case = S.GaussianPoisson("amr_small")
+    o, g = pair(case, precision)
+    rng = np.random.default_rng(7)
+    src = rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb))
+    tgt0 = rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb))
+    fs, ft = g.field(src), g.field(tgt0)
+    for level in range(o.base_level, o.depth):
+        ref = o.fmm_apply(src, tgt0, level, nlas, 0.75, 1)
+        g.upload(ft, tgt0)
+        g.fmm_apply(fs, ft, level, nlas, 0.75, B.AMR2AMR)
+        out = g.download(ft)
+        assert rel_linf(out - tgt0, ref - tgt0) < tol, (level, rel_linf(out - tgt0, ref - tgt0))
+
+
+@pytest.mark.parametrize("n_levels", [0, 1])
+def test_poisson_vortex_ring(n_levels):
+    case = S.VortexRingPoisson(n_levels)
+    o, g = pair(case)
+    src, ex = case.fields(o)
+    ref = o.apply_lgf(src)
+    fs, ft = g.field(src), g.field()
+    g.apply_lgf(fs, ft)
+    out = g.download(ft)
+    assert rel_linf(out, ref) < 1e-12
+    assert case.finest_linf(g, out, ex) < case.exp_linf
+
+
+@pytest.mark.parametrize("name", ["uniform_small", "amr_small", "uniform_64"])
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_poisson_gaussian(name, precision, tol):
+    case = S.GaussianPoisson(name)
+    o, g = pair(case, precision)
+    src = case.fields(o)
+    ref = o.apply_lgf(src)
+    fs, ft = g.field(src), g.field()
+    g.apply_lgf(fs, ft)
+    out = g.download(ft)
+    assert rel_linf(out, ref) < tol
+    # a second solve on the same context (cached plans and spectra) is identical
+    g.zero(ft)
+    g.apply_lgf(fs, ft)
+    assert np.array_equal(g.download(ft), out)
+
+
+def test_capi_errors_are_status_codes():
+    g = B.Solver((-24,) * 3, (48,) * 3, 6, 1.0, [((-24,) * 3, (48,) * 3)])
+    with pytest.raises(B.IblgfError):
+        g.fmm_apply(0, 99, g.base_level, 1)
+    with pytest.raises(B.IblgfError):
+        g.fmm_apply(0, 0, g.depth + 3, 1)
+    with pytest.raises(B.IblgfError):
+        g.upload(0, np.zeros(5))
