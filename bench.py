@@ -117,6 +117,7 @@ def main():
     ap.add_argument("--workload", default="amr_3level")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -214,7 +215,7 @@ def main():
 
     # ---- FP64 plain path on the same input, and accuracy of this run against it
     extra = {}
-    if rank == 0 and prec == B.FP32:
+    if rank == 0 and prec == B.FP32 and not args.no_fp64:
         g64 = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                        n_levels=case.n_levels, predicate=case.predicate, precision=B.FP64, device=local,
                        stream=stream.cuda_stream)

@@ -119,6 +119,15 @@ int iblgf_domain_add_blocks(iblgf_ctx* x, int n, const int* base, const int* ext
     });
 }
 
+int iblgf_domain_import(iblgf_ctx* x, int n, const uint64_t* keys, const int* flags)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
+        if (n <= 0 || !keys || !flags) throw iblgf_b200::Error(IBLGF_EINVAL, "bad import arguments");
+        c.tree.import_octants(n, keys, flags);
+    });
+}
+
 int iblgf_domain_init_refine(iblgf_ctx* x, int n_ref, int global_refinement, iblgf_refine_fn pred, void* user)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
@@ -243,6 +252,15 @@ int iblgf_poisson_apply_lgf(iblgf_ctx* x, int source, int target, int fmm_type)
     });
 }
 
+int iblgf_poisson_apply_if(iblgf_ctx* x, int source, int target, double alpha_base, int fmm_type)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, source);
+        need_field(c, target);
+        iblgf_b200::apply_if(c, source, target, alpha_base, fmm_type);
+    });
+}
+
 int iblgf_poisson_options(iblgf_ctx* x, int use_correction, int subtract_non_leaf)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
@@ -250,6 +268,24 @@ int iblgf_poisson_options(iblgf_ctx* x, int use_correction, int subtract_non_lea
         if (c.finalized && (subtract_non_leaf != 0) != c.subtract_non_leaf)
             throw iblgf_b200::Error(IBLGF_EINVAL, "subtract_non_leaf is fixed at finalize (masks depend on it)");
         c.subtract_non_leaf = subtract_non_leaf != 0;
+    });
+}
+
+int iblgf_op_apply(iblgf_ctx* x, int op, const int* in, int n_in, const int* out, int n_out, int level, double scale)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!in || !out) throw iblgf_b200::Error(IBLGF_EINVAL, "null field list");
+        for (int i = 0; i < n_in; ++i) need_field(c, in[i]);
+        for (int i = 0; i < n_out; ++i) need_field(c, out[i]);
+        iblgf_b200::apply_op(c, op, in, n_in, out, n_out, level, scale);
+    });
+}
+
+int iblgf_buffer_exchange(iblgf_ctx* x, int field, int level)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, field);
+        iblgf_b200::buffer_exchange(c, field, level);
     });
 }
 

@@ -5,6 +5,7 @@
 #include <array>
 #include <cstdint>
 #include <map>
+#include <tuple>
 #include <unordered_map>
 #include <memory>
 #include <stdexcept>
@@ -105,6 +106,7 @@ struct HostTree
     void refine(int i, bool ratio_2to1);
     void init_refine(int n_ref, int level_up_max, iblgf_refine_fn pred, void* user);
     void mark_correction();
+    void import_octants(int n, const u64* keys, const int* flags);
     std::vector<int> canonical() const;  // has_data octants, (level, key) order
 };
 
@@ -194,7 +196,13 @@ struct Ctx
     // per-sweep work buffers (sized on demand)
     DevBuf<char> d_src_spec, d_acc, d_w;
 
-    std::map<std::pair<int, int>, std::unique_ptr<FmmPlan>> plans;
+    std::map<std::tuple<int, int, int>, std::unique_ptr<FmmPlan>> plans;
+    // integrating-factor kernels: e^{-2 alpha} I_n(2 alpha), n < ge_stride, one
+    // table per alpha (LGF_GE::build_lt / compute_lgf)
+    std::map<double, int> ge_index;
+    std::vector<double> ge_host;
+    DevBuf<double> d_ge;
+    int ge_stride = 0;
     long long launches = 0;
     bool profile = false;
     std::vector<std::array<cudaEvent_t, 5>> prof_events;
@@ -212,7 +220,9 @@ struct Ctx
 void ctx_init(Ctx& c);
 void domain_finalize(Ctx& c);
 int field_create(Ctx& c);
-void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int fmm_type);
+void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int fmm_type, int ge = -1);
+int ge_table(Ctx& c, double alpha);
+void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type);
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);
 int mask_idx_gen(int type, int refinement_level, int nlas);
 
@@ -235,6 +245,10 @@ void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat
 void launch_halo(Ctx& c, double* f, const int* list, int n);
 void launch_source_correction(Ctx& c, const double* target_tmp, double* corr, const int* list, int n,
                               double inv_dx2);
+void launch_op(Ctx& c, int op, const double* const* in, int n_in, double* const* out, int n_out, const int* list,
+               const double* dx, int n, double scale);
+void buffer_exchange(Ctx& c, int field, int level);
+void apply_op(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, int level, double scale);
 void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* out, double scale);
 
 }  // namespace iblgf_b200

@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(256) fwd_xy_kernel(const double* __restrict__ 
                                                      const int* __restrict__ item_oct,
                                                      const int* __restrict__ desc,
                                                      const double* __restrict__ table,
-                                                     const R* __restrict__ tw, cx<R>* __restrict__ W)
+                                                     const R* __restrict__ tw, cx<R>* __restrict__ W,
+                                                     const double* __restrict__ ge, int ge_stride)
 {
     constexpr int P = 2 * NB - 1;
     __shared__ cx<R> s_tw[P];
@@ -67,12 +68,28 @@ __global__ void __launch_bounds__(256) fwd_xy_kernel(const double* __restrict__ 
     }
     else if (MODE == kFromLgf)
     {
-        const int ld = desc[4 * item], st = 1 << ld;
+        // desc[0] >= 0: LGF_GL at stride 2^level_diff (lgf.hpp:222-262);
+        // desc[0] < 0: LGF_GE table -desc[0]-1, E(n) = f[|n1|] f[|n2|] f[|n3|]
+        const int ld = desc[4 * item];
         const int bx = desc[4 * item + 1], by = desc[4 * item + 2], bz = desc[4 * item + 3];
-        for (int i = threadIdx.x; i < NIN * NIN; i += blockDim.x)
+        if (ld >= 0)
         {
-            const int x = i % NIN, y = i / NIN;
-            s_in[i] = (R)lgf_get_dev((bx + x) * st, (by + y) * st, (bz + z) * st, table);
+            const int st = 1 << ld;
+            for (int i = threadIdx.x; i < NIN * NIN; i += blockDim.x)
+            {
+                const int x = i % NIN, y = i / NIN;
+                s_in[i] = (R)lgf_get_dev((bx + x) * st, (by + y) * st, (bz + z) * st, table);
+            }
+        }
+        else
+        {
+            const double* f = ge + (size_t)(-ld - 1) * ge_stride;
+            const double fz = f[abs(bz + z)];
+            for (int i = threadIdx.x; i < NIN * NIN; i += blockDim.x)
+            {
+                const int x = i % NIN, y = i / NIN;
+                s_in[i] = (R)(f[abs(bx + x)] * f[abs(by + y)] * fz);
+            }
         }
     }
     else
@@ -194,8 +211,11 @@ __global__ void __launch_bounds__(256) group_mac_kernel(
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);  // [343][F]
     cx<R>* Ss = Gs + 343 * F;                       // [n_src][F]
-    const int tile = blockIdx.y;
-    const long long f0 = (long long)blockIdx.x * F;
+    // grid.x = tile (fast), grid.y = frequency chunk: CTAs resident together
+    // work on the same chunk, so the chunk's spectra and source values are
+    // read from HBM once and then served from L2 to every tile
+    const int tile = blockIdx.x;
+    const long long f0 = (long long)blockIdx.y * F;
     const int lane = threadIdx.x % F, row = threadIdx.x / F, rows = blockDim.x / F;
     const cx<R> zero = mk<R>(0, 0);
     const int* su = spec_u + 343 * tile_tab[tile];
@@ -213,7 +233,7 @@ __global__ void __launch_bounds__(256) group_mac_kernel(
         Ss[i] = ff < NC ? S[(size_t)tile_src[s0 + i / F] * NC + ff] : zero;
     }
     __syncthreads();
-    const bool coarse = tile_coarse[tile] != 0;
+    const int mode = tile_coarse[tile];  // 0 all, 1 non-adjacent only, 2 adjacent only
     const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
     const long long f = f0 + lane;
     for (int gb = g0 + row * M; gb < g1; gb += rows * M)
@@ -240,10 +260,11 @@ __global__ void __launch_bounds__(256) group_mac_kernel(
             for (int c = 0; c < 8; ++c)
             {
                 const int u = c_group_u[c * 216 + k];
-                if (coarse)
+                if (mode)
                 {
                     const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
-                    if (ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1) continue;
+                    const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
+                    if (adj == (mode == 1)) continue;
                 }
                 const cx<R> gv = Gs[u * F + lane];
 #pragma unroll
@@ -368,7 +389,7 @@ struct Conv
         if (!n) return;
         cx<R>* W = (cx<R>*)c.d_w.p;
         fwd_xy_kernel<R, NB, NB, kFromField><<<dim3(n, NB), 256, 0, c.stream>>>(field, d_item_oct, nullptr,
-                                                                              nullptr, tw(c), W);
+                                                                              nullptr, tw(c), W, nullptr, 0);
         fwd_z_kernel<R, R, NB, NB><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, tw(c), nullptr,
                                                                                   (cx<R>*)spec);
         c.launches += 2;
@@ -382,10 +403,10 @@ struct Conv
         double2* W = (double2*)c.d_w.p;
         if (dense)
             fwd_xy_kernel<double, NB, P, kFromDense><<<dim3(n, P), 256, 0, c.stream>>>(
-                dense, nullptr, nullptr, nullptr, c.d_tw64.p, W);
+                dense, nullptr, nullptr, nullptr, c.d_tw64.p, W, nullptr, 0);
         else
             fwd_xy_kernel<double, NB, P, kFromLgf><<<dim3(n, P), 256, 0, c.stream>>>(
-                nullptr, nullptr, d_desc, c.d_lgf_table.p, c.d_tw64.p, W);
+                nullptr, nullptr, d_desc, c.d_lgf_table.p, c.d_tw64.p, W, c.d_ge.p, c.ge_stride);
         fwd_z_kernel<double, R, NB, P><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, c.d_tw64.p, d_slot,
                                                                                       (cx<R>*)spec);
         c.launches += 2;
@@ -410,7 +431,7 @@ struct Conv
         const size_t smem = (size_t)(343 + p.max_tile_src) * GF * sizeof(cx<R>);
         auto kfn = group_mac_kernel<R, GF, GM>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        dim3 grid((unsigned)((c.NC + GF - 1) / GF), p.n_tiles);
+        dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
         kfn<<<grid, 256, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.tile_gptr.p,
                                            p.tile_sptr.p, p.tile_src.p, p.tile_tab.p, p.tile_coarse.p,
                                            p.spec_u.p, p.grp_src.p, p.grp_tgt.p, (cx<R>*)acc);

@@ -331,9 +331,11 @@ void upload_tasks(Ctx& c, TpTasks& tt, const std::vector<int>& dst, const std::v
     tt.task_cid.upload(cid, c.stream);
 }
 
-FmmPlan& get_plan(Ctx& c, int level, int idx)
+// ge < 0: LGF_GL sweep (Fmm::apply full branch); ge >= 0: LGF_GE sweep with
+// the integrating-factor table `ge` (neighbour-only branch, fmm.hpp:754-770)
+FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
 {
-    auto key = std::make_pair(idx, level);
+    auto key = std::make_tuple(idx, level, ge);
     auto it = c.plans.find(key);
     if (it != c.plans.end()) return *it->second;
     auto plan = std::make_unique<FmmPlan>();
@@ -343,12 +345,16 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
     const auto& m = c.masks[idx];
     auto S = [&](int o) { return m[2 * o] != 0; };
     auto T = [&](int o) { return m[2 * o + 1] != 0; };
+    const bool neighbor_only = ge >= 0;
     std::vector<int> zs, zt, cs, at, srcs, tgts;
     for (int lv = level; lv >= 0; --lv)
         for (int o : c.level_octs[lv])
         {
-            if (S(o)) zs.push_back(o), srcs.push_back(o);
-            if (T(o)) zt.push_back(o), tgts.push_back(o);
+            if (S(o)) zs.push_back(o);
+            if (T(o)) zt.push_back(o);
+            if (neighbor_only && lv != level) continue;
+            if (S(o)) srcs.push_back(o);
+            if (T(o)) tgts.push_back(o);
         }
     for (int o : c.level_octs[level])
     {
@@ -360,7 +366,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
     p.copy_s.upload(cs, c.stream);
     p.add_t.upload(at, c.stream);
     // anterpolation, levels level-1 .. 0
-    for (int lv = level - 1; lv >= 0; --lv)
+    for (int lv = level - 1; lv >= 0 && !neighbor_only; --lv)
     {
         std::vector<int> dst;
         std::vector<std::vector<std::pair<int, int>>> tasks;
@@ -379,7 +385,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
         upload_tasks(c, p.antrp.back(), dst, tasks);
     }
     // interpolation, levels 1 .. level-1 (parent level)
-    for (int lv = 1; lv < level; ++lv)
+    for (int lv = 1; lv < level && !neighbor_only; ++lv)
     {
         std::vector<int> dst;
         std::vector<std::vector<std::pair<int, int>>> tasks;
@@ -427,7 +433,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
         TP x{t, {}, {}};
         auto add_pair = [&](int s, int lvd) {
             x.src.push_back(src_slot[s]);
-            x.spec.push_back(slot_of({lvd, c.bbase[3 * t] - c.bbase[3 * s] - (Nb - 1),
+            x.spec.push_back(slot_of({neighbor_only ? -1 - ge : lvd, c.bbase[3 * t] - c.bbase[3 * s] - (Nb - 1),
                                       c.bbase[3 * t + 1] - c.bbase[3 * s + 1] - (Nb - 1),
                                       c.bbase[3 * t + 2] - c.bbase[3 * s + 2] - (Nb - 1)}));
         };
@@ -437,7 +443,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
                 const int n = c.nbr[27 * t + i];
                 if (n >= 0 && S(n)) add_pair(n, 0);
             }
-        for (int i = 0; i < c.n_infl[t]; ++i)
+        for (int i = 0; i < c.n_infl[t] && !neighbor_only; ++i)
         {
             const int n = c.infl[189 * t + i];
             if (n >= 0 && S(n)) add_pair(n, ld);
@@ -486,9 +492,13 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
                         cand[k] = (o >= 0 && S(o)) ? src_slot[o] : -1;
                     }
                 }
+        const int mode = neighbor_only ? 2 : (ld == 0 ? 0 : 1);
+        auto valid = [&](int kk) {
+            return mode == 0 || (mode == 1 && !adjacent(cc, kk)) || (mode == 2 && adjacent(cc, kk));
+        };
         std::vector<int> mine;
         for (int kk = 0; kk < 216; ++kk)
-            if (cand[kk] >= 0 && (ld == 0 || !adjacent(cc, kk))) mine.push_back(cand[kk]);
+            if (cand[kk] >= 0 && valid(kk)) mine.push_back(cand[kk]);
         std::vector<int> ref = tp[i].src;
         std::sort(mine.begin(), mine.end());
         std::sort(ref.begin(), ref.end());
@@ -512,7 +522,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
             g = it->second;
         groups[g].tgt[cc] = (int)i;  // temporary: index into tp
         for (int kk = 0; kk < 216; ++kk)
-            if (cand[kk] >= 0 && (ld == 0 || !adjacent(cc, kk))) groups[g].used[kk] = true;
+            if (cand[kk] >= 0 && valid(kk)) groups[g].used[kk] = true;
         in_group[i] = 1;
     }
     // target slots: pair-list targets first, then group targets in group order
@@ -552,7 +562,8 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
         for (int u = 0; u < 343; ++u)
         {
             const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
-            const std::array<int, 4> k{gr.ld, ux * e - (Nb - 1), uy * e - (Nb - 1), uz * e - (Nb - 1)};
+            const std::array<int, 4> k{neighbor_only ? -1 - ge : gr.ld, ux * e - (Nb - 1), uy * e - (Nb - 1),
+                                       uz * e - (Nb - 1)};
             auto it = c.spec_slot.find(k);
             spec_u.push_back(it == c.spec_slot.end() ? -1 : it->second);
         }
@@ -569,7 +580,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx)
         tgptr.push_back((int)gtgt.size() / 8);
         tsptr.push_back((int)tsrc.size());
         ttab.push_back(tab_of_ld[cur_ld]);
-        tcoarse.push_back(cur_ld > 0 ? 1 : 0);
+        tcoarse.push_back(neighbor_only ? 2 : (cur_ld > 0 ? 1 : 0));
         max_src = std::max(max_src, (int)local.size());
         local.clear();
         ngrp = 0;
@@ -684,7 +695,7 @@ struct Timer
 };
 }  // namespace
 
-void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_scale, int fmm_type)
+void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_scale, int fmm_type, int ge)
 {
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (level < c.tree.base_level || level >= c.tree.depth) throw Error(IBLGF_EINVAL, "level out of range");
@@ -692,7 +703,7 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     const int idx = fmm_type == IBLGF_STREAM ? mask_idx_gen(IBLGF_STREAM, 0, 0)
                                               : mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0);
     upload_group_offsets();
-    FmmPlan& p = get_plan(c, level, idx);
+    FmmPlan& p = get_plan(c, level, idx, ge);
     c.stats[0] += 1;
     c.stats[1] += p.n_src;
     c.stats[2] += p.n_tgt;
@@ -722,7 +733,8 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     tm.mark(3);
     if (!p.empty())
     {
-        const double scale = dx_level * dx_level / ((double)c.P * c.P * c.P);
+        // compute_influence_field (fmm.hpp:1021-1026): dx^2 for LGF_GL, 1 for LGF_GE
+        const double scale = (ge >= 0 ? 1.0 : dx_level * dx_level) / ((double)c.P * c.P * c.P);
         launch_inverse_add(c, p, c.d_acc.p, ft, scale);
     }
     for (auto& t : p.intrp) launch_tp(c, t, ft, ft, 0, 1);
@@ -804,7 +816,150 @@ PoissonLists& poisson_lists(Ctx& c)
 }
 }  // namespace
 
-void poisson_release(const Ctx* c) { g_plists.erase(c); }
+namespace
+{
+// per level (and "all levels" at index kMaxLevel+1): block list and dx per block
+struct OpLists
+{
+    std::vector<DevBuf<int>> list;
+    std::vector<DevBuf<double>> dx;
+};
+std::map<const Ctx*, std::unique_ptr<OpLists>> g_oplists;
+
+OpLists& op_lists(Ctx& c)
+{
+    auto it = g_oplists.find(&c);
+    if (it != g_oplists.end()) return *it->second;
+    auto ol = std::make_unique<OpLists>();
+    const int L = kMaxLevel + 2;
+    ol->list.resize(L);
+    ol->dx.resize(L);
+    std::vector<int> all;
+    std::vector<double> alldx;
+    for (int l = 0; l <= kMaxLevel; ++l)
+    {
+        std::vector<double> dx;
+        const double d = c.cfg.dx_base / std::pow(2.0, l - c.tree.base_level);
+        for (int o : c.level_octs[l])
+        {
+            dx.push_back(d);
+            all.push_back(o);
+            alldx.push_back(d);
+        }
+        ol->list[l].upload(c.level_octs[l], c.stream);
+        ol->dx[l].upload(dx, c.stream);
+    }
+    ol->list[L - 1].upload(all, c.stream);
+    ol->dx[L - 1].upload(alldx, c.stream);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    auto& ref = *ol;
+    g_oplists.emplace(&c, std::move(ol));
+    return ref;
+}
+}  // namespace
+
+void buffer_exchange(Ctx& c, int field, int level)
+{
+    if (level < 0 || level > kMaxLevel) throw Error(IBLGF_EINVAL, "level out of range");
+    OpLists& ol = op_lists(c);
+    launch_halo(c, c.field(field), ol.list[level].p, (int)ol.list[level].n);
+}
+
+void apply_op(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, int level, double scale)
+{
+    static const int need_in[6] = {1, 1, 3, 3, 3, 6}, need_out[6] = {1, 3, 1, 3, 3, 3};
+    if (op < 0 || op > 5) throw Error(IBLGF_EINVAL, "unknown operator");
+    if (n_in != need_in[op] || n_out != need_out[op]) throw Error(IBLGF_EINVAL, "wrong number of component fields");
+    if (level > kMaxLevel) throw Error(IBLGF_EINVAL, "level out of range");
+    OpLists& ol = op_lists(c);
+    const int li = level < 0 ? kMaxLevel + 1 : level;
+    const double* pin[6] = {};
+    double* pout[3] = {};
+    for (int i = 0; i < n_in; ++i) pin[i] = c.field(in[i]);
+    for (int i = 0; i < n_out; ++i)
+    {
+        pout[i] = c.field(out[i]);
+        for (int j = 0; j < n_in; ++j)
+            if (out[i] == in[j]) throw Error(IBLGF_EINVAL, "operator output aliases an input");
+    }
+    launch_op(c, op, pin, n_in, pout, n_out, ol.list[li].p, ol.dx[li].p, (int)ol.list[li].n, scale);
+}
+
+// e^{-2 alpha} I_n(2 alpha), n = 0..stride-1, by Miller's backward recurrence
+// normalised with e^x = I_0 + 2 sum I_k (A&S 9.6.26, 9.6.37)
+int ge_table(Ctx& c, double alpha)
+{
+    auto it = c.ge_index.find(alpha);
+    if (it != c.ge_index.end()) return it->second;
+    if (!(alpha > 0.0)) throw Error(IBLGF_EINVAL, "integrating-factor alpha must be positive");
+    c.ge_stride = 4 * c.Nb + 9;
+    const int nmax = c.ge_stride - 1;
+    const double x = 2.0 * alpha;
+    std::vector<double> f(c.ge_stride, 0.0);
+    const int m = nmax + 30 + (int)std::ceil(std::sqrt(90.0 * x));
+    double a = 0.0, b = 1e-280, sum = 0.0;
+    for (int k = m; k >= 1; --k)
+    {
+        const double cc = a + (2.0 * k / x) * b;
+        sum += b;
+        if (k <= nmax) f[k] = b;
+        a = b;
+        b = cc;
+        if (std::fabs(b) > 1e250)
+        {
+            a *= 1e-250;
+            b *= 1e-250;
+            sum *= 1e-250;
+            for (int n = k; n <= nmax; ++n) f[n] *= 1e-250;
+        }
+    }
+    f[0] = b;
+    const double norm = b + 2.0 * sum;
+    for (auto& v : f) v /= norm;
+    const int idx = (int)c.ge_index.size();
+    c.ge_index.emplace(alpha, idx);
+    c.ge_host.insert(c.ge_host.end(), f.begin(), f.end());
+    c.d_ge.upload(c.ge_host, c.stream);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    return idx;
+}
+
+// PoissonSolver::apply_lgf_IF / apply_if (poisson.hpp:428-494), AMR2AMR
+void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (fmm_type != IBLGF_AMR2AMR) throw Error(IBLGF_EINVAL, "apply_if supports AMR2AMR");
+    PoissonLists& pl = poisson_lists(c);
+    OpLists& ol = op_lists(c);
+    double* st = c.field(c.f_source_tmp);
+    double* tt = c.field(c.f_target_tmp);
+    const size_t bytes = c.field_elems() * sizeof(double);
+    IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
+    IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
+    launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
+    const int bl = c.tree.base_level, depth = c.tree.depth;
+    for (int ls = depth - 2; ls >= bl; --ls) launch_tp(c, pl.coarsify[ls], st, st, 4, 0);
+    // intrp_to_correction_buffer (poisson.hpp:1015-1069)
+    for (int l = depth - 2; l >= bl; --l)
+    {
+        launch_halo(c, st, ol.list[l].p, (int)ol.list[l].n);
+        launch_tp(c, pl.corr_intrp[l], st, st, 2, 2);
+    }
+    for (int l = bl; l < depth; ++l)
+    {
+        // LGF_GE::change_level_impl: alpha = alpha_base * 4^(l - base)
+        const int ge = ge_table(c, alpha_base * std::pow(4.0, l - bl));
+        fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, false, 1.0, IBLGF_AMR2AMR, ge);
+        if (!c.subtract_non_leaf) fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, true, 1.0, IBLGF_AMR2AMR, ge);
+        launch_axpy_blocks(c, tt, c.field(tgt), pl.level_all[l].p, (int)pl.level_all[l].n, 1.0, true);
+    }
+}
+
+void poisson_release(const Ctx* c)
+{
+    g_plists.erase(c);
+    g_oplists.erase(c);
+}
 
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
 {

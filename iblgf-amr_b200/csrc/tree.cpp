@@ -308,6 +308,21 @@ void HostTree::mark_correction()
     }
 }
 
+void HostTree::import_octants(int n, const u64* keys, const int* flags)
+{
+    if (o.size() != 1 || o[0].has_data) throw Error(IBLGF_EINVAL, "import needs an empty tree");
+    for (int i = 0; i < n; ++i)
+    {
+        const int lv = key_level(keys[i]);
+        if (lv > kMaxLevel) throw Error(IBLGF_EINVAL, "key level out of range");
+        const int x = insert(keys[i]);
+        if (o[x].key != keys[i]) throw Error(IBLGF_EINVAL, "malformed key");
+        alloc(x, lv - base_level);
+        o[x].leaf = (flags[i] & 1) != 0;
+        o[x].correction = (flags[i] & 2) != 0;
+    }
+}
+
 std::vector<int> HostTree::canonical() const
 {
     std::vector<std::pair<std::pair<int, u64>, int>> v;

@@ -30,11 +30,11 @@ class Config(ctypes.Structure):
 
 EXPORTS = [
     "iblgf_create", "iblgf_destroy", "iblgf_last_error", "iblgf_synchronize",
-    "iblgf_domain_add_blocks", "iblgf_domain_init_refine", "iblgf_domain_finalize",
+    "iblgf_domain_add_blocks", "iblgf_domain_import", "iblgf_domain_init_refine", "iblgf_domain_finalize",
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
-    "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf",
-    "iblgf_poisson_options", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block",
+    "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
+    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -58,6 +58,7 @@ def lib():
     L.iblgf_synchronize.argtypes = [vp]
     L.iblgf_domain_add_blocks.argtypes = [vp, ci, vp, vp]
     L.iblgf_domain_init_refine.argtypes = [vp, ci, ci, REFINE_FN, vp]
+    L.iblgf_domain_import.argtypes = [vp, ci, vp, vp]
     L.iblgf_domain_finalize.argtypes = [vp, ci]
     L.iblgf_domain_info.argtypes = [vp, vp, vp, vp]
     L.iblgf_domain_octants.argtypes = [vp, vp, vp, vp, vp]
@@ -71,7 +72,10 @@ def lib():
     L.iblgf_fmm_apply.argtypes = [vp, ci, ci, ci, ci, cd, ci]
     L.iblgf_poisson_apply_lgf.argtypes = [vp, ci, ci, ci]
     L.iblgf_poisson_options.argtypes = [vp, ci, ci]
+    L.iblgf_poisson_apply_if.argtypes = [vp, ci, ci, cd, ci]
     L.iblgf_lgf_table.argtypes = [vp, vp, sz]
+    L.iblgf_op_apply.argtypes = [vp, ci, vp, ci, vp, ci, ci, cd]
+    L.iblgf_buffer_exchange.argtypes = [vp, ci, ci]
     L.iblgf_lgf_get.argtypes = [vp, vp, sz, vp]
     L.iblgf_conv_block.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -102,7 +106,7 @@ class Solver:
 
     def __init__(self, bd_base, bd_extent, block_extent, dx_base, blocks, n_levels=0,
                  global_refinement=0, predicate=None, precision=FP64, subtract_non_leaf=False,
-                 intrp_order=5, device=0, stream=None, use_correction=True):
+                 intrp_order=5, device=0, stream=None, use_correction=True, import_octants=None):
         L = lib()
         cfg = Config(block_extent, (ctypes.c_int * 3)(*bd_base), (ctypes.c_int * 3)(*bd_extent),
                      float(dx_base), int(precision), int(device), int(intrp_order),
@@ -115,16 +119,25 @@ class Solver:
         self.Nb = block_extent + 2
         self.block_extent = block_extent
         self.precision = precision
-        bb = np.array([b[0] for b in blocks], np.int32).ravel()
-        be = np.array([b[1] for b in blocks], np.int32).ravel()
-        self._check(L.iblgf_domain_add_blocks(self.h, len(blocks), _p(bb), _p(be)))
+        if import_octants is not None:
+            keys = np.ascontiguousarray(import_octants[0], dtype=np.uint64)
+            flags = np.ascontiguousarray(import_octants[1], dtype=np.int32)
+            self._check(L.iblgf_domain_import(self.h, len(keys), _p(keys), _p(flags)))
+            n_levels, global_refinement, predicate = 0, 0, None
+            self._imported = True
+        else:
+            bb = np.array([b[0] for b in blocks], np.int32).ravel()
+            be = np.array([b[1] for b in blocks], np.int32).ravel()
+            self._check(L.iblgf_domain_add_blocks(self.h, len(blocks), _p(bb), _p(be)))
+            self._imported = False
         if predicate is not None:
             def cb(user, base, ext, rl, diff):
                 return 1 if predicate((base[0], base[1], base[2]), (ext[0], ext[1], ext[2]), rl, diff) else 0
             self._cb = REFINE_FN(cb)
         else:
             self._cb = REFINE_FN(lambda *a: 0)
-        self._check(L.iblgf_domain_init_refine(self.h, int(n_levels), int(global_refinement), self._cb, None))
+        if not self._imported:
+            self._check(L.iblgf_domain_init_refine(self.h, int(n_levels), int(global_refinement), self._cb, None))
         self._check(L.iblgf_domain_finalize(self.h, 1 if subtract_non_leaf else 0))
         self._check(L.iblgf_poisson_options(self.h, 1 if use_correction else 0, 1 if subtract_non_leaf else 0))
         bl, dp, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -208,6 +221,22 @@ class Solver:
 
     def apply_lgf(self, src, tgt, fmm_type=AMR2AMR):
         self._check(lib().iblgf_poisson_apply_lgf(self.h, src, tgt, int(fmm_type)))
+
+    LAPLACE, GRADIENT, DIVERGENCE, CURL, CURL_TRANSPOSE, NONLINEAR = range(6)
+
+    def op(self, op, inputs, outputs, level=-1, scale=1.0):
+        """Mimetic block operator on field ids (Operator::laplace ... nonlinear)."""
+        fi = np.array(inputs, np.int32)
+        fo = np.array(outputs, np.int32)
+        self._check(lib().iblgf_op_apply(self.h, int(op), _p(fi), len(fi), _p(fo), len(fo), int(level),
+                                         float(scale)))
+
+    def buffer_exchange(self, fid, level):
+        self._check(lib().iblgf_buffer_exchange(self.h, int(fid), int(level)))
+
+    def apply_if(self, src, tgt, alpha_base, fmm_type=AMR2AMR):
+        """PoissonSolver::apply_lgf_IF (integrating factor, LGF_GE)."""
+        self._check(lib().iblgf_poisson_apply_if(self.h, src, tgt, float(alpha_base), int(fmm_type)))
 
     def lgf_table(self):
         out = np.zeros(176851)

@@ -119,9 +119,11 @@ class GaussianPoisson:
         if name == "uniform_64":
             half = 32
             self.n_levels = 0
-        elif name == "amr_3level":
+        elif name in ("amr_3level", "amr_2level"):
+            # amr_2level: the same source and base mesh with one refinement
+            # level (a medium-size case for profiling)
             half = 64
-            self.n_levels = 2
+            self.n_levels = 2 if name == "amr_3level" else 1
             n_random = 16
         elif name in ("uniform_small", "amr_small"):
             # reduced parity cases: 4x4x4 base blocks of 6^3 cells

@@ -70,6 +70,13 @@ int iblgf_synchronize(iblgf_ctx* ctx);
 int iblgf_domain_add_blocks(iblgf_ctx* ctx, int n, const int* base, const int* extent);
 int iblgf_domain_init_refine(iblgf_ctx* ctx, int n_ref, int global_refinement,
                              iblgf_refine_fn pred, void* user);
+/* Imports an octree built elsewhere (the reference's Domain after
+ * init_refine / mark_correction) instead of add_blocks + init_refine: the
+ * keys of every octant that holds data (Octant::has_data) and their flags
+ * (bit 0 leaf, bit 1 correction). Block bases follow
+ * Tree::octant_to_level_coordinate (domain.hpp:196-201). Call once, before
+ * iblgf_domain_finalize. */
+int iblgf_domain_import(iblgf_ctx* ctx, int n, const uint64_t* keys, const int* flags);
 /* Builds the neighbour / influence lists on the device, the FMM masks
  * (FmmMaskBuilder::fmm_lgf_mask_build, fmm_vortex_streamfun_mask) and
  * allocates the working fields. subtract_non_leaf as in the reference. */
@@ -96,8 +103,31 @@ int iblgf_fmm_apply(iblgf_ctx* ctx, int source, int target, int level,
 /* PoissonSolver::apply_lgf<Source,Target>(fmm_type) for one scalar field —
  * include/iblgf/solver/poisson/poisson.hpp:131-135, 587-894 */
 int iblgf_poisson_apply_lgf(iblgf_ctx* ctx, int source, int target, int fmm_type);
+/* PoissonSolver::apply_lgf_IF<Source,Target>(alpha_base, fmm_type) for one
+ * scalar field — the integrating factor e^{alpha L} with the LGF_GE kernel
+ * (include/iblgf/lgf/lgf_ge.hpp:33-190), neighbour-only FMM branch
+ * (fmm.hpp:754-770), alpha = alpha_base * 4^(level - base_level)
+ * (poisson.hpp:428-494). */
+int iblgf_poisson_apply_if(iblgf_ctx* ctx, int source, int target, double alpha_base, int fmm_type);
 /* PoissonSolver::use_correction() / subtract_non_leaf() (poisson.hpp:1494-1498) */
 int iblgf_poisson_options(iblgf_ctx* ctx, int use_correction, int subtract_non_leaf);
+
+/* ---- mimetic block operators (include/iblgf/operators/operators.hpp) ----
+ * Applied to the interior of every block of tree level `level` (all levels if
+ * level < 0) with dx_level = dx_base / 2^(level - base_level); the one-cell
+ * buffers are read, so exchange them first as the reference's level wrappers
+ * do. Vector fields are 3 component field ids (face: normal components x,y,z;
+ * edge: x,y,z). op: 0 laplace (:1386, cell->cell, 1 in / 1 out),
+ * 1 gradient (:1421, cell->face, 1/3), 2 divergence (:1448, face->cell, 3/1),
+ * 3 curl (:1479, face->edge, 3/3), 4 curl_transpose (:2416, edge->face, 3/3,
+ * times scale), 5 nonlinear (:2455, face u + edge omega -> face, 6/3).
+ * Outputs must not alias inputs. */
+int iblgf_op_apply(iblgf_ctx* ctx, int op, const int* in, int n_in, const int* out, int n_out,
+                   int level, double scale);
+/* client::buffer_exchange<Field>(level) (domain/decomposition/client.hpp:1120):
+ * every buffer cell of the level's blocks takes the overlapping interior
+ * value of its same-level neighbour. */
+int iblgf_buffer_exchange(iblgf_ctx* ctx, int field, int level);
 
 /* ---- LGF kernel (include/iblgf/lgf/lgf_gl_lookup.hpp:33-52) ------------ */
 /* Copies the 176851-entry N_max = 100 table (positive integrals; get() = -value)

@@ -165,6 +165,58 @@ int orc_apply_lgf(void* hp, const double* src, double* tgt, int use_correction, 
     });
 }
 
+int orc_apply_if(void* hp, const double* src, double* tgt, double alpha_base, int subtract_non_leaf)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Field s(src, src + n), t(tgt, tgt + n);
+        h->s->apply_if(s, t, alpha_base, subtract_non_leaf != 0);
+        std::memcpy(tgt, t.data(), n * sizeof(double));
+    });
+}
+
+int orc_fmm_apply_ge(void* hp, const double* src, double* tgt, int level, int nlas, double scale, double alpha)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Field s(src, src + n), t(tgt, tgt + n);
+        h->s->fmm_apply_ge(s, t, level, nlas != 0, scale, alpha);
+        std::memcpy(tgt, t.data(), n * sizeof(double));
+    });
+}
+
+double orc_lgf_ge_get(void* hp, int x, int y, int z, double alpha) { return static_cast<Handle*>(hp)->s->lgf_ge_get(x, y, z, alpha); }
+
+// in/out: arrays of pointers to whole fields (n_oct * Nb^3 each)
+int orc_op(void* hp, int op, int n_in, const double* const* in, int n_out, double* const* out, int level,
+           double scale)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        std::vector<Field> fin(n_in), fout(n_out);
+        std::vector<const Field*> pin;
+        std::vector<Field*> pout;
+        for (int i = 0; i < n_in; ++i) fin[i].assign(in[i], in[i] + n), pin.push_back(&fin[i]);
+        for (int i = 0; i < n_out; ++i) fout[i].assign(out[i], out[i] + n), pout.push_back(&fout[i]);
+        apply_op(*h->d, op, pin, pout, level, scale);
+        for (int i = 0; i < n_out; ++i) std::memcpy(out[i], fout[i].data(), n * sizeof(double));
+    });
+}
+
+int orc_buffer_exchange(void* hp, double* f, int level)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Field x(f, f + n);
+        buffer_exchange(*h->d, x, level);
+        std::memcpy(f, x.data(), n * sizeof(double));
+    });
+}
+
 // Single-block linear convolution with the reference's Convolution contract
 // (convolution.hpp:225-304): kernel holds P^3 values (P = 2Nb-1, x fastest),
 // out (Nb^3) += scale * window[Nb-1, 2Nb-2]^3 of (kernel (*) zero-padded src).

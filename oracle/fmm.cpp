@@ -717,3 +717,205 @@ void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_corr
 }
 
 }  // namespace orc
+
+// ---------------------------------------------------------------------------
+// Integrating-factor kernel LGF_GE (include/iblgf/lgf/lgf_ge.hpp:33-190):
+// E(n; alpha) = e^{-6 alpha} I_n1(2 alpha) I_n2(2 alpha) I_n3(2 alpha)
+//             = prod_i e^{-2 alpha} I_ni(2 alpha), neighbour-only, alpha scaled
+// by 4^level_diff (change_level_impl :81-84); the FMM takes the short branch
+// of Fmm::apply (fmm.hpp:754-770) with scale 1 (no dx^2).
+namespace orc
+{
+double Solver::lgf_ge_get(int x, int y, int z, double alpha)
+{
+    const int nmax = 4 * Nb + 8;
+    if (alpha != ge_alpha || (int)ge_f.size() < nmax + 1)
+    {
+        ge_f.assign(nmax + 1, 0.0);
+        bessel_ie_all(2.0 * alpha, nmax, ge_f.data());
+        ge_alpha = alpha;
+    }
+    x = std::abs(x);
+    y = std::abs(y);
+    z = std::abs(z);
+    if (x > nmax || y > nmax || z > nmax) throw std::runtime_error("LGF_GE offset out of range");
+    return ge_f[x] * ge_f[y] * ge_f[z];
+}
+
+const std::vector<cplx>& Solver::lgf_ge_spectrum(double alpha, int bx, int by, int bz)
+{
+    const auto key = std::make_tuple(alpha, bx, by, bz);
+    auto it = spectra_ge.find(key);
+    if (it != spectra_ge.end()) return it->second;
+    const int H = P / 2 + 1;
+    std::vector<cplx> x((size_t)P * P * P);
+    for (int k = 0; k < P; ++k)
+        for (int j = 0; j < P; ++j)
+            for (int i = 0; i < P; ++i)
+                x[i + (size_t)P * (j + (size_t)P * k)] = lgf_ge_get(bx + i, by + j, bz + k, alpha);
+    fft3(fft, P, x.data(), true);
+    std::vector<cplx> h((size_t)H * P * P);
+    for (int k = 0; k < P; ++k)
+        for (int j = 0; j < P; ++j)
+            for (int i = 0; i < H; ++i)
+                h[i + (size_t)H * (j + (size_t)P * k)] = x[i + (size_t)P * (j + (size_t)P * k)];
+    return spectra_ge.emplace(key, std::move(h)).first->second;
+}
+
+void Solver::fmm_apply_ge(const Field& src, Field& tgt, int level, bool nlas, double add_with_scale,
+                          double alpha)
+{
+    const size_t B = (size_t)Nb * Nb * Nb;
+    const int H = P / 2 + 1;
+    const size_t NC = (size_t)H * P * P;
+    const int rl = level - d->base_level;
+    const int idx = fmm_mask_idx_gen(AMR2AMR, rl, nlas ? 1 : 0);
+    if (fmm_s.size() != d->octs.size() * B) fmm_s.assign(d->octs.size() * B, 0.0);
+    if (fmm_t.size() != d->octs.size() * B) fmm_t.assign(d->octs.size() * B, 0.0);
+    auto Sm = [&](Octant* o) { return o->mask[idx][0]; };
+    auto Tm = [&](Octant* o) { return o->mask[idx][1]; };
+    for (int lv = level; lv >= 0; --lv)
+        for (auto& kv : d->level_maps[lv])
+        {
+            Octant* o = kv.second;
+            if (o->has_data && Sm(o)) std::fill(&fmm_s[o->idx * B], &fmm_s[o->idx * B] + B, 0.0);
+            if (o->has_data && Tm(o)) std::fill(&fmm_t[o->idx * B], &fmm_t[o->idx * B] + B, 0.0);
+        }
+    for (auto& kv : d->level_maps[level])
+    {
+        Octant* o = kv.second;
+        if (!(o->has_data && Sm(o))) continue;
+        for (int k = 1; k < Nb - 1; ++k)
+            for (int j = 1; j < Nb - 1; ++j)
+                for (int i = 1; i < Nb - 1; ++i)
+                {
+                    const size_t c = i + (size_t)Nb * (j + (size_t)Nb * k);
+                    fmm_s[o->idx * B + c] = src[o->idx * B + c];
+                }
+    }
+    std::vector<Octant*> targets, sources;
+    for (auto& kv : d->level_maps[level])
+    {
+        if (kv.second->has_data && Tm(kv.second)) targets.push_back(kv.second);
+        if (kv.second->has_data && Sm(kv.second)) sources.push_back(kv.second);
+    }
+    std::map<Octant*, int> sidx;
+    for (int i = 0; i < (int)sources.size(); ++i) sidx[sources[i]] = i;
+    std::vector<std::vector<cplx>> sspec(sources.size());
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < (int)sources.size(); ++i) fwd_half(&fmm_s[sources[i]->idx * B], sspec[i]);
+    struct Pair { int s; const std::vector<cplx>* g; };
+    std::vector<std::vector<Pair>> plist(targets.size());
+    for (size_t ti = 0; ti < targets.size(); ++ti)
+    {
+        Octant* t = targets[ti];
+        for (int i = 0; i < 27; ++i)
+        {
+            Octant* n = t->neighbor[i];
+            if (!n || !Sm(n)) continue;
+            plist[ti].push_back({sidx.at(n), &lgf_ge_spectrum(alpha, t->bbase[0] - n->bbase[0] - (Nb - 1),
+                                                              t->bbase[1] - n->bbase[1] - (Nb - 1),
+                                                              t->bbase[2] - n->bbase[2] - (Nb - 1))});
+        }
+    }
+    const double scale = 1.0 / ((double)P * P * P);
+#pragma omp parallel for schedule(dynamic)
+    for (int ti = 0; ti < (int)targets.size(); ++ti)
+    {
+        if (plist[ti].empty()) continue;
+        std::vector<cplx> acc(NC, 0.0);
+        for (auto& pr : plist[ti])
+        {
+            const cplx* g = pr.g->data();
+            const cplx* s = sspec[pr.s].data();
+            for (size_t f = 0; f < NC; ++f) acc[f] += g[f] * s[f];
+        }
+        for (size_t f = 0; f < NC; ++f) acc[f] *= scale;
+        std::vector<cplx> x((size_t)P * P * P);
+        for (int k = 0; k < P; ++k)
+            for (int j = 0; j < P; ++j)
+                for (int i = 0; i < P; ++i)
+                {
+                    cplx v;
+                    if (i < H) v = acc[i + (size_t)H * (j + (size_t)P * k)];
+                    else v = std::conj(acc[(P - i) + (size_t)H * ((P - j) % P + (size_t)P * ((P - k) % P))]);
+                    x[i + (size_t)P * (j + (size_t)P * k)] = v;
+                }
+        fft3(fft, P, x.data(), false);
+        double* out = &fmm_t[targets[ti]->idx * B];
+        for (int k = 0; k < Nb; ++k)
+            for (int j = 0; j < Nb; ++j)
+                for (int i = 0; i < Nb; ++i)
+                    out[i + (size_t)Nb * (j + (size_t)Nb * k)] +=
+                        x[(i + Nb - 1) + (size_t)P * ((j + Nb - 1) + (size_t)P * (k + Nb - 1))].real();
+    }
+    for (auto& kv : d->level_maps[level])
+    {
+        Octant* o = kv.second;
+        if (!(o->has_data && Tm(o))) continue;
+        for (size_t c = 0; c < B; ++c) tgt[o->idx * B + c] += fmm_t[o->idx * B + c] * add_with_scale;
+    }
+}
+
+void Solver::coarsify_all(Field& f)
+{
+    const size_t B = (size_t)Nb * Nb * Nb;
+    for (int ls = d->depth - 2; ls >= d->base_level; --ls)
+        for (auto& kv : d->level_maps[ls])
+        {
+            Octant* p = kv.second;
+            for (int c = 0; c < 8; ++c)
+            {
+                Octant* ch = p->child[c].get();
+                if (!ch || !ch->has_data) continue;
+                tp_antrp(Nb, cc_antrp[2 + (c & 1)].data(), cc_antrp[2 + ((c >> 1) & 1)].data(),
+                         cc_antrp[2 + ((c >> 2) & 1)].data(), &f[ch->idx * B], &f[p->idx * B]);
+            }
+        }
+}
+
+void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_only)
+{
+    const size_t B = (size_t)Nb * Nb * Nb;
+    for (auto& kv : d->level_maps[level])
+    {
+        Octant* p = kv.second;
+        for (int c = 0; c < 8; ++c)
+        {
+            Octant* ch = p->child[c].get();
+            if (!ch || !ch->has_data) continue;
+            if (correction_only && !ch->correction) continue;
+            tp_interp(Nb, cc_intrp[2 + (c & 1)].data(), cc_intrp[2 + ((c >> 1) & 1)].data(),
+                      cc_intrp[2 + ((c >> 2) & 1)].data(), &from[p->idx * B], &to[ch->idx * B], false);
+        }
+    }
+}
+
+// PoissonSolver::apply_if (poisson.hpp:436-494) for AMR2AMR
+void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf)
+{
+    const size_t B = (size_t)Nb * Nb * Nb;
+    const size_t N = d->octs.size() * B;
+    Field source_tmp(N, 0.0), target_tmp(N, 0.0);
+    for (Octant* o : d->octs)
+        if (o->leaf) std::copy(&src[o->idx * B], &src[o->idx * B] + B, &source_tmp[o->idx * B]);
+    coarsify_all(source_tmp);
+    // intrp_to_correction_buffer (poisson.hpp:1015-1069)
+    for (int l = d->depth - 2; l >= d->base_level; --l)
+    {
+        buffer_exchange(*d, source_tmp, l);
+        cc_intrp_level(source_tmp, source_tmp, l, true);
+    }
+    for (int l = d->base_level; l < d->depth; ++l)
+    {
+        const double alpha = alpha_base * std::pow(4.0, l - d->base_level);
+        fmm_apply_ge(source_tmp, target_tmp, l, false, 1.0, alpha);
+        if (!subtract_non_leaf) fmm_apply_ge(source_tmp, target_tmp, l, true, 1.0, alpha);
+        for (auto& kv : d->level_maps[l])
+        {
+            Octant* o = kv.second;
+            std::copy(&target_tmp[o->idx * B], &target_tmp[o->idx * B] + B, &tgt[o->idx * B]);
+        }
+    }
+}
+}  // namespace orc

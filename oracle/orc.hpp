@@ -144,6 +144,10 @@ struct Solver
     std::vector<double> cc_intrp[4], cc_antrp[4];
     // LGF spectra cache: (level_diff, base offset) -> half spectrum
     std::map<std::array<int, 4>, std::vector<cplx>> spectra;
+    // LGF_GE spectra cache: (alpha, base offset) -> half spectrum
+    std::map<std::tuple<double, int, int, int>, std::vector<cplx>> spectra_ge;
+    double ge_alpha = -1.0;
+    std::vector<double> ge_f;  // e^{-2 alpha} I_n(2 alpha)
     Field fmm_s, fmm_t;
     explicit Solver(Domain* d, int intrp_order = 5);
 
@@ -153,9 +157,20 @@ struct Solver
                    double add_with_scale, int fmm_type);
     void apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_correction,
                    bool subtract_non_leaf);
+    // integrating factor (LGF_GE, neighbour only): lgf_ge.hpp, fmm.hpp:754-770
+    double lgf_ge_get(int x, int y, int z, double alpha);
+    const std::vector<cplx>& lgf_ge_spectrum(double alpha, int bx, int by, int bz);
+    void fmm_apply_ge(const Field& src, Field& tgt, int level, bool non_leaf_as_source,
+                      double add_with_scale, double alpha);
+    void apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf);
+    void cc_intrp_level(Field& from, Field& to, int level, bool correction_only);
+    void coarsify_all(Field& f);
 };
 
 void nli_matrix(int Nb, int pts_cap, double* mat /* Nb x 2Nb, (p,c) at p*2Nb+c */);
+void buffer_exchange(Domain& d, Field& f, int level);
+void apply_op(Domain& d, int op, const std::vector<const Field*>& in, const std::vector<Field*>& out,
+              int level, double scale);
 void cc_matrix(int Nb, int pts_cap, int relpos, double* mat);
 
 }  // namespace orc

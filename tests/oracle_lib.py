@@ -50,6 +50,12 @@ def lib():
         L.orc_fmm_apply.argtypes = [vp, vp, vp, ci, ci, cd, ci]
         L.orc_apply_lgf.argtypes = [vp, vp, vp, ci, ci]
         L.orc_block_conv.argtypes = [ci, vp, vp, vp, cd]
+        L.orc_op.argtypes = [vp, ci, ci, vp, ci, vp, ci, cd]
+        L.orc_buffer_exchange.argtypes = [vp, vp, ci]
+        L.orc_apply_if.argtypes = [vp, vp, vp, cd, ci]
+        L.orc_fmm_apply_ge.argtypes = [vp, vp, vp, ci, ci, cd, cd]
+        L.orc_lgf_ge_get.argtypes = [vp, ci, ci, ci, cd]
+        L.orc_lgf_ge_get.restype = cd
         _lib = L
     return _lib
 
@@ -149,6 +155,36 @@ class Domain:
         _check(lib().orc_fmm_apply(self.h, _p(src), _p(out), int(level), int(non_leaf_as_source),
                                    float(scale), int(fmm_type)))
         return out
+
+    def op(self, op, inputs, outputs, level=-1, scale=1.0):
+        """Mimetic block operator; inputs/outputs are lists of fields."""
+        ins = [np.ascontiguousarray(a, dtype=np.float64) for a in inputs]
+        outs = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in outputs]
+        pin = (ctypes.c_void_p * len(ins))(*[a.ctypes.data for a in ins])
+        pout = (ctypes.c_void_p * len(outs))(*[a.ctypes.data for a in outs])
+        _check(lib().orc_op(self.h, int(op), len(ins), pin, len(outs), pout, int(level), float(scale)))
+        return outs
+
+    def buffer_exchange(self, f, level):
+        x = np.ascontiguousarray(f, dtype=np.float64).copy()
+        _check(lib().orc_buffer_exchange(self.h, _p(x), int(level)))
+        return x
+
+    def apply_if(self, src, alpha_base, tgt=None, subtract_non_leaf=False):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        out = self.zeros() if tgt is None else np.ascontiguousarray(tgt, dtype=np.float64).copy()
+        _check(lib().orc_apply_if(self.h, _p(src), _p(out), float(alpha_base), int(subtract_non_leaf)))
+        return out
+
+    def fmm_apply_ge(self, src, tgt, level, non_leaf_as_source, scale, alpha):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        out = np.ascontiguousarray(tgt, dtype=np.float64).copy()
+        _check(lib().orc_fmm_apply_ge(self.h, _p(src), _p(out), int(level), int(non_leaf_as_source),
+                                      float(scale), float(alpha)))
+        return out
+
+    def lgf_ge_get(self, x, y, z, alpha):
+        return lib().orc_lgf_ge_get(self.h, int(x), int(y), int(z), float(alpha))
 
     def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False):
         src = np.ascontiguousarray(src, dtype=np.float64)

@@ -38,3 +38,12 @@ def test_create_without_device_reports_status():
 def test_null_config_is_rejected():
     h = ctypes.c_void_p()
     assert B.lib().iblgf_create(None, ctypes.byref(h)) == 1
+
+
+def test_cpp_adapter_builds():
+    """include/iblgf_b200/adapter.hpp (reference-style PoissonSolver<Setup>)
+    compiles against a stand-in of the reference's domain types and links to
+    the library."""
+    import subprocess
+    subprocess.run(["make", "-s", "-B", "-C", os.path.join(ROOT, "tests", "cpp")], check=True)
+    assert os.path.exists(os.path.join(ROOT, "tests", "cpp", "adapter_mock"))

@@ -173,3 +173,85 @@ def test_capi_errors_are_status_codes():
         g.fmm_apply(0, 0, g.depth + 3, 1)
     with pytest.raises(B.IblgfError):
         g.upload(0, np.zeros(5))
+
+
+@pytest.mark.parametrize("name", ["vr1", "amr_small"])
+def test_domain_import_matches(name):
+    """iblgf_domain_import (the drop-in path: the reference's Domain builds the
+    tree) gives the same octants, lists and masks as building it here."""
+    case = {"vr1": lambda: S.VortexRingPoisson(1), "amr_small": lambda: S.GaussianPoisson("amr_small")}[name]()
+    o, g = pair(case)
+    gi = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                  import_octants=(o.keys[::-1].copy(), o.flags[::-1].copy()))
+    assert np.array_equal(gi.keys, o.keys) and np.array_equal(gi.flags, o.flags)
+    assert np.array_equal(gi.bbase, o.bbase) and np.array_equal(gi.levels, o.levels)
+    for a, b in zip(o.lists(), gi.lists()):
+        assert np.array_equal(a, b)
+    for idx in [0] + [15 + 2 * r + n for r in range(gi.depth - gi.base_level) for n in (0, 1)]:
+        assert np.array_equal(o.masks(idx), gi.masks(idx)), idx
+
+
+def test_cpp_adapter_poisson_solve(tmp_path):
+    """The reference-style C++ adapter (PoissonSolver<Setup>::solve<Src,Tgt>)
+    over a stand-in domain in shuffled iteration order reproduces the oracle."""
+    import struct
+    import subprocess
+    case = S.GaussianPoisson("amr_small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(o)
+    ref = o.apply_lgf(src)
+    fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
+    with open(fin, "wb") as f:
+        f.write(struct.pack("7i", case.block_extent, *case.bd_base, *case.bd_extent))
+        f.write(struct.pack("d", case.dx_base))
+        f.write(struct.pack("i", o.n))
+        f.write(o.keys.astype(np.uint64).tobytes())
+        f.write(o.flags.astype(np.int32).tobytes())
+        f.write(np.ascontiguousarray(src).tobytes())
+    root = os.path.dirname(HERE)
+    subprocess.run(["make", "-s", "-C", os.path.join(root, "tests", "cpp")], check=True)
+    subprocess.run([os.path.join(root, "tests", "cpp", "adapter_mock"), str(fin), str(fout)], check=True)
+    out = np.fromfile(fout, dtype=np.float64).reshape(ref.shape)
+    # leaves carry the solution (poisson.hpp:761-781); non-leaf targets stay 0
+    assert rel_linf(out, ref) < 1e-12
+
+
+@pytest.mark.parametrize("op,n_in,n_out", [(0, 1, 1), (1, 1, 3), (2, 3, 1), (3, 3, 3), (4, 3, 3), (5, 6, 3)])
+def test_mimetic_operators(op, n_in, n_out):
+    """Operator::laplace/gradient/divergence/curl/curl_transpose/nonlinear after a
+    same-level buffer exchange, every level, against the oracle."""
+    case = S.GaussianPoisson("amr_small")
+    o, g = pair(case)
+    rng = np.random.default_rng(11 + op)
+    ins = [rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb)) for _ in range(n_in)]
+    outs0 = [rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb)) for _ in range(n_out)]
+    # buffers from the exchange on every level, as the level wrappers do
+    ref_in = ins
+    for lv in range(o.depth):
+        ref_in = [o.buffer_exchange(a, lv) for a in ref_in]
+    ref = o.op(op, ref_in, outs0, -1, 0.7)
+    fi = [g.field(a) for a in ins]
+    fo = [g.field(a) for a in outs0]
+    for lv in range(g.depth):
+        for f in fi:
+            g.buffer_exchange(f, lv)
+    for f, r in zip(fi, ref_in):
+        assert np.array_equal(g.download(f), r)
+    g.op(op, fi, fo, -1, 0.7)
+    for f, r in zip(fo, ref):
+        assert rel_linf(g.download(f), r) < 1e-13
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+@pytest.mark.parametrize("alpha", [0.05, 0.8])
+def test_integrating_factor_apply_if(precision, tol, alpha):
+    """apply_lgf_IF: LGF_GE neighbour-only FMM per level (alpha x 4^level) with
+    the leaf copy, coarsification and correction-buffer interpolation."""
+    case = S.GaussianPoisson("amr_small")
+    o, g = pair(case, precision)
+    src = case.fields(o)
+    ref = o.apply_if(src, alpha)
+    fs, ft = g.field(src), g.field()
+    g.apply_if(fs, ft, alpha)
+    assert rel_linf(g.download(ft), ref) < tol

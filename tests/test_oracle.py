@@ -126,3 +126,18 @@ def test_poisson_vortex_ring(n_levels):
     src, ex = case.fields(d)
     num = d.apply_lgf(src)
     assert case.finest_linf(d, num, ex) < case.exp_linf
+
+
+def test_lgf_ge_matches_bessel_and_conserves_mass():
+    """LGF_GE E(n; alpha) = e^{-6a} I_n1(2a) I_n2(2a) I_n3(2a) (lgf_ge.hpp:158-167):
+    against scipy's scaled Bessel functions (the reference uses Boost.Math's
+    cyl_bessel_i, not available here) and sum_n E = 1 (heat-kernel mass)."""
+    sp = pytest.importorskip("scipy.special")
+    case = S.GaussianPoisson("uniform_small")
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks)
+    for a in (0.05, 0.37, 2.5):
+        for n in [(0, 0, 0), (1, 2, 3), (7, 0, 25), (30, 3, 1)]:
+            ref = sp.ive(n[0], 2 * a) * sp.ive(n[1], 2 * a) * sp.ive(n[2], 2 * a)
+            assert abs(d.lgf_ge_get(*n, a) - ref) <= 1e-13 * ref
+        r = range(-20, 21)
+        assert abs(sum(d.lgf_ge_get(x, y, z, a) for x in r for y in r for z in r) - 1.0) < 1e-12
