@@ -280,7 +280,8 @@ def main():
                            "precision": args.precision + " FFT/MAC, f64 fields and LGF table",
                            "l2": "inputs larger than L2 (fields %.0f MB, spectra cache > 126 MB)" % (g.n * g.Nb ** 3 * 8 / 1e6),
                            "parallelism": "replicas" if world > 1 else "single GPU",
-                           "sweeps_per_step": sweeps, "pairs_per_step": npairs},
+                           "sweeps_per_step": sweeps, "pairs_per_step": npairs,
+                           "targets_per_step": ntgt, "group_mac_targets_per_step": int(stats[7]) / args.steps},
                 "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s",
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
                 "gpu_launches": int(launches),

@@ -25,6 +25,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda_pipeline.h>
+
 #include "cplx.cuh"
 #include "ctx.hpp"
 #include "lgf_dev.cuh"
@@ -201,48 +203,79 @@ __global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, c
 // and one load of S feeds 8.
 __constant__ short c_group_u[8 * 216];  // offset index (ux+3)+7(uy+3)+49(uz+3)
 
+// Launch shape: 128 threads = RW rows x F frequency lanes, each row owns M
+// groups; F x sizeof(complex) = 64 B per staged row (four 16-byte cp.async
+// chunks), so a tile of up to kTileSrc sources plus the 343 spectra fits in
+// ~96 KB and two CTAs share an SM: one stages while the other computes.
 template<class R, int F, int M>
-__global__ void __launch_bounds__(256) group_mac_kernel(
+__global__ void __launch_bounds__(128, 2) group_mac_kernel(
     const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, const int* __restrict__ tile_gptr,
     const int* __restrict__ tile_sptr, const int* __restrict__ tile_src, const int* __restrict__ tile_tab,
     const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
     const unsigned short* __restrict__ grp_src, const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
 {
+    static_assert(F * sizeof(cx<R>) == 64, "staged rows are 64 bytes");
+    constexpr int RW = 128 / F;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);  // [343][F]
-    cx<R>* Ss = Gs + 343 * F;                       // [n_src][F]
-    // grid.x = tile (fast), grid.y = frequency chunk: CTAs resident together
-    // work on the same chunk, so the chunk's spectra and source values are
-    // read from HBM once and then served from L2 to every tile
+    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);          // [343][F]
+    unsigned short* Js = reinterpret_cast<unsigned short*>(Gs + 343 * F);  // [RW*M][216]
+    cx<R>* Ss = reinterpret_cast<cx<R>*>(Js + RW * M * 216 + (RW * M * 216 % 8 ? 8 - RW * M * 216 % 8 : 0));
     const int tile = blockIdx.x;
     const long long f0 = (long long)blockIdx.y * F;
-    const int lane = threadIdx.x % F, row = threadIdx.x / F, rows = blockDim.x / F;
-    const cx<R> zero = mk<R>(0, 0);
-    const int* su = spec_u + 343 * tile_tab[tile];
-    for (int i = threadIdx.x; i < 343 * F; i += blockDim.x)
-    {
-        const int u = i / F;
-        const long long ff = f0 + (i % F);
-        const int slot = su[u];
-        Gs[i] = (slot >= 0 && ff < NC) ? G[(size_t)slot * NC + ff] : zero;
-    }
-    const int s0 = tile_sptr[tile], ns = tile_sptr[tile + 1] - s0;
-    for (int i = threadIdx.x; i < ns * F; i += blockDim.x)
-    {
-        const long long ff = f0 + (i % F);
-        Ss[i] = ff < NC ? S[(size_t)tile_src[s0 + i / F] * NC + ff] : zero;
-    }
-    __syncthreads();
+    const int lane = threadIdx.x % F, row = threadIdx.x / F;
     const int mode = tile_coarse[tile];  // 0 all, 1 non-adjacent only, 2 adjacent only
+    const int* su = spec_u + 343 * tile_tab[tile];
+    const int s0 = tile_sptr[tile], ns = tile_sptr[tile + 1] - s0;
     const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
-    const long long f = f0 + lane;
-    for (int gb = g0 + row * M; gb < g1; gb += rows * M)
+    const cx<R> zero = mk<R>(0, 0);
+    const bool full = f0 + F <= NC;
+    // ---- staging: 16-byte asynchronous copies, 4 per 64-byte row
+    const int nrow = 343 + ns;
+    for (int q = threadIdx.x; q < nrow * 4; q += blockDim.x)
     {
+        const int r = q >> 2, part = q & 3;
+        const cx<R>* src;
+        cx<R>* dst;
+        if (r < 343)
+        {
+            const int slot = su[r];
+            dst = Gs + r * F;
+            src = slot >= 0 ? G + (size_t)slot * NC + f0 : nullptr;
+        }
+        else
+        {
+            dst = Ss + (r - 343) * F;
+            src = S + (size_t)tile_src[s0 + r - 343] * NC + f0;
+        }
+        constexpr int per = 16 / sizeof(cx<R>);
+        if (src && full)
+            __pipeline_memcpy_async(dst + part * per, src + part * per, 16);
+        else
+            for (int e = 0; e < per; ++e)
+            {
+                const int l = part * per + e;
+                dst[l] = (src && f0 + l < NC) ? src[l] : zero;
+            }
+    }
+    __pipeline_commit();
+    // candidate source indices of this CTA's groups
+    for (int i = threadIdx.x; i < RW * M * 216; i += blockDim.x)
+    {
+        const int g = g0 + i / 216;
+        Js[i] = g < g1 ? grp_src[(size_t)g * 216 + (i % 216)] : (unsigned short)0xFFFF;
+    }
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    const long long f = f0 + lane;
+    for (int gb = g0 + row * M; gb < g1; gb += RW * M)
+    {
+        const unsigned short* jr = Js + (gb - g0) * 216;
         cx<R> acc[M][8];
 #pragma unroll
         for (int m = 0; m < M; ++m)
 #pragma unroll
             for (int c = 0; c < 8; ++c) acc[m][c] = zero;
+#pragma unroll 2
         for (int k = 0; k < 216; ++k)
         {
             cx<R> sv[M];
@@ -250,8 +283,7 @@ __global__ void __launch_bounds__(256) group_mac_kernel(
 #pragma unroll
             for (int m = 0; m < M; ++m)
             {
-                const int g = gb + m;
-                const unsigned short j = g < g1 ? grp_src[(size_t)g * 216 + k] : (unsigned short)0xFFFF;
+                const unsigned short j = jr[m * 216 + k];
                 sv[m] = j != 0xFFFF ? Ss[j * F + lane] : zero;
                 any = any || j != 0xFFFF;
             }
@@ -289,33 +321,40 @@ __global__ void __launch_bounds__(256) group_mac_kernel(
     }
 }
 
-// inv_z: V[t][z'][p] = sum_kz ACC[t][kz][p] e^{+2 pi i kz (z'+NB-1)/P}, z' < NB
-template<class R, int NB>
-__global__ void __launch_bounds__(128) inv_z_kernel(const cx<R>* __restrict__ ACC, const R* __restrict__ tw,
-                                                    cx<R>* __restrict__ V)
+// inv_z: V[t][z'][p] = sum_kz ACC[t][kz][p] e^{+2 pi i kz (z'+NB-1)/P}, z' < NB.
+// The accumulators arrive in the working precision RA; the inverse transforms
+// run in RC = FP64 on both paths: cancellation in the c2r amplifies FP32
+// rounding of the twiddled sums far more than in the forward transforms.
+template<class RA, class RC, int NB>
+__global__ void __launch_bounds__(128) inv_z_kernel(const cx<RA>* __restrict__ ACC, const RC* __restrict__ tw,
+                                                    cx<RC>* __restrict__ V)
 {
     constexpr int P = 2 * NB - 1;
     constexpr int NP = P * NB;
-    __shared__ cx<R> s_tw[P];
-    load_tw<R>(s_tw, tw, P);
+    __shared__ cx<RC> s_tw[P];
+    load_tw<RC>(s_tw, tw, P);
     __syncthreads();
     const int t = blockIdx.x;
     const int p = blockIdx.y * blockDim.x + threadIdx.x;
     if (p >= NP) return;
-    const cx<R>* a = ACC + (size_t)t * P * NP + p;
-    cx<R> v[P];
+    const cx<RA>* a = ACC + (size_t)t * P * NP + p;
+    cx<RC> v[P];
 #pragma unroll
-    for (int kz = 0; kz < P; ++kz) v[kz] = a[(size_t)kz * NP];
-    cx<R>* out = V + (size_t)t * NB * NP + p;
+    for (int kz = 0; kz < P; ++kz)
+    {
+        const cx<RA> x = a[(size_t)kz * NP];
+        v[kz] = mk<RC>((RC)x.x, (RC)x.y);
+    }
+    cx<RC>* out = V + (size_t)t * NB * NP + p;
     for (int zo = 0; zo < NB; ++zo)
     {
         const int zz = zo + NB - 1;
-        cx<R> s = mk<R>(0, 0);
+        cx<RC> s = mk<RC>(0, 0);
         int j = 0;
 #pragma unroll
         for (int kz = 0; kz < P; ++kz)
         {
-            cmac_conj<R>(s, v[kz], s_tw[j]);
+            cmac_conj<RC>(s, v[kz], s_tw[j]);
             j += zz;
             if (j >= P) j -= P;
         }
@@ -422,17 +461,20 @@ struct Conv
         c.launches += 1;
     }
 
-    static constexpr int GF = std::is_same<R, float>::value ? 16 : 8;
-    static constexpr int GM = std::is_same<R, float>::value ? 2 : 1;
+    static constexpr int GF = std::is_same<R, float>::value ? 8 : 4;
+    static constexpr int GM = std::is_same<R, float>::value ? 2 : 1;  // rows x M = 32 groups per CTA
 
     static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc)
     {
         if (!p.n_tiles) return;
-        const size_t smem = (size_t)(343 + p.max_tile_src) * GF * sizeof(cx<R>);
+        constexpr int RW = 128 / GF;
+        const size_t js = RW * GM * 216 * sizeof(unsigned short);
+        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + ((js + 15) / 16) * 16 +
+                            (size_t)p.max_tile_src * GF * sizeof(cx<R>);
         auto kfn = group_mac_kernel<R, GF, GM>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
-        kfn<<<grid, 256, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.tile_gptr.p,
+        kfn<<<grid, 128, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.tile_gptr.p,
                                            p.tile_sptr.p, p.tile_src.p, p.tile_tab.p, p.tile_coarse.p,
                                            p.spec_u.p, p.grp_src.p, p.grp_tgt.p, (cx<R>*)acc);
         c.launches += 1;
@@ -441,9 +483,10 @@ struct Conv
     static void inverse(Ctx& c, const void* acc, const int* d_tgt_oct, int n_tgt, double scale, double* target)
     {
         if (!n_tgt) return;
-        cx<R>* V = (cx<R>*)c.d_w.p;
-        inv_z_kernel<R, NB><<<dim3(n_tgt, (NP + 127) / 128), 128, 0, c.stream>>>((const cx<R>*)acc, tw(c), V);
-        inv_yx_kernel<R, NB><<<dim3(n_tgt, NB), 256, 0, c.stream>>>(V, tw(c), d_tgt_oct, scale, target);
+        double2* V = (double2*)c.d_w.p;
+        inv_z_kernel<R, double, NB><<<dim3(n_tgt, (NP + 127) / 128), 128, 0, c.stream>>>((const cx<R>*)acc,
+                                                                                        c.d_tw64.p, V);
+        inv_yx_kernel<double, NB><<<dim3(n_tgt, NB), 256, 0, c.stream>>>(V, c.d_tw64.p, d_tgt_oct, scale, target);
         c.launches += 2;
     }
 };
@@ -551,7 +594,7 @@ void upload_group_offsets()
 
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale)
 {
-    ensure(c.d_w, (size_t)p.n_tgt * c.Nb * c.P * c.Nb * c.cplx_bytes());
+    ensure(c.d_w, (size_t)p.n_tgt * c.Nb * c.P * c.Nb * 16);
     dispatch(c, [&](auto cv) {
         using CV = decltype(cv);
         CV::inverse(c, acc, p.tgt_oct.p, p.n_tgt, scale, fmm_t);
@@ -567,7 +610,7 @@ void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* 
     sspec.alloc(c.NC * cb);
     acc.alloc(c.NC * cb);
     ensure(c.d_w, (size_t)c.P * c.P * c.Nb * 16);
-    std::vector<int> zero{0}, ptr{0, 1};
+    std::vector<int> zero{0}, ptr{0, 1};  // the FP64 inverse of one block fits: Nb*P*Nb <= P*P*Nb
     DevBuf<int> d_zero, d_ptr;
     d_zero.upload(zero, c.stream);
     d_ptr.upload(ptr, c.stream);

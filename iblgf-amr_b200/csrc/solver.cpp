@@ -570,7 +570,9 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
     }
     // tiles: consecutive groups of one level distance while the union of their
     // sources fits the staging budget
-    const int kScap = 1152, kGcap = 32;
+    // a tile: up to 32 sibling groups (16 rows x 2 per row of the MAC CTA) whose
+    // union of candidate sources fits the 64-byte-row staging budget
+    const int kScap = 1024, kGcap = 32;
     std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
     std::vector<unsigned short> gsrc;
     std::map<int, int> local;
@@ -711,6 +713,7 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     c.stats[4] += p.n_spec_unique;
     for (auto& t : p.antrp) c.stats[5] += t.n_tasks;
     for (auto& t : p.intrp) c.stats[6] += t.n_tasks;
+    c.stats[7] += p.n_tgt - p.n_csr_tgt;
     const double dx_level = c.cfg.dx_base / std::pow(2.0, rl);
     double* fs = c.field(c.f_fmm_s);
     double* ft = c.field(c.f_fmm_t);

@@ -156,7 +156,8 @@ int iblgf_profile_read(iblgf_ctx* ctx, double* out4);
 /* Work counters since the last iblgf_profile call: [0] FMM sweeps,
  * [1] source blocks transformed, [2] target blocks, [3] (target, source)
  * pairs, [4] distinct LGF spectra used per sweep (summed), [5] anterpolation
- * block transfers, [6] interpolation block transfers, [7] reserved. */
+ * block transfers, [6] interpolation block transfers, [7] targets handled by
+ * the sibling-group MAC (the rest use the general pair-list MAC). */
 int iblgf_stats(iblgf_ctx* ctx, long long* out8);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the
