@@ -35,6 +35,9 @@ int guard(F&& f)
 
 extern "C" {
 
+int orc_apply_lgf_type(void* hp, const double* src, double* tgt, int use_correction, int subtract_non_leaf,
+                       int fmm_type);
+
 const char* orc_last_error() { return g_err.c_str(); }
 
 double orc_lgf_get(int x, int y, int z) { return lgf_get(x, y, z); }
@@ -156,11 +159,17 @@ int orc_fmm_apply(void* hp, const double* src, double* tgt, int level, int nlas,
 
 int orc_apply_lgf(void* hp, const double* src, double* tgt, int use_correction, int subtract_non_leaf)
 {
+    return orc_apply_lgf_type(hp, src, tgt, use_correction, subtract_non_leaf, AMR2AMR);
+}
+
+int orc_apply_lgf_type(void* hp, const double* src, double* tgt, int use_correction, int subtract_non_leaf,
+                       int fmm_type)
+{
     auto* h = static_cast<Handle*>(hp);
     return guard([&] {
         const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
         Field s(src, src + n), t(tgt, tgt + n);
-        h->s->apply_lgf(s, t, AMR2AMR, use_correction != 0, subtract_non_leaf != 0);
+        h->s->apply_lgf(s, t, fmm_type, use_correction != 0, subtract_non_leaf != 0);
         std::memcpy(tgt, t.data(), n * sizeof(double));
     });
 }

@@ -597,11 +597,37 @@ void Solver::fmm_apply(const Field& src, Field& tgt, int level, bool nlas,
 void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_correction,
                        bool subtract_non_leaf)
 {
-    if (fmm_type != AMR2AMR) throw std::runtime_error("oracle: apply_lgf supports AMR2AMR");
+    if (fmm_type != AMR2AMR && fmm_type != STREAM) throw std::runtime_error("oracle: unsupported fmm_type");
     const size_t B = (size_t)Nb * Nb * Nb;
     const size_t N = d->octs.size() * B;
     Field source_tmp(N, 0.0), target_tmp(N, 0.0), correction_tmp(N, 0.0);
     auto blk = [&](Field& f, Octant* o) { return &f[o->idx * B]; };
+    if (fmm_type == STREAM)
+    {
+        // poisson.hpp:612-614 (copy_level, interior only), l = base level only,
+        // one sweep with the stream mask (:749-752), leaves copied (:761-781)
+        for (auto& kv : d->level_maps[d->base_level])
+        {
+            Octant* o = kv.second;
+            for (int k = 1; k < Nb - 1; ++k)
+                for (int j = 1; j < Nb - 1; ++j)
+                    for (int i = 1; i < Nb - 1; ++i)
+                    {
+                        const size_t c = i + (size_t)Nb * (j + (size_t)Nb * k);
+                        source_tmp[o->idx * B + c] = src[o->idx * B + c];
+                    }
+        }
+        if (!subtract_non_leaf)
+        {
+            fmm_apply(source_tmp, target_tmp, d->base_level, false, 1.0, STREAM);
+            for (auto& kv : d->level_maps[d->base_level])
+            {
+                Octant* o = kv.second;
+                if (o->leaf) std::copy(blk(target_tmp, o), blk(target_tmp, o) + B, &tgt[o->idx * B]);
+            }
+        }
+        return;
+    }
     // copy_leaf (with buffer)
     for (Octant* o : d->octs)
         if (o->leaf) std::copy(&src[o->idx * B], &src[o->idx * B] + B, blk(source_tmp, o));

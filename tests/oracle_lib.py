@@ -49,6 +49,7 @@ def lib():
         L.orc_solver_create.argtypes = [vp, ci]
         L.orc_fmm_apply.argtypes = [vp, vp, vp, ci, ci, cd, ci]
         L.orc_apply_lgf.argtypes = [vp, vp, vp, ci, ci]
+        L.orc_apply_lgf_type.argtypes = [vp, vp, vp, ci, ci, ci]
         L.orc_block_conv.argtypes = [ci, vp, vp, vp, cd]
         L.orc_op.argtypes = [vp, ci, ci, vp, ci, vp, ci, cd]
         L.orc_buffer_exchange.argtypes = [vp, vp, ci]
@@ -186,9 +187,9 @@ class Domain:
     def lgf_ge_get(self, x, y, z, alpha):
         return lib().orc_lgf_ge_get(self.h, int(x), int(y), int(z), float(alpha))
 
-    def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False):
+    def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False, fmm_type=1):
         src = np.ascontiguousarray(src, dtype=np.float64)
         out = self.zeros() if tgt is None else np.ascontiguousarray(tgt, dtype=np.float64).copy()
-        _check(lib().orc_apply_lgf(self.h, _p(src), _p(out), int(use_correction),
-                                   int(subtract_non_leaf)))
+        _check(lib().orc_apply_lgf_type(self.h, _p(src), _p(out), int(use_correction),
+                                        int(subtract_non_leaf), int(fmm_type)))
         return out
