@@ -121,6 +121,10 @@ struct TpTasks  // tensor-product transfer tasks of one tree level
     DevBuf<int> task_cid;       // child id (0..7)
 };
 
+// sibling groups per group-MAC tile; the kernel's thread rows x groups per
+// row cover exactly this many
+constexpr int kGroupTileCap = 32;
+
 struct FmmPlan
 {
     int level = 0, mask_idx = 0;
@@ -234,7 +238,6 @@ void launch_build_lists(Ctx& c, const u64* d_sorted_keys, const int* d_sorted_id
 void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots);
 void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, int n_src, void* src_spec);
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
-void upload_group_offsets();
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale);
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);

@@ -194,21 +194,21 @@ __global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, c
 // Sibling-group MAC. At a sweep's base level the neighbours and the influence
 // list of a target together are exactly the children of its parent's 27
 // neighbours; coarser targets see the non-adjacent ones. The 8 siblings of a
-// parent therefore share one candidate source set (216 = 27 x 8), and the
-// offset of (child c, candidate k = (n, c')) is u = c - c' - 2n in [-3,3]^3.
-// One CTA = (tile of sibling groups, chunk of F frequencies): the tile's LGF
-// spectra (343 offsets) and the union of its groups' sources are staged in
-// shared memory; each thread keeps the accumulators of M groups x 8 children
-// for one frequency, so one shared-memory load of G[u] feeds M complex MACs
-// and one load of S feeds 8.
-__constant__ short c_group_u[8 * 216];  // offset index (ux+3)+7(uy+3)+49(uz+3)
-
-// Launch shape: 128 threads = RW rows x F frequency lanes, each row owns M
-// groups; F x sizeof(complex) = 64 B per staged row (four 16-byte cp.async
-// chunks), so a tile of up to kTileSrc sources plus the 343 spectra fits in
-// ~96 KB and two CTAs share an SM: one stages while the other computes.
+// parent therefore share one candidate source set (216 = 27 x 8 candidates
+// k = (n, c')), and the offset of (child c, candidate (n, c')) is
+// u = c - c' - 2n in [-3,3]^3 (343 LGF spectra per tile).
+// For one neighbour parent n the 64 (c, c') pairs use only the 27 offsets
+// u = d - 2n, d = c - c' in [-1,1]^3, so the kernel walks n and, per z-slab
+// (c'z, cz), keeps the 9 spectra of that slab and the 4 sources with that c'z
+// in registers for 16 x M complex MACs.
+// Adjacency filtering (coarse targets take only non-adjacent sources, the
+// integrating factor only adjacent ones) depends on u alone, so it is applied
+// once when the tile's spectra are staged: excluded offsets become zero rows.
+// One CTA = (tile of up to 32 sibling groups, chunk of F frequencies); the
+// tile's spectra (64-byte rows) and the groups' candidate rows live in shared
+// memory (~50 KB, four CTAs per SM); source spectra are read through L1/L2.
 template<class R, int F, int M>
-__global__ void __launch_bounds__(128, 2) group_mac_kernel(
+__global__ void __launch_bounds__(128, 4) group_mac_kernel(
     const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, const int* __restrict__ tile_gptr,
     const int* __restrict__ tile_sptr, const int* __restrict__ tile_src, const int* __restrict__ tile_tab,
     const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
@@ -217,90 +217,100 @@ __global__ void __launch_bounds__(128, 2) group_mac_kernel(
     static_assert(F * sizeof(cx<R>) == 64, "staged rows are 64 bytes");
     constexpr int RW = 128 / F;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);          // [343][F]
-    unsigned short* Js = reinterpret_cast<unsigned short*>(Gs + 343 * F);  // [RW*M][216]
-    cx<R>* Ss = reinterpret_cast<cx<R>*>(Js + RW * M * 216 + (RW * M * 216 % 8 ? 8 - RW * M * 216 % 8 : 0));
+    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);                              // [343][F]
+    int* Jr = reinterpret_cast<int*>(Gs + 343 * F);                          // [RW*M][216] source rows
     const int tile = blockIdx.x;
     const long long f0 = (long long)blockIdx.y * F;
     const int lane = threadIdx.x % F, row = threadIdx.x / F;
     const int mode = tile_coarse[tile];  // 0 all, 1 non-adjacent only, 2 adjacent only
     const int* su = spec_u + 343 * tile_tab[tile];
-    const int s0 = tile_sptr[tile], ns = tile_sptr[tile + 1] - s0;
+    const int s0 = tile_sptr[tile];
     const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
     const cx<R> zero = mk<R>(0, 0);
     const bool full = f0 + F <= NC;
-    // ---- staging: 16-byte asynchronous copies, 4 per 64-byte row
-    const int nrow = 343 + ns;
-    for (int q = threadIdx.x; q < nrow * 4; q += blockDim.x)
+    constexpr int per = 16 / sizeof(cx<R>);
+    for (int q = threadIdx.x; q < 343 * 4; q += blockDim.x)
     {
         const int r = q >> 2, part = q & 3;
-        const cx<R>* src;
-        cx<R>* dst;
-        if (r < 343)
-        {
-            const int slot = su[r];
-            dst = Gs + r * F;
-            src = slot >= 0 ? G + (size_t)slot * NC + f0 : nullptr;
-        }
-        else
-        {
-            dst = Ss + (r - 343) * F;
-            src = S + (size_t)tile_src[s0 + r - 343] * NC + f0;
-        }
-        constexpr int per = 16 / sizeof(cx<R>);
-        if (src && full)
-            __pipeline_memcpy_async(dst + part * per, src + part * per, 16);
+        const int ux = r % 7 - 3, uy = (r / 7) % 7 - 3, uz = r / 49 - 3;
+        const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
+        const int slot = (mode == 1 && adj) || (mode == 2 && !adj) ? -1 : su[r];
+        cx<R>* dst = Gs + r * F + part * per;
+        const cx<R>* src = slot >= 0 ? G + (size_t)slot * NC + f0 + part * per : nullptr;
+        if (src && full) __pipeline_memcpy_async(dst, src, 16);
         else
             for (int e = 0; e < per; ++e)
-            {
-                const int l = part * per + e;
-                dst[l] = (src && f0 + l < NC) ? src[l] : zero;
-            }
+                dst[e] = (src && f0 + part * per + e < NC) ? src[e] : zero;
     }
     __pipeline_commit();
-    // candidate source indices of this CTA's groups
     for (int i = threadIdx.x; i < RW * M * 216; i += blockDim.x)
     {
         const int g = g0 + i / 216;
-        Js[i] = g < g1 ? grp_src[(size_t)g * 216 + (i % 216)] : (unsigned short)0xFFFF;
+        const unsigned short j = g < g1 ? grp_src[(size_t)g * 216 + (i % 216)] : (unsigned short)0xFFFF;
+        Jr[i] = j != 0xFFFF ? tile_src[s0 + j] : -1;
     }
     __pipeline_wait_prior(0);
     __syncthreads();
     const long long f = f0 + lane;
+    const long long fc = f < NC ? f : NC - 1;  // clamped column for the tail chunk
+    const cx<R>* Sf = S + fc;
     for (int gb = g0 + row * M; gb < g1; gb += RW * M)
     {
-        const unsigned short* jr = Js + (gb - g0) * 216;
+        const int* jr = Jr + (gb - g0) * 216;
         cx<R> acc[M][8];
 #pragma unroll
         for (int m = 0; m < M; ++m)
 #pragma unroll
             for (int c = 0; c < 8; ++c) acc[m][c] = zero;
-#pragma unroll 2
-        for (int k = 0; k < 216; ++k)
+        for (int n = 0; n < 27; ++n)
         {
-            cx<R> sv[M];
+            int jj[M][8];
             bool any = false;
 #pragma unroll
             for (int m = 0; m < M; ++m)
-            {
-                const unsigned short j = jr[m * 216 + k];
-                sv[m] = j != 0xFFFF ? Ss[j * F + lane] : zero;
-                any = any || j != 0xFFFF;
-            }
-            if (!any) continue;
 #pragma unroll
-            for (int c = 0; c < 8; ++c)
-            {
-                const int u = c_group_u[c * 216 + k];
-                if (mode)
+                for (int cp = 0; cp < 8; ++cp)
                 {
-                    const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
-                    const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
-                    if (adj == (mode == 1)) continue;
+                    jj[m][cp] = jr[m * 216 + n * 8 + cp];
+                    any = any || jj[m][cp] >= 0;
                 }
-                const cx<R> gv = Gs[u * F + lane];
+            if (!any) continue;
+            // row of u = -2n; d = (dx, dy, dz) adds dx + 7 dy + 49 dz
+            const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
+            const cx<R>* gn = Gs + ((3 - 2 * nx) + 7 * (3 - 2 * ny) + 49 * (3 - 2 * nz)) * F + lane;
 #pragma unroll
-                for (int m = 0; m < M; ++m) cmac<R>(acc[m][c], gv, sv[m]);
+            for (int cpz = 0; cpz < 2; ++cpz)
+            {
+                cx<R> sv[M][4];
+#pragma unroll
+                for (int m = 0; m < M; ++m)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                    {
+                        const int j = jj[m][4 * cpz + q];
+                        sv[m][q] = j >= 0 ? __ldg(Sf + (size_t)j * NC) : zero;
+                    }
+#pragma unroll
+                for (int cz = 0; cz < 2; ++cz)
+                {
+                    const int dz = cz - cpz;
+                    cx<R> gv[9];
+#pragma unroll
+                    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                        for (int dx = -1; dx <= 1; ++dx)
+                            gv[(dy + 1) * 3 + dx + 1] = gn[(dx + 7 * dy + 49 * dz) * F];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)  // c' = 4 cpz + q
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)  // c = 4 cz + r
+                        {
+                            const int dx = (r & 1) - (q & 1), dy = (r >> 1) - (q >> 1);
+                            const cx<R> g = gv[(dy + 1) * 3 + dx + 1];
+#pragma unroll
+                            for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][q]);
+                        }
+                }
             }
         }
         if (f < NC)
@@ -468,9 +478,8 @@ struct Conv
     {
         if (!p.n_tiles) return;
         constexpr int RW = 128 / GF;
-        const size_t js = RW * GM * 216 * sizeof(unsigned short);
-        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + ((js + 15) / 16) * 16 +
-                            (size_t)p.max_tile_src * GF * sizeof(cx<R>);
+        static_assert(RW * GM == kGroupTileCap, "one pass of thread rows covers a tile");
+        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)RW * GM * 216 * sizeof(int);
         auto kfn = group_mac_kernel<R, GF, GM>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
@@ -571,25 +580,6 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
         CV::group_mac(c, p, src_spec, acc);
     });
     IBLGF_CUDA(cudaGetLastError());
-}
-
-void upload_group_offsets()
-{
-    static bool done = false;
-    if (done) return;
-    short tab[8 * 216];
-    for (int cc = 0; cc < 8; ++cc)
-        for (int k = 0; k < 216; ++k)
-        {
-            const int n = k / 8, cp = k % 8;
-            const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
-            const int ux = (cc & 1) - (cp & 1) - 2 * nx;
-            const int uy = ((cc >> 1) & 1) - ((cp >> 1) & 1) - 2 * ny;
-            const int uz = ((cc >> 2) & 1) - ((cp >> 2) & 1) - 2 * nz;
-            tab[cc * 216 + k] = (short)((ux + 3) + 7 * (uy + 3) + 49 * (uz + 3));
-        }
-    IBLGF_CUDA(cudaMemcpyToSymbol(c_group_u, tab, sizeof(tab)));
-    done = true;
 }
 
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale)

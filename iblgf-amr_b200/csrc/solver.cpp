@@ -572,7 +572,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
     // sources fits the staging budget
     // a tile: up to 32 sibling groups (16 rows x 2 per row of the MAC CTA) whose
     // union of candidate sources fits the 64-byte-row staging budget
-    const int kScap = 1024, kGcap = 32;
+    const int kScap = 1024, kGcap = kGroupTileCap;
     std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
     std::vector<unsigned short> gsrc;
     std::map<int, int> local;
@@ -704,7 +704,6 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     const int rl = level - c.tree.base_level;
     const int idx = fmm_type == IBLGF_STREAM ? mask_idx_gen(IBLGF_STREAM, 0, 0)
                                               : mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0);
-    upload_group_offsets();
     FmmPlan& p = get_plan(c, level, idx, ge);
     c.stats[0] += 1;
     c.stats[1] += p.n_src;
@@ -967,7 +966,8 @@ void poisson_release(const Ctx* c)
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
 {
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
-    if (fmm_type != IBLGF_AMR2AMR) throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR");
+    if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_STREAM)
+        throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR and STREAM");
     PoissonLists& pl = poisson_lists(c);
     double* st = c.field(c.f_source_tmp);
     double* tt = c.field(c.f_target_tmp);
@@ -976,6 +976,19 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
     IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    if (fmm_type == IBLGF_STREAM)
+    {
+        // base level only: copy_level (interior), one sweep with the stream
+        // mask, leaves copied out (poisson.hpp:612-614, 749-781)
+        const int bl = c.tree.base_level;
+        launch_copy_interior(c, c.field(src), st, pl.level_all[bl].p, (int)pl.level_all[bl].n);
+        if (!c.subtract_non_leaf)
+        {
+            fmm_apply(c, c.f_source_tmp, c.f_target_tmp, bl, false, 1.0, IBLGF_STREAM);
+            launch_axpy_blocks(c, tt, c.field(tgt), pl.level_leaves[bl].p, (int)pl.level_leaves[bl].n, 1.0, true);
+        }
+        return;
+    }
     launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
     const int bl = c.tree.base_level, depth = c.tree.depth;
     for (int ls = depth - 2; ls >= bl; --ls) launch_tp(c, pl.coarsify[ls], st, st, 4, 0);

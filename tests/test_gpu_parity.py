@@ -255,3 +255,16 @@ def test_integrating_factor_apply_if(precision, tol, alpha):
     fs, ft = g.field(src), g.field()
     g.apply_if(fs, ft, alpha)
     assert rel_linf(g.download(ft), ref) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_poisson_stream_mask(precision, tol):
+    """apply_lgf with MASK_TYPE::STREAM (base level only, stream mask: sources
+    are the non-correction base blocks) as pad_velocity uses it."""
+    case = S.GaussianPoisson("amr_small")
+    o, g = pair(case, precision)
+    src = case.fields(o)
+    ref = o.apply_lgf(src, fmm_type=0)
+    fs, ft = g.field(src), g.field()
+    g.apply_lgf(fs, ft, fmm_type=B.STREAM)
+    assert rel_linf(g.download(ft), ref) < tol
