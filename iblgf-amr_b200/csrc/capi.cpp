@@ -323,6 +323,14 @@ int iblgf_conv_block(iblgf_ctx* x, const double* src, const double* kernel, doub
     });
 }
 
+int iblgf_conv_block_noalloc(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!src || !kernel || !out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        iblgf_b200::launch_conv_block_noalloc(c, src, kernel, out, scale);
+    });
+}
+
 int iblgf_kernel_launches(iblgf_ctx* x, long long* count)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { *count = c.launches; });

@@ -253,5 +253,6 @@ void launch_op(Ctx& c, int op, const double* const* in, int n_in, double* const*
 void buffer_exchange(Ctx& c, int field, int level);
 void apply_op(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, int level, double scale);
 void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* out, double scale);
+void launch_conv_block_noalloc(Ctx& c, const double* src, const double* kernel, double* out, double scale);
 
 }  // namespace iblgf_b200

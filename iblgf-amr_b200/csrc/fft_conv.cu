@@ -22,6 +22,7 @@
 // inputs zero and half of the outputs discarded they cost about as much as a
 // mixed-radix FFT of length 35 and map onto regular loops.
 #include <cmath>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -425,6 +426,8 @@ __global__ void __launch_bounds__(256) inv_yx_kernel(const cx<R>* __restrict__ V
 template<class R, int NB>
 struct Conv
 {
+    using Real = R;
+    static constexpr int Nb = NB;
     static constexpr int P = 2 * NB - 1;
     static constexpr int NP = P * NB;
 
@@ -614,6 +617,113 @@ void launch_conv_block(Ctx& c, const double* src, const double* kernel, double* 
     });
     IBLGF_CUDA(cudaGetLastError());
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// ---------------------------------------------------------------------------
+// Single-block convolution without any device allocation. The per-call
+// temporaries of launch_conv_block (LGF, source and product spectra, the
+// transform work array, two index arrays) live instead in one file-scope
+// device array of kNoAllocScratchBytes (2 MiB). At the largest supported
+// block (Nb = 18, FP64) a call needs 1.41 MB of it.
+//
+// Who needs it: a host application that has already reserved the device
+// memory for its own block pool, or that calls the solve from a section in
+// which it must not allocate — cudaMalloc can fail there, and cudaFree
+// synchronises the whole device, which stalls every other stream the
+// application keeps busy. The context (twiddles) is created beforehand as
+// usual; this call itself performs no cudaMalloc, cudaFree or library
+// allocation, and it enqueues on the context stream without synchronising.
+//
+// Limits: the scratch is one array per device, shared by every context and
+// stream of that device, so calls that overlap in time on different streams
+// race on it; serialise them (one stream, or a host lock). The first call on a
+// device performs the one-time set-up (symbol address, index arrays), so make
+// it before any stream capture begins. No scratch byte needs to start at zero:
+// every byte a kernel reads is written earlier in the same call, and the two
+// index arrays are written once at set-up.
+constexpr size_t kNoAllocScratchBytes = size_t(2) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace
+{
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// index arrays of the one-block pair list: zero = {0}, ptr = {0, 1}
+__global__ void noalloc_index_kernel(int* idx)
+{
+    if (threadIdx.x == 0)
+    {
+        idx[0] = 0;
+        idx[1] = 0;
+        idx[2] = 1;
+    }
+}
+
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+unsigned char* noalloc_scratch(Ctx& c)
+{
+    int dev = -1;
+    IBLGF_CUDA(cudaGetDevice(&dev));
+    if (dev != c.cfg.device) IBLGF_CUDA(cudaSetDevice(c.cfg.device));
+    IBLGF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error(IBLGF_EINVAL, "device ordinal beyond the scratch table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev])
+    {
+        void* ptr = nullptr;
+        IBLGF_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        if (!ptr) throw Error(IBLGF_ECUDA, "cudaGetSymbolAddress returned a null scratch address");
+        noalloc_index_kernel<<<1, 32, 0, c.stream>>>(static_cast<int*>(ptr));
+        IBLGF_CUDA(cudaGetLastError());
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+void launch_conv_block_noalloc(Ctx& c, const double* src, const double* kernel, double* out, double scale)
+{
+    // scratch layout: [index ints | LGF spectrum | source spectrum | product | work]
+    const size_t spec = round256((size_t)c.NC * 16);  // sized for FP64 spectra
+    const size_t work = round256((size_t)c.P * c.P * c.Nb * 16);
+    const size_t need = 256 + 3 * spec + work;
+    if (need > kNoAllocScratchBytes)
+        throw Error(IBLGF_EINVAL, "block too large for the static convolution scratch (needs " +
+                                      std::to_string(need) + " bytes, limit " +
+                                      std::to_string(kNoAllocScratchBytes) + ")");
+    unsigned char* base = noalloc_scratch(c);
+    const int* d_zero = reinterpret_cast<const int*>(base);
+    const int* d_ptr = d_zero + 1;
+    unsigned char* gspec = base + 256;
+    unsigned char* sspec = gspec + spec;
+    unsigned char* acc = sspec + spec;
+    unsigned char* W = acc + spec;
+    const double s = scale / ((double)c.P * c.P * c.P);
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        using R = typename CV::Real;
+        constexpr int NB = CV::Nb, P = CV::P, NP = CV::NP;
+        fwd_xy_kernel<double, NB, P, kFromDense><<<dim3(1, P), 256, 0, c.stream>>>(
+            kernel, nullptr, nullptr, nullptr, c.d_tw64.p, (double2*)W, nullptr, 0);
+        fwd_z_kernel<double, R, NB, P><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
+            (const double2*)W, c.d_tw64.p, nullptr, (cx<R>*)gspec);
+        fwd_xy_kernel<R, NB, NB, kFromField><<<dim3(1, NB), 256, 0, c.stream>>>(
+            src, d_zero, nullptr, nullptr, CV::tw(c), (cx<R>*)W, nullptr, 0);
+        fwd_z_kernel<R, R, NB, NB><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
+            (const cx<R>*)W, CV::tw(c), nullptr, (cx<R>*)sspec);
+        mac_kernel<R><<<dim3((unsigned)((c.NC + 127) / 128), 1), 128, 0, c.stream>>>(
+            (const cx<R>*)gspec, (const cx<R>*)sspec, d_ptr, d_zero, d_zero, c.NC, (cx<R>*)acc);
+        inv_z_kernel<R, double, NB><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
+            (const cx<R>*)acc, c.d_tw64.p, (double2*)W);
+        inv_yx_kernel<double, NB><<<dim3(1, NB), 256, 0, c.stream>>>((const double2*)W, c.d_tw64.p, d_zero, s,
+                                                                       out);
+        c.launches += 7;
+    });
+    IBLGF_CUDA(cudaGetLastError());
 }
 
 }  // namespace iblgf_b200

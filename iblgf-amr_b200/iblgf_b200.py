@@ -34,7 +34,7 @@ EXPORTS = [
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
-    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block",
+    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -78,6 +78,7 @@ def lib():
     L.iblgf_buffer_exchange.argtypes = [vp, ci, ci]
     L.iblgf_lgf_get.argtypes = [vp, vp, sz, vp]
     L.iblgf_conv_block.argtypes = [vp, vp, vp, vp, cd]
+    L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
     L.iblgf_profile_read.argtypes = [vp, vp]

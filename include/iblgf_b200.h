@@ -142,6 +142,18 @@ int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out)
  * Nb must equal the context's block size. */
 int iblgf_conv_block(iblgf_ctx* ctx, const double* src, const double* kernel, double* out,
                      double scale);
+/* Same result as iblgf_conv_block, but the call allocates no device memory:
+ * its temporaries live in a 2 MiB static device array (1.41 MB used at
+ * Nb = 18); a block needing more is rejected with IBLGF_EINVAL. For hosts
+ * that must not allocate at call time (device memory already reserved for
+ * their own pool, or no device-wide synchronisation from cudaFree allowed).
+ * Enqueues on the context stream and returns without synchronising. The
+ * scratch is shared by all contexts on a device: calls overlapping in time on
+ * different streams race. The first call on a device runs a one-time set-up;
+ * make it before any stream capture. No reference counterpart: the
+ * reference's fft::Convolution owns FFTW buffers allocated at construction. */
+int iblgf_conv_block_noalloc(iblgf_ctx* ctx, const double* src, const double* kernel, double* out,
+                             double scale);
 
 /* ---- timing / introspection ------------------------------------------- */
 /* Number of kernels this library launched on the context stream so far. */
