@@ -118,6 +118,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
+    ap.add_argument("--no-ns", action="store_true", help="skip the IF-HERK step measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -271,6 +272,8 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case)
+    if rank == 0 and not args.no_ns:
+        extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -293,6 +296,43 @@ def main():
     g.close()
     if dist:
         dist.destroy_process_group()
+
+
+def ns_bench(B, stream, device, steps, warmup):
+    """IF-HERK time step (NS step ms) on the vortex-ring configuration: FP32
+    FFT/MAC path and FP64 plain path from the same initial velocity, each
+    timed with CUDA events over `steps` steps after `warmup` steps, and the
+    FP32 velocity's relative L-inf deviation from FP64 after the same steps."""
+    import torch
+    case = S.VortexRingNS("c4")
+    dt = case.dt()
+    out = {}
+    res = {}
+    for name, prec in (("fp32", B.FP32), ("fp64", B.FP64)):
+        g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                     n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=device,
+                     stream=stream.cuda_stream)
+        u0 = case.initial_velocity(g)
+        uf = [g.field(u0[k]) for k in range(3)]
+        pf = g.field()
+        T = g.ns_step(uf, pf, dt, case.Re, 0.0, warmup)
+        g.synchronize()
+        l0 = g.launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        T = g.ns_step(uf, pf, dt, case.Re, T, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out["ms_per_step_" + name] = e0.elapsed_time(e1) / steps
+        out["launches_per_step"] = (g.launches() - l0) / steps
+        res[name] = np.stack([g.download(uf[k]) for k in range(3)])
+        out["octants"], out["leaves"] = int(g.n), int(np.count_nonzero(g.leaf))
+        g.close()
+    out.update({"workload": "vortex ring R=1, sigma=0.2R, Re=1000, dx_finest=R/32, 16^3 blocks, 3 mesh levels",
+                "dt": dt, "Re": case.Re, "steps": steps, "warmup": warmup,
+                "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
+                "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
+    return out
 
 
 def cpu_baseline(case):

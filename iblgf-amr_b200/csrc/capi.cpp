@@ -82,6 +82,7 @@ int iblgf_destroy(iblgf_ctx* x)
     if (!x) return IBLGF_EINVAL;
     cudaStreamSynchronize(x->c.stream);
     iblgf_b200::poisson_release(&x->c);
+    iblgf_b200::ns_release(&x->c);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
     return IBLGF_OK;
@@ -320,6 +321,15 @@ int iblgf_conv_block(iblgf_ctx* x, const double* src, const double* kernel, doub
     return guard(x, [&](iblgf_b200::Ctx& c) {
         if (!src || !kernel || !out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
         iblgf_b200::launch_conv_block(c, src, kernel, out, scale);
+    });
+}
+
+int iblgf_ns_step(iblgf_ctx* x, const int* u_fields, int p_field, double dt, double Re, double* T, int n_steps)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!u_fields || !T) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        if (n_steps < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative step count");
+        iblgf_b200::ns_step(c, u_fields, p_field, dt, Re, T, n_steps);
     });
 }
 

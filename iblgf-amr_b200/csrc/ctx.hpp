@@ -189,7 +189,11 @@ struct Ctx
     DevBuf<double> d_lgf_table;
     DevBuf<double> d_tw64;  // 2P doubles: cos, -sin interleaved (forward)
     DevBuf<float> d_tw32;
-    DevBuf<double> d_mats;  // Nb*Nb matrices: [0,1] FMM Nli, [2,3] cell intrp, [4,5] coarsify
+    // Nb*Nb matrices (child bit 0 / 1): [0,1] FMM Nli, cell-centred transfers with
+    // relative position 1: [2,3] interpolation, [4,5] coarsification; relative
+    // position 0: [6,7] interpolation, [8,9] coarsification (injection)
+    DevBuf<double> d_mats;
+    std::vector<double> h_mats;  // host copy (transfer kernels take them as launch parameters)
 
     // spectra cache: key (level_diff, bx, by, bz) -> slot; storage in the
     // working precision, NC complex per slot
@@ -226,7 +230,30 @@ void domain_finalize(Ctx& c);
 int field_create(Ctx& c);
 void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int fmm_type, int ge = -1);
 int ge_table(Ctx& c, double alpha);
-void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type);
+// rp: relative position per axis of the field's mesh object (cell {1,1,1} when null)
+void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp = nullptr);
+
+// device block lists of the Poisson level loop and of the level-wise operators
+struct PoissonLists
+{
+    DevBuf<int> all, leaves;
+    std::vector<DevBuf<int>> level_all, level_leaves;
+    std::vector<TpTasks> coarsify;       // per level ls (dst parents at ls)
+    std::vector<TpTasks> cc_intrp;       // per level l: children of level-l octants
+    std::vector<TpTasks> corr_intrp;     // per level l: correction children
+    std::vector<DevBuf<int>> children;   // per level l: children (with data) of level-l octants
+};
+struct OpLists
+{
+    std::vector<DevBuf<int>> list;
+    std::vector<DevBuf<double>> dx;
+};
+PoissonLists& poisson_lists(Ctx& c);
+// IF-HERK time steps (ifherk.hpp:1078-1200) of the face velocity u[3] and the
+// cell pressure p; T advances by dt per step
+void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n_steps);
+void ns_release(const Ctx* c);
+OpLists& op_lists(Ctx& c);
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);
 int mask_idx_gen(int type, int refinement_level, int nlas);
 
@@ -245,6 +272,8 @@ void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list,
                         bool assign);
 void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base,
                int mode /*0 antrp add, 1 intrp add, 2 intrp assign*/);
+// per-axis matrix pairs (mat_base[3]): face / edge components of the cell-centred transfers
+void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode);
 void launch_halo(Ctx& c, double* f, const int* list, int n);
 void launch_source_correction(Ctx& c, const double* target_tmp, double* corr, const int* list, int n,
                               double inv_dx2);

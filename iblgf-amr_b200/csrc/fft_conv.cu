@@ -279,18 +279,19 @@ __global__ void __launch_bounds__(128, 4) group_mac_kernel(
             // row of u = -2n; d = (dx, dy, dz) adds dx + 7 dy + 49 dz
             const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
             const cx<R>* gn = Gs + ((3 - 2 * nx) + 7 * (3 - 2 * ny) + 49 * (3 - 2 * nz)) * F + lane;
+            // all 8 x M source values of parent n in flight at once
+            cx<R> sv[M][8];
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                {
+                    const int j = jj[m][q];
+                    sv[m][q] = j >= 0 ? __ldg(Sf + (size_t)j * NC) : zero;
+                }
 #pragma unroll
             for (int cpz = 0; cpz < 2; ++cpz)
             {
-                cx<R> sv[M][4];
-#pragma unroll
-                for (int m = 0; m < M; ++m)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                    {
-                        const int j = jj[m][4 * cpz + q];
-                        sv[m][q] = j >= 0 ? __ldg(Sf + (size_t)j * NC) : zero;
-                    }
 #pragma unroll
                 for (int cz = 0; cz < 2; ++cz)
                 {
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(128, 4) group_mac_kernel(
                             const int dx = (r & 1) - (q & 1), dy = (r >> 1) - (q >> 1);
                             const cx<R> g = gv[(dy + 1) * 3 + dx + 1];
 #pragma unroll
-                            for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][q]);
+                            for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][4 * cpz + q]);
                         }
                 }
             }

@@ -1,0 +1,358 @@
+// IF-HERK time step of the incompressible Navier-Stokes solver on the device,
+// Ifherk::time_step (include/iblgf/solver/time_integration/ifherk.hpp:
+// 1078-1200) with its helpers: up_and_down (:992-1015), clean (:1309-1352),
+// clean_leaf_correction_boundary (:1355-1405), lin_sys_with_ib_solve
+// (:1451-1517), nonlinear (:1638-1692), divergence (:1738-1763), gradient
+// (:1766-1795), add / copy (:1878-1960). Every stage runs on the context
+// stream from device-resident component fields: the Poisson and integrating-
+// factor solves, the mimetic operators, buffer exchanges and level transfers
+// are the library's own kernels, with no host round trip inside a step.
+//
+// Scope: no immersed boundary (the Schur-complement solve, smearing and the
+// IB2xIB / IB2AMR pieces act on an empty point set and change none of the
+// fields the step reads), no adaptation, no body force, frame velocity 0.
+// The velocity-refresh branch (pad_velocity + adapt_corr_time_step, taken
+// once (T - T_last_refresh) 3.3 / (Re dx_base^2) > 7) is rejected.
+#include <cmath>
+#include <map>
+#include <memory>
+
+#include "ctx.hpp"
+
+namespace iblgf_b200
+{
+void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only);
+void launch_axpby(Ctx& c, double* to, const double* from, double a, int mode);
+void launch_smooth(Ctx& c, double* f, const int* list, const int* ptr, const int* dirs, int n, int reps);
+
+namespace
+{
+enum Mesh { kCell = 0, kFace = 1, kEdge = 2 };
+
+// component field ids of a cell (1) or face / edge (3) field
+struct VF
+{
+    int mesh = kCell;
+    int n = 1;
+    int id[3] = {-1, -1, -1};
+};
+
+// relative positions of a component (cell_center_nli_intrp.hpp:349-365)
+void relpos(int mesh, int comp, int rp[3])
+{
+    for (int a = 0; a < 3; ++a) rp[a] = 1;
+    if (mesh == kFace) rp[comp] = 0;
+    else if (mesh == kEdge)
+    {
+        for (int a = 0; a < 3; ++a) rp[a] = 0;
+        rp[comp] = 1;
+    }
+}
+
+struct NsState
+{
+    VF q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
+    DevBuf<int> leaf;                // 1 for leaves, per octant
+    std::vector<DevBuf<int>> corr;   // per level: correction blocks
+    // smooth2zero lists of the base level for leaf_only_boundary false / true
+    DevBuf<int> sm_list[2], sm_ptr[2], sm_dirs[2];
+    int sm_n[2] = {0, 0};
+    double T_last_vel_refresh = 0.0;  // ifherk.hpp:1980
+};
+std::map<const Ctx*, std::unique_ptr<NsState>> g_ns;
+
+VF make_vf(Ctx& c, int mesh)
+{
+    VF f;
+    f.mesh = mesh;
+    f.n = mesh == kCell ? 1 : 3;
+    for (int k = 0; k < f.n; ++k) f.id[k] = field_create(c);
+    return f;
+}
+
+NsState& ns_state(Ctx& c)
+{
+    auto it = g_ns.find(&c);
+    if (it != g_ns.end()) return *it->second;
+    auto s = std::make_unique<NsState>();
+    s->q_i = make_vf(c, kFace);
+    s->g_i = make_vf(c, kFace);
+    s->d_i = make_vf(c, kCell);
+    s->r_i = make_vf(c, kFace);
+    s->u_i = make_vf(c, kFace);
+    s->w_1 = make_vf(c, kFace);
+    s->w_2 = make_vf(c, kFace);
+    s->cell_aux = make_vf(c, kCell);
+    s->face_aux = make_vf(c, kFace);
+    s->edge_aux = make_vf(c, kEdge);
+    std::vector<int> leaf(c.n_oct);
+    for (int i = 0; i < c.n_oct; ++i) leaf[i] = c.flags[i] & 1;
+    s->leaf.upload(leaf, c.stream);
+    s->corr.resize(c.level_octs.size());
+    for (size_t l = 0; l < c.level_octs.size(); ++l)
+    {
+        std::vector<int> v;
+        for (int o : c.level_octs[l])
+            if (c.flags[o] & 2) v.push_back(o);
+        s->corr[l].upload(v, c.stream);
+    }
+    const int bl = c.tree.base_level;
+    for (int lo = 0; lo < 2; ++lo)
+    {
+        std::vector<int> list, ptr{0}, dirs;
+        for (int o : c.level_octs[bl])
+        {
+            const size_t d0 = dirs.size();
+            for (int i = 0; i < 27; ++i)
+            {
+                const int q = c.nbr[27 * (size_t)o + i];
+                if (q < 0 || (lo && (c.flags[q] & 2))) dirs.push_back(i);
+            }
+            if (dirs.size() == d0) continue;
+            list.push_back(o);
+            ptr.push_back((int)dirs.size());
+        }
+        s->sm_n[lo] = (int)list.size();
+        s->sm_list[lo].upload(list, c.stream);
+        s->sm_ptr[lo].upload(ptr, c.stream);
+        s->sm_dirs[lo].upload(dirs, c.stream);
+    }
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    auto& ref = *s;
+    g_ns.emplace(&c, std::move(s));
+    return ref;
+}
+
+class Step
+{
+  public:
+    Step(Ctx& c_, NsState& s_, double dt_, double Re_)
+    : c(c_), s(s_), pl(poisson_lists(c_)), ol(op_lists(c_)), dt(dt_), Re(Re_)
+    {
+        bl = c.tree.base_level;
+        depth = c.tree.depth;
+        // ifherk.hpp:164-173
+        const double tmp = Re * c.cfg.dx_base * c.cfg.dx_base / dt;
+        for (int k = 0; k < 3; ++k) alpha[k] = (cc[k + 1] - cc[k]) / tmp;
+    }
+
+    void time_step(const VF& u, const VF& p)
+    {
+        up_and_down(u);
+        copy(u, s.q_i, 1.0);
+        // stage 1
+        clean(s.g_i, false);
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        clean(s.face_aux, false);
+        nonlinear(u, s.g_i, coeff_a(1, 1) * (-dt));
+        copy(s.q_i, s.r_i, 1.0);
+        add(s.g_i, s.r_i, 1.0);
+        lin_sys(alpha[0]);
+        // stage 2
+        clean(s.r_i, false);
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        add(s.g_i, s.face_aux, -1.0);
+        copy(s.face_aux, s.w_1, -1.0 / dt / coeff_a(1, 1));
+        apply_if(s.q_i, s.q_i, alpha[0]);
+        apply_if(s.w_1, s.w_1, alpha[0]);
+        add(s.q_i, s.r_i, 1.0);
+        add(s.w_1, s.r_i, dt * coeff_a(2, 1));
+        up_and_down(s.u_i);
+        nonlinear(s.u_i, s.g_i, coeff_a(2, 2) * (-dt));
+        add(s.g_i, s.r_i, 1.0);
+        lin_sys(alpha[1]);
+        // stage 3
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        clean(s.w_2, false);
+        add(s.g_i, s.face_aux, -1.0);
+        copy(s.face_aux, s.w_2, -1.0 / dt / coeff_a(2, 2));
+        copy(s.q_i, s.r_i, 1.0);
+        add(s.w_1, s.r_i, dt * coeff_a(3, 1));
+        add(s.w_2, s.r_i, dt * coeff_a(3, 2));
+        apply_if(s.r_i, s.r_i, alpha[1]);
+        up_and_down(s.u_i);
+        nonlinear(s.u_i, s.g_i, coeff_a(3, 3) * (-dt));
+        add(s.g_i, s.r_i, 1.0);
+        lin_sys(alpha[2]);
+        copy(s.u_i, u, 1.0);
+        copy(s.d_i, p, 1.0 / coeff_a(3, 3) / dt);
+    }
+
+  private:
+    Ctx& c;
+    NsState& s;
+    PoissonLists& pl;
+    OpLists& ol;
+    double dt, Re;
+    int bl = 0, depth = 0;
+    // ifherk.hpp:2010-2011
+    const double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
+    const double cc[4] = {0.0, 1.0 / 3, 1.0, 1.0};
+    double alpha[3] = {0.0, 0.0, 0.0};
+
+    double coeff_a(int i, int j) const { return a[i * (i - 1) / 2 + j - 1]; }
+    double* F(int id) { return c.field(id); }
+
+    void clean(const VF& f, bool non_leaf_only)
+    {
+        for (int k = 0; k < f.n; ++k) launch_clean(c, F(f.id[k]), s.leaf.p, non_leaf_only);
+    }
+    void copy(const VF& from, const VF& to, double a_)
+    {
+        for (int k = 0; k < from.n; ++k) launch_axpby(c, F(to.id[k]), F(from.id[k]), a_, 0);
+    }
+    void add(const VF& from, const VF& to, double a_)
+    {
+        for (int k = 0; k < from.n; ++k) launch_axpby(c, F(to.id[k]), F(from.id[k]), a_, 1);
+    }
+    void scale(const VF& f, double a_)
+    {
+        for (int k = 0; k < f.n; ++k) launch_axpby(c, F(f.id[k]), nullptr, a_, 2);
+    }
+    void exchange(const VF& f, int l)
+    {
+        for (int k = 0; k < f.n; ++k) launch_halo(c, F(f.id[k]), ol.list[l].p, (int)ol.list[l].n);
+    }
+    // source_coarsify (poisson.hpp:1136-1194) into the field itself
+    void up(const VF& f)
+    {
+        for (int k = 0; k < f.n; ++k)
+        {
+            int rp[3], m[3];
+            relpos(f.mesh, k, rp);
+            for (int a_ = 0; a_ < 3; ++a_) m[a_] = rp[a_] ? 4 : 8;
+            for (int ls = depth - 2; ls >= bl; --ls) launch_tp_axes(c, pl.coarsify[ls], F(f.id[k]), F(f.id[k]), m, 0);
+        }
+    }
+    // intrp_to_correction_buffer (poisson.hpp:1015-1069), correction children only
+    void down_to_correction(const VF& f)
+    {
+        for (int k = 0; k < f.n; ++k)
+        {
+            int rp[3], m[3];
+            relpos(f.mesh, k, rp);
+            for (int a_ = 0; a_ < 3; ++a_) m[a_] = rp[a_] ? 2 : 6;
+            for (int l = depth - 2; l >= bl; --l)
+            {
+                launch_halo(c, F(f.id[k]), ol.list[l].p, (int)ol.list[l].n);
+                launch_tp_axes(c, pl.corr_intrp[l], F(f.id[k]), F(f.id[k]), m, 2);
+            }
+        }
+    }
+    void up_and_down(const VF& f)
+    {
+        clean(f, true);
+        up(f);
+        down_to_correction(f);
+    }
+    void op(int o, std::initializer_list<const VF*> in, const VF& out, int l, double sc)
+    {
+        const double* pin[6] = {};
+        double* pout[3] = {};
+        int n_in = 0;
+        for (const VF* v : in)
+            for (int k = 0; k < v->n; ++k) pin[n_in++] = F(v->id[k]);
+        for (int k = 0; k < out.n; ++k) pout[k] = F(out.id[k]);
+        launch_op(c, o, pin, n_in, pout, out.n, ol.list[l].p, ol.dx[l].p, (int)ol.list[l].n, sc);
+    }
+    void clean_leaf_correction_boundary(const VF& f, int l, bool leaf_only_boundary)
+    {
+        if (leaf_only_boundary)
+            for (int k = 0; k < f.n; ++k) launch_zero_blocks(c, F(f.id[k]), s.corr[l].p, (int)s.corr[l].n);
+        if (l != bl) return;
+        const int v = leaf_only_boundary ? 1 : 0;
+        // smooth2zero scales every component; the reference calls it once per component
+        for (int k = 0; k < f.n; ++k)
+            launch_smooth(c, F(f.id[k]), s.sm_list[v].p, s.sm_ptr[v].p, s.sm_dirs[v].p, s.sm_n[v], f.n);
+    }
+    void nonlinear(const VF& src, const VF& tgt, double sc)
+    {
+        clean(s.edge_aux, false);
+        clean(tgt, false);
+        clean(s.face_aux, false);
+        for (int l = bl; l < depth; ++l)
+        {
+            exchange(src, l);
+            op(3, {&src}, s.edge_aux, l, 1.0);
+        }
+        copy(src, s.face_aux, 1.0);
+        for (int l = bl; l < depth; ++l)
+        {
+            exchange(s.edge_aux, l);
+            clean_leaf_correction_boundary(s.edge_aux, l, false);
+            op(5, {&s.face_aux, &s.edge_aux}, tgt, l, 1.0);
+        }
+        scale(tgt, sc);
+    }
+    void divergence(const VF& src, const VF& tgt)
+    {
+        up_and_down(src);
+        for (int l = bl; l < depth; ++l)
+        {
+            exchange(src, l);
+            op(2, {&src}, tgt, l, 1.0);
+            clean_leaf_correction_boundary(tgt, l, true);
+        }
+    }
+    void gradient(const VF& src, const VF& tgt)
+    {
+        clean(tgt, false);
+        for (int l = bl; l < depth; ++l)
+        {
+            op(1, {&src}, tgt, l, 1.0);
+            exchange(tgt, l);
+        }
+    }
+    void apply_if(const VF& src, const VF& tgt, double alpha_base)
+    {
+        for (int k = 0; k < src.n; ++k)
+        {
+            int rp[3];
+            relpos(src.mesh, k, rp);
+            iblgf_b200::apply_if(c, src.id[k], tgt.id[k], alpha_base, IBLGF_AMR2AMR, rp);
+        }
+    }
+    void lin_sys(double alpha_k)
+    {
+        divergence(s.r_i, s.cell_aux);
+        poisson_apply_lgf(c, s.cell_aux.id[0], s.d_i.id[0], IBLGF_AMR2AMR);
+        gradient(s.d_i, s.face_aux);
+        add(s.face_aux, s.r_i, -1.0);
+        if (std::fabs(alpha_k) > 1e-14) apply_if(s.r_i, s.u_i, alpha_k);
+        else copy(s.r_i, s.u_i, 1.0);
+    }
+};
+}  // namespace
+
+void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n_steps)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (!(dt > 0.0) || !(Re > 0.0)) throw Error(IBLGF_EINVAL, "dt and Re must be positive");
+    const int nf = (int)c.fields.size();
+    for (int k = 0; k < 3; ++k)
+        if (u[k] < 0 || u[k] >= nf) throw Error(IBLGF_EINVAL, "bad velocity field id");
+    if (p < 0 || p >= nf) throw Error(IBLGF_EINVAL, "bad pressure field id");
+    NsState& s = ns_state(c);
+    VF uf, pf;
+    uf.mesh = kFace;
+    uf.n = 3;
+    for (int k = 0; k < 3; ++k) uf.id[k] = u[k];
+    pf.id[0] = p;
+    Step st(c, s, dt, Re);
+    const double dx = c.cfg.dx_base;
+    for (int i = 0; i < n_steps; ++i)
+    {
+        if ((*T - s.T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
+            throw Error(IBLGF_EINVAL, "velocity refresh (pad_velocity) branch is not supported");
+        st.time_step(uf, pf);
+        *T += dt;
+    }
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void ns_release(const Ctx* c) { g_ns.erase(c); }
+
+}  // namespace iblgf_b200

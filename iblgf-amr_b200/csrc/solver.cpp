@@ -127,7 +127,18 @@ void ctx_init(Ctx& c)
                 if (col == 2 * p - 1 || col == 2 * p) simple[(size_t)h * c.Nb * c.Nb + p * c.Nb + j] = 0.5;
             }
     mats.insert(mats.end(), simple.begin(), simple.end());
+    // relative position 0 (face normal / edge transverse axes): Lagrange
+    // interpolation on coincident nodes, injection for coarsification
+    // (cell_center_nli_intrp.hpp:82-83, 109-118, 158-161)
+    append_halves(mats, lagrange_matrix(c.Nb, c.cfg.intrp_order, 0), c.Nb);
+    std::vector<double> inject((size_t)c.Nb * c.Nb * 2, 0.0);
+    for (int h = 0; h < 2; ++h)
+        for (int p = 1; p < c.Nb - 1; ++p)
+            for (int j = 1; j < c.Nb - 1; ++j)
+                if (j + h * (c.Nb - 2) == 2 * p - 1) inject[(size_t)h * c.Nb * c.Nb + p * c.Nb + j] = 1.0;
+    mats.insert(mats.end(), inject.begin(), inject.end());
     c.d_mats.upload(mats, c.stream);
+    c.h_mats = mats;
     c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
     launch_lgf_table(c);
 }
@@ -747,16 +758,8 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
 // --------------------------------------------------------------- Poisson
 namespace
 {
-struct PoissonLists
-{
-    DevBuf<int> all, leaves;
-    std::vector<DevBuf<int>> level_all, level_leaves;
-    std::vector<TpTasks> coarsify;       // per level ls (dst parents at ls)
-    std::vector<TpTasks> cc_intrp;       // per level l: children of level-l octants
-    std::vector<TpTasks> corr_intrp;     // per level l: correction children
-    std::vector<DevBuf<int>> children;   // per level l: children (with data) of level-l octants
-};
 std::map<const Ctx*, std::unique_ptr<PoissonLists>> g_plists;
+}  // namespace
 
 PoissonLists& poisson_lists(Ctx& c)
 {
@@ -816,17 +819,12 @@ PoissonLists& poisson_lists(Ctx& c)
     g_plists.emplace(&c, std::move(pl));
     return ref;
 }
-}  // namespace
 
 namespace
 {
 // per level (and "all levels" at index kMaxLevel+1): block list and dx per block
-struct OpLists
-{
-    std::vector<DevBuf<int>> list;
-    std::vector<DevBuf<double>> dx;
-};
 std::map<const Ctx*, std::unique_ptr<OpLists>> g_oplists;
+}  // namespace
 
 OpLists& op_lists(Ctx& c)
 {
@@ -858,7 +856,6 @@ OpLists& op_lists(Ctx& c)
     g_oplists.emplace(&c, std::move(ol));
     return ref;
 }
-}  // namespace
 
 void buffer_exchange(Ctx& c, int field, int level)
 {
@@ -927,8 +924,14 @@ int ge_table(Ctx& c, double alpha)
 }
 
 // PoissonSolver::apply_lgf_IF / apply_if (poisson.hpp:428-494), AMR2AMR
-void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type)
+void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp)
 {
+    static const int cell[3] = {1, 1, 1};
+    if (!rp) rp = cell;
+    // cell-centred transfer matrices per axis: relative position 1 -> [4,5]
+    // coarsify / [2,3] interpolate, relative position 0 -> [8,9] / [6,7]
+    const int coarse_m[3] = {rp[0] ? 4 : 8, rp[1] ? 4 : 8, rp[2] ? 4 : 8};
+    const int intrp_m[3] = {rp[0] ? 2 : 6, rp[1] ? 2 : 6, rp[2] ? 2 : 6};
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (fmm_type != IBLGF_AMR2AMR) throw Error(IBLGF_EINVAL, "apply_if supports AMR2AMR");
     PoissonLists& pl = poisson_lists(c);
@@ -940,12 +943,12 @@ void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type)
     IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
     launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
     const int bl = c.tree.base_level, depth = c.tree.depth;
-    for (int ls = depth - 2; ls >= bl; --ls) launch_tp(c, pl.coarsify[ls], st, st, 4, 0);
+    for (int ls = depth - 2; ls >= bl; --ls) launch_tp_axes(c, pl.coarsify[ls], st, st, coarse_m, 0);
     // intrp_to_correction_buffer (poisson.hpp:1015-1069)
     for (int l = depth - 2; l >= bl; --l)
     {
         launch_halo(c, st, ol.list[l].p, (int)ol.list[l].n);
-        launch_tp(c, pl.corr_intrp[l], st, st, 2, 2);
+        launch_tp_axes(c, pl.corr_intrp[l], st, st, intrp_m, 2);
     }
     for (int l = bl; l < depth; ++l)
     {

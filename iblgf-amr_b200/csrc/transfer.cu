@@ -14,75 +14,102 @@
 //   correction    add_source_correction (cell_center_nli_intrp.hpp:171-238)
 //   zero / copy_interior / axpy over block lists (fmm.hpp:1029-1106,
 //                 poisson.hpp:921-1013)
+#include <cstring>
+
 #include "ctx.hpp"
 
 namespace iblgf_b200
 {
 namespace
 {
-// One pass of a separable transfer along axis d: out[..m..] = sum_n T(m,n) in[..n..]
-// with T(m,n) = M(m,n) (anterpolation) or M(n,m) (interpolation).
+// The Nb x Nb matrices of a transfer per axis and child bit, passed by
+// value: they sit in the constant bank, and with the passes fully unrolled
+// every matrix entry is an FMA operand at a fixed offset (no shared-memory
+// loads). Face and edge components use different matrices per axis.
 template<int NB>
-__device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* __restrict__ out,
-                                        const double* __restrict__ M, int axis, bool transpose)
+struct TpMats
 {
-    constexpr int N3 = NB * NB * NB;
-    const int stride = axis == 0 ? 1 : (axis == 1 ? NB : NB * NB);
-    for (int i = threadIdx.x; i < N3; i += blockDim.x)
+    double m[3][2][NB * NB];
+};
+
+template<int NB>
+constexpr int tp_threads()
+{
+    return (NB * NB + 31) / 32 * 32;
+}
+
+// One pass along the fastest axis of `in`: thread p owns the pencil
+// in[p*NB + n] and writes out[m*NB^2 + p] = sum_n T(m,n) in[p*NB + n] with
+// T(m,n) = M_K(m,n) (anterpolation) or M_K(n,m) (interpolation). Writing the
+// result with the axes rotated ([z][y][x] -> [x][z][y]) makes the next axis
+// the fastest one, so all three passes read contiguous pencils; after three
+// passes the layout is back to [z][y][x]. The last pass adds into the
+// thread's accumulators instead of writing shared memory.
+template<int NB, int A, int K, bool TR, bool LAST>
+__device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* __restrict__ out,
+                                        const TpMats<NB>& mt, int p, double* acc)
+{
+    double v[NB];
+#pragma unroll
+    for (int n = 0; n < NB; ++n) v[n] = in[p * NB + n];
+#pragma unroll
+    for (int m = 0; m < NB; ++m)
     {
-        const int m = (i / stride) % NB;
-        const int base = i - m * stride;
         double s = 0.0;
-#pragma unroll 6
-        for (int n = 0; n < NB; ++n)
-        {
-            const double t = transpose ? M[n * NB + m] : M[m * NB + n];
-            s = fma(t, in[base + n * stride], s);
-        }
-        out[i] = s;
+#pragma unroll
+        for (int n = 0; n < NB; ++n) s = fma(TR ? mt.m[A][K][n * NB + m] : mt.m[A][K][m * NB + n], v[n], s);
+        if (LAST) acc[m] += s;
+        else out[m * NB * NB + p] = s;
     }
+}
+
+template<int NB, int A, bool TR, bool LAST>
+__device__ __forceinline__ void tp_pass_bit(int bit, const double* in, double* out, const TpMats<NB>& mt, int p,
+                                            double* acc)
+{
+    if (bit) tp_pass<NB, A, 1, TR, LAST>(in, out, mt, p, acc);
+    else tp_pass<NB, A, 0, TR, LAST>(in, out, mt, p, acc);
 }
 
 // mode 0: dst[group] += sum_tasks A(src)        (anterpolation / coarsify)
 // mode 1: dst[group] += I(src)                  (FMM interpolation)
 // mode 2: dst[group]  = I(src)                  (cell-centred interpolation)
-template<int NB>
-__global__ void __launch_bounds__(256) tp_kernel(const int* __restrict__ gptr, const int* __restrict__ gdst,
-                                                 const int* __restrict__ tsrc, const int* __restrict__ tcid,
-                                                 const double* __restrict__ src, double* __restrict__ dst,
-                                                 const double* __restrict__ mats, int mode)
+// One CTA per receiving block, one thread per pencil; the sending blocks of
+// a group are applied in child order into per-thread accumulators.
+template<int NB, bool TR>
+__global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
+    const int* __restrict__ gptr, const int* __restrict__ gdst, const int* __restrict__ tsrc,
+    const int* __restrict__ tcid, const double* __restrict__ src, double* __restrict__ dst,
+    const __grid_constant__ TpMats<NB> mt, int mode)
 {
     constexpr int N3 = NB * NB * NB;
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) double sm[];
     double* a = sm;
     double* b = a + N3;
-    double* acc = b + N3;
-    double* mat = acc + N3;  // 2 matrices
     const int g = blockIdx.x;
-    for (int i = threadIdx.x; i < 2 * NB * NB; i += blockDim.x) mat[i] = mats[i];
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) acc[i] = 0.0;
-    const bool tr = mode != 0;
+    const int p = threadIdx.x;
+    const bool active = p < NB * NB;
+    // accumulate onto the receiving block in task order (dst += r_0, += r_1, ...)
+    double* d = dst + (size_t)gdst[g] * N3 + p;
+    double acc[NB];
+#pragma unroll
+    for (int m = 0; m < NB; ++m) acc[m] = (active && mode != 2) ? d[m * NB * NB] : 0.0;
     for (int t = gptr[g]; t < gptr[g + 1]; ++t)
     {
-        const double* s = src + (size_t)tsrc[t] * N3;
+        const double2* s2 = reinterpret_cast<const double2*>(src + (size_t)tsrc[t] * N3);
         const int cid = tcid[t];
+        for (int i = threadIdx.x; i < N3 / 2; i += blockDim.x) reinterpret_cast<double2*>(a)[i] = s2[i];
         __syncthreads();
-        for (int i = threadIdx.x; i < N3; i += blockDim.x) a[i] = s[i];
+        if (active) tp_pass_bit<NB, 0, TR, false>(cid & 1, a, b, mt, p, acc);
         __syncthreads();
-        tp_pass<NB>(a, b, mat + ((cid >> 0) & 1) * NB * NB, 0, tr);
+        if (active) tp_pass_bit<NB, 1, TR, false>((cid >> 1) & 1, b, a, mt, p, acc);
         __syncthreads();
-        tp_pass<NB>(b, a, mat + ((cid >> 1) & 1) * NB * NB, 1, tr);
+        if (active) tp_pass_bit<NB, 2, TR, true>((cid >> 2) & 1, a, nullptr, mt, p, acc);
         __syncthreads();
-        tp_pass<NB>(a, b, mat + ((cid >> 2) & 1) * NB * NB, 2, tr);
-        __syncthreads();
-        for (int i = threadIdx.x; i < N3; i += blockDim.x) acc[i] += b[i];
     }
-    __syncthreads();
-    double* d = dst + (size_t)gdst[g] * N3;
-    if (mode == 2)
-        for (int i = threadIdx.x; i < N3; i += blockDim.x) d[i] = acc[i];
-    else
-        for (int i = threadIdx.x; i < N3; i += blockDim.x) d[i] += acc[i];
+    if (!active) return;
+#pragma unroll
+    for (int m = 0; m < NB; ++m) d[m * NB * NB] = acc[m];
 }
 
 template<int NB>
@@ -182,20 +209,31 @@ void nb_dispatch(int Nb, F&& f)
 
 void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base, int mode)
 {
+    const int bases[3] = {mat_base, mat_base, mat_base};
+    launch_tp_axes(c, t, src, dst, bases, mode);
+}
+
+void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode)
+{
     if (!t.n_groups) return;
     nb_dispatch(c.Nb, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
-        const size_t smem = (3 * (size_t)NB * NB * NB + 2 * NB * NB) * sizeof(double);
-        static bool attr = false;
-        if (!attr)
+        static_assert((NB * NB * NB) % 2 == 0, "blocks are copied as double2");
+        TpMats<NB> mt;
+        for (int a = 0; a < 3; ++a)
         {
-            IBLGF_CUDA(cudaFuncSetAttribute(tp_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
-            attr = true;
+            const size_t off = (size_t)mat_base[a] * NB * NB;
+            if (c.h_mats.size() < off + 2 * NB * NB) throw Error(IBLGF_EINTERNAL, "transfer matrices missing");
+            std::memcpy(mt.m[a], c.h_mats.data() + off, sizeof(mt.m[a]));
         }
-        tp_kernel<NB><<<t.n_groups, 256, smem, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
-                                                           t.task_cid.p, src, dst,
-                                                           c.d_mats.p + (size_t)mat_base * NB * NB, mode);
+        const size_t smem = 2 * (size_t)NB * NB * NB * sizeof(double);
+        auto launch = [&](auto kfn) {
+            IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kfn<<<t.n_groups, tp_threads<NB>(), smem, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
+                                                                  t.task_cid.p, src, dst, mt, mode);
+        };
+        if (mode == 0) launch(tp_kernel<NB, false>);
+        else launch(tp_kernel<NB, true>);
     });
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());

@@ -34,7 +34,7 @@ EXPORTS = [
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
-    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_conv_block", "iblgf_conv_block_noalloc",
+    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_ns_step", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -78,6 +78,7 @@ def lib():
     L.iblgf_buffer_exchange.argtypes = [vp, ci, ci]
     L.iblgf_lgf_get.argtypes = [vp, vp, sz, vp]
     L.iblgf_conv_block.argtypes = [vp, vp, vp, vp, cd]
+    L.iblgf_ns_step.argtypes = [vp, vp, ci, cd, cd, vp, ci]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -249,6 +250,14 @@ class Solver:
         out = np.zeros(c.shape[0])
         self._check(lib().iblgf_lgf_get(self.h, _p(c), c.shape[0], _p(out)))
         return out
+
+    def ns_step(self, u_fields, p_field, dt, Re, T, n_steps=1):
+        """IF-HERK steps (ifherk.hpp:1078-1200); returns the new time T."""
+        uf = np.ascontiguousarray(np.asarray(u_fields, dtype=np.int32))
+        t = ctypes.c_double(T)
+        self._check(lib().iblgf_ns_step(self.h, _p(uf), int(p_field), float(dt), float(Re), ctypes.byref(t),
+                                        int(n_steps)))
+        return t.value
 
     def conv_block(self, src_dptr, kernel_dptr, out_dptr, scale=1.0):
         self._check(lib().iblgf_conv_block(self.h, ctypes.c_void_p(src_dptr), ctypes.c_void_p(kernel_dptr),

@@ -205,3 +205,97 @@ class ImpulseFmm:
         i0 = next(int(i) for i in order if octs.leaf[i] and not octs.correction[i])
         src[i0, 1, 1, 1] = 1.0
         return src, i0, np.array(octs.bbase[i0])
+
+
+class VortexRingNS:
+    """Vortex-ring flow for the IF-HERK time step (the incompressible NS
+    setups, e.g. setups/ns_amr_lgf: one ring of radius R = 1 in the z = 0
+    plane, Gaussian core sigma = 0.2 R, Re = 1000).
+
+    The initial face velocity is the curl of the vector potential
+    A = a0 exp(-d^2 / sigma_A^2) (-y, x, 0), d = distance to the core circle,
+    evaluated at the face centres (synthetic stand-in for the reference's
+    vorticity-to-velocity initialisation; peak speed about Gamma / (2 pi sigma)
+    * 0.64 for circulation Gamma = 1). The mesh refines where the core factor
+    exp(-d^2 / sigma^2) on the block grown by 2 cells exceeds thresh[rl].
+
+    c4:    dx_base = R/8, 16^3 blocks, box +-3R, two refinement levels
+           (dx_finest = R/32), 3 mesh levels
+    small: dx_base = R/4, 6^3 blocks, box +-3R, one refinement level (parity)
+    """
+
+    def __init__(self, name="c4"):
+        self.name = name
+        self.R, self.sigma, self.Re, self.cfl = 1.0, 0.2, 1000.0, 0.35
+        if name == "c4":
+            self.block_extent, self.dx_base, self.n_levels = 16, 1.0 / 8, 2
+            self.thresh = (2e-3, 2e-2)
+        elif name == "small":
+            self.block_extent, self.dx_base, self.n_levels = 6, 1.0 / 4, 1
+            self.thresh = (1e-2,)
+        else:
+            raise ValueError(name)
+        half = int(round(3.0 * self.R / self.dx_base))
+        half = -(-half // self.block_extent) * self.block_extent
+        self.bd_base = (-2 * half,) * 3
+        self.bd_extent = (4 * half,) * 3
+        self.blocks = [((-half,) * 3, (2 * half,) * 3)]
+        self.sigma_a = 1.5 * self.sigma
+        self.a0 = 1.0
+        self.a0 = 0.5 / self._umax_probe()
+
+    def _core(self, X, Y, Z):
+        rho = np.sqrt(X * X + Y * Y)
+        return np.exp(-((rho - self.R) ** 2 + Z * Z) / self.sigma ** 2)
+
+    def _A(self, X, Y, Z):
+        rho = np.sqrt(X * X + Y * Y)
+        g = self.a0 * np.exp(-((rho - self.R) ** 2 + Z * Z) / self.sigma_a ** 2)
+        return -Y * g, X * g, np.zeros_like(g)
+
+    def velocity(self, X, Y, Z, comp, h=1e-6):
+        """Component comp of curl A by central differences of the analytic A."""
+        def d(axis, k):
+            e = [0.0, 0.0, 0.0]
+            e[axis] = h
+            p = self._A(X + e[0], Y + e[1], Z + e[2])[k]
+            m = self._A(X - e[0], Y - e[1], Z - e[2])[k]
+            return (p - m) / (2 * h)
+        if comp == 0:
+            return d(1, 2) - d(2, 1)
+        if comp == 1:
+            return d(2, 0) - d(0, 2)
+        return d(0, 1) - d(1, 0)
+
+    def _umax_probe(self):
+        x = np.linspace(-2.0, 2.0, 81)
+        X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+        return float(max(np.abs(self.velocity(X, Y, Z, k)).max() for k in range(3)))
+
+    def predicate(self, base, extent, rl, diff_level):
+        e = extent[0]
+        dxl = self.dx_base / 2 ** rl
+        i = np.arange(e + 4) - 2
+        x, y, z = ((base[a] + i + 0.5) * dxl for a in range(3))
+        g = self._core(x[:, None, None], y[None, :, None], z[None, None, :])
+        return bool(rl < len(self.thresh) and (g > self.thresh[rl]).any())
+
+    def initial_velocity(self, octs):
+        """(3, n, Nb, Nb, Nb) face velocity on every block, buffers included:
+        component d sits on the cell face normal to d at the lower side,
+        x_d = (b_d + i - 1) dx, the other coordinates at cell centres."""
+        Nb = self.block_extent + 2
+        u = np.zeros((3, octs.n, Nb, Nb, Nb))
+        i = np.arange(Nb) - 1.0
+        for o in range(octs.n):
+            rl = int(octs.levels[o]) - octs.base_level
+            dxl = self.dx_base / 2 ** rl
+            b = octs.bbase[o]
+            for comp in range(3):
+                c = [(b[a] + i + (0.0 if a == comp else 0.5)) * dxl for a in range(3)]
+                u[comp, o] = self.velocity(c[0][None, None, :], c[1][None, :, None], c[2][:, None, None], comp)
+        return u
+
+    def dt(self):
+        dx_finest = self.dx_base / 2 ** self.n_levels
+        return self.cfl * dx_finest / 0.5

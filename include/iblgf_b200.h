@@ -136,6 +136,17 @@ int iblgf_lgf_table(iblgf_ctx* ctx, double* host_out, size_t count);
 /* G(n) for n host coordinate triples (x,y,z), evaluated on the device. */
 int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out);
 
+/* ---- IF-HERK time step (Ifherk::time_step, ifherk.hpp:1078-1200, with the
+ * time_march loop's T += dt) -------------------------------------------------
+ * Advances the face velocity (three component fields u_fields[0..2], x/y/z
+ * normal components) by n_steps steps of size dt at Reynolds number Re and
+ * writes the pressure of the last step into p_field; *T is the simulation time
+ * (in/out). Scope: no immersed boundary, adaptation or body force, frame
+ * velocity 0. The velocity-refresh branch (taken once (T - 0) 3.3 / (Re
+ * dx_base^2) > 7) returns IBLGF_EINVAL. */
+int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, double Re, double* T,
+                  int n_steps);
+
 /* ---- single-block convolution (fft::Convolution, convolution.hpp:141-328)
  * out (Nb^3, device) += scale * window [Nb-1, 2Nb-2]^3 of the linear
  * convolution of src (Nb^3, device) with kernel (P^3, device, P = 2Nb-1).

@@ -226,6 +226,23 @@ int orc_buffer_exchange(void* hp, double* f, int level)
     });
 }
 
+// n_steps IF-HERK steps (ifherk.hpp:1078-1200) from time T0: u holds the
+// three face-velocity component fields back to back (in/out), p the pressure
+// (out).
+int orc_ns_step(void* hp, double dt, double Re, double T0, double* u, double* p, int n_steps)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        Ifherk ns(h->d.get(), h->s.get(), dt, Re);
+        ns.T = T0;
+        for (int k = 0; k < 3; ++k) ns.u.c[k].assign(u + k * n, u + (k + 1) * n);
+        for (int st = 0; st < n_steps; ++st) ns.time_step();
+        for (int k = 0; k < 3; ++k) std::memcpy(u + k * n, ns.u.c[k].data(), n * sizeof(double));
+        std::memcpy(p, ns.p.c[0].data(), n * sizeof(double));
+    });
+}
+
 // Single-block linear convolution with the reference's Convolution contract
 // (convolution.hpp:225-304): kernel holds P^3 values (P = 2Nb-1, x fastest),
 // out (Nb^3) += scale * window[Nb-1, 2Nb-2]^3 of (kernel (*) zero-padded src).

@@ -883,9 +883,11 @@ void Solver::fmm_apply_ge(const Field& src, Field& tgt, int level, bool nlas, do
     }
 }
 
-void Solver::coarsify_all(Field& f)
+void Solver::coarsify_all(Field& f, const int* rp)
 {
     const size_t B = (size_t)Nb * Nb * Nb;
+    static const int cell[3] = {1, 1, 1};
+    if (!rp) rp = cell;
     for (int ls = d->depth - 2; ls >= d->base_level; --ls)
         for (auto& kv : d->level_maps[ls])
         {
@@ -894,15 +896,17 @@ void Solver::coarsify_all(Field& f)
             {
                 Octant* ch = p->child[c].get();
                 if (!ch || !ch->has_data) continue;
-                tp_antrp(Nb, cc_antrp[2 + (c & 1)].data(), cc_antrp[2 + ((c >> 1) & 1)].data(),
-                         cc_antrp[2 + ((c >> 2) & 1)].data(), &f[ch->idx * B], &f[p->idx * B]);
+                tp_antrp(Nb, cc_antrp[2 * rp[0] + (c & 1)].data(), cc_antrp[2 * rp[1] + ((c >> 1) & 1)].data(),
+                         cc_antrp[2 * rp[2] + ((c >> 2) & 1)].data(), &f[ch->idx * B], &f[p->idx * B]);
             }
         }
 }
 
-void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_only)
+void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_only, const int* rp)
 {
     const size_t B = (size_t)Nb * Nb * Nb;
+    static const int cell[3] = {1, 1, 1};
+    if (!rp) rp = cell;
     for (auto& kv : d->level_maps[level])
     {
         Octant* p = kv.second;
@@ -911,26 +915,27 @@ void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_o
             Octant* ch = p->child[c].get();
             if (!ch || !ch->has_data) continue;
             if (correction_only && !ch->correction) continue;
-            tp_interp(Nb, cc_intrp[2 + (c & 1)].data(), cc_intrp[2 + ((c >> 1) & 1)].data(),
-                      cc_intrp[2 + ((c >> 2) & 1)].data(), &from[p->idx * B], &to[ch->idx * B], false);
+            tp_interp(Nb, cc_intrp[2 * rp[0] + (c & 1)].data(), cc_intrp[2 * rp[1] + ((c >> 1) & 1)].data(),
+                      cc_intrp[2 * rp[2] + ((c >> 2) & 1)].data(), &from[p->idx * B], &to[ch->idx * B], false);
         }
     }
 }
 
-// PoissonSolver::apply_if (poisson.hpp:436-494) for AMR2AMR
-void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf)
+// PoissonSolver::apply_if (poisson.hpp:436-494) for AMR2AMR; rp: relative
+// positions of the field's mesh object (cell {1,1,1} when null)
+void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf, const int* rp)
 {
     const size_t B = (size_t)Nb * Nb * Nb;
     const size_t N = d->octs.size() * B;
     Field source_tmp(N, 0.0), target_tmp(N, 0.0);
     for (Octant* o : d->octs)
         if (o->leaf) std::copy(&src[o->idx * B], &src[o->idx * B] + B, &source_tmp[o->idx * B]);
-    coarsify_all(source_tmp);
+    coarsify_all(source_tmp, rp);
     // intrp_to_correction_buffer (poisson.hpp:1015-1069)
     for (int l = d->depth - 2; l >= d->base_level; --l)
     {
         buffer_exchange(*d, source_tmp, l);
-        cc_intrp_level(source_tmp, source_tmp, l, true);
+        cc_intrp_level(source_tmp, source_tmp, l, true, rp);
     }
     for (int l = d->base_level; l < d->depth; ++l)
     {

@@ -162,9 +162,58 @@ struct Solver
     const std::vector<cplx>& lgf_ge_spectrum(double alpha, int bx, int by, int bz);
     void fmm_apply_ge(const Field& src, Field& tgt, int level, bool non_leaf_as_source,
                       double add_with_scale, double alpha);
-    void apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf);
-    void cc_intrp_level(Field& from, Field& to, int level, bool correction_only);
-    void coarsify_all(Field& f);
+    void apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf,
+                  const int* rp = nullptr);
+    // cell_center_nli transfers; rp = relative position per axis (0: node
+    // coincides with the child's, 1: half a cell off), cell {1,1,1} when null
+    void cc_intrp_level(Field& from, Field& to, int level, bool correction_only, const int* rp = nullptr);
+    void coarsify_all(Field& f, const int* rp = nullptr);
+};
+
+// ---------------------------------------------------------------- IF-HERK
+// Mesh objects of a field's components (domain::MeshObject) and their
+// relative positions for the cell-centred transfers.
+enum MeshType { MESH_CELL = 0, MESH_FACE = 1, MESH_EDGE = 2 };
+void mesh_relpos(int mesh, int comp, int rp[3]);
+
+struct VField
+{
+    int mesh = MESH_CELL;
+    std::vector<Field> c;  // 1 (cell) or 3 (face, edge) component fields
+};
+
+// Ifherk::time_step without immersed boundary (ifherk.hpp:1078-1200)
+struct Ifherk
+{
+    Domain* d;
+    Solver* s;
+    double dt, Re;
+    double T = 0.0, T_last_vel_refresh = 0.0;
+    double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
+    double c[4] = {0.0, 1.0 / 3, 1.0, 1.0};
+    double alpha[3] = {0.0, 0.0, 0.0};
+    VField u, p, q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
+
+    Ifherk(Domain* d, Solver* s, double dt, double Re);
+    double coeff_a(int i, int j) const;
+    void time_step();
+
+    void clean(VField& f, bool non_leaf_only);
+    void up(VField& f);
+    void down_to_correction(VField& f);
+    void up_and_down(VField& f);
+    void smooth2zero(VField& f, Octant* o, int ngb);
+    void clean_leaf_correction_boundary(VField& f, int l, bool leaf_only_boundary);
+    void op_level(int op, const std::vector<const Field*>& in, const std::vector<Field*>& out, int l,
+                  double scale);
+    void exchange(VField& f, int l);
+    void copy(const VField& from, VField& to, double scale);
+    void add(const VField& from, VField& to, double scale);
+    void nonlinear(VField& src, VField& tgt, double scale);
+    void divergence(VField& src, VField& tgt);
+    void gradient(VField& src, VField& tgt);
+    void apply_if(const VField& src, VField& tgt, double alpha_base);
+    void lin_sys(double alpha_k);
 };
 
 void nli_matrix(int Nb, int pts_cap, double* mat /* Nb x 2Nb, (p,c) at p*2Nb+c */);

@@ -57,6 +57,7 @@ def lib():
         L.orc_fmm_apply_ge.argtypes = [vp, vp, vp, ci, ci, cd, cd]
         L.orc_lgf_ge_get.argtypes = [vp, ci, ci, ci, cd]
         L.orc_lgf_ge_get.restype = cd
+        L.orc_ns_step.argtypes = [vp, cd, cd, cd, vp, vp, ci]
         _lib = L
     return _lib
 
@@ -186,6 +187,14 @@ class Domain:
 
     def lgf_ge_get(self, x, y, z, alpha):
         return lib().orc_lgf_ge_get(self.h, int(x), int(y), int(z), float(alpha))
+
+    def ns_step(self, u, dt, Re, T0=0.0, n_steps=1):
+        """IF-HERK steps (ifherk.hpp:1078-1200); u: (3, n, Nb, Nb, Nb) face
+        velocity. Returns (u, p) after n_steps."""
+        uu = np.ascontiguousarray(u, dtype=np.float64).copy()
+        p = self.zeros()
+        _check(lib().orc_ns_step(self.h, float(dt), float(Re), float(T0), _p(uu), _p(p), int(n_steps)))
+        return uu, p
 
     def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False, fmm_type=1):
         src = np.ascontiguousarray(src, dtype=np.float64)

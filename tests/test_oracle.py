@@ -141,3 +141,24 @@ def test_lgf_ge_matches_bessel_and_conserves_mass():
             assert abs(d.lgf_ge_get(*n, a) - ref) <= 1e-13 * ref
         r = range(-20, 21)
         assert abs(sum(d.lgf_ge_get(x, y, z, a) for x in r for y in r for z in r) - 1.0) < 1e-12
+
+
+def test_ns_step_oracle_projects_and_conserves_scale():
+    """One IF-HERK step (ifherk.hpp:1078-1200) of the vortex-ring flow: the
+    projection leaves the leaves' velocity (nearly) divergence free and the
+    step changes the velocity by O(dt)."""
+    case = S.VortexRingNS("small")
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    u0 = case.initial_velocity(d)
+    u1, p = d.ns_step(u0, case.dt(), case.Re, 0.0, 1)
+    lf = d.leaf & ~d.correction
+
+    def div_max(u):
+        div = d.op(2, [u[0], u[1], u[2]], [d.zeros()])[0]
+        return float(np.abs(div[lf][:, 2:-2, 2:-2, 2:-2]).max())
+
+    assert div_max(u1) < 0.05 * div_max(u0)
+    du = float(np.abs(u1 - u0)[:, lf].max())
+    assert 0.0 < du < 0.1 * float(np.abs(u0[:, lf]).max())
+    assert np.isfinite(p).all()
