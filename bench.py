@@ -119,6 +119,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
     ap.add_argument("--no-ns", action="store_true", help="skip the IF-HERK step measurement")
+    ap.add_argument("--ns-only", action="store_true", help="only the IF-HERK step measurement (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -156,6 +157,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
+    if args.ns_only:
+        if rank == 0:
+            print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
+        return
     prec = B.FP32 if args.precision == "fp32" else B.FP64
     g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                  n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=local,
