@@ -120,6 +120,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
     ap.add_argument("--no-ns", action="store_true", help="skip the IF-HERK step measurement")
     ap.add_argument("--ns-only", action="store_true", help="only the IF-HERK step measurement (profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
+    ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -160,6 +162,10 @@ def main():
     if args.ns_only:
         if rank == 0:
             print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
+        return
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps({"batch": batch_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
         return
     prec = B.FP32 if args.precision == "fp32" else B.FP64
     g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
@@ -279,6 +285,8 @@ def main():
         cpu = cpu_baseline(case)
     if rank == 0 and not args.no_ns:
         extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
+    if rank == 0 and not args.no_batch:
+        extra["batch"] = batch_bench(B, stream, local, args.steps, args.warmup)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -337,6 +345,64 @@ def ns_bench(B, stream, device, steps, warmup):
                 "dt": dt, "Re": case.Re, "steps": steps, "warmup": warmup,
                 "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
                 "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
+    return out
+
+
+def batch_bench(B, stream, device, steps, warmup):
+    """Batch of 256 independent Poisson problems of 1..64 blocks of 16^3
+    cells: one batched apply_lgf (every sweep stage one launch for all
+    problems) in FP32, timed with CUDA events over `steps` solves after
+    `warmup`, against the same problems solved one after another through
+    single-problem contexts on the same stream, and against the FP64 batch."""
+    import torch
+    case = S.BatchPoisson("c3")
+    out = {"workload": "256 unbounded Poisson problems, 1..64 blocks of 16^3 cells (log-uniform, seeded), dx = 1",
+           "problems": len(case.problems), "blocks": int(sum(p["n_blocks"] for p in case.problems))}
+
+    def timed(run):
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    res = {}
+    for name, prec in (("fp32", B.FP32), ("fp64", B.FP64)):
+        g = B.BatchSolver(case.block_extent, case.dx_base, case.problems, precision=prec, device=device,
+                          stream=stream.cuda_stream)
+        src = g.zeros()
+        for i in range(len(case.problems)):
+            v = g.problem(i)
+            src[v.offset:v.offset + v.n] = case.fields(v, i)
+        fs, ft = g.field(src), g.field()
+        l0 = g.launches()
+        g.apply_lgf(fs, ft)
+        g.synchronize()
+        out["launches_per_solve"] = g.launches() - l0
+        ms = timed(lambda: g.apply_lgf(fs, ft))
+        cells = int(np.count_nonzero(g.leaf)) * case.block_extent ** 3
+        out["cells_per_solve"] = cells
+        out["ms_per_solve_" + name] = ms
+        out["cells_per_s_" + name] = cells / (ms * 1e-3)
+        res[name] = g.download(ft)
+        g.close()
+    out["rel_linf_fp32_vs_fp64"] = float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())
+    # the same problems one context each, solved one after another (FP32)
+    solvers = []
+    for i, p in enumerate(case.problems):
+        s = B.Solver(p["bd_base"], p["bd_extent"], case.block_extent, case.dx_base, p["blocks"], precision=B.FP32,
+                     device=device, stream=stream.cuda_stream)
+        solvers.append((s, s.field(case.fields(s, i)), s.field()))
+    ms_seq = timed(lambda: [s.apply_lgf(a, b) for s, a, b in solvers])
+    out["ms_per_solve_sequential_fp32"] = ms_seq
+    out["speedup_batched_vs_sequential"] = ms_seq / out["ms_per_solve_fp32"]
+    for s, _, _ in solvers:
+        s.close()
     return out
 
 

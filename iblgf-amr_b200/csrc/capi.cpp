@@ -83,6 +83,7 @@ int iblgf_destroy(iblgf_ctx* x)
     cudaStreamSynchronize(x->c.stream);
     iblgf_b200::poisson_release(&x->c);
     iblgf_b200::ns_release(&x->c);
+    iblgf_b200::batch_release(&x->c);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
     return IBLGF_OK;
@@ -98,40 +99,27 @@ int iblgf_synchronize(iblgf_ctx* x)
 int iblgf_domain_add_blocks(iblgf_ctx* x, int n, const int* base, const int* extent)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
-        if (n < 0 || (n && (!base || !extent))) throw iblgf_b200::Error(IBLGF_EINVAL, "bad block arguments");
-        const int e = c.cfg.block_extent;
-        std::vector<std::array<int, 3>> nb;
-        for (int b = 0; b < n; ++b)
-        {
-            for (int d = 0; d < 3; ++d)
-            {
-                if (extent[3 * b + d] <= 0 || extent[3 * b + d] % e)
-                    throw iblgf_b200::Error(IBLGF_EINVAL, "Domain: Extent of blocks are not evenly divisible");
-                if (std::abs(base[3 * b + d]) % e)
-                    throw iblgf_b200::Error(IBLGF_EINVAL, "Domain: Base of blocks are not evenly divisible");
-            }
-            for (int k = 0; k < extent[3 * b + 2] / e; ++k)
-                for (int j = 0; j < extent[3 * b + 1] / e; ++j)
-                    for (int i = 0; i < extent[3 * b] / e; ++i)
-                        nb.push_back({base[3 * b] / e + i, base[3 * b + 1] / e + j, base[3 * b + 2] / e + k});
-        }
-        c.tree.add_base_blocks(nb);
+        iblgf_b200::add_blocks(c, n, base, extent);
     });
 }
 
 int iblgf_domain_import(iblgf_ctx* x, int n, const uint64_t* keys, const int* flags)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
         if (n <= 0 || !keys || !flags) throw iblgf_b200::Error(IBLGF_EINVAL, "bad import arguments");
         c.tree.import_octants(n, keys, flags);
+        c.has_blocks = true;
     });
 }
 
 int iblgf_domain_init_refine(iblgf_ctx* x, int n_ref, int global_refinement, iblgf_refine_fn pred, void* user)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
         if (n_ref < 0 || global_refinement < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative refinement");
         c.tree.init_refine(n_ref, global_refinement, pred, user);
@@ -141,6 +129,7 @@ int iblgf_domain_init_refine(iblgf_ctx* x, int n_ref, int global_refinement, ibl
 int iblgf_domain_finalize(iblgf_ctx* x, int subtract_non_leaf)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
         c.subtract_non_leaf = subtract_non_leaf != 0;
         iblgf_b200::domain_finalize(c);
@@ -150,6 +139,7 @@ int iblgf_domain_finalize(iblgf_ctx* x, int subtract_non_leaf)
 int iblgf_domain_info(iblgf_ctx* x, int* base_level, int* depth, int* n_octants)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
         if (base_level) *base_level = c.tree.base_level;
         if (depth) *depth = c.tree.depth;
@@ -160,6 +150,7 @@ int iblgf_domain_info(iblgf_ctx* x, int* base_level, int* depth, int* n_octants)
 int iblgf_domain_octants(iblgf_ctx* x, uint64_t* keys, int* levels, int* flags, int* bbase)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
         for (int i = 0; i < c.n_oct; ++i)
         {
@@ -175,6 +166,7 @@ int iblgf_domain_octants(iblgf_ctx* x, uint64_t* keys, int* levels, int* flags, 
 int iblgf_domain_lists(iblgf_ctx* x, int* nbr, int* infl, int* n_infl)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
         if (nbr) std::memcpy(nbr, c.nbr.data(), c.nbr.size() * sizeof(int));
         if (infl) std::memcpy(infl, c.infl.data(), c.infl.size() * sizeof(int));
@@ -185,6 +177,7 @@ int iblgf_domain_lists(iblgf_ctx* x, int* nbr, int* infl, int* n_infl)
 int iblgf_domain_masks(iblgf_ctx* x, int mask_idx, unsigned char* st)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
         if (!c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain not finalized");
         if (mask_idx < 0 || mask_idx >= (int)c.masks.size()) throw iblgf_b200::Error(IBLGF_EINVAL, "bad mask index");
         std::memcpy(st, c.masks[mask_idx].data(), c.masks[mask_idx].size());
@@ -331,6 +324,59 @@ int iblgf_ns_step(iblgf_ctx* x, const int* u_fields, int p_field, double dt, dou
         if (n_steps < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative step count");
         iblgf_b200::ns_step(c, u_fields, p_field, dt, Re, T, n_steps);
     });
+}
+
+int iblgf_batch_add_problem(iblgf_ctx* x, const int* bd_base, const int* bd_extent, int n_boxes, const int* base,
+                            const int* extent, int n_ref, iblgf_refine_fn pred, void* user, int* problem)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        const int id = iblgf_b200::batch_add_problem(c, bd_base, bd_extent, n_boxes, base, extent, n_ref, pred, user);
+        if (problem) *problem = id;
+    });
+}
+
+int iblgf_batch_finalize(iblgf_ctx* x, int subtract_non_leaf)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        c.subtract_non_leaf = subtract_non_leaf != 0;
+        iblgf_b200::batch_finalize(c);
+    });
+}
+
+int iblgf_batch_problem_info(iblgf_ctx* x, int problem, int* info)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.batch || !c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "batch not finalized");
+        if (problem < 0 || problem >= (int)c.sub.size() || !info)
+            throw iblgf_b200::Error(IBLGF_EINVAL, "bad problem index");
+        const iblgf_b200::Ctx& s = *c.sub[problem];
+        info[0] = c.sub_off[problem];
+        info[1] = s.n_oct;
+        info[2] = s.tree.base_level;
+        info[3] = s.tree.depth;
+    });
+}
+
+int iblgf_batch_problem_octants(iblgf_ctx* x, int problem, uint64_t* keys, int* levels, int* flags, int* bbase)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!c.batch || !c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "batch not finalized");
+        if (problem < 0 || problem >= (int)c.sub.size()) throw iblgf_b200::Error(IBLGF_EINVAL, "bad problem index");
+        const iblgf_b200::Ctx& s = *c.sub[problem];
+        for (int i = 0; i < s.n_oct; ++i)
+        {
+            if (keys) keys[i] = s.keys[i];
+            if (levels) levels[i] = s.levels[i];
+            if (flags) flags[i] = s.flags[i];
+            if (bbase)
+                for (int d = 0; d < 3; ++d) bbase[3 * i + d] = s.bbase[3 * i + d];
+        }
+    });
+}
+
+int iblgf_batch_apply_lgf(iblgf_ctx* x, int src, int tgt)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::batch_apply_lgf(c, src, tgt); });
 }
 
 int iblgf_conv_block_noalloc(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)

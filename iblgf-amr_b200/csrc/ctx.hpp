@@ -150,6 +150,31 @@ struct FmmPlan
     bool empty() const { return n_tgt == 0; }
 };
 
+// Host side of a sweep plan: octant indices, source / target slots and LGF
+// spectrum keys (level_diff or -1-ge, block offset). upload_plan() maps the
+// keys to slots of a context's spectra cache and moves the lists to the
+// device; merge_plans() concatenates the plans of independent octrees.
+struct HostTasks
+{
+    std::vector<int> ptr{0}, src, cid, dst;  // receiving blocks with at least one task
+};
+struct HostPlan
+{
+    int level = 0, mask_idx = 0, ge = -1;
+    std::vector<int> zs, zt, cs, at, srcs;
+    std::vector<HostTasks> antrp, intrp;
+    std::vector<int> tgt_list;  // pair-list targets first, then group targets
+    int n_csr_tgt = 0;
+    std::vector<int> ptr{0}, psrc;
+    std::vector<std::array<int, 4>> pkey;      // keys of the pair-list (CSR) targets' pairs
+    std::vector<std::array<int, 4>> all_keys;  // keys of every target's pairs: spectra to compute
+    std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
+    std::vector<unsigned short> gsrc;
+    std::vector<std::array<int, 4>> tab_keys;  // 343 per table
+    int n_groups = 0, max_tile_src = 0, n_spec_unique = 0;
+    long long n_pairs = 0;
+};
+
 struct Field
 {
     DevBuf<double> d;
@@ -218,6 +243,13 @@ struct Ctx
     // unique spectra per sweep, anterpolation tasks, interpolation tasks
     long long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
+    // batch of independent problems (iblgf_batch_*): each problem's octree,
+    // lists and masks live in a topology-only sub-context; fields, spectra and
+    // work buffers live here, the problems' octants back to back
+    bool batch = false, topology_only = false, has_blocks = false;
+    std::vector<std::unique_ptr<Ctx>> sub;
+    std::vector<int> sub_off;
+
     size_t block_elems() const { return (size_t)Nb * Nb * Nb; }
     size_t field_elems() const { return (size_t)n_oct * block_elems(); }
     size_t cplx_bytes() const { return cfg.precision == IBLGF_FP32 ? 8 : 16; }
@@ -229,6 +261,21 @@ void ctx_init(Ctx& c);
 void domain_finalize(Ctx& c);
 int field_create(Ctx& c);
 void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int fmm_type, int ge = -1);
+// one FMM sweep of a ready plan: zero / copy / anterpolate, forward transforms,
+// MAC, inverse transforms + add, interpolate, add into tgt (fmm.hpp:729-870)
+void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add_with_scale, int ge);
+HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge);
+std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h);
+void host_tasks(HostTasks& ht, const std::vector<int>& dst, const std::vector<std::vector<std::pair<int, int>>>& tasks);
+void upload_host_tasks(Ctx& c, TpTasks& tt, const HostTasks& ht);
+void add_blocks(Ctx& c, int n, const int* base, const int* extent);
+void need_single(const Ctx& c);
+// batches of independent problems (batch.cpp)
+int batch_add_problem(Ctx& c, const int* bd_base, const int* bd_extent, int n, const int* base, const int* extent,
+                      int n_ref, iblgf_refine_fn pred, void* user);
+void batch_finalize(Ctx& c);
+void batch_apply_lgf(Ctx& c, int src, int tgt);
+void batch_release(const Ctx* c);
 int ge_table(Ctx& c, double alpha);
 // rp: relative position per axis of the field's mesh object (cell {1,1,1} when null)
 void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp = nullptr);

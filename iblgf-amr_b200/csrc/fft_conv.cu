@@ -208,6 +208,48 @@ __global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, c
 // One CTA = (tile of up to 32 sibling groups, chunk of F frequencies); the
 // tile's spectra (64-byte rows) and the groups' candidate rows live in shared
 // memory (~50 KB, four CTAs per SM); source spectra are read through L1/L2.
+// The 64 (c, c') sibling pairs of one neighbour parent n, z-slab by z-slab:
+// the 9 spectra of a slab stay in registers for 16 x M complex MACs. MASKED
+// skips the pairs a tile excludes (mode 1: adjacent ones, mode 2: all but the
+// adjacent ones); the conditions are uniform across the CTA.
+template<class R, int F, int M, bool MASKED>
+__device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&sv)[M][8], cx<R> (&acc)[M][8],
+                                                 int mode, int nx, int ny, int nz)
+{
+#pragma unroll
+    for (int cpz = 0; cpz < 2; ++cpz)
+    {
+#pragma unroll
+        for (int cz = 0; cz < 2; ++cz)
+        {
+            const int dz = cz - cpz;
+            const bool adj_z = abs(dz - 2 * nz) <= 1;
+            if (MASKED && mode == 2 && !adj_z) continue;
+            cx<R> gv[9];
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx)
+                    gv[(dy + 1) * 3 + dx + 1] = gn[(dx + 7 * dy + 49 * dz) * F];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)  // c' = 4 cpz + q
+#pragma unroll
+                for (int r = 0; r < 4; ++r)  // c = 4 cz + r
+                {
+                    const int dx = (r & 1) - (q & 1), dy = (r >> 1) - (q >> 1);
+                    if (MASKED)
+                    {
+                        const bool adj = adj_z && abs(dx - 2 * nx) <= 1 && abs(dy - 2 * ny) <= 1;
+                        if (adj == (mode == 1)) continue;
+                    }
+                    const cx<R> g = gv[(dy + 1) * 3 + dx + 1];
+#pragma unroll
+                    for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][4 * cpz + q]);
+                }
+        }
+    }
+}
+
 template<class R, int F, int M>
 __global__ void __launch_bounds__(128, 4) group_mac_kernel(
     const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, const int* __restrict__ tile_gptr,
@@ -289,31 +331,8 @@ __global__ void __launch_bounds__(128, 4) group_mac_kernel(
                     const int j = jj[m][q];
                     sv[m][q] = j >= 0 ? __ldg(Sf + (size_t)j * NC) : zero;
                 }
-#pragma unroll
-            for (int cpz = 0; cpz < 2; ++cpz)
-            {
-#pragma unroll
-                for (int cz = 0; cz < 2; ++cz)
-                {
-                    const int dz = cz - cpz;
-                    cx<R> gv[9];
-#pragma unroll
-                    for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-                        for (int dx = -1; dx <= 1; ++dx)
-                            gv[(dy + 1) * 3 + dx + 1] = gn[(dx + 7 * dy + 49 * dz) * F];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)  // c' = 4 cpz + q
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)  // c = 4 cz + r
-                        {
-                            const int dx = (r & 1) - (q & 1), dy = (r >> 1) - (q >> 1);
-                            const cx<R> g = gv[(dy + 1) * 3 + dx + 1];
-#pragma unroll
-                            for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][4 * cpz + q]);
-                        }
-                }
-            }
+            if (mode == 0) group_mac_parent<R, F, M, false>(gn, sv, acc, 0, nx, ny, nz);
+            else group_mac_parent<R, F, M, true>(gn, sv, acc, mode, nx, ny, nz);
         }
         if (f < NC)
         {

@@ -329,6 +329,7 @@ class Step
 
 void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n_steps)
 {
+    need_single(c);
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (!(dt > 0.0) || !(Re > 0.0)) throw Error(IBLGF_EINVAL, "dt and Re must be positive");
     const int nf = (int)c.fields.size();

@@ -100,6 +100,11 @@ void ctx_init(Ctx& c)
         IBLGF_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
     }
+    if (c.topology_only)
+    {
+        c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
+        return;
+    }
     // twiddles e^{-2 pi i j / P}
     std::vector<double> tw(2 * c.P);
     std::vector<float> tw32(2 * c.P);
@@ -309,6 +314,8 @@ void domain_finalize(Ctx& c)
     c.d_bbase.upload(c.bbase, c.stream);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     build_masks(c);
+    c.finalized = true;
+    if (c.topology_only) return;
     c.f_source_tmp = field_create(c);
     c.f_target_tmp = field_create(c);
     c.f_correction_tmp = field_create(c);
@@ -344,38 +351,58 @@ void upload_tasks(Ctx& c, TpTasks& tt, const std::vector<int>& dst, const std::v
 
 // ge < 0: LGF_GL sweep (Fmm::apply full branch); ge >= 0: LGF_GE sweep with
 // the integrating-factor table `ge` (neighbour-only branch, fmm.hpp:754-770)
-FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
+}  // namespace
+
+void host_tasks(HostTasks& ht, const std::vector<int>& dst, const std::vector<std::vector<std::pair<int, int>>>& tasks)
 {
-    auto key = std::make_tuple(idx, level, ge);
-    auto it = c.plans.find(key);
-    if (it != c.plans.end()) return *it->second;
-    auto plan = std::make_unique<FmmPlan>();
-    FmmPlan& p = *plan;
+    for (size_t g = 0; g < dst.size(); ++g)
+    {
+        if (tasks[g].empty()) continue;
+        ht.dst.push_back(dst[g]);
+        for (auto& t : tasks[g])
+        {
+            ht.src.push_back(t.first);
+            ht.cid.push_back(t.second);
+        }
+        ht.ptr.push_back((int)ht.src.size());
+    }
+}
+
+void upload_host_tasks(Ctx& c, TpTasks& tt, const HostTasks& ht)
+{
+    tt.n_groups = (int)ht.dst.size();
+    tt.n_tasks = (int)ht.src.size();
+    tt.group_ptr.upload(ht.ptr, c.stream);
+    tt.group_dst.upload(ht.dst, c.stream);
+    tt.task_src.upload(ht.src, c.stream);
+    tt.task_cid.upload(ht.cid, c.stream);
+}
+
+HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
+{
+    HostPlan p;
     p.level = level;
     p.mask_idx = idx;
+    p.ge = ge;
     const auto& m = c.masks[idx];
     auto S = [&](int o) { return m[2 * o] != 0; };
     auto T = [&](int o) { return m[2 * o + 1] != 0; };
     const bool neighbor_only = ge >= 0;
-    std::vector<int> zs, zt, cs, at, srcs, tgts;
+    std::vector<int> tgts;
     for (int lv = level; lv >= 0; --lv)
         for (int o : c.level_octs[lv])
         {
-            if (S(o)) zs.push_back(o);
-            if (T(o)) zt.push_back(o);
+            if (S(o)) p.zs.push_back(o);
+            if (T(o)) p.zt.push_back(o);
             if (neighbor_only && lv != level) continue;
-            if (S(o)) srcs.push_back(o);
+            if (S(o)) p.srcs.push_back(o);
             if (T(o)) tgts.push_back(o);
         }
     for (int o : c.level_octs[level])
     {
-        if (S(o)) cs.push_back(o);
-        if (T(o)) at.push_back(o);
+        if (S(o)) p.cs.push_back(o);
+        if (T(o)) p.at.push_back(o);
     }
-    p.zero_s.upload(zs, c.stream);
-    p.zero_t.upload(zt, c.stream);
-    p.copy_s.upload(cs, c.stream);
-    p.add_t.upload(at, c.stream);
     // anterpolation, levels level-1 .. 0
     for (int lv = level - 1; lv >= 0 && !neighbor_only; --lv)
     {
@@ -393,7 +420,7 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
             }
         }
         p.antrp.emplace_back();
-        upload_tasks(c, p.antrp.back(), dst, tasks);
+        host_tasks(p.antrp.back(), dst, tasks);
     }
     // interpolation, levels 1 .. level-1 (parent level)
     for (int lv = 1; lv < level && !neighbor_only; ++lv)
@@ -414,28 +441,18 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
             }
         }
         p.intrp.emplace_back();
-        upload_tasks(c, p.intrp.back(), dst, tasks);
+        host_tasks(p.intrp.back(), dst, tasks);
     }
     // sources and pair list
     std::vector<int> src_slot(c.n_oct, -1);
-    for (size_t i = 0; i < srcs.size(); ++i) src_slot[srcs[i]] = (int)i;
-    p.n_src = (int)srcs.size();
-    p.src_oct.upload(srcs, c.stream);
-    std::vector<std::array<int, 5>> new_slots;
+    for (size_t i = 0; i < p.srcs.size(); ++i) src_slot[p.srcs[i]] = (int)i;
     const int Nb = c.Nb, e = c.cfg.block_extent;
-    auto slot_of = [&](const std::array<int, 4>& k) {
-        auto it = c.spec_slot.find(k);
-        if (it != c.spec_slot.end()) return it->second;
-        const int slot = (int)c.spec_slot.size();
-        c.spec_slot.emplace(k, slot);
-        new_slots.push_back({slot, k[0], k[1], k[2], k[3]});
-        return slot;
-    };
     // reference pair list of every target (fmm.hpp:988-1027, fmm_tt :1167-1195)
     struct TP
     {
         int t;
-        std::vector<int> src, spec;
+        std::vector<int> src;
+        std::vector<std::array<int, 4>> key;
     };
     std::vector<TP> tp;
     for (int t : tgts)
@@ -444,9 +461,9 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
         TP x{t, {}, {}};
         auto add_pair = [&](int s, int lvd) {
             x.src.push_back(src_slot[s]);
-            x.spec.push_back(slot_of({neighbor_only ? -1 - ge : lvd, c.bbase[3 * t] - c.bbase[3 * s] - (Nb - 1),
-                                      c.bbase[3 * t + 1] - c.bbase[3 * s + 1] - (Nb - 1),
-                                      c.bbase[3 * t + 2] - c.bbase[3 * s + 2] - (Nb - 1)}));
+            x.key.push_back({neighbor_only ? -1 - ge : lvd, c.bbase[3 * t] - c.bbase[3 * s] - (Nb - 1),
+                             c.bbase[3 * t + 1] - c.bbase[3 * s + 1] - (Nb - 1),
+                             c.bbase[3 * t + 2] - c.bbase[3 * s + 2] - (Nb - 1)});
         };
         if (c.levels[t] == level)
             for (int i = 0; i < 27; ++i)
@@ -537,18 +554,17 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
         in_group[i] = 1;
     }
     // target slots: pair-list targets first, then group targets in group order
-    std::vector<int> tgt_list, ptr{0}, psrc, pspec;
     std::vector<int> slot_of_tp(tp.size(), -1);
     for (size_t i = 0; i < tp.size(); ++i)
     {
         if (in_group[i]) continue;
-        slot_of_tp[i] = (int)tgt_list.size();
-        tgt_list.push_back(tp[i].t);
-        psrc.insert(psrc.end(), tp[i].src.begin(), tp[i].src.end());
-        pspec.insert(pspec.end(), tp[i].spec.begin(), tp[i].spec.end());
-        ptr.push_back((int)psrc.size());
+        slot_of_tp[i] = (int)p.tgt_list.size();
+        p.tgt_list.push_back(tp[i].t);
+        p.psrc.insert(p.psrc.end(), tp[i].src.begin(), tp[i].src.end());
+        p.pkey.insert(p.pkey.end(), tp[i].key.begin(), tp[i].key.end());
+        p.ptr.push_back((int)p.psrc.size());
     }
-    p.n_csr_tgt = (int)tgt_list.size();
+    p.n_csr_tgt = (int)p.tgt_list.size();
     // groups ordered by (sweep level distance, parent key): spatially coherent tiles
     std::vector<int> gorder(groups.size());
     for (size_t g = 0; g < groups.size(); ++g) gorder[g] = (int)g;
@@ -560,12 +576,11 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
         {
             const int i = groups[g].tgt[cc];
             if (i < 0) continue;
-            slot_of_tp[i] = (int)tgt_list.size();
-            tgt_list.push_back(tp[i].t);
+            slot_of_tp[i] = (int)p.tgt_list.size();
+            p.tgt_list.push_back(tp[i].t);
         }
     // per-ld spectrum slot tables over the 343 offsets
     std::map<int, int> tab_of_ld;
-    std::vector<int> spec_u;
     for (auto& gr : groups)
     {
         if (tab_of_ld.count(gr.ld)) continue;
@@ -573,10 +588,8 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
         for (int u = 0; u < 343; ++u)
         {
             const int ux = u % 7 - 3, uy = (u / 7) % 7 - 3, uz = u / 49 - 3;
-            const std::array<int, 4> k{neighbor_only ? -1 - ge : gr.ld, ux * e - (Nb - 1), uy * e - (Nb - 1),
-                                       uz * e - (Nb - 1)};
-            auto it = c.spec_slot.find(k);
-            spec_u.push_back(it == c.spec_slot.end() ? -1 : it->second);
+            p.tab_keys.push_back({neighbor_only ? -1 - ge : gr.ld, ux * e - (Nb - 1), uy * e - (Nb - 1),
+                                  uz * e - (Nb - 1)});
         }
     }
     // tiles: consecutive groups of one level distance while the union of their
@@ -584,8 +597,13 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
     // a tile: up to 32 sibling groups (16 rows x 2 per row of the MAC CTA) whose
     // union of candidate sources fits the 64-byte-row staging budget
     const int kScap = 1024, kGcap = kGroupTileCap;
-    std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
-    std::vector<unsigned short> gsrc;
+    std::vector<int>& tgptr = p.tgptr;
+    std::vector<int>& tsptr = p.tsptr;
+    std::vector<int>& tsrc = p.tsrc;
+    std::vector<int>& ttab = p.ttab;
+    std::vector<int>& tcoarse = p.tcoarse;
+    std::vector<int>& gtgt = p.gtgt;
+    std::vector<unsigned short>& gsrc = p.gsrc;
     std::map<int, int> local;
     int cur_ld = -1, ngrp = 0, max_src = 0;
     auto close_tile = [&]() {
@@ -630,28 +648,78 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
     }
     close_tile();
     p.n_groups = (int)groups.size();
-    p.n_tiles = (int)ttab.size();
     p.max_tile_src = max_src;
-    p.tile_gptr.upload(tgptr, c.stream);
-    p.tile_sptr.upload(tsptr, c.stream);
-    p.tile_src.upload(tsrc, c.stream);
-    p.tile_tab.upload(ttab, c.stream);
-    p.tile_coarse.upload(tcoarse, c.stream);
-    p.spec_u.upload(spec_u, c.stream);
-    p.grp_src.upload(gsrc, c.stream);
-    p.grp_tgt.upload(gtgt, c.stream);
-    p.n_tgt = (int)tgt_list.size();
-    p.n_pairs = 0;
+    for (auto& x : tp) p.all_keys.insert(p.all_keys.end(), x.key.begin(), x.key.end());
     for (auto& x : tp) p.n_pairs += (long long)x.src.size();
     {
-        std::vector<int> u;
-        for (auto& x : tp) u.insert(u.end(), x.spec.begin(), x.spec.end());
+        std::vector<std::array<int, 4>> u;
+        for (auto& x : tp) u.insert(u.end(), x.key.begin(), x.key.end());
         std::sort(u.begin(), u.end());
         p.n_spec_unique = (int)(std::unique(u.begin(), u.end()) - u.begin());
     }
-    p.tgt_oct.upload(tgt_list, c.stream);
-    p.pair_ptr.upload(ptr, c.stream);
-    p.pair_src.upload(psrc, c.stream);
+    return p;
+}
+
+std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
+{
+    auto plan = std::make_unique<FmmPlan>();
+    FmmPlan& p = *plan;
+    p.level = h.level;
+    p.mask_idx = h.mask_idx;
+    p.zero_s.upload(h.zs, c.stream);
+    p.zero_t.upload(h.zt, c.stream);
+    p.copy_s.upload(h.cs, c.stream);
+    p.add_t.upload(h.at, c.stream);
+    for (auto& t : h.antrp)
+    {
+        p.antrp.emplace_back();
+        upload_host_tasks(c, p.antrp.back(), t);
+    }
+    for (auto& t : h.intrp)
+    {
+        p.intrp.emplace_back();
+        upload_host_tasks(c, p.intrp.back(), t);
+    }
+    p.n_src = (int)h.srcs.size();
+    p.src_oct.upload(h.srcs, c.stream);
+    // LGF spectrum slots: every pair's key gets a slot (new ones are computed
+    // below); the group tables reference registered keys only (-1: zero row)
+    std::vector<std::array<int, 5>> new_slots;
+    auto slot_of = [&](const std::array<int, 4>& k) {
+        auto it = c.spec_slot.find(k);
+        if (it != c.spec_slot.end()) return it->second;
+        const int slot = (int)c.spec_slot.size();
+        c.spec_slot.emplace(k, slot);
+        new_slots.push_back({slot, k[0], k[1], k[2], k[3]});
+        return slot;
+    };
+    for (auto& k : h.all_keys) slot_of(k);
+    std::vector<int> pspec(h.pkey.size());
+    for (size_t i = 0; i < h.pkey.size(); ++i) pspec[i] = slot_of(h.pkey[i]);
+    std::vector<int> spec_u(h.tab_keys.size());
+    for (size_t i = 0; i < h.tab_keys.size(); ++i)
+    {
+        auto it = c.spec_slot.find(h.tab_keys[i]);
+        spec_u[i] = it == c.spec_slot.end() ? -1 : it->second;
+    }
+    p.n_csr_tgt = h.n_csr_tgt;
+    p.n_groups = h.n_groups;
+    p.n_tiles = (int)h.ttab.size();
+    p.max_tile_src = h.max_tile_src;
+    p.tile_gptr.upload(h.tgptr, c.stream);
+    p.tile_sptr.upload(h.tsptr, c.stream);
+    p.tile_src.upload(h.tsrc, c.stream);
+    p.tile_tab.upload(h.ttab, c.stream);
+    p.tile_coarse.upload(h.tcoarse, c.stream);
+    p.spec_u.upload(spec_u, c.stream);
+    p.grp_src.upload(h.gsrc, c.stream);
+    p.grp_tgt.upload(h.gtgt, c.stream);
+    p.n_tgt = (int)h.tgt_list.size();
+    p.n_pairs = h.n_pairs;
+    p.n_spec_unique = h.n_spec_unique;
+    p.tgt_oct.upload(h.tgt_list, c.stream);
+    p.pair_ptr.upload(h.ptr, c.stream);
+    p.pair_src.upload(h.psrc, c.stream);
     p.pair_spec.upload(pspec, c.stream);
     // grow the spectra cache and fill the new slots
     if (!new_slots.empty())
@@ -673,6 +741,17 @@ FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
         c.spec_used = need;
     }
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    return plan;
+}
+
+namespace
+{
+FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
+{
+    auto key = std::make_tuple(idx, level, ge);
+    auto it = c.plans.find(key);
+    if (it != c.plans.end()) return *it->second;
+    auto plan = upload_plan(c, build_host_plan(c, level, idx, ge));
     auto& ref = *plan;
     c.plans.emplace(key, std::move(plan));
     return ref;
@@ -708,14 +787,50 @@ struct Timer
 };
 }  // namespace
 
+// Domain::construct_basemesh_blocks (domain.hpp:405-488): blocks given as
+// boxes of base cells, each split into block_extent^3 base blocks
+void add_blocks(Ctx& c, int n, const int* base, const int* extent)
+{
+    if (n < 0 || (n && (!base || !extent))) throw Error(IBLGF_EINVAL, "bad block arguments");
+    const int e = c.cfg.block_extent;
+    std::vector<std::array<int, 3>> nb;
+    for (int b = 0; b < n; ++b)
+    {
+        for (int d = 0; d < 3; ++d)
+        {
+            if (extent[3 * b + d] <= 0 || extent[3 * b + d] % e)
+                throw Error(IBLGF_EINVAL, "Domain: Extent of blocks are not evenly divisible");
+            if (std::abs(base[3 * b + d]) % e)
+                throw Error(IBLGF_EINVAL, "Domain: Base of blocks are not evenly divisible");
+        }
+        for (int k = 0; k < extent[3 * b + 2] / e; ++k)
+            for (int j = 0; j < extent[3 * b + 1] / e; ++j)
+                for (int i = 0; i < extent[3 * b] / e; ++i)
+                    nb.push_back({base[3 * b] / e + i, base[3 * b + 1] / e + j, base[3 * b + 2] / e + k});
+    }
+    c.tree.add_base_blocks(nb);
+    c.has_blocks = true;
+}
+
+void need_single(const Ctx& c)
+{
+    if (c.batch) throw Error(IBLGF_EINVAL, "the context holds a batch of problems (use the iblgf_batch_* calls)");
+}
+
 void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_scale, int fmm_type, int ge)
 {
+    need_single(c);
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (level < c.tree.base_level || level >= c.tree.depth) throw Error(IBLGF_EINVAL, "level out of range");
     const int rl = level - c.tree.base_level;
     const int idx = fmm_type == IBLGF_STREAM ? mask_idx_gen(IBLGF_STREAM, 0, 0)
                                               : mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0);
     FmmPlan& p = get_plan(c, level, idx, ge);
+    run_sweep(c, p, src, tgt, c.cfg.dx_base / std::pow(2.0, rl), add_with_scale, ge);
+}
+
+void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add_with_scale, int ge)
+{
     c.stats[0] += 1;
     c.stats[1] += p.n_src;
     c.stats[2] += p.n_tgt;
@@ -724,7 +839,6 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     for (auto& t : p.antrp) c.stats[5] += t.n_tasks;
     for (auto& t : p.intrp) c.stats[6] += t.n_tasks;
     c.stats[7] += p.n_tgt - p.n_csr_tgt;
-    const double dx_level = c.cfg.dx_base / std::pow(2.0, rl);
     double* fs = c.field(c.f_fmm_s);
     double* ft = c.field(c.f_fmm_t);
     Timer tm(c);
@@ -859,6 +973,7 @@ OpLists& op_lists(Ctx& c)
 
 void buffer_exchange(Ctx& c, int field, int level)
 {
+    need_single(c);
     if (level < 0 || level > kMaxLevel) throw Error(IBLGF_EINVAL, "level out of range");
     OpLists& ol = op_lists(c);
     launch_halo(c, c.field(field), ol.list[level].p, (int)ol.list[level].n);
@@ -866,6 +981,7 @@ void buffer_exchange(Ctx& c, int field, int level)
 
 void apply_op(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, int level, double scale)
 {
+    need_single(c);
     static const int need_in[6] = {1, 1, 3, 3, 3, 6}, need_out[6] = {1, 3, 1, 3, 3, 3};
     if (op < 0 || op > 5) throw Error(IBLGF_EINVAL, "unknown operator");
     if (n_in != need_in[op] || n_out != need_out[op]) throw Error(IBLGF_EINVAL, "wrong number of component fields");
@@ -926,6 +1042,7 @@ int ge_table(Ctx& c, double alpha)
 // PoissonSolver::apply_lgf_IF / apply_if (poisson.hpp:428-494), AMR2AMR
 void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp)
 {
+    need_single(c);
     static const int cell[3] = {1, 1, 1};
     if (!rp) rp = cell;
     // cell-centred transfer matrices per axis: relative position 1 -> [4,5]
@@ -968,6 +1085,7 @@ void poisson_release(const Ctx* c)
 
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
 {
+    need_single(c);
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_STREAM)
         throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR and STREAM");

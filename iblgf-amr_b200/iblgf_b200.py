@@ -34,7 +34,9 @@ EXPORTS = [
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
-    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get", "iblgf_ns_step", "iblgf_conv_block", "iblgf_conv_block_noalloc",
+    "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
+    "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
+    "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -79,6 +81,11 @@ def lib():
     L.iblgf_lgf_get.argtypes = [vp, vp, sz, vp]
     L.iblgf_conv_block.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_ns_step.argtypes = [vp, vp, ci, cd, cd, vp, ci]
+    L.iblgf_batch_add_problem.argtypes = [vp, vp, vp, ci, vp, vp, ci, REFINE_FN, vp, vp]
+    L.iblgf_batch_finalize.argtypes = [vp, ci]
+    L.iblgf_batch_problem_info.argtypes = [vp, ci, vp]
+    L.iblgf_batch_problem_octants.argtypes = [vp, ci, vp, vp, vp, vp]
+    L.iblgf_batch_apply_lgf.argtypes = [vp, ci, ci]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -291,3 +298,87 @@ def from_case(case, **kw):
     """Build a Solver for an iblgf_setups case object."""
     return Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                   n_levels=getattr(case, "n_levels", 0), predicate=getattr(case, "predicate", None), **kw)
+
+
+class ProblemView:
+    """Octants of one problem of a batch (the attributes an iblgf_setups case
+    reads when it builds fields): n, levels, flags, bbase, base_level, leaf."""
+
+    def __init__(self, offset, n, base_level, depth, keys, levels, flags, bbase):
+        self.offset, self.n, self.base_level, self.depth = offset, n, base_level, depth
+        self.keys, self.levels, self.flags, self.bbase = keys, levels, flags, bbase
+
+    @property
+    def leaf(self):
+        return (self.flags & 1) != 0
+
+    @property
+    def correction(self):
+        return (self.flags & 2) != 0
+
+
+class BatchSolver(Solver):
+    """Many independent unbounded Poisson problems in one context
+    (iblgf_batch_*): problems = list of dicts with bd_base, bd_extent, blocks
+    and optionally n_levels / predicate. Fields hold the problems' octants back
+    to back; problem(i) gives the octant range and arrays of problem i."""
+
+    def __init__(self, block_extent, dx_base, problems, precision=FP64, device=0, stream=None,
+                 subtract_non_leaf=False, use_correction=True, intrp_order=5):
+        L = lib()
+        cfg = Config(block_extent, (ctypes.c_int * 3)(0, 0, 0), (ctypes.c_int * 3)(0, 0, 0),
+                     float(dx_base), int(precision), int(device), int(intrp_order),
+                     ctypes.c_void_p(stream) if stream else None)
+        h = ctypes.c_void_p()
+        rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+        self.h = h
+        self.Nb = block_extent + 2
+        self.block_extent = block_extent
+        self.precision = precision
+        self._cbs = []
+        for pr in problems:
+            bb = np.array([b[0] for b in pr["blocks"]], np.int32).ravel()
+            be = np.array([b[1] for b in pr["blocks"]], np.int32).ravel()
+            pred = pr.get("predicate")
+            if pred is not None:
+                def cb(user, base, ext, rl, diff, pred=pred):
+                    return 1 if pred((base[0], base[1], base[2]), (ext[0], ext[1], ext[2]), rl, diff) else 0
+                fn = REFINE_FN(cb)
+            else:
+                fn = REFINE_FN(lambda *a: 0)
+            self._cbs.append(fn)
+            pid = ctypes.c_int()
+            self._check(L.iblgf_batch_add_problem(self.h, _p(np.array(pr["bd_base"], np.int32)),
+                                                  _p(np.array(pr["bd_extent"], np.int32)), len(pr["blocks"]),
+                                                  _p(bb), _p(be), int(pr.get("n_levels", 0)), fn, None,
+                                                  ctypes.byref(pid)))
+        self._check(L.iblgf_batch_finalize(self.h, 1 if subtract_non_leaf else 0))
+        self._check(L.iblgf_poisson_options(self.h, 1 if use_correction else 0, 1 if subtract_non_leaf else 0))
+        self.views = []
+        for i in range(len(problems)):
+            info = np.zeros(4, np.int32)
+            self._check(L.iblgf_batch_problem_info(self.h, i, _p(info)))
+            n = int(info[1])
+            keys, levels = np.zeros(n, np.uint64), np.zeros(n, np.int32)
+            flags, bbase = np.zeros(n, np.int32), np.zeros((n, 3), np.int32)
+            self._check(L.iblgf_batch_problem_octants(self.h, i, _p(keys), _p(levels), _p(flags), _p(bbase)))
+            self.views.append(ProblemView(int(info[0]), n, int(info[2]), int(info[3]), keys, levels, flags, bbase))
+        self.n = sum(v.n for v in self.views)
+        self.flags = np.concatenate([v.flags for v in self.views])
+        self.levels = np.concatenate([v.levels for v in self.views])
+        self.bbase = np.concatenate([v.bbase for v in self.views])
+
+    def problem(self, i):
+        return self.views[i]
+
+    def split(self, arr):
+        """Per-problem slices of a batch field array."""
+        return [arr[v.offset:v.offset + v.n] for v in self.views]
+
+    def apply_lgf(self, src, tgt, fmm_type=AMR2AMR):
+        if fmm_type != AMR2AMR:
+            raise IblgfError("batches support the AMR2AMR mask")
+        self._check(lib().iblgf_batch_apply_lgf(self.h, src, tgt))
+

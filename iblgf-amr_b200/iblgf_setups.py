@@ -299,3 +299,82 @@ class VortexRingNS:
     def dt(self):
         dx_finest = self.dx_base / 2 ** self.n_levels
         return self.cfl * dx_finest / 0.5
+
+
+class BatchPoisson:
+    """Batch of independent unbounded Poisson problems of uneven size.
+
+    c3:    256 problems, 16^3-cell blocks, dx = 1; block count per problem
+           n = floor(exp(U[0, ln 64])) clipped to [1, 64] (log-uniform); the
+           n blocks fill the most compact near-cube box a x b x c (x fastest),
+           a = ceil(n^(1/3)), b = ceil(sqrt(n / a)), c = ceil(n / (a b));
+           source = 4 Gaussians per problem, sigma ~ U[2, 6] cells, amplitude
+           ~ U[-1, 1], centres uniform in the problem's block box
+           (numpy PCG64, seed 20261203); one mesh level.
+    small: 6 problems of 1..27 blocks of 6^3 cells (parity case).
+    """
+
+    def __init__(self, name="c3", seed=20261203):
+        self.name = name
+        rng = np.random.Generator(np.random.PCG64(seed))
+        if name == "c3":
+            self.block_extent, n_prob, nmax, sig = 16, 256, 64, (2.0, 6.0)
+            counts = [int(min(max(np.floor(np.exp(rng.uniform(0.0, np.log(nmax)))), 1), nmax))
+                      for _ in range(n_prob)]
+        elif name == "small":
+            self.block_extent, sig = 6, (0.8, 2.0)
+            counts = [1, 27, 5, 12, 2, 8]
+        else:
+            raise ValueError(name)
+        self.dx_base = 1.0
+        e = self.block_extent
+        self.problems = []
+        for n in counts:
+            a = int(np.ceil(round(n ** (1.0 / 3.0), 9)))
+            b = int(np.ceil(np.sqrt(n / a)))
+            c = int(np.ceil(n / (a * b)))
+            dims = (a, b, c)
+            start = [-((d + 1) // 2) * e for d in dims]
+            blocks = []
+            for i in range(n):
+                pos = (i % a, (i // a) % b, i // (a * b))
+                blocks.append((tuple(start[k] + pos[k] * e for k in range(3)), (e, e, e)))
+            m = 1
+            while m < max(dims):
+                m *= 2
+            half = max(m * e // 2, e)
+            lo = np.array(start, float)
+            hi = lo + np.array(dims, float) * e
+            g = []
+            for _ in range(4):
+                s = rng.uniform(*sig)
+                amp = rng.uniform(-1.0, 1.0)
+                ctr = tuple(rng.uniform(lo[k], hi[k]) for k in range(3))
+                g.append((amp, s, ctr))
+            self.problems.append({"bd_base": (-2 * half,) * 3, "bd_extent": (4 * half,) * 3, "blocks": blocks,
+                                  "gaussians": g, "n_blocks": n})
+
+    @staticmethod
+    def _f(gauss, X, Y, Z):
+        out = np.zeros(np.broadcast(X, Y, Z).shape)
+        for a, s, c in gauss:
+            out += a * np.exp(-((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) / (2.0 * s * s))
+        return out
+
+    def fields(self, octs, i):
+        """Source of problem i on its leaves (interior nodes), octs = that
+        problem's octants (a BatchSolver problem view or an oracle Domain)."""
+        e = self.block_extent
+        Nb = e + 2
+        src = np.zeros((octs.n, Nb, Nb, Nb))
+        x = np.arange(e) + 0.5
+        for o in range(octs.n):
+            if not octs.leaf[o]:
+                continue
+            b = octs.bbase[o]
+            src[o, 1:-1, 1:-1, 1:-1] = self._f(self.problems[i]["gaussians"], (b[0] + x)[None, None, :],
+                                               (b[1] + x)[None, :, None], (b[2] + x)[:, None, None])
+        return src
+
+    def n_cells(self, octs):
+        return int(np.count_nonzero(octs.leaf)) * self.block_extent ** 3

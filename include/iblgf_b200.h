@@ -147,6 +147,30 @@ int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out)
 int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, double Re, double* T,
                   int n_steps);
 
+/* ---- batches of independent problems -----------------------------------
+ * Many unbounded Poisson problems of uneven size solved together: each is
+ * PoissonSolver::apply_lgf (poisson.hpp:587-894) on its own octree
+ * (Domain::construct_basemesh_blocks / init_refine, domain.hpp:405-488,
+ * 878-939), while every stage of a sweep (anterpolation per level, forward
+ * transforms, spectral MAC, inverse transforms, interpolation) runs as one
+ * launch over all problems. A context becomes a batch with its first
+ * iblgf_batch_add_problem (instead of iblgf_domain_add_blocks); all problems
+ * share the context's block_extent, dx_base and precision, and each has its
+ * own bounding box (bd_base / bd_extent), block boxes and refinement.
+ * Fields (iblgf_field_*) of a batch hold the problems' octants back to back:
+ * problem p occupies octants [info[0], info[0] + info[1]) of
+ * iblgf_batch_problem_info, in that problem's canonical order. */
+int iblgf_batch_add_problem(iblgf_ctx* ctx, const int* bd_base, const int* bd_extent, int n_boxes,
+                            const int* base, const int* extent, int n_ref, iblgf_refine_fn pred, void* user,
+                            int* problem);
+int iblgf_batch_finalize(iblgf_ctx* ctx, int subtract_non_leaf);
+/* info[0] first octant in the batch, [1] octants, [2] base level, [3] depth */
+int iblgf_batch_problem_info(iblgf_ctx* ctx, int problem, int* info);
+int iblgf_batch_problem_octants(iblgf_ctx* ctx, int problem, uint64_t* keys, int* levels, int* flags,
+                                int* bbase);
+/* apply_lgf of every problem (AMR2AMR mask) from field src into field tgt */
+int iblgf_batch_apply_lgf(iblgf_ctx* ctx, int src, int tgt);
+
 /* ---- single-block convolution (fft::Convolution, convolution.hpp:141-328)
  * out (Nb^3, device) += scale * window [Nb-1, 2Nb-2]^3 of the linear
  * convolution of src (Nb^3, device) with kernel (P^3, device, P = 2Nb-1).
