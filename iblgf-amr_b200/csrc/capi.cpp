@@ -84,6 +84,7 @@ int iblgf_destroy(iblgf_ctx* x)
     iblgf_b200::poisson_release(&x->c);
     iblgf_b200::ns_release(&x->c);
     iblgf_b200::batch_release(&x->c);
+    iblgf_b200::ib_release(&x->c);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
     return IBLGF_OK;
@@ -377,6 +378,29 @@ int iblgf_batch_problem_octants(iblgf_ctx* x, int problem, uint64_t* keys, int* 
 int iblgf_batch_apply_lgf(iblgf_ctx* x, int src, int tgt)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::batch_apply_lgf(c, src, tgt); });
+}
+
+int iblgf_ib_set_points(iblgf_ctx* x, int n, const double* coords, double Re)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_set_points(c, n, coords, Re); });
+}
+
+int iblgf_ib_flags(iblgf_ctx* x, int* flags)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!flags) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        iblgf_b200::ib_flags(c, flags);
+    });
+}
+
+int iblgf_ib_solve(iblgf_ctx* x, const int* u_fields, double alpha, double threshold, int max_iter, double* force,
+                   int* iters)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!u_fields || !force) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        if (max_iter < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative iteration limit");
+        iblgf_b200::ib_solve(c, u_fields, alpha, threshold, max_iter, force, iters);
+    });
 }
 
 int iblgf_conv_block_noalloc(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)

@@ -276,6 +276,17 @@ int batch_add_problem(Ctx& c, const int* bd_base, const int* bd_extent, int n, c
 void batch_finalize(Ctx& c);
 void batch_apply_lgf(Ctx& c, int src, int tgt);
 void batch_release(const Ctx* c);
+// immersed boundary (ibsolve.cpp)
+void build_ib_masks(Ctx& c, std::vector<int>& ib);
+void ib_set_points(Ctx& c, int n, const double* X, double Re);
+void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters);
+void ib_flags(Ctx& c, int* flags);
+void ib_release(const Ctx* c);
+void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const long long* at, const double* w,
+                          int n, double* f);
+void launch_ib_smearing(Ctx& c, double* const* u, const long long* node_at, const int* nptr, const int* npt,
+                        const int* nent, const double* w, int n_nodes, const double* f);
+void launch_face_planes(Ctx& c, double* f, const int* list, const unsigned char* faces, int n, int width);
 int ge_table(Ctx& c, double alpha);
 // rp: relative position per axis of the field's mesh object (cell {1,1,1} when null)
 void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp = nullptr);

@@ -1,0 +1,356 @@
+// Immersed-boundary force solve on the device:
+//   points, flags and influence lists: IB::init / ib_block_overlap /
+//     yang3 (include/iblgf/domain/ib.hpp:70-120, 652-705),
+//     ServerBase::update_ib_flag (domain/decomposition/server.hpp:544-576),
+//     Client::update_ib_rank_and_infl (client.hpp:1262-1320)
+//   masks: FmmMaskBuilder IB2xIB / xIB2IB / IB2AMR (fmm/fmm.hpp:70-190)
+//   solve: LinSysSolver::ib_solve, CG_solve, ET_H_S_E, apply_Schur,
+//     projection, smearing (solver/linsys/linsys.hpp:113-450)
+// The delta weights of every (point, influence node, component) are computed
+// here once; projection and smearing run as deterministic device gathers. The
+// Schur operator's divergence, masked LGF solve, gradient and integrating
+// factor are the library's own kernels on device fields. CG vectors and dot
+// products are FP64 on the host (3 n values per iteration).
+#include <cmath>
+#include <map>
+#include <memory>
+
+#include "ctx.hpp"
+
+namespace iblgf_b200
+{
+void launch_axpby(Ctx& c, double* to, const double* from, double a, int mode);
+
+namespace
+{
+double yang3(double x)
+{
+    const double r = std::fabs(x);
+    if (r > 2) return 0.0;
+    const double r2 = r * r, s3 = std::sqrt(3.0);
+    if (r <= 1.0)
+        return 17.0 / 48.0 + s3 * M_PI / 108.0 + r / 4.0 - r2 / 4.0 +
+               (1.0 - 2.0 * r) / 16 * std::sqrt(-12.0 * r2 + 12.0 * r + 1.0) -
+               s3 / 12.0 * std::asin(s3 / 2.0 * (2.0 * r - 1.0));
+    return 55.0 / 48.0 - s3 * M_PI / 108.0 - 13.0 * r / 12.0 + r2 / 4.0 +
+           (2.0 * r - 3.0) / 48.0 * std::sqrt(-12.0 * r2 + 36.0 * r - 23.0) +
+           s3 / 36.0 * std::asin(s3 / 2.0 * (2 * r - 3.0));
+}
+
+struct IbState
+{
+    int n = 0;
+    std::vector<double> X;
+    std::vector<int> flags;  // per octant: bit0 is_ib (parents of IB blocks included), bit1 is_extended_ib
+    // projection: per point CSR over entries (field offset, 3 weights)
+    DevBuf<int> ptr;
+    DevBuf<long long> at;
+    DevBuf<double> w;
+    // smearing: per node CSR over (point, entry)
+    DevBuf<long long> node_at;
+    DevBuf<int> nptr, npt, nent;
+    int n_nodes = 0;
+    // face-plane cleaning at the finest level: IB region (width 2) and the
+    // operator's correction-boundary clean (width 2)
+    DevBuf<int> ibc_list, cb_list, corr_list;
+    DevBuf<unsigned char> ibc_faces, cb_faces;
+    int n_ibc = 0, n_cb = 0, n_corr = 0;
+    bool clean_base = false;
+    int face_aux[3] = {-1, -1, -1}, face_aux2[3] = {-1, -1, -1}, cell_aux2 = -1;
+    DevBuf<double> d_f;  // 3 n forces (smearing input / projection output)
+};
+std::map<const Ctx*, std::unique_ptr<IbState>> g_ib;
+
+// face neighbour direction -> face bit (0 z-, 1 y-, 2 x-, 3 x+, 4 y+, 5 z+)
+int face_bit(int i)
+{
+    switch (i)
+    {
+        case 4: return 0;
+        case 10: return 1;
+        case 12: return 2;
+        case 14: return 3;
+        case 16: return 4;
+        case 22: return 5;
+        default: return -1;
+    }
+}
+
+IbState& state(Ctx& c)
+{
+    auto it = g_ib.find(&c);
+    if (it == g_ib.end()) throw Error(IBLGF_EINVAL, "no immersed-boundary points set");
+    return *it->second;
+}
+}  // namespace
+
+void ib_set_points(Ctx& c, int n, const double* X, double Re)
+{
+    need_single(c);
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (n <= 0 || !X) throw Error(IBLGF_EINVAL, "no points");
+    if (!(Re > 0)) throw Error(IBLGF_EINVAL, "Re must be positive");
+    auto s = std::make_unique<IbState>();
+    s->n = n;
+    s->X.assign(X, X + 3 * (size_t)n);
+    const int l_max = c.tree.depth - 1, bl = c.tree.base_level;
+    const int ib_level = l_max - bl;
+    const int e = c.cfg.block_extent, Nb = c.Nb;
+    const double dx_base = c.cfg.dx_base;
+    const double dx_ib = dx_base / std::pow(2, ib_level);
+    const double ddf_radius = 4.5, safety = 5.0 / (Re * dx_ib) + 1.0;
+    auto overlap = [&](int i, int o, int radius_level) {
+        double r = 0;
+        if (radius_level == 2) r = ddf_radius + safety + 10.0;
+        else if (radius_level == 1) r = ddf_radius + 5.0;
+        const double sc = std::pow(2, ib_level - (c.levels[o] - bl));
+        const double factor = std::pow(2, ib_level) / dx_base;
+        for (int q = 0; q < 3; ++q)
+        {
+            const double base = c.bbase[3 * o + q] * sc - r;
+            const double mx = base + e * sc + 2 * r - 1;
+            if (mx + 1 < X[3 * i + q] * factor || base >= X[3 * i + q] * factor) return false;
+        }
+        return true;
+    };
+    s->flags.assign(c.n_oct, 0);
+    for (int i = 0; i < n; ++i)
+        for (int o : c.level_octs[l_max])
+            if (overlap(i, o, 2))
+            {
+                s->flags[o] |= 2;
+                if (overlap(i, o, 1) && (c.flags[o] & 1)) s->flags[o] |= 1;
+            }
+    std::vector<int> ibm = s->flags;
+    build_ib_masks(c, ibm);
+    s->flags = ibm;
+    // influence lists / nodes / weights (client.hpp:1262-1320, operators.hpp:841-861)
+    std::vector<int> ptr{0};
+    std::vector<long long> at;
+    std::vector<double> w;
+    std::vector<int> ent_pt;
+    const size_t B = c.block_elems();
+    for (int i = 0; i < n; ++i)
+    {
+        for (int o : c.level_octs[l_max])
+        {
+            if (!(c.flags[o] & 1) || !overlap(i, o, 1)) continue;
+            const double sc = std::pow(2, c.levels[o] - bl) / dx_base;
+            for (int k = 0; k < e; ++k)
+                for (int j = 0; j < e; ++j)
+                    for (int a = 0; a < e; ++a)
+                    {
+                        const int nd[3] = {c.bbase[3 * o] + a, c.bbase[3 * o + 1] + j, c.bbase[3 * o + 2] + k};
+                        double dist[3];
+                        bool in = true;
+                        for (int q = 0; q < 3; ++q)
+                        {
+                            dist[q] = nd[q] - X[3 * i + q] * sc;
+                            if (std::fabs(dist[q]) >= ddf_radius + 1.0) in = false;
+                        }
+                        if (!in) continue;
+                        at.push_back((long long)o * B + (a + 1) + (size_t)Nb * ((j + 1) + (size_t)Nb * (k + 1)));
+                        for (int cc = 0; cc < 3; ++cc)
+                            w.push_back(yang3(dist[0] + (cc == 0 ? 0.0 : 0.5)) *
+                                        yang3(dist[1] + (cc == 1 ? 0.0 : 0.5)) *
+                                        yang3(dist[2] + (cc == 2 ? 0.0 : 0.5)));
+                        ent_pt.push_back(i);
+                    }
+        }
+        ptr.push_back((int)at.size());
+    }
+    // node-major view for the smearing gather, points in increasing order
+    std::map<long long, std::vector<int>> by_node;
+    for (size_t e_ = 0; e_ < at.size(); ++e_) by_node[at[e_]].push_back((int)e_);
+    std::vector<long long> node_at;
+    std::vector<int> nptr{0}, npt, nent;
+    for (auto& kv : by_node)
+    {
+        node_at.push_back(kv.first);
+        for (int e_ : kv.second)
+        {
+            npt.push_back(ent_pt[e_]);
+            nent.push_back(e_);
+        }
+        nptr.push_back((int)npt.size());
+    }
+    s->ptr.upload(ptr, c.stream);
+    s->at.upload(at, c.stream);
+    s->w.upload(w, c.stream);
+    s->node_at.upload(node_at, c.stream);
+    s->nptr.upload(nptr, c.stream);
+    s->npt.upload(npt, c.stream);
+    s->nent.upload(nent, c.stream);
+    s->n_nodes = (int)node_at.size();
+    // face-plane cleaning lists at the finest level
+    std::vector<int> ibc_list, cb_list, corr;
+    std::vector<unsigned char> ibc_faces, cb_faces;
+    for (int o : c.level_octs[l_max])
+    {
+        unsigned char m1 = 0, m2 = 0;
+        for (int i = 0; i < 27; ++i)
+        {
+            const int b = face_bit(i);
+            if (b < 0) continue;
+            const int q = c.nbr[27 * (size_t)o + i];
+            if (q < 0 || !(ibm[q] & 1)) m1 |= (unsigned char)(1u << b);
+            if (q < 0 || (c.flags[q] & 2)) m2 |= (unsigned char)(1u << b);
+        }
+        if (m1)
+        {
+            ibc_list.push_back(o);
+            ibc_faces.push_back(m1);
+        }
+        if (m2)
+        {
+            cb_list.push_back(o);
+            cb_faces.push_back(m2);
+        }
+        if (c.flags[o] & 2) corr.push_back(o);
+    }
+    s->clean_base = l_max == bl;
+    s->ibc_list.upload(ibc_list, c.stream);
+    s->ibc_faces.upload(ibc_faces, c.stream);
+    s->cb_list.upload(cb_list, c.stream);
+    s->cb_faces.upload(cb_faces, c.stream);
+    s->corr_list.upload(corr, c.stream);
+    s->n_ibc = (int)ibc_list.size();
+    s->n_cb = (int)cb_list.size();
+    s->n_corr = (int)corr.size();
+    auto old = g_ib.find(&c);
+    if (old != g_ib.end())
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            s->face_aux[k] = old->second->face_aux[k];
+            s->face_aux2[k] = old->second->face_aux2[k];
+        }
+        s->cell_aux2 = old->second->cell_aux2;
+    }
+    else
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            s->face_aux[k] = field_create(c);
+            s->face_aux2[k] = field_create(c);
+        }
+        s->cell_aux2 = field_create(c);
+    }
+    s->d_f.alloc(3 * (size_t)n);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    g_ib[&c] = std::move(s);
+}
+
+void ib_flags(Ctx& c, int* flags)
+{
+    IbState& s = state(c);
+    for (int o = 0; o < c.n_oct; ++o) flags[o] = s.flags[o];
+}
+
+namespace
+{
+void projection(Ctx& c, IbState& s, const int* u, std::vector<double>& f)
+{
+    const double* pu[3] = {c.field(u[0]), c.field(u[1]), c.field(u[2])};
+    launch_ib_projection(c, pu, s.ptr.p, s.at.p, s.w.p, s.n, s.d_f.p);
+    f.resize(3 * (size_t)s.n);
+    IBLGF_CUDA(cudaMemcpyAsync(f.data(), s.d_f.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void smearing(Ctx& c, IbState& s, const std::vector<double>& f, const int* u)
+{
+    IBLGF_CUDA(cudaMemcpyAsync(s.d_f.p, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    double* pu[3] = {c.field(u[0]), c.field(u[1]), c.field(u[2])};
+    for (int k = 0; k < 3; ++k) IBLGF_CUDA(cudaMemsetAsync(pu[k], 0, c.field_elems() * sizeof(double), c.stream));
+    launch_ib_smearing(c, pu, s.node_at.p, s.nptr.p, s.npt.p, s.nent.p, s.w.p, s.n_nodes, s.d_f.p);
+}
+
+// apply_Schur<Source, Target>(xIB2IB), linsys.hpp:299-330
+void apply_schur(Ctx& c, IbState& s, const int* src, const int* tgt)
+{
+    OpLists& ol = op_lists(c);
+    const int l = c.tree.depth - 1;
+    for (int k = 0; k < 3; ++k) launch_halo(c, c.field(src[k]), ol.list[l].p, (int)ol.list[l].n);
+    const double* pin[3] = {c.field(src[0]), c.field(src[1]), c.field(src[2])};
+    double* pc[1] = {c.field(s.cell_aux2)};
+    launch_op(c, 2, pin, 3, pc, 1, ol.list[l].p, ol.dx[l].p, (int)ol.list[l].n, 1.0);
+    // Operator::clean_leaf_correction_boundary<cell_aux2>(l, true, 2)
+    launch_zero_blocks(c, pc[0], s.corr_list.p, s.n_corr);
+    if (s.clean_base) launch_face_planes(c, pc[0], s.cb_list.p, s.cb_faces.p, s.n_cb, 2);
+    launch_face_planes(c, pc[0], s.ibc_list.p, s.ibc_faces.p, s.n_ibc, 2);
+    poisson_apply_lgf(c, s.cell_aux2, s.cell_aux2, IBLGF_xIB2IB);
+    const double* pg[1] = {c.field(s.cell_aux2)};
+    double* pt[3] = {c.field(tgt[0]), c.field(tgt[1]), c.field(tgt[2])};
+    launch_op(c, 1, pg, 1, pt, 3, ol.list[l].p, ol.dx[l].p, (int)ol.list[l].n, 1.0);
+    for (int k = 0; k < 3; ++k)
+    {
+        launch_halo(c, pt[k], ol.list[l].p, (int)ol.list[l].n);
+        launch_face_planes(c, pt[k], s.ibc_list.p, s.ibc_faces.p, s.n_ibc, 2);
+    }
+}
+
+void et_h_s_e(Ctx& c, IbState& s, const std::vector<double>& fin, std::vector<double>& fout, double alpha)
+{
+    for (int k = 0; k < 3; ++k)
+        IBLGF_CUDA(cudaMemsetAsync(c.field(s.face_aux[k]), 0, c.field_elems() * sizeof(double), c.stream));
+    smearing(c, s, fin, s.face_aux2);
+    if (std::fabs(alpha) > 1e-14)
+        for (int k = 0; k < 3; ++k)
+        {
+            int rp[3] = {1, 1, 1};
+            rp[k] = 0;  // face component k
+            apply_if(c, s.face_aux2[k], s.face_aux2[k], alpha, IBLGF_IB2xIB, rp);
+        }
+    apply_schur(c, s, s.face_aux2, s.face_aux);
+    for (int k = 0; k < 3; ++k) launch_axpby(c, c.field(s.face_aux2[k]), c.field(s.face_aux[k]), -1.0, 1);
+    projection(c, s, s.face_aux2, fout);
+}
+}  // namespace
+
+void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters)
+{
+    IbState& s = state(c);
+    const int nf = (int)c.fields.size();
+    for (int k = 0; k < 3; ++k)
+        if (u[k] < 0 || u[k] >= nf) throw Error(IBLGF_EINVAL, "bad velocity field id");
+    const size_t m = 3 * (size_t)s.n;
+    std::vector<double> uc, Ax, r(m), p, Ap, fv(f, f + m);
+    projection(c, s, u, uc);
+    for (int k = 0; k < 3; ++k)
+        IBLGF_CUDA(cudaMemsetAsync(c.field(s.face_aux2[k]), 0, c.field_elems() * sizeof(double), c.stream));
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+        double t = 0.0;
+        for (size_t i = 0; i < m; ++i) t += a[i] * b[i];
+        return t;
+    };
+    et_h_s_e(c, s, fv, Ax, alpha);
+    for (size_t i = 0; i < m; ++i) r[i] = uc[i] - Ax[i];
+    p = r;
+    double rsold = dot(r, r);
+    int it = 0;
+    for (int k = 0; k < max_iter; ++k)
+    {
+        et_h_s_e(c, s, p, Ap, alpha);
+        ++it;
+        const double pAp = dot(p, Ap);
+        if (pAp == 0.0) break;
+        const double a = rsold / pAp;
+        for (size_t i = 0; i < m; ++i)
+        {
+            fv[i] = fv[i] + p[i] * a;
+            r[i] = r[i] + Ap[i] * -a;
+        }
+        const double rsnew = dot(r, r);
+        const double f2 = dot(fv, fv);
+        if (std::sqrt(rsnew / f2) < threshold) break;
+        for (size_t i = 0; i < m; ++i) p[i] = r[i] + p[i] * (rsnew / rsold);
+        rsold = rsnew;
+    }
+    for (size_t i = 0; i < m; ++i) f[i] = fv[i];
+    if (iters) *iters = it;
+}
+
+void ib_release(const Ctx* c) { g_ib.erase(c); }
+
+}  // namespace iblgf_b200

@@ -25,6 +25,9 @@ int mask_idx_gen(int type, int refinement_level, int nlas)
 {
     if (type == IBLGF_STREAM) return 0;
     if (type == IBLGF_AMR2AMR) return refinement_level * 2 + nlas + 15;
+    if (type == IBLGF_IB2xIB) return 1;
+    if (type == IBLGF_xIB2IB) return 2;
+    if (type == IBLGF_IB2AMR) return refinement_level + 4;
     throw Error(IBLGF_EINVAL, "unsupported fmm_type");
 }
 
@@ -252,6 +255,51 @@ void build_masks(Ctx& c)
     upward_pass(c, bl, st);
 }
 }  // namespace
+
+// FmmMaskBuilder::fmm_IB2xIB_mask / fmm_xIB2IB_mask / fmm_IB2AMR_mask
+// (fmm.hpp:70-190) from per-octant flags (bit0 is_ib, bit1 is_extended_ib);
+// IB2AMR marks the parents of IB blocks as IB (flags updated in place)
+void build_ib_masks(Ctx& c, std::vector<int>& ib)
+{
+    const int l = c.tree.depth - 1, bl = c.tree.base_level;
+    for (int t = IBLGF_IB2xIB; t <= IBLGF_xIB2IB; ++t)
+    {
+        MaskView mv{c.masks[mask_idx_gen(t, 0, 0)]};
+        std::fill(mv.m.begin(), mv.m.end(), 0);
+        for (int o : c.level_octs[l])
+        {
+            if (ib[o] & 1) mv.set(o, true, true);
+            if (ib[o] & 2)
+            {
+                if (t == IBLGF_IB2xIB) mv.m[2 * o + 1] = 1;
+                else mv.m[2 * o] = 1;
+            }
+        }
+        upward_pass(c, l, mv);
+        clean_no_inf(c, l, mv);
+    }
+    for (int lv = l - 1; lv >= bl; --lv)
+        for (int o : c.level_octs[lv])
+            for (int k = 0; k < 8; ++k)
+            {
+                const int ch = c.child[8 * o + k];
+                if (ch >= 0 && (ib[ch] & 1)) ib[o] |= 1;
+            }
+    for (int lv = l; lv >= bl; --lv)
+    {
+        MaskView mv{c.masks[mask_idx_gen(IBLGF_IB2AMR, lv - bl, 0)]};
+        std::fill(mv.m.begin(), mv.m.end(), 0);
+        for (int o : c.level_octs[lv]) mv.set(o, (ib[o] & 1) != 0, true);
+        upward_pass(c, lv, mv);
+    }
+    // plans built from the previous masks are stale
+    for (auto it = c.plans.begin(); it != c.plans.end();)
+    {
+        const int idx = std::get<0>(it->first);
+        if (idx >= 1 && idx < 15) it = c.plans.erase(it);
+        else ++it;
+    }
+}
 
 int field_create(Ctx& c)
 {
@@ -823,8 +871,8 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double add_with_s
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
     if (level < c.tree.base_level || level >= c.tree.depth) throw Error(IBLGF_EINVAL, "level out of range");
     const int rl = level - c.tree.base_level;
-    const int idx = fmm_type == IBLGF_STREAM ? mask_idx_gen(IBLGF_STREAM, 0, 0)
-                                              : mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0);
+    const int idx = fmm_type == IBLGF_AMR2AMR ? mask_idx_gen(IBLGF_AMR2AMR, rl, nlas ? 1 : 0)
+                                               : mask_idx_gen(fmm_type, rl, 0);
     FmmPlan& p = get_plan(c, level, idx, ge);
     run_sweep(c, p, src, tgt, c.cfg.dx_base / std::pow(2.0, rl), add_with_scale, ge);
 }
@@ -1050,7 +1098,8 @@ void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const i
     const int coarse_m[3] = {rp[0] ? 4 : 8, rp[1] ? 4 : 8, rp[2] ? 4 : 8};
     const int intrp_m[3] = {rp[0] ? 2 : 6, rp[1] ? 2 : 6, rp[2] ? 2 : 6};
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
-    if (fmm_type != IBLGF_AMR2AMR) throw Error(IBLGF_EINVAL, "apply_if supports AMR2AMR");
+    if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_IB2xIB)
+        throw Error(IBLGF_EINVAL, "apply_if supports AMR2AMR and IB2xIB");
     PoissonLists& pl = poisson_lists(c);
     OpLists& ol = op_lists(c);
     double* st = c.field(c.f_source_tmp);
@@ -1058,8 +1107,19 @@ void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const i
     const size_t bytes = c.field_elems() * sizeof(double);
     IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
-    launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
     const int bl = c.tree.base_level, depth = c.tree.depth;
+    if (fmm_type == IBLGF_IB2xIB)
+    {
+        // poisson.hpp:447-448, 465-494: finest level only, interior copy, the
+        // non-leaf-as-source sweep with the IB2xIB mask, level copied out
+        const int l = depth - 1;
+        launch_copy_interior(c, c.field(src), st, pl.level_all[l].p, (int)pl.level_all[l].n);
+        const int ge = ge_table(c, alpha_base * std::pow(4.0, l - bl));
+        if (!c.subtract_non_leaf) fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, true, 1.0, IBLGF_IB2xIB, ge);
+        launch_axpy_blocks(c, tt, c.field(tgt), pl.level_all[l].p, (int)pl.level_all[l].n, 1.0, true);
+        return;
+    }
+    launch_axpy_blocks(c, c.field(src), st, pl.leaves.p, (int)pl.leaves.n, 1.0, true);
     for (int ls = depth - 2; ls >= bl; --ls) launch_tp_axes(c, pl.coarsify[ls], st, st, coarse_m, 0);
     // intrp_to_correction_buffer (poisson.hpp:1015-1069)
     for (int l = depth - 2; l >= bl; --l)
@@ -1087,8 +1147,9 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
 {
     need_single(c);
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
-    if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_STREAM)
-        throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR and STREAM");
+    if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_STREAM && fmm_type != IBLGF_xIB2IB &&
+        fmm_type != IBLGF_IB2xIB)
+        throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR, STREAM, IB2xIB and xIB2IB");
     PoissonLists& pl = poisson_lists(c);
     double* st = c.field(c.f_source_tmp);
     double* tt = c.field(c.f_target_tmp);
@@ -1097,6 +1158,19 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
     IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    if (fmm_type == IBLGF_xIB2IB || fmm_type == IBLGF_IB2xIB)
+    {
+        // finest level only: copy_level (interior), one sweep with the IB
+        // mask, leaves of that level assigned (poisson.hpp:615-616, 702-745)
+        const int l = c.tree.depth - 1;
+        launch_copy_interior(c, c.field(src), st, pl.level_all[l].p, (int)pl.level_all[l].n);
+        if (!c.subtract_non_leaf)
+        {
+            fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, false, 1.0, fmm_type);
+            launch_axpy_blocks(c, tt, c.field(tgt), pl.level_leaves[l].p, (int)pl.level_leaves[l].n, 1.0, true);
+        }
+        return;
+    }
     if (fmm_type == IBLGF_STREAM)
     {
         // base level only: copy_level (interior), one sweep with the stream

@@ -36,7 +36,8 @@ EXPORTS = [
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
-    "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_conv_block", "iblgf_conv_block_noalloc",
+    "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
+    "iblgf_ib_solve", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -86,6 +87,9 @@ def lib():
     L.iblgf_batch_problem_info.argtypes = [vp, ci, vp]
     L.iblgf_batch_problem_octants.argtypes = [vp, ci, vp, vp, vp, vp]
     L.iblgf_batch_apply_lgf.argtypes = [vp, ci, ci]
+    L.iblgf_ib_set_points.argtypes = [vp, ci, vp, cd]
+    L.iblgf_ib_flags.argtypes = [vp, vp]
+    L.iblgf_ib_solve.argtypes = [vp, vp, cd, cd, ci, vp, vp]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -265,6 +269,25 @@ class Solver:
         self._check(lib().iblgf_ns_step(self.h, _p(uf), int(p_field), float(dt), float(Re), ctypes.byref(t),
                                         int(n_steps)))
         return t.value
+
+    def ib_set_points(self, X, Re):
+        """IB points (n, 3) on the finest level (ib.hpp / server.hpp / client.hpp)."""
+        self._ib_X = np.ascontiguousarray(X, dtype=np.float64)
+        self._check(lib().iblgf_ib_set_points(self.h, len(self._ib_X), _p(self._ib_X), float(Re)))
+
+    def ib_flags(self):
+        out = np.zeros(self.n, np.int32)
+        self._check(lib().iblgf_ib_flags(self.h, _p(out)))
+        return out
+
+    def ib_solve(self, u_fields, alpha, threshold=1e-3, max_iter=40, f0=None):
+        """IB force solve (linsys.hpp:113-230); returns (force (n, 3), CG iterations)."""
+        uf = np.ascontiguousarray(np.asarray(u_fields, dtype=np.int32))
+        f = np.zeros((len(self._ib_X), 3)) if f0 is None else np.ascontiguousarray(f0, dtype=np.float64).copy()
+        it = ctypes.c_int()
+        self._check(lib().iblgf_ib_solve(self.h, _p(uf), float(alpha), float(threshold), int(max_iter), _p(f),
+                                         ctypes.byref(it)))
+        return f, it.value
 
     def conv_block(self, src_dptr, kernel_dptr, out_dptr, scale=1.0):
         self._check(lib().iblgf_conv_block(self.h, ctypes.c_void_p(src_dptr), ctypes.c_void_p(kernel_dptr),

@@ -378,3 +378,76 @@ class BatchPoisson:
 
     def n_cells(self, octs):
         return int(np.count_nonzero(octs.leaf)) * self.block_extent ** 3
+
+
+class SphereIB:
+    """Immersed-boundary sphere (the reference's geometry=sphere, ib.hpp:179-210:
+    R = 0.5 at the origin, Fibonacci points at spacing ibph * dx_ib) in a
+    block-refined box; the IB lives on the finest level.
+
+    small: 6^3 blocks, dx_base = 1/8, box +-1.5, one refinement level around
+           the sphere (dx_ib = 1/16), ibph 1.5 (413 points), Re = 300
+    c5:    16^3 blocks, dx_base = 1/10, box +-3.2 x +-3.2 x [-3.2, 6.4) with a
+           wake, two refinement levels (dx_ib = D/40), ibph 1.7 (2009 points),
+           Re = 300
+    """
+
+    def __init__(self, name="small"):
+        self.name, self.Re = name, 300.0
+        if name == "small":
+            self.block_extent, self.dx_base, self.n_levels, self.ibph = 6, 1.0 / 8, 1, 1.5
+            lo, hi = (-12, -12, -12), (12, 12, 12)
+            self.radii = (1.1,)
+        elif name == "c5":
+            self.block_extent, self.dx_base, self.n_levels, self.ibph = 16, 1.0 / 10, 2, 1.7
+            lo, hi = (-32, -32, -32), (64, 32, 32)
+            self.radii = (1.6, 1.0)
+        else:
+            raise ValueError(name)
+        e = self.block_extent
+        self.blocks = [(lo, tuple(h - l for l, h in zip(lo, hi)))]
+        m = 1
+        while m * e < max(max(abs(v) for v in lo), max(abs(v) for v in hi)):
+            m *= 2
+        half = m * e
+        self.bd_base = (-2 * half,) * 3
+        self.bd_extent = (4 * half,) * 3
+
+    def points(self):
+        import oracle_lib as O  # noqa: F401  (tests only)
+        raise NotImplementedError
+
+    def predicate(self, base, extent, rl, diff_level):
+        """Refine blocks (grown by 2 cells) that reach within radii[rl] of the
+        sphere centre; the c5 wake extends the base-level region downstream."""
+        if rl >= len(self.radii):
+            return False
+        dxl = self.dx_base / 2 ** rl
+        lo = [(base[d] - 2) * dxl for d in range(3)]
+        hi = [(base[d] + extent[d] + 2) * dxl for d in range(3)]
+        r = self.radii[rl]
+        if self.name == "c5" and rl == 0:
+            # wake: a cylinder of radius r behind the sphere up to x = 4
+            q = [min(max(0.0, lo[1]), hi[1]), min(max(0.0, lo[2]), hi[2])]
+            if hi[0] > -r and lo[0] < 4.0 and q[0] ** 2 + q[1] ** 2 < r * r:
+                return True
+        c = [min(max(0.0, lo[d]), hi[d]) for d in range(3)]
+        return c[0] ** 2 + c[1] ** 2 + c[2] ** 2 < r * r
+
+    def velocity(self, octs, U=(1.0, 0.0, 0.0), seed=5):
+        """Face velocity: the uniform stream U plus a smooth seeded
+        perturbation, on every block (buffers included)."""
+        rng = np.random.Generator(np.random.PCG64(seed))
+        k = rng.uniform(0.5, 2.0, size=(3, 3))
+        Nb = self.block_extent + 2
+        u = np.zeros((3, octs.n, Nb, Nb, Nb))
+        i = np.arange(Nb) - 1.0
+        for o in range(octs.n):
+            rl = int(octs.levels[o]) - octs.base_level
+            dxl = self.dx_base / 2 ** rl
+            b = octs.bbase[o]
+            for c in range(3):
+                x = [(b[a] + i + (0.0 if a == c else 0.5)) * dxl for a in range(3)]
+                X, Y, Z = x[0][None, None, :], x[1][None, :, None], x[2][:, None, None]
+                u[c, o] = U[c] + 0.1 * np.sin(k[c, 0] * X) * np.cos(k[c, 1] * Y) * np.cos(k[c, 2] * Z)
+        return u

@@ -37,7 +37,10 @@ enum
 enum { IBLGF_FP64 = 0, IBLGF_FP32 = 1 };
 
 /* octant_t::MASK_TYPE (include/iblgf/domain/octree/octant.hpp:69-78) */
-enum { IBLGF_STREAM = 0, IBLGF_AMR2AMR = 1 };
+/* mask types (octant.hpp MASK_TYPE): STREAM, AMR2AMR, and the immersed-
+ * boundary ones IB2xIB (IB blocks -> IB and extended-IB blocks), xIB2IB
+ * (IB and extended-IB -> IB), IB2AMR (IB -> all blocks of a level) */
+enum { IBLGF_STREAM = 0, IBLGF_AMR2AMR = 1, IBLGF_IB2xIB = 2, IBLGF_xIB2IB = 3, IBLGF_IB2AMR = 4 };
 
 typedef struct
 {
@@ -146,6 +149,22 @@ int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out)
  * dx_base^2) > 7) returns IBLGF_EINVAL. */
 int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, double Re, double* T,
                   int n_steps);
+
+/* ---- immersed boundary (ib.hpp, linsys.hpp) ------------------------------
+ * iblgf_ib_set_points: the IB points (n x 3 coordinates, the reference's
+ * IB::coordinates_) on the finest mesh level, with IB::init's delta radius
+ * 4.5 and safety distance 5 / (Re dx_ib) + 1; marks IB / extended-IB blocks
+ * (ServerBase::update_ib_flag, server.hpp:544-576), builds the IB2xIB /
+ * xIB2IB / IB2AMR masks (fmm.hpp:70-190) and the influence lists and yang3
+ * delta weights (client.hpp:1262-1320). iblgf_ib_flags: per octant bit0
+ * is_ib, bit1 is_extended_ib. iblgf_ib_solve: LinSysSolver::ib_solve +
+ * CG_solve (linsys.hpp:113-230) for the face velocity u_fields[0..2] (a body
+ * at rest in the frame); force (n x 3) is the initial guess in and the IB
+ * force out, iters the CG iteration count. */
+int iblgf_ib_set_points(iblgf_ctx* ctx, int n, const double* coords, double Re);
+int iblgf_ib_flags(iblgf_ctx* ctx, int* flags);
+int iblgf_ib_solve(iblgf_ctx* ctx, const int* u_fields, double alpha, double threshold, int max_iter,
+                   double* force, int* iters);
 
 /* ---- batches of independent problems -----------------------------------
  * Many unbounded Poisson problems of uneven size solved together: each is

@@ -243,6 +243,47 @@ int orc_ns_step(void* hp, double dt, double Re, double T0, double* u, double* p,
     });
 }
 
+// IB force solve (linsys.hpp:113-230) for n points X (n x 3): u holds the
+// three face-velocity component fields back to back; f (n x 3) is the initial
+// guess in and the force out; flags (optional, per octant) gets bit0 is_ib,
+// bit1 is_extended_ib; iters gets the CG iteration count.
+int orc_ib_solve(void* hp, int n, const double* X, double Re, const double* u, double alpha, double threshold,
+                 int max_iter, double* f, int* flags, int* iters)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t N = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        std::vector<std::array<double, 3>> pts(n), force(n);
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c)
+            {
+                pts[i][c] = X[3 * i + c];
+                force[i][c] = f[3 * i + c];
+            }
+        IbSystem ib(h->d.get(), h->s.get(), pts, Re);
+        VField uf;
+        uf.mesh = MESH_FACE;
+        for (int k = 0; k < 3; ++k) uf.c.emplace_back(u + k * N, u + (k + 1) * N);
+        ib.solve(uf, alpha, force, threshold, max_iter);
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) f[3 * i + c] = force[i][c];
+        if (flags)
+            for (size_t i = 0; i < h->d->octs.size(); ++i)
+                flags[i] = (h->d->octs[i]->ib ? 1 : 0) | (h->d->octs[i]->ext_ib ? 2 : 0);
+        if (iters) *iters = ib.iterations;
+    });
+}
+
+int orc_sphere_points(double dx_base, int ib_level, double ibph, double* X, int cap)
+{
+    const auto v = sphere_points(dx_base, ib_level, ibph);
+    for (int i = 0; i < (int)v.size() && i < cap; ++i)
+        for (int c = 0; c < 3; ++c) X[3 * i + c] = v[i][c];
+    return (int)v.size();
+}
+
+double orc_yang3(double x) { return yang3(x); }
+
 // Single-block linear convolution with the reference's Convolution contract
 // (convolution.hpp:225-304): kernel holds P^3 values (P = 2Nb-1, x fastest),
 // out (Nb^3) += scale * window[Nb-1, 2Nb-2]^3 of (kernel (*) zero-padded src).

@@ -184,6 +184,44 @@ void fmm_stream_mask_build(Domain& d)
     upward_pass(d, d.base_level, idx);
 }
 
+void fmm_ib_mask_build(Domain& d)
+{
+    const int l = d.depth - 1;
+    for (int t = IB2xIB; t <= xIB2IB; ++t)
+    {
+        const int idx = fmm_mask_idx_gen(t);
+        for (auto& o : d.octs) o->mask[idx] = {false, false};
+        for (auto& kv : d.level_maps[l])
+        {
+            Octant* o = kv.second;
+            if (o->ib) o->mask[idx] = {true, true};
+            if (o->ext_ib)
+            {
+                if (t == IB2xIB) o->mask[idx][T] = true;
+                else o->mask[idx][S] = true;
+            }
+        }
+        upward_pass(d, l, idx);
+        clean_no_inf(d, l, idx);
+    }
+    for (int lv = d.depth - 2; lv >= d.base_level; --lv)
+        for (auto& kv : d.level_maps[lv])
+            for (auto& c : kv.second->child)
+                if (c && c->has_data && c->ib) kv.second->ib = true;
+    for (int lv = d.depth - 1; lv >= d.base_level; --lv)
+    {
+        const int idx = fmm_mask_idx_gen(IB2AMR, lv - d.base_level);
+        for (auto& o : d.octs) o->mask[idx] = {false, false};
+        for (auto& kv : d.level_maps[lv])
+        {
+            Octant* o = kv.second;
+            o->mask[idx][T] = true;
+            if (o->ib) o->mask[idx][S] = true;
+        }
+        upward_pass(d, lv, idx);
+    }
+}
+
 // fmm_nli.hpp:319-374; mat is Nb x 2Nb with (p, c) at p*2Nb + c
 void nli_matrix(int Nb, int pts_cap, double* mat)
 {
@@ -449,6 +487,8 @@ void Solver::fmm_apply(const Field& src, Field& tgt, int level, bool nlas,
     int idx;
     if (fmm_type == STREAM) idx = fmm_mask_idx_gen(STREAM);
     else if (fmm_type == AMR2AMR) idx = fmm_mask_idx_gen(AMR2AMR, rl, nlas ? 1 : 0);
+    else if (fmm_type == IB2xIB || fmm_type == xIB2IB) idx = fmm_mask_idx_gen(fmm_type);
+    else if (fmm_type == IB2AMR) idx = fmm_mask_idx_gen(IB2AMR, rl);
     else throw std::runtime_error("oracle: unsupported fmm_type");
     if (fmm_s.size() != d->octs.size() * B) fmm_s.assign(d->octs.size() * B, 0.0);
     if (fmm_t.size() != d->octs.size() * B) fmm_t.assign(d->octs.size() * B, 0.0);
@@ -597,7 +637,8 @@ void Solver::fmm_apply(const Field& src, Field& tgt, int level, bool nlas,
 void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_correction,
                        bool subtract_non_leaf)
 {
-    if (fmm_type != AMR2AMR && fmm_type != STREAM) throw std::runtime_error("oracle: unsupported fmm_type");
+    if (fmm_type != AMR2AMR && fmm_type != STREAM && fmm_type != xIB2IB && fmm_type != IB2xIB)
+        throw std::runtime_error("oracle: unsupported fmm_type");
     const size_t B = (size_t)Nb * Nb * Nb;
     const size_t N = d->octs.size() * B;
     Field source_tmp(N, 0.0), target_tmp(N, 0.0), correction_tmp(N, 0.0);
@@ -621,6 +662,23 @@ void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_corr
         {
             fmm_apply(source_tmp, target_tmp, d->base_level, false, 1.0, STREAM);
             for (auto& kv : d->level_maps[d->base_level])
+            {
+                Octant* o = kv.second;
+                if (o->leaf) std::copy(blk(target_tmp, o), blk(target_tmp, o) + B, &tgt[o->idx * B]);
+            }
+        }
+        return;
+    }
+    if (fmm_type == xIB2IB || fmm_type == IB2xIB)
+    {
+        // poisson.hpp:615-616, 648-650, 702-745: finest level only, interior
+        // copy, one sweep with the IB mask, leaves of that level assigned
+        const int l = d->depth - 1;
+        copy_level_interior(src, source_tmp, l);
+        if (!subtract_non_leaf)
+        {
+            fmm_apply(source_tmp, target_tmp, l, false, 1.0, fmm_type);
+            for (auto& kv : d->level_maps[l])
             {
                 Octant* o = kv.second;
                 if (o->leaf) std::copy(blk(target_tmp, o), blk(target_tmp, o) + B, &tgt[o->idx * B]);
@@ -789,13 +847,13 @@ const std::vector<cplx>& Solver::lgf_ge_spectrum(double alpha, int bx, int by, i
 }
 
 void Solver::fmm_apply_ge(const Field& src, Field& tgt, int level, bool nlas, double add_with_scale,
-                          double alpha)
+                          double alpha, int fmm_type)
 {
     const size_t B = (size_t)Nb * Nb * Nb;
     const int H = P / 2 + 1;
     const size_t NC = (size_t)H * P * P;
     const int rl = level - d->base_level;
-    const int idx = fmm_mask_idx_gen(AMR2AMR, rl, nlas ? 1 : 0);
+    const int idx = fmm_type == AMR2AMR ? fmm_mask_idx_gen(AMR2AMR, rl, nlas ? 1 : 0) : fmm_mask_idx_gen(fmm_type, rl);
     if (fmm_s.size() != d->octs.size() * B) fmm_s.assign(d->octs.size() * B, 0.0);
     if (fmm_t.size() != d->octs.size() * B) fmm_t.assign(d->octs.size() * B, 0.0);
     auto Sm = [&](Octant* o) { return o->mask[idx][0]; };
@@ -923,30 +981,56 @@ void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_o
 
 // PoissonSolver::apply_if (poisson.hpp:436-494) for AMR2AMR; rp: relative
 // positions of the field's mesh object (cell {1,1,1} when null)
-void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf, const int* rp)
+void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf, const int* rp,
+                      int fmm_type)
 {
     const size_t B = (size_t)Nb * Nb * Nb;
     const size_t N = d->octs.size() * B;
     Field source_tmp(N, 0.0), target_tmp(N, 0.0);
-    for (Octant* o : d->octs)
-        if (o->leaf) std::copy(&src[o->idx * B], &src[o->idx * B] + B, &source_tmp[o->idx * B]);
-    coarsify_all(source_tmp, rp);
-    // intrp_to_correction_buffer (poisson.hpp:1015-1069)
-    for (int l = d->depth - 2; l >= d->base_level; --l)
+    if (fmm_type == AMR2AMR)
     {
-        buffer_exchange(*d, source_tmp, l);
-        cc_intrp_level(source_tmp, source_tmp, l, true, rp);
+        for (Octant* o : d->octs)
+            if (o->leaf) std::copy(&src[o->idx * B], &src[o->idx * B] + B, &source_tmp[o->idx * B]);
+        coarsify_all(source_tmp, rp);
+        // intrp_to_correction_buffer (poisson.hpp:1015-1069)
+        for (int l = d->depth - 2; l >= d->base_level; --l)
+        {
+            buffer_exchange(*d, source_tmp, l);
+            cc_intrp_level(source_tmp, source_tmp, l, true, rp);
+        }
     }
-    for (int l = d->base_level; l < d->depth; ++l)
+    else if (fmm_type == IB2xIB)
+        copy_level_interior(src, source_tmp, d->depth - 1);
+    else
+        throw std::runtime_error("oracle: apply_if supports AMR2AMR and IB2xIB");
+    const int l_min = fmm_type == IB2xIB ? d->depth - 1 : d->base_level;
+    for (int l = l_min; l < d->depth; ++l)
     {
         const double alpha = alpha_base * std::pow(4.0, l - d->base_level);
-        fmm_apply_ge(source_tmp, target_tmp, l, false, 1.0, alpha);
-        if (!subtract_non_leaf) fmm_apply_ge(source_tmp, target_tmp, l, true, 1.0, alpha);
+        if (fmm_type == AMR2AMR) fmm_apply_ge(source_tmp, target_tmp, l, false, 1.0, alpha, fmm_type);
+        if (!subtract_non_leaf) fmm_apply_ge(source_tmp, target_tmp, l, true, 1.0, alpha, fmm_type);
         for (auto& kv : d->level_maps[l])
         {
             Octant* o = kv.second;
             std::copy(&target_tmp[o->idx * B], &target_tmp[o->idx * B] + B, &tgt[o->idx * B]);
         }
+    }
+}
+
+// copy_level(l, with_buffer = false): interior nodes of every block of level l
+void Solver::copy_level_interior(const Field& src, Field& dst, int l) const
+{
+    for (auto& kv : d->level_maps[l])
+    {
+        Octant* o = kv.second;
+        const size_t B = (size_t)Nb * Nb * Nb;
+        for (int k = 1; k < Nb - 1; ++k)
+            for (int j = 1; j < Nb - 1; ++j)
+                for (int i = 1; i < Nb - 1; ++i)
+                {
+                    const size_t c = i + (size_t)Nb * (j + (size_t)Nb * k);
+                    dst[o->idx * B + c] = src[o->idx * B + c];
+                }
     }
 }
 }  // namespace orc

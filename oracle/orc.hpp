@@ -78,6 +78,7 @@ struct Octant
     int bbase[3] = {0, 0, 0};  // block base (level cell units, no buffer)
     int data_level = 0;        // refinement level given at allocation
     bool leaf = false, correction = false, physical = false, aim_deletion = false;
+    bool ib = false, ext_ib = false;  // immersed-boundary blocks (server.hpp:544-576)
     std::array<Octant*, 27> neighbor{};
     std::array<Octant*, 189> influence{};
     int n_infl = 0;
@@ -131,6 +132,9 @@ enum MaskType { STREAM = 0, AMR2AMR = 1, IB2xIB = 2, xIB2IB = 3, IB2AMR = 4 };
 int fmm_mask_idx_gen(int type, int refinement_level = 0, int non_leaf_as_source = 0);
 void fmm_lgf_mask_build(Domain& d, bool subtract_non_leaf);
 void fmm_stream_mask_build(Domain& d);
+// IB2xIB, xIB2IB and IB2AMR masks from the octants' ib / ext_ib flags
+// (fmm.hpp:70-190); IB2AMR also marks the parents of IB blocks as IB
+void fmm_ib_mask_build(Domain& d);
 
 struct Solver
 {
@@ -161,13 +165,14 @@ struct Solver
     double lgf_ge_get(int x, int y, int z, double alpha);
     const std::vector<cplx>& lgf_ge_spectrum(double alpha, int bx, int by, int bz);
     void fmm_apply_ge(const Field& src, Field& tgt, int level, bool non_leaf_as_source,
-                      double add_with_scale, double alpha);
+                      double add_with_scale, double alpha, int fmm_type = AMR2AMR);
     void apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf,
-                  const int* rp = nullptr);
+                  const int* rp = nullptr, int fmm_type = AMR2AMR);
     // cell_center_nli transfers; rp = relative position per axis (0: node
     // coincides with the child's, 1: half a cell off), cell {1,1,1} when null
     void cc_intrp_level(Field& from, Field& to, int level, bool correction_only, const int* rp = nullptr);
     void coarsify_all(Field& f, const int* rp = nullptr);
+    void copy_level_interior(const Field& src, Field& dst, int l) const;
 };
 
 // ---------------------------------------------------------------- IF-HERK
@@ -215,6 +220,38 @@ struct Ifherk
     void apply_if(const VField& src, VField& tgt, double alpha_base);
     void lin_sys(double alpha_k);
 };
+
+// ---------------------------------------------------------------- IB
+// Immersed boundary on the finest level (ib.hpp, client.hpp:1262-1320,
+// server.hpp:544-576) and its force solve (linsys.hpp:113-531).
+double yang3(double x);  // ib.hpp:690-705
+struct IbSystem
+{
+    Domain* d;
+    Solver* s;
+    int ib_level = 0;            // refinement level of the IB (the finest)
+    double Re = 1.0;
+    double ddf_radius = 4.5, safety_dis = 0.0;
+    std::vector<std::array<double, 3>> X;                       // point coordinates
+    std::vector<std::vector<Octant*>> infl;                     // leaf blocks per point
+    std::vector<std::vector<std::vector<std::array<int, 3>>>> pts;  // interior nodes (local index) per block
+    VField face_aux, face_aux2, cell_aux2;
+    int iterations = 0;
+
+    IbSystem(Domain* d, Solver* s, const std::vector<std::array<double, 3>>& X, double Re);
+    bool overlap(int i, const Octant* o, int radius_level) const;   // ib_block_overlap
+    void projection(const VField& u, std::vector<std::array<double, 3>>& f) const;
+    void smearing(const std::vector<std::array<double, 3>>& f, VField& u) const;
+    void clean_ib_region_boundary(VField& f, int l, int width) const;
+    void clean_face_boundary(VField& f, int l, bool leaf_only_boundary, int width) const;
+    void apply_schur(VField& src, VField& tgt);
+    void et_h_s_e(const std::vector<std::array<double, 3>>& fin, std::vector<std::array<double, 3>>& fout,
+                  double alpha);
+    // ib_solve (linsys.hpp:113-129) + CG_solve (:170-230); f: initial guess in, force out
+    void solve(const VField& u, double alpha, std::vector<std::array<double, 3>>& f, double threshold,
+               int max_iter);
+};
+std::vector<std::array<double, 3>> sphere_points(double dx_base, int ib_level, double ibph);
 
 void nli_matrix(int Nb, int pts_cap, double* mat /* Nb x 2Nb, (p,c) at p*2Nb+c */);
 void buffer_exchange(Domain& d, Field& f, int level);

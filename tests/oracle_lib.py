@@ -58,6 +58,11 @@ def lib():
         L.orc_lgf_ge_get.argtypes = [vp, ci, ci, ci, cd]
         L.orc_lgf_ge_get.restype = cd
         L.orc_ns_step.argtypes = [vp, cd, cd, cd, vp, vp, ci]
+        L.orc_ib_solve.argtypes = [vp, ci, vp, cd, vp, cd, cd, ci, vp, vp, vp]
+        L.orc_sphere_points.argtypes = [cd, ci, cd, vp, ci]
+        L.orc_sphere_points.restype = ci
+        L.orc_yang3.argtypes = [cd]
+        L.orc_yang3.restype = cd
         _lib = L
     return _lib
 
@@ -73,6 +78,14 @@ def _check(rc):
 
 def lgf_get(x, y, z):
     return lib().orc_lgf_get(int(x), int(y), int(z))
+
+
+def sphere_points(dx_base, ib_level, ibph):
+    """ib.hpp:179-210: Fibonacci points on the sphere R = 0.5."""
+    n = lib().orc_sphere_points(float(dx_base), int(ib_level), float(ibph), None, 0)
+    X = np.zeros((n, 3))
+    lib().orc_sphere_points(float(dx_base), int(ib_level), float(ibph), _p(X), n)
+    return X
 
 
 def block_conv(src, kernel, scale=1.0):
@@ -195,6 +208,18 @@ class Domain:
         p = self.zeros()
         _check(lib().orc_ns_step(self.h, float(dt), float(Re), float(T0), _p(uu), _p(p), int(n_steps)))
         return uu, p
+
+    def ib_solve(self, X, Re, u, alpha, threshold=1e-3, max_iter=40, f0=None):
+        """IB force solve (linsys.hpp:113-230): returns (force (n, 3), flags per
+        octant (bit0 is_ib, bit1 is_extended_ib), CG iterations)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        f = np.zeros((len(X), 3)) if f0 is None else np.ascontiguousarray(f0, dtype=np.float64).copy()
+        flags = np.zeros(self.n, np.int32)
+        it = ctypes.c_int()
+        _check(lib().orc_ib_solve(self.h, len(X), _p(X), float(Re), _p(uu), float(alpha), float(threshold),
+                                  int(max_iter), _p(f), _p(flags), ctypes.byref(it)))
+        return f, flags, it.value
 
     def apply_lgf(self, src, tgt=None, use_correction=True, subtract_non_leaf=False, fmm_type=1):
         src = np.ascontiguousarray(src, dtype=np.float64)
