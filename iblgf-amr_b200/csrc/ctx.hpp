@@ -4,6 +4,7 @@
 
 #include <array>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <tuple>
 #include <unordered_map>
@@ -281,6 +282,11 @@ void build_ib_masks(Ctx& c, std::vector<int>& ib);
 void ib_set_points(Ctx& c, int n, const double* X, double Re);
 void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters);
 void ib_flags(Ctx& c, int* flags);
+bool ib_active(const Ctx& c);
+const int* ib_face_aux2(Ctx& c);
+void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
+                 const std::function<void()>& gradient_d);
+void ib_force(Ctx& c, int stage, double* out);
 void ib_release(const Ctx* c);
 void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const long long* at, const double* w,
                           int n, double* f);
@@ -310,6 +316,8 @@ PoissonLists& poisson_lists(Ctx& c);
 // IF-HERK time steps (ifherk.hpp:1078-1200) of the face velocity u[3] and the
 // cell pressure p; T advances by dt per step
 void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n_steps);
+// constant frame velocity and IB CG settings of the IF-HERK step
+void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter);
 void ns_release(const Ctx* c);
 OpLists& op_lists(Ctx& c);
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);

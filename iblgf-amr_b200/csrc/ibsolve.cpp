@@ -12,6 +12,7 @@
 // factor are the library's own kernels on device fields. CG vectors and dot
 // products are FP64 on the host (3 n values per iteration).
 #include <cmath>
+#include <functional>
 #include <map>
 #include <memory>
 
@@ -58,6 +59,7 @@ struct IbState
     bool clean_base = false;
     int face_aux[3] = {-1, -1, -1}, face_aux2[3] = {-1, -1, -1}, cell_aux2 = -1;
     DevBuf<double> d_f;  // 3 n forces (smearing input / projection output)
+    std::vector<double> force_prev[4];  // IB::force_prev per IF-HERK stage (CG warm start)
 };
 std::map<const Ctx*, std::unique_ptr<IbState>> g_ib;
 
@@ -237,6 +239,7 @@ void ib_set_points(Ctx& c, int n, const double* X, double Re)
         s->cell_aux2 = field_create(c);
     }
     s->d_f.alloc(3 * (size_t)n);
+    for (auto& fp : s->force_prev) fp.assign(3 * (size_t)n, 0.0);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     g_ib[&c] = std::move(s);
 }
@@ -258,11 +261,12 @@ void projection(Ctx& c, IbState& s, const int* u, std::vector<double>& f)
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-void smearing(Ctx& c, IbState& s, const std::vector<double>& f, const int* u)
+void smearing(Ctx& c, IbState& s, const std::vector<double>& f, const int* u, bool cleaning = true)
 {
     IBLGF_CUDA(cudaMemcpyAsync(s.d_f.p, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     double* pu[3] = {c.field(u[0]), c.field(u[1]), c.field(u[2])};
-    for (int k = 0; k < 3; ++k) IBLGF_CUDA(cudaMemsetAsync(pu[k], 0, c.field_elems() * sizeof(double), c.stream));
+    if (cleaning)
+        for (int k = 0; k < 3; ++k) IBLGF_CUDA(cudaMemsetAsync(pu[k], 0, c.field_elems() * sizeof(double), c.stream));
     launch_ib_smearing(c, pu, s.node_at.p, s.nptr.p, s.npt.p, s.nent.p, s.w.p, s.n_nodes, s.d_f.p);
 }
 
@@ -307,6 +311,45 @@ void et_h_s_e(Ctx& c, IbState& s, const std::vector<double>& fin, std::vector<do
     projection(c, s, s.face_aux2, fout);
 }
 }  // namespace
+
+bool ib_active(const Ctx& c) { return g_ib.count(&c) != 0; }
+
+const int* ib_face_aux2(Ctx& c) { return state(c).face_aux2; }
+
+// lin_sys_with_ib_solve's IB part (ifherk.hpp:1474-1494) after face_aux2 =
+// r_i - grad d_i (+ IF): CG warm-started from the stage's previous force,
+// pressure correction of d, then face_aux = grad d + E f (the caller
+// subtracts it from r_i)
+void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
+                 const std::function<void()>& gradient_d)
+{
+    IbState& s = state(c);
+    std::vector<double> f = s.force_prev[stage];
+    ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), nullptr);
+    s.force_prev[stage] = f;
+    // LinSysSolver::pressure_correction (linsys.hpp:131-145)
+    OpLists& ol = op_lists(c);
+    const int l = c.tree.depth - 1;
+    IBLGF_CUDA(cudaMemsetAsync(c.field(s.cell_aux2), 0, c.field_elems() * sizeof(double), c.stream));
+    smearing(c, s, f, s.face_aux2);
+    for (int k = 0; k < 3; ++k) launch_halo(c, c.field(s.face_aux2[k]), ol.list[l].p, (int)ol.list[l].n);
+    const double* pin[3] = {c.field(s.face_aux2[0]), c.field(s.face_aux2[1]), c.field(s.face_aux2[2])};
+    double* pc[1] = {c.field(s.cell_aux2)};
+    launch_op(c, 2, pin, 3, pc, 1, ol.list[l].p, ol.dx[l].p, (int)ol.list[l].n, 1.0);
+    launch_zero_blocks(c, pc[0], s.corr_list.p, s.n_corr);
+    if (s.clean_base) launch_face_planes(c, pc[0], s.cb_list.p, s.cb_faces.p, s.n_cb, 2);
+    poisson_apply_lgf(c, s.cell_aux2, s.cell_aux2, IBLGF_IB2AMR);
+    launch_axpby(c, c.field(d_field), c.field(s.cell_aux2), -1.0, 1);
+    gradient_d();
+    smearing(c, s, f, face_aux, false);
+}
+
+void ib_force(Ctx& c, int stage, double* out)
+{
+    IbState& s = state(c);
+    if (stage < 1 || stage > 3) throw Error(IBLGF_EINVAL, "stage must be 1, 2 or 3");
+    for (size_t i = 0; i < s.force_prev[stage].size(); ++i) out[i] = s.force_prev[stage][i];
+}
 
 void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters)
 {

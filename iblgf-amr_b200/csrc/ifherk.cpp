@@ -59,6 +59,14 @@ struct NsState
     int sm_n[2] = {0, 0};
     double T_last_vel_refresh = 0.0;  // ifherk.hpp:1980
 };
+// per context: constant frame velocity and IB CG settings (set any time)
+struct NsOptions
+{
+    double frame_vel[3] = {0.0, 0.0, 0.0};
+    double cg_threshold = 1e-3;
+    int cg_max_iter = 40;
+};
+std::map<const Ctx*, NsOptions> g_nsopt;
 std::map<const Ctx*, std::unique_ptr<NsState>> g_ns;
 
 VF make_vf(Ctx& c, int mesh)
@@ -127,7 +135,7 @@ class Step
 {
   public:
     Step(Ctx& c_, NsState& s_, double dt_, double Re_)
-    : c(c_), s(s_), pl(poisson_lists(c_)), ol(op_lists(c_)), dt(dt_), Re(Re_)
+    : c(c_), s(s_), pl(poisson_lists(c_)), ol(op_lists(c_)), dt(dt_), Re(Re_), opt(g_nsopt[&c_])
     {
         bl = c.tree.base_level;
         depth = c.tree.depth;
@@ -148,6 +156,7 @@ class Step
         nonlinear(u, s.g_i, coeff_a(1, 1) * (-dt));
         copy(s.q_i, s.r_i, 1.0);
         add(s.g_i, s.r_i, 1.0);
+        stage = 1;
         lin_sys(alpha[0]);
         // stage 2
         clean(s.r_i, false);
@@ -162,6 +171,7 @@ class Step
         up_and_down(s.u_i);
         nonlinear(s.u_i, s.g_i, coeff_a(2, 2) * (-dt));
         add(s.g_i, s.r_i, 1.0);
+        stage = 2;
         lin_sys(alpha[1]);
         // stage 3
         clean(s.d_i, false);
@@ -176,6 +186,7 @@ class Step
         up_and_down(s.u_i);
         nonlinear(s.u_i, s.g_i, coeff_a(3, 3) * (-dt));
         add(s.g_i, s.r_i, 1.0);
+        stage = 3;
         lin_sys(alpha[2]);
         copy(s.u_i, u, 1.0);
         copy(s.d_i, p, 1.0 / coeff_a(3, 3) / dt);
@@ -187,7 +198,8 @@ class Step
     PoissonLists& pl;
     OpLists& ol;
     double dt, Re;
-    int bl = 0, depth = 0;
+    NsOptions opt;
+    int bl = 0, depth = 0, stage = 0;
     // ifherk.hpp:2010-2011
     const double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
     const double cc[4] = {0.0, 1.0 / 3, 1.0, 1.0};
@@ -279,6 +291,9 @@ class Step
             op(3, {&src}, s.edge_aux, l, 1.0);
         }
         copy(src, s.face_aux, 1.0);
+        // add_field_expression(frame_vel, -1): a constant frame velocity
+        for (int k = 0; k < 3; ++k)
+            if (opt.frame_vel[k] != 0.0) launch_axpby(c, F(s.face_aux.id[k]), nullptr, -opt.frame_vel[k], 3);
         for (int l = bl; l < depth; ++l)
         {
             exchange(s.edge_aux, l);
@@ -319,6 +334,30 @@ class Step
     {
         divergence(s.r_i, s.cell_aux);
         poisson_apply_lgf(c, s.cell_aux.id[0], s.d_i.id[0], IBLGF_AMR2AMR);
+        if (ib_active(c))
+        {
+            // lin_sys_with_ib_solve (ifherk.hpp:1451-1517)
+            VF fa2;
+            fa2.mesh = kFace;
+            fa2.n = 3;
+            for (int k = 0; k < 3; ++k) fa2.id[k] = ib_face_aux2(c)[k];
+            copy(s.r_i, fa2, 1.0);
+            gradient(s.d_i, s.face_aux);
+            add(s.face_aux, fa2, -1.0);
+            if (std::fabs(alpha_k) > 1e-14)
+                for (int k = 0; k < 3; ++k)
+                {
+                    int rp[3];
+                    relpos(kFace, k, rp);
+                    iblgf_b200::apply_if(c, fa2.id[k], fa2.id[k], alpha_k, IBLGF_IB2xIB, rp);
+                }
+            ns_ib_stage(c, stage, alpha_k, opt.cg_threshold, opt.cg_max_iter, s.d_i.id[0], s.face_aux.id,
+                        [&]() { gradient(s.d_i, s.face_aux); });
+            add(s.face_aux, s.r_i, -1.0);
+            if (std::fabs(alpha_k) > 1e-14) apply_if(s.r_i, s.u_i, alpha_k);
+            else copy(s.r_i, s.u_i, 1.0);
+            return;
+        }
         gradient(s.d_i, s.face_aux);
         add(s.face_aux, s.r_i, -1.0);
         if (std::fabs(alpha_k) > 1e-14) apply_if(s.r_i, s.u_i, alpha_k);
@@ -354,6 +393,19 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
     IBLGF_CUDA(cudaGetLastError());
 }
 
-void ns_release(const Ctx* c) { g_ns.erase(c); }
+void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter)
+{
+    if (!(cg_threshold > 0) || cg_max_iter < 0) throw Error(IBLGF_EINVAL, "bad CG settings");
+    NsOptions& o = g_nsopt[&c];
+    for (int k = 0; k < 3; ++k) o.frame_vel[k] = frame_vel ? frame_vel[k] : 0.0;
+    o.cg_threshold = cg_threshold;
+    o.cg_max_iter = cg_max_iter;
+}
+
+void ns_release(const Ctx* c)
+{
+    g_ns.erase(c);
+    g_nsopt.erase(c);
+}
 
 }  // namespace iblgf_b200

@@ -35,14 +35,15 @@ __global__ void clean_kernel(double* __restrict__ f, const int* __restrict__ lea
     }
 }
 
-// mode 0: to = a * from; 1: to += a * from; 2: to *= a
+// mode 0: to = a * from; 1: to += a * from; 2: to *= a; 3: to += a
 __global__ void axpby_kernel(double* __restrict__ to, const double* __restrict__ from, double a, size_t n, int mode)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     {
         if (mode == 0) to[i] = from[i] * a;
         else if (mode == 1) to[i] += from[i] * a;
-        else to[i] *= a;
+        else if (mode == 2) to[i] *= a;
+        else to[i] += a;
     }
 }
 

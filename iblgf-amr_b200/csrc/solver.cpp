@@ -1147,9 +1147,7 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
 {
     need_single(c);
     if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
-    if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_STREAM && fmm_type != IBLGF_xIB2IB &&
-        fmm_type != IBLGF_IB2xIB)
-        throw Error(IBLGF_EINVAL, "apply_lgf supports AMR2AMR, STREAM, IB2xIB and xIB2IB");
+    if (fmm_type < IBLGF_STREAM || fmm_type > IBLGF_IB2AMR) throw Error(IBLGF_EINVAL, "unknown fmm_type");
     PoissonLists& pl = poisson_lists(c);
     double* st = c.field(c.f_source_tmp);
     double* tt = c.field(c.f_target_tmp);
@@ -1158,6 +1156,21 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
     IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
     IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    if (fmm_type == IBLGF_IB2AMR)
+    {
+        // finest-level interior copy, coarsified (cell mesh), one sweep per
+        // level with the IB2AMR mask, leaves assigned, no source correction
+        // (poisson.hpp:617-618, 632-634, 702-745)
+        const int bl = c.tree.base_level, depth = c.tree.depth;
+        launch_copy_interior(c, c.field(src), st, pl.level_all[depth - 1].p, (int)pl.level_all[depth - 1].n);
+        for (int ls = depth - 2; ls >= bl; --ls) launch_tp(c, pl.coarsify[ls], st, st, 4, 0);
+        for (int l = bl; l < depth && !c.subtract_non_leaf; ++l)
+        {
+            fmm_apply(c, c.f_source_tmp, c.f_target_tmp, l, false, 1.0, IBLGF_IB2AMR);
+            launch_axpy_blocks(c, tt, c.field(tgt), pl.level_leaves[l].p, (int)pl.level_leaves[l].n, 1.0, true);
+        }
+        return;
+    }
     if (fmm_type == IBLGF_xIB2IB || fmm_type == IBLGF_IB2xIB)
     {
         // finest level only: copy_level (interior), one sweep with the IB

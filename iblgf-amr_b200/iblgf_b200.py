@@ -37,7 +37,7 @@ EXPORTS = [
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
-    "iblgf_ib_solve", "iblgf_conv_block", "iblgf_conv_block_noalloc",
+    "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -90,6 +90,8 @@ def lib():
     L.iblgf_ib_set_points.argtypes = [vp, ci, vp, cd]
     L.iblgf_ib_flags.argtypes = [vp, vp]
     L.iblgf_ib_solve.argtypes = [vp, vp, cd, cd, ci, vp, vp]
+    L.iblgf_ns_options.argtypes = [vp, vp, cd, ci]
+    L.iblgf_ib_force.argtypes = [vp, ci, vp]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -269,6 +271,15 @@ class Solver:
         self._check(lib().iblgf_ns_step(self.h, _p(uf), int(p_field), float(dt), float(Re), ctypes.byref(t),
                                         int(n_steps)))
         return t.value
+
+    def ns_options(self, frame_vel=(0.0, 0.0, 0.0), cg_threshold=1e-3, cg_max_iter=40):
+        fv = np.ascontiguousarray(frame_vel, dtype=np.float64)
+        self._check(lib().iblgf_ns_options(self.h, _p(fv), float(cg_threshold), int(cg_max_iter)))
+
+    def ib_force(self, stage):
+        out = np.zeros((len(self._ib_X), 3))
+        self._check(lib().iblgf_ib_force(self.h, int(stage), _p(out)))
+        return out
 
     def ib_set_points(self, X, Re):
         """IB points (n, 3) on the finest level (ib.hpp / server.hpp / client.hpp)."""

@@ -144,11 +144,21 @@ int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out)
  * Advances the face velocity (three component fields u_fields[0..2], x/y/z
  * normal components) by n_steps steps of size dt at Reynolds number Re and
  * writes the pressure of the last step into p_field; *T is the simulation time
- * (in/out). Scope: no immersed boundary, adaptation or body force, frame
- * velocity 0. The velocity-refresh branch (taken once (T - 0) 3.3 / (Re
- * dx_base^2) > 7) returns IBLGF_EINVAL. */
+ * (in/out). The immersed boundary and the frame velocity come from
+ * iblgf_ib_set_points / iblgf_ns_options. Not covered: adaptation, body
+ * force, moving bodies (boundary velocity 0) and the velocity-refresh branch
+ * (taken once (T - 0) 3.3 / (Re dx_base^2) > 7), which returns IBLGF_EINVAL. */
 int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, double Re, double* T,
                   int n_steps);
+/* Constant frame velocity (frame_vel[3], subtracted from the convecting
+ * velocity as add_field_expression(frame_vel, -1) in Ifherk::nonlinear,
+ * ifherk.hpp:1667-1668; NULL = 0) and the IB CG settings (cg_threshold,
+ * cg_max_itr; defaults 1e-3, 40). With IB points set (iblgf_ib_set_points)
+ * each stage of iblgf_ns_step runs lin_sys_with_ib_solve with the IB
+ * (ifherk.hpp:1451-1517), warm-started from that stage's previous force. */
+int iblgf_ns_options(iblgf_ctx* ctx, const double* frame_vel, double cg_threshold, int cg_max_iter);
+/* IB force of the last step's stage 1, 2 or 3 (IB::force_prev), n x 3 */
+int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out);
 
 /* ---- immersed boundary (ib.hpp, linsys.hpp) ------------------------------
  * iblgf_ib_set_points: the IB points (n x 3 coordinates, the reference's

@@ -243,6 +243,36 @@ int orc_ns_step(void* hp, double dt, double Re, double T0, double* u, double* p,
     });
 }
 
+// IF-HERK steps with an immersed boundary of n_pts points X and a constant
+// frame velocity; forces (3 stages x n_pts x 3) gets the stage forces of the
+// last step.
+int orc_ns_step_ib(void* hp, double dt, double Re, double T0, double* u, double* p, int n_steps, int n_pts,
+                   const double* X, const double* frame_vel, double threshold, int max_iter, double* forces)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        std::vector<std::array<double, 3>> pts(n_pts);
+        for (int i = 0; i < n_pts; ++i)
+            for (int c = 0; c < 3; ++c) pts[i][c] = X[3 * i + c];
+        IbSystem ib(h->d.get(), h->s.get(), pts, Re);
+        Ifherk ns(h->d.get(), h->s.get(), dt, Re);
+        ns.T = T0;
+        ns.ib = &ib;
+        ns.cg_threshold = threshold;
+        ns.cg_max_iter = max_iter;
+        for (int k = 0; k < 3; ++k) ns.frame_vel[k] = frame_vel[k];
+        for (auto& fp : ns.force_prev) fp.assign(n_pts, {0.0, 0.0, 0.0});
+        for (int k = 0; k < 3; ++k) ns.u.c[k].assign(u + k * n, u + (k + 1) * n);
+        for (int st = 0; st < n_steps; ++st) ns.time_step();
+        for (int k = 0; k < 3; ++k) std::memcpy(u + k * n, ns.u.c[k].data(), n * sizeof(double));
+        std::memcpy(p, ns.p.c[0].data(), n * sizeof(double));
+        for (int sidx = 1; sidx <= 3; ++sidx)
+            for (int i = 0; i < n_pts; ++i)
+                for (int c = 0; c < 3; ++c) forces[((sidx - 1) * n_pts + i) * 3 + c] = ns.force_prev[sidx][i][c];
+    });
+}
+
 // IB force solve (linsys.hpp:113-230) for n points X (n x 3): u holds the
 // three face-velocity component fields back to back; f (n x 3) is the initial
 // guess in and the force out; flags (optional, per octant) gets bit0 is_ib,

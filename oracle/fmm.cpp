@@ -637,7 +637,8 @@ void Solver::fmm_apply(const Field& src, Field& tgt, int level, bool nlas,
 void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_correction,
                        bool subtract_non_leaf)
 {
-    if (fmm_type != AMR2AMR && fmm_type != STREAM && fmm_type != xIB2IB && fmm_type != IB2xIB)
+    if (fmm_type != AMR2AMR && fmm_type != STREAM && fmm_type != xIB2IB && fmm_type != IB2xIB &&
+        fmm_type != IB2AMR)
         throw std::runtime_error("oracle: unsupported fmm_type");
     const size_t B = (size_t)Nb * Nb * Nb;
     const size_t N = d->octs.size() * B;
@@ -678,6 +679,24 @@ void Solver::apply_lgf(const Field& src, Field& tgt, int fmm_type, bool use_corr
         if (!subtract_non_leaf)
         {
             fmm_apply(source_tmp, target_tmp, l, false, 1.0, fmm_type);
+            for (auto& kv : d->level_maps[l])
+            {
+                Octant* o = kv.second;
+                if (o->leaf) std::copy(blk(target_tmp, o), blk(target_tmp, o) + B, &tgt[o->idx * B]);
+            }
+        }
+        return;
+    }
+    if (fmm_type == IB2AMR)
+    {
+        // poisson.hpp:617-618, 632-634, 702-745: finest-level interior copy,
+        // coarsified (cell mesh), one sweep per level with the IB2AMR mask,
+        // leaves assigned; no source correction
+        copy_level_interior(src, source_tmp, d->depth - 1);
+        coarsify_all(source_tmp);
+        for (int l = d->base_level; l < d->depth && !subtract_non_leaf; ++l)
+        {
+            fmm_apply(source_tmp, target_tmp, l, false, 1.0, IB2AMR);
             for (auto& kv : d->level_maps[l])
             {
                 Octant* o = kv.second;

@@ -154,11 +154,12 @@ void IbSystem::projection(const VField& u, std::vector<std::array<double, 3>>& f
         }
 }
 
-void IbSystem::smearing(const std::vector<std::array<double, 3>>& f, VField& u) const
+void IbSystem::smearing(const std::vector<std::array<double, 3>>& f, VField& u, bool cleaning) const
 {
     const int Nb = d->Nb;
     const size_t B = (size_t)Nb * Nb * Nb;
-    for (auto& c : u.c) std::fill(c.begin(), c.end(), 0.0);
+    if (cleaning)
+        for (auto& c : u.c) std::fill(c.begin(), c.end(), 0.0);
     for (size_t i = 0; i < X.size(); ++i)
         for (size_t b = 0; b < infl[i].size(); ++b)
         {
@@ -269,6 +270,19 @@ void IbSystem::et_h_s_e(const std::vector<std::array<double, 3>>& fin, std::vect
     for (int k = 0; k < 3; ++k)
         for (size_t i = 0; i < face_aux2.c[k].size(); ++i) face_aux2.c[k][i] += face_aux.c[k][i] * -1.0;
     projection(face_aux2, fout);
+}
+
+void IbSystem::pressure_correction(const std::vector<std::array<double, 3>>& f, VField& p)
+{
+    const int l = d->depth - 1;
+    for (auto& c : cell_aux2.c) std::fill(c.begin(), c.end(), 0.0);
+    smearing(f, face_aux2);
+    for (auto& c : face_aux2.c) buffer_exchange(*d, c, l);
+    apply_op(*d, 2, {&face_aux2.c[0], &face_aux2.c[1], &face_aux2.c[2]}, {&cell_aux2.c[0]}, l, 1.0);
+    clean_face_boundary(cell_aux2, l, true, 2);
+    const Field in = cell_aux2.c[0];
+    s->apply_lgf(in, cell_aux2.c[0], IB2AMR, true, false);
+    for (size_t i = 0; i < p.c[0].size(); ++i) p.c[0][i] += cell_aux2.c[0][i] * -1.0;
 }
 
 void IbSystem::solve(const VField& u, double alpha, std::vector<std::array<double, 3>>& f, double threshold,

@@ -200,6 +200,10 @@ void Ifherk::nonlinear(VField& src, VField& tgt, double scale)
         op_level(3, {&src.c[0], &src.c[1], &src.c[2]}, {&edge_aux.c[0], &edge_aux.c[1], &edge_aux.c[2]}, l, 1.0);
     }
     copy(src, face_aux, 1.0);
+    // add_field_expression(frame_vel, -1): a constant frame velocity
+    for (int k = 0; k < 3; ++k)
+        if (frame_vel[k] != 0.0)
+            for (double& v : face_aux.c[k]) v += frame_vel[k] * -1.0;
     for (int l = d->base_level; l < d->depth; ++l)
     {
         exchange(edge_aux, l);
@@ -248,6 +252,33 @@ void Ifherk::lin_sys(double alpha_k)
 {
     divergence(r_i, cell_aux);
     s->apply_lgf(cell_aux.c[0], d_i.c[0], AMR2AMR, true, false);
+    if (ib)
+    {
+        // lin_sys_with_ib_solve (ifherk.hpp:1451-1517)
+        VField& fa2 = ib->face_aux2;
+        copy(r_i, fa2, 1.0);
+        gradient(d_i, face_aux);
+        add(face_aux, fa2, -1.0);
+        if (std::fabs(alpha_k) > 1e-14)
+            for (int k = 0; k < 3; ++k)
+            {
+                int rp[3];
+                mesh_relpos(MESH_FACE, k, rp);
+                const Field in = fa2.c[k];
+                s->apply_if(in, fa2.c[k], alpha_k, false, rp, IB2xIB);
+            }
+        std::vector<std::array<double, 3>> force = force_prev[stage_idx];
+        const VField uin = fa2;
+        ib->solve(uin, alpha_k, force, cg_threshold, cg_max_iter);
+        force_prev[stage_idx] = force;
+        ib->pressure_correction(force, d_i);
+        gradient(d_i, face_aux);
+        ib->smearing(force, face_aux, false);
+        add(face_aux, r_i, -1.0);
+        if (std::fabs(alpha_k) > 1e-14) apply_if(r_i, u_i, alpha_k);
+        else copy(r_i, u_i, 1.0);
+        return;
+    }
     gradient(d_i, face_aux);
     add(face_aux, r_i, -1.0);
     if (std::fabs(alpha_k) > 1e-14) apply_if(r_i, u_i, alpha_k);
@@ -269,6 +300,7 @@ void Ifherk::time_step()
     nonlinear(u, g_i, coeff_a(1, 1) * (-dt));
     copy(q_i, r_i, 1.0);
     add(g_i, r_i, 1.0);
+    stage_idx = 1;
     lin_sys(alpha[0]);
     // stage 2
     clean(r_i, false);
@@ -283,6 +315,7 @@ void Ifherk::time_step()
     up_and_down(u_i);
     nonlinear(u_i, g_i, coeff_a(2, 2) * (-dt));
     add(g_i, r_i, 1.0);
+    stage_idx = 2;
     lin_sys(alpha[1]);
     // stage 3
     clean(d_i, false);
@@ -297,6 +330,7 @@ void Ifherk::time_step()
     up_and_down(u_i);
     nonlinear(u_i, g_i, coeff_a(3, 3) * (-dt));
     add(g_i, r_i, 1.0);
+    stage_idx = 3;
     lin_sys(alpha[2]);
     copy(u_i, u, 1.0);
     copy(d_i, p, 1.0 / coeff_a(3, 3) / dt);

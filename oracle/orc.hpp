@@ -195,6 +195,13 @@ struct Ifherk
     double dt, Re;
     double T = 0.0, T_last_vel_refresh = 0.0;
     double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
+    // immersed boundary (optional): force of the previous step per stage
+    // (IB::force_prev, the CG warm start), CG settings, frame velocity
+    struct IbSystem* ib = nullptr;
+    std::vector<std::array<double, 3>> force_prev[4];
+    double cg_threshold = 1e-3;
+    int cg_max_iter = 40, stage_idx = 0;
+    double frame_vel[3] = {0.0, 0.0, 0.0};
     double c[4] = {0.0, 1.0 / 3, 1.0, 1.0};
     double alpha[3] = {0.0, 0.0, 0.0};
     VField u, p, q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
@@ -241,7 +248,7 @@ struct IbSystem
     IbSystem(Domain* d, Solver* s, const std::vector<std::array<double, 3>>& X, double Re);
     bool overlap(int i, const Octant* o, int radius_level) const;   // ib_block_overlap
     void projection(const VField& u, std::vector<std::array<double, 3>>& f) const;
-    void smearing(const std::vector<std::array<double, 3>>& f, VField& u) const;
+    void smearing(const std::vector<std::array<double, 3>>& f, VField& u, bool cleaning = true) const;
     void clean_ib_region_boundary(VField& f, int l, int width) const;
     void clean_face_boundary(VField& f, int l, bool leaf_only_boundary, int width) const;
     void apply_schur(VField& src, VField& tgt);
@@ -250,6 +257,8 @@ struct IbSystem
     // ib_solve (linsys.hpp:113-129) + CG_solve (:170-230); f: initial guess in, force out
     void solve(const VField& u, double alpha, std::vector<std::array<double, 3>>& f, double threshold,
                int max_iter);
+    // LinSysSolver::pressure_correction (linsys.hpp:131-145): p -= L^-1 div E f
+    void pressure_correction(const std::vector<std::array<double, 3>>& f, VField& p);
 };
 std::vector<std::array<double, 3>> sphere_points(double dx_base, int ib_level, double ibph);
 

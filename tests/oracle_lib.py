@@ -59,6 +59,7 @@ def lib():
         L.orc_lgf_ge_get.restype = cd
         L.orc_ns_step.argtypes = [vp, cd, cd, cd, vp, vp, ci]
         L.orc_ib_solve.argtypes = [vp, ci, vp, cd, vp, cd, cd, ci, vp, vp, vp]
+        L.orc_ns_step_ib.argtypes = [vp, cd, cd, cd, vp, vp, ci, ci, vp, vp, cd, ci, vp]
         L.orc_sphere_points.argtypes = [cd, ci, cd, vp, ci]
         L.orc_sphere_points.restype = ci
         L.orc_yang3.argtypes = [cd]
@@ -208,6 +209,19 @@ class Domain:
         p = self.zeros()
         _check(lib().orc_ns_step(self.h, float(dt), float(Re), float(T0), _p(uu), _p(p), int(n_steps)))
         return uu, p
+
+    def ns_step_ib(self, u, dt, Re, X, frame_vel=(0.0, 0.0, 0.0), T0=0.0, n_steps=1, threshold=1e-3,
+                   max_iter=40):
+        """IF-HERK steps with an immersed boundary (ifherk.hpp:1451-1517);
+        returns (u, p, stage forces (3, n, 3) of the last step)."""
+        uu = np.ascontiguousarray(u, dtype=np.float64).copy()
+        p = self.zeros()
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        fv = np.ascontiguousarray(frame_vel, dtype=np.float64)
+        forces = np.zeros((3, len(X), 3))
+        _check(lib().orc_ns_step_ib(self.h, float(dt), float(Re), float(T0), _p(uu), _p(p), int(n_steps), len(X),
+                                    _p(X), _p(fv), float(threshold), int(max_iter), _p(forces)))
+        return uu, p, forces
 
     def ib_solve(self, X, Re, u, alpha, threshold=1e-3, max_iter=40, f0=None):
         """IB force solve (linsys.hpp:113-230): returns (force (n, 3), flags per

@@ -45,3 +45,31 @@ def test_ib_solve_needs_points():
     g._ib_X = np.zeros((4, 3))
     with pytest.raises(B.IblgfError):
         g.ib_solve(uf, 0.0)
+
+
+@pytest.mark.parametrize("precision,tol,ptol", [(B.FP64, 1e-9, 1e-9), (B.FP32, 1e-4, 5e-4)])
+def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
+    """Two IF-HERK steps past the sphere in a uniform stream (frame velocity
+    (-1, 0, 0): the body at rest, the fluid moving at +1): velocity, pressure
+    and the three stage forces of the last step against the oracle. In FP32
+    the pressure (d_i / (a33 dt), a factor 400 here) carries the FP32
+    perturbation of the IB CG iterates: 5e-4 for it, 1e-4 for velocity."""
+    case = S.SphereIB("small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=precision)
+    X = O.sphere_points(case.dx_base, o.depth - 1 - o.base_level, case.ibph)
+    u0 = case.velocity(o)
+    dt, fv = 0.01, (-1.0, 0.0, 0.0)
+    ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, 0.0, 2)
+    g.ib_set_points(X, case.Re)
+    g.ns_options(fv)
+    uf = [g.field(u0[k]) for k in range(3)]
+    pf = g.field()
+    g.ns_step(uf, pf, dt, case.Re, 0.0, 2)
+    for k in range(3):
+        assert rel_linf(g.download(uf[k]), ur[k]) < tol, (k, rel_linf(g.download(uf[k]), ur[k]))
+    assert rel_linf(g.download(pf), pr) < ptol, rel_linf(g.download(pf), pr)
+    for st in range(3):
+        assert rel_linf(g.ib_force(st + 1), fr[st]) < tol * 10, (st, rel_linf(g.ib_force(st + 1), fr[st]))
