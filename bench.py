@@ -122,6 +122,8 @@ def main():
     ap.add_argument("--ns-only", action="store_true", help="only the IF-HERK step measurement (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
+    ap.add_argument("--no-ib", action="store_true", help="skip the immersed-boundary NS step measurement")
+    ap.add_argument("--ib-only", action="store_true", help="only the immersed-boundary NS step measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -162,6 +164,10 @@ def main():
     if args.ns_only:
         if rank == 0:
             print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
+        return
+    if args.ib_only:
+        if rank == 0:
+            print(json.dumps({"ns_step_ib": ib_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
         return
     if args.batch_only:
         if rank == 0:
@@ -285,6 +291,8 @@ def main():
         cpu = cpu_baseline(case)
     if rank == 0 and not args.no_ns:
         extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
+    if rank == 0 and not args.no_ib:
+        extra["ns_step_ib"] = ib_bench(B, stream, local, args.steps, args.warmup)
     if rank == 0 and not args.no_batch:
         extra["batch"] = batch_bench(B, stream, local, args.steps, args.warmup)
 
@@ -346,6 +354,64 @@ def ns_bench(B, stream, device, steps, warmup):
                 "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
                 "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
     return out
+
+
+def ib_bench(B, stream, device, steps, warmup):
+    """IF-HERK step with the immersed boundary, flow past a sphere (D = 1,
+    Re = 300, uniform stream via frame velocity, dx_finest = D/40, 2009 IB
+    points, wake refinement): step time (CUDA events) and IB CG iterations per
+    step, FP32 and FP64, warm start = previous step's force per stage."""
+    import torch
+    case = S.SphereIB("c5")
+    out = {"workload": "sphere D=1, Re=300, uniform stream, dx_finest=D/40, 16^3 blocks, 3 mesh levels, "
+                       "2009 IB points, CG threshold 1e-3, max 40"}
+    dt = 0.35 * case.dx_base / 4 / 1.0
+    res = {}
+    for name, prec in (("fp32", B.FP32), ("fp64", B.FP64)):
+        g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                     n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=device,
+                     stream=stream.cuda_stream)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        X = sphere_points(case.dx_base, g.depth - 1 - g.base_level, case.ibph)
+        g.ib_set_points(X, case.Re)
+        g.ns_options((-1.0, 0.0, 0.0))
+        u0 = case.velocity(g, U=(0.0, 0.0, 0.0))
+        uf = [g.field(u0[k]) for k in range(3)]
+        pf = g.field()
+        T = 0.0
+        for _ in range(warmup):
+            T = g.ns_step(uf, pf, dt, case.Re, T, 1)
+        torch.cuda.synchronize()
+        its = []
+        ms = 0.0
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            T = g.ns_step(uf, pf, dt, case.Re, T, 1)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            its.append(sum(g.ib_iterations()))
+        out["ms_per_step_" + name] = ms / steps
+        out["cg_iterations_per_step_" + name] = float(np.mean(its))
+        out["octants"], out["leaves"], out["ib_points"] = int(g.n), int(np.count_nonzero(g.leaf)), len(X)
+        res[name] = np.stack([g.download(uf[k]) for k in range(3)])
+        g.close()
+    out.update({"dt": dt, "steps": steps, "warmup": warmup,
+                "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
+                "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
+    return out
+
+
+def sphere_points(dx_base, ib_level, ibph):
+    """IB points on the sphere R = 0.5 (ib.hpp:179-210), Fibonacci order."""
+    dx = dx_base / 2 ** ib_level * ibph
+    n = int(np.floor(np.pi / (dx * dx * 0.86602540378))) + 1
+    lam = (1.0 + np.sqrt(5.0)) / 2.0
+    x = np.arange(n) + 0.5
+    phi = np.arccos(1.0 - 2 * x / n)
+    theta = 2 * np.pi * x / lam
+    return np.stack([0.5 * np.cos(theta) * np.sin(phi), 0.5 * np.sin(theta) * np.sin(phi), 0.5 * np.cos(phi)], 1)
 
 
 def batch_bench(B, stream, device, steps, warmup):

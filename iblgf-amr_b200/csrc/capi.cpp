@@ -385,12 +385,9 @@ int iblgf_ns_options(iblgf_ctx* x, const double* frame_vel, double cg_threshold,
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ns_options(c, frame_vel, cg_threshold, cg_max_iter); });
 }
 
-int iblgf_ib_force(iblgf_ctx* x, int stage, double* out)
+int iblgf_ib_force(iblgf_ctx* x, int stage, double* out, int* iters)
 {
-    return guard(x, [&](iblgf_b200::Ctx& c) {
-        if (!out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
-        iblgf_b200::ib_force(c, stage, out);
-    });
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_force(c, stage, out, iters); });
 }
 
 int iblgf_ib_set_points(iblgf_ctx* x, int n, const double* coords, double Re)

@@ -286,7 +286,7 @@ bool ib_active(const Ctx& c);
 const int* ib_face_aux2(Ctx& c);
 void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
                  const std::function<void()>& gradient_d);
-void ib_force(Ctx& c, int stage, double* out);
+void ib_force(Ctx& c, int stage, double* out, int* iters);
 void ib_release(const Ctx* c);
 void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const long long* at, const double* w,
                           int n, double* f);

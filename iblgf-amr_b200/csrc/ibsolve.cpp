@@ -60,6 +60,7 @@ struct IbState
     int face_aux[3] = {-1, -1, -1}, face_aux2[3] = {-1, -1, -1}, cell_aux2 = -1;
     DevBuf<double> d_f;  // 3 n forces (smearing input / projection output)
     std::vector<double> force_prev[4];  // IB::force_prev per IF-HERK stage (CG warm start)
+    int iters[4] = {0, 0, 0, 0};        // CG iterations of the last step's stages
 };
 std::map<const Ctx*, std::unique_ptr<IbState>> g_ib;
 
@@ -325,7 +326,7 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
 {
     IbState& s = state(c);
     std::vector<double> f = s.force_prev[stage];
-    ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), nullptr);
+    ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
     s.force_prev[stage] = f;
     // LinSysSolver::pressure_correction (linsys.hpp:131-145)
     OpLists& ol = op_lists(c);
@@ -344,11 +345,13 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
     smearing(c, s, f, face_aux, false);
 }
 
-void ib_force(Ctx& c, int stage, double* out)
+void ib_force(Ctx& c, int stage, double* out, int* iters)
 {
     IbState& s = state(c);
     if (stage < 1 || stage > 3) throw Error(IBLGF_EINVAL, "stage must be 1, 2 or 3");
-    for (size_t i = 0; i < s.force_prev[stage].size(); ++i) out[i] = s.force_prev[stage][i];
+    if (out)
+        for (size_t i = 0; i < s.force_prev[stage].size(); ++i) out[i] = s.force_prev[stage][i];
+    if (iters) *iters = s.iters[stage];
 }
 
 void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters)

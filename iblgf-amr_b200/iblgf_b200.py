@@ -91,7 +91,7 @@ def lib():
     L.iblgf_ib_flags.argtypes = [vp, vp]
     L.iblgf_ib_solve.argtypes = [vp, vp, cd, cd, ci, vp, vp]
     L.iblgf_ns_options.argtypes = [vp, vp, cd, ci]
-    L.iblgf_ib_force.argtypes = [vp, ci, vp]
+    L.iblgf_ib_force.argtypes = [vp, ci, vp, vp]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -278,7 +278,16 @@ class Solver:
 
     def ib_force(self, stage):
         out = np.zeros((len(self._ib_X), 3))
-        self._check(lib().iblgf_ib_force(self.h, int(stage), _p(out)))
+        self._check(lib().iblgf_ib_force(self.h, int(stage), _p(out), None))
+        return out
+
+    def ib_iterations(self):
+        """CG iterations of stages 1..3 of the last step."""
+        out = []
+        for st in (1, 2, 3):
+            it = ctypes.c_int()
+            self._check(lib().iblgf_ib_force(self.h, st, None, ctypes.byref(it)))
+            out.append(it.value)
         return out
 
     def ib_set_points(self, X, Re):

@@ -157,8 +157,9 @@ int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, d
  * each stage of iblgf_ns_step runs lin_sys_with_ib_solve with the IB
  * (ifherk.hpp:1451-1517), warm-started from that stage's previous force. */
 int iblgf_ns_options(iblgf_ctx* ctx, const double* frame_vel, double cg_threshold, int cg_max_iter);
-/* IB force of the last step's stage 1, 2 or 3 (IB::force_prev), n x 3 */
-int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out);
+/* IB force (IB::force_prev, n x 3) and CG iteration count of the last
+ * step's stage 1, 2 or 3; either output may be NULL */
+int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out, int* iters);
 
 /* ---- immersed boundary (ib.hpp, linsys.hpp) ------------------------------
  * iblgf_ib_set_points: the IB points (n x 3 coordinates, the reference's
