@@ -390,6 +390,29 @@ int iblgf_ib_force(iblgf_ctx* x, int stage, double* out, int* iters)
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_force(c, stage, out, iters); });
 }
 
+int iblgf_ib_warmstart(iblgf_ctx* x, int mode, int train_steps, int epochs, double lr, unsigned seed)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_warmstart(c, mode, train_steps, epochs, lr, seed); });
+}
+
+int iblgf_ib_warmstart_info(iblgf_ctx* x, double* info)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!info) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        iblgf_b200::ib_warmstart_info(c, info);
+    });
+}
+
+int iblgf_ws_check(iblgf_ctx* x, int n_samples, int n_points, const float* params, const float* inputs,
+                   const float* targets, float* outputs, float* grads, float* loss)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (n_samples <= 0 || n_points <= 0 || !params || !inputs || !targets || !outputs || !grads || !loss)
+            throw iblgf_b200::Error(IBLGF_EINVAL, "bad arguments");
+        iblgf_b200::ws_check(c, n_samples, n_points, params, inputs, targets, outputs, grads, loss);
+    });
+}
+
 int iblgf_ib_set_points(iblgf_ctx* x, int n, const double* coords, double Re)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_set_points(c, n, coords, Re); });

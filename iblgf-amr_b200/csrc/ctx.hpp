@@ -293,6 +293,18 @@ void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const 
 void launch_ib_smearing(Ctx& c, double* const* u, const long long* node_at, const int* nptr, const int* npt,
                         const int* nent, const double* w, int n_nodes, const double* f);
 void launch_face_planes(Ctx& c, double* f, const int* list, const unsigned char* faces, int n, int width);
+// learned warm start network (warmstart.cu)
+constexpr int kWsChannels = 64, kWsInputs = 9;
+void ws_offsets(int* off);  // 7 offsets: W1 b1 W2 b2 W3 b3 end
+void ws_forward(Ctx& c, const float* params, const float* x, int S, int N, float* h1, float* h2, float* y);
+float ws_backward(Ctx& c, const float* params, const float* x, const float* tgt, int S, int N, const float* h1,
+                  const float* h2, const float* y, float* dy, float* dh2, float* dh1, float* grads,
+                  DevBuf<float>& partial);
+void ws_adam(Ctx& c, float* params, const float* grads, float* m, float* v, int n, float lr, int step);
+void ib_warmstart(Ctx& c, int mode, int train_steps, int epochs, double lr, unsigned seed);
+void ib_warmstart_info(Ctx& c, double* info);
+void ws_check(Ctx& c, int S, int N, const float* params, const float* x, const float* tgt, float* y, float* grads,
+              float* loss);
 int ge_table(Ctx& c, double alpha);
 // rp: relative position per axis of the field's mesh object (cell {1,1,1} when null)
 void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const int* rp = nullptr);

@@ -11,10 +11,12 @@
 // Schur operator's divergence, masked LGF solve, gradient and integrating
 // factor are the library's own kernels on device fields. CG vectors and dot
 // products are FP64 on the host (3 n values per iteration).
+#include <algorithm>
 #include <cmath>
 #include <functional>
 #include <map>
 #include <memory>
+#include <random>
 
 #include "ctx.hpp"
 
@@ -37,6 +39,24 @@ double yang3(double x)
            (2.0 * r - 3.0) / 48.0 * std::sqrt(-12.0 * r2 + 36.0 * r - 23.0) +
            s3 / 36.0 * std::asin(s3 / 2.0 * (2 * r - 3.0));
 }
+
+// learned warm start (see warmstart.cu): samples of the first train_steps
+// steps, then a network trained on them predicts f0 - f_prev per stage
+struct WarmStart
+{
+    int mode = 0;  // 0: previous step's force of the stage (the reference), 1: learned
+    int train_steps = 0, epochs = 0, steps_seen = 0, n_params = 0;
+    float lr = 1e-3f;
+    unsigned seed = 1;
+    bool trained = false;
+    float loss_first = 0.0f, loss_last = 0.0f, sb = 1.0f, sf = 1.0f;
+    std::vector<std::vector<double>> s_duc, s_fprev, s_dfp, s_f;  // samples
+    std::vector<double> f_prev2[4];                          // force two steps back per stage
+    float sd = 1.0f, st = 1.0f;  // input / target scales
+    std::vector<double> uc_prev[4];                          // right-hand side of the previous step per stage
+    std::vector<int> order;                                  // network position -> IB point (Morton order)
+    DevBuf<float> params, grads, m, v, x, t, h1, h2, y, dy, dh1, dh2, partial;
+};
 
 struct IbState
 {
@@ -61,6 +81,7 @@ struct IbState
     DevBuf<double> d_f;  // 3 n forces (smearing input / projection output)
     std::vector<double> force_prev[4];  // IB::force_prev per IF-HERK stage (CG warm start)
     int iters[4] = {0, 0, 0, 0};        // CG iterations of the last step's stages
+    WarmStart ws;
 };
 std::map<const Ctx*, std::unique_ptr<IbState>> g_ib;
 
@@ -315,6 +336,215 @@ void et_h_s_e(Ctx& c, IbState& s, const std::vector<double>& fin, std::vector<do
 
 bool ib_active(const Ctx& c) { return g_ib.count(&c) != 0; }
 
+namespace
+{
+void ws_init(WarmStart& w, Ctx& c)
+{
+    int o[7];
+    ws_offsets(o);
+    w.n_params = o[6];
+    std::vector<float> p(o[6], 0.0f);
+    std::mt19937 rng(w.seed);
+    const int C = kWsChannels;
+    auto fill = [&](int a, int b, int fan_in, float gain) {
+        std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+        const float bound = gain / std::sqrt((float)fan_in);
+        for (int i = a; i < b; ++i) p[i] = bound * U(rng);
+    };
+    fill(o[0], o[1], kWsInputs * 5, std::sqrt(6.0f));
+    fill(o[2], o[3], C * 5, std::sqrt(6.0f));
+    fill(o[4], o[5], C * 5, 0.1f);
+    w.params.upload(p, c.stream);
+    std::vector<float> z(o[6], 0.0f);
+    w.grads.upload(z, c.stream);
+    w.m.upload(z, c.stream);
+    w.v.upload(z, c.stream);
+}
+
+// x [S][9][N] = ((uc - uc_prev) / sb, f_prev / sf, (f_prev - f_prev2) / sd),
+// points in network order
+std::vector<float> ws_inputs(const WarmStart& w, const std::vector<const std::vector<double>*>& duc,
+                             const std::vector<const std::vector<double>*>& fp,
+                             const std::vector<const std::vector<double>*>& dfp, int N)
+{
+    const int I = kWsInputs;
+    std::vector<float> x(duc.size() * I * (size_t)N);
+    for (size_t s_ = 0; s_ < duc.size(); ++s_)
+        for (int ch = 0; ch < 3; ++ch)
+            for (int q = 0; q < N; ++q)
+            {
+                const int i = w.order[q];
+                x[(s_ * I + ch) * N + q] = (float)((*duc[s_])[3 * i + ch] / w.sb);
+                x[(s_ * I + 3 + ch) * N + q] = (float)((*fp[s_])[3 * i + ch] / w.sf);
+                x[(s_ * I + 6 + ch) * N + q] = (float)((*dfp[s_])[3 * i + ch] / w.sd);
+            }
+    return x;
+}
+
+void ws_train(Ctx& c, WarmStart& w, int N)
+{
+    const int S = (int)w.s_duc.size();
+    if (!S) return;
+    double sb = 0, sf = 0, sd = 0;
+    for (int s_ = 0; s_ < S; ++s_)
+        for (int i = 0; i < 3 * N; ++i)
+        {
+            sb += w.s_duc[s_][i] * w.s_duc[s_][i];
+            sf += w.s_f[s_][i] * w.s_f[s_][i];
+            sd += w.s_dfp[s_][i] * w.s_dfp[s_][i];
+        }
+    w.sd = (float)std::sqrt(sd / (S * 3.0 * N));
+    if (!(w.sd > 0)) w.sd = 1.0f;
+    double st = 0;
+    for (int s_ = 0; s_ < S; ++s_)
+        for (int i = 0; i < 3 * N; ++i)
+        {
+            const double d = w.s_f[s_][i] - w.s_fprev[s_][i];
+            st += d * d;
+        }
+    w.st = (float)std::sqrt(st / (S * 3.0 * N));
+    if (!(w.st > 0)) w.st = 1.0f;
+    w.sb = (float)std::sqrt(sb / (S * 3.0 * N));
+    w.sf = (float)std::sqrt(sf / (S * 3.0 * N));
+    if (!(w.sb > 0)) w.sb = 1.0f;
+    if (!(w.sf > 0)) w.sf = 1.0f;
+    std::vector<const std::vector<double>*> duc, fp, dfp;
+    for (int s_ = 0; s_ < S; ++s_)
+    {
+        duc.push_back(&w.s_duc[s_]);
+        fp.push_back(&w.s_fprev[s_]);
+        dfp.push_back(&w.s_dfp[s_]);
+    }
+    std::vector<float> x = ws_inputs(w, duc, fp, dfp, N), t(S * 3 * (size_t)N);
+    for (int s_ = 0; s_ < S; ++s_)
+        for (int ch = 0; ch < 3; ++ch)
+            for (int q = 0; q < N; ++q)
+            {
+                const int i = w.order[q];
+                t[((size_t)s_ * 3 + ch) * N + q] =
+                    (float)((w.s_f[s_][3 * i + ch] - w.s_fprev[s_][3 * i + ch]) / w.st);
+            }
+    w.x.upload(x, c.stream);
+    w.t.upload(t, c.stream);
+    const size_t hs = (size_t)S * kWsChannels * N;
+    w.h1.alloc(hs);
+    w.h2.alloc(hs);
+    w.dh1.alloc(hs);
+    w.dh2.alloc(hs);
+    w.y.alloc((size_t)S * 3 * N);
+    w.dy.alloc((size_t)S * 3 * N);
+    for (int ep = 0; ep < w.epochs; ++ep)
+    {
+        ws_forward(c, w.params.p, w.x.p, S, N, w.h1.p, w.h2.p, w.y.p);
+        const float l = ws_backward(c, w.params.p, w.x.p, w.t.p, S, N, w.h1.p, w.h2.p, w.y.p, w.dy.p, w.dh2.p,
+                                    w.dh1.p, w.grads.p, w.partial);
+        if (ep == 0) w.loss_first = l;
+        w.loss_last = l;
+        ws_adam(c, w.params.p, w.grads.p, w.m.p, w.v.p, w.n_params, w.lr, ep + 1);
+    }
+    w.trained = true;
+}
+
+// f0 = f_prev + st * net(...), st the rms of f - f_prev in the samples
+std::vector<double> ws_predict(Ctx& c, WarmStart& w, const std::vector<double>& duc, const std::vector<double>& fp,
+                               const std::vector<double>& dfp, int N)
+{
+    std::vector<float> x = ws_inputs(w, {&duc}, {&fp}, {&dfp}, N);
+    DevBuf<float> dx, h1, h2, y;
+    dx.upload(x, c.stream);
+    h1.alloc((size_t)kWsChannels * N);
+    h2.alloc((size_t)kWsChannels * N);
+    y.alloc(3 * (size_t)N);
+    ws_forward(c, w.params.p, dx.p, 1, N, h1.p, h2.p, y.p);
+    std::vector<float> hy(3 * (size_t)N);
+    IBLGF_CUDA(cudaMemcpyAsync(hy.data(), y.p, hy.size() * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<double> f0(fp);
+    for (int ch = 0; ch < 3; ++ch)
+        for (int q = 0; q < N; ++q) f0[3 * w.order[q] + ch] += (double)w.st * hy[(size_t)ch * N + q];
+    return f0;
+}
+}  // namespace
+
+void ib_warmstart(Ctx& c, int mode, int train_steps, int epochs, double lr, unsigned seed)
+{
+    IbState& s = state(c);
+    if (mode != 0 && mode != 1) throw Error(IBLGF_EINVAL, "warm-start mode must be 0 or 1");
+    if (mode == 1 && (train_steps <= 0 || epochs <= 0 || !(lr > 0)))
+        throw Error(IBLGF_EINVAL, "learned warm start needs train_steps, epochs and lr > 0");
+    WarmStart& w = s.ws;
+    w = WarmStart();
+    w.mode = mode;
+    w.train_steps = train_steps;
+    w.epochs = epochs;
+    w.lr = (float)lr;
+    w.seed = seed;
+    // network order: Morton order of the points (10 bits per axis over their
+    // bounding box), so that the convolution's neighbours are spatial ones
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < s.n; ++i)
+        for (int q = 0; q < 3; ++q)
+        {
+            lo[q] = std::min(lo[q], s.X[3 * i + q]);
+            hi[q] = std::max(hi[q], s.X[3 * i + q]);
+        }
+    std::vector<std::pair<unsigned long long, int>> key(s.n);
+    for (int i = 0; i < s.n; ++i)
+    {
+        unsigned long long k = 0;
+        unsigned v[3];
+        for (int q = 0; q < 3; ++q)
+        {
+            const double span = hi[q] > lo[q] ? hi[q] - lo[q] : 1.0;
+            v[q] = (unsigned)std::min(1023.0, std::floor((s.X[3 * i + q] - lo[q]) / span * 1023.0));
+        }
+        for (int b = 9; b >= 0; --b)
+            for (int q = 2; q >= 0; --q) k = (k << 1) | ((v[q] >> b) & 1u);
+        key[i] = {k, i};
+    }
+    std::sort(key.begin(), key.end());
+    w.order.resize(s.n);
+    for (int q = 0; q < s.n; ++q) w.order[q] = key[q].second;
+    if (mode == 1) ws_init(w, c);
+}
+
+void ib_warmstart_info(Ctx& c, double* info)
+{
+    IbState& s = state(c);
+    const WarmStart& w = s.ws;
+    info[0] = w.mode;
+    info[1] = w.trained ? 1 : 0;
+    info[2] = (double)w.s_duc.size();
+    info[3] = w.loss_first;
+    info[4] = w.loss_last;
+    info[5] = w.n_params;
+}
+
+void ws_check(Ctx& c, int S, int N, const float* params, const float* x, const float* tgt, float* y, float* grads,
+              float* loss)
+{
+    int o[7];
+    ws_offsets(o);
+    DevBuf<float> dp, dx, dt, h1, h2, dy_, yy, dh1, dh2, g, part;
+    dp.upload(std::vector<float>(params, params + o[6]), c.stream);
+    dx.upload(std::vector<float>(x, x + (size_t)S * kWsInputs * N), c.stream);
+    dt.upload(std::vector<float>(tgt, tgt + (size_t)S * 3 * N), c.stream);
+    const size_t hs = (size_t)S * kWsChannels * N;
+    h1.alloc(hs);
+    h2.alloc(hs);
+    dh1.alloc(hs);
+    dh2.alloc(hs);
+    yy.alloc((size_t)S * 3 * N);
+    dy_.alloc((size_t)S * 3 * N);
+    g.alloc(o[6]);
+    ws_forward(c, dp.p, dx.p, S, N, h1.p, h2.p, yy.p);
+    const float l = ws_backward(c, dp.p, dx.p, dt.p, S, N, h1.p, h2.p, yy.p, dy_.p, dh2.p, dh1.p, g.p, part);
+    IBLGF_CUDA(cudaMemcpyAsync(y, yy.p, (size_t)S * 3 * N * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaMemcpyAsync(grads, g.p, o[6] * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    *loss = l;
+}
+
 const int* ib_face_aux2(Ctx& c) { return state(c).face_aux2; }
 
 // lin_sys_with_ib_solve's IB part (ifherk.hpp:1474-1494) after face_aux2 =
@@ -325,8 +555,34 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
                  const std::function<void()>& gradient_d)
 {
     IbState& s = state(c);
+    WarmStart& w = s.ws;
     std::vector<double> f = s.force_prev[stage];
-    ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
+    if (w.mode == 1)
+    {
+        std::vector<double> uc, duc, dfp(s.force_prev[stage]);
+        projection(c, s, s.face_aux2, uc);
+        duc = uc;
+        if (!w.uc_prev[stage].empty())
+            for (size_t i = 0; i < duc.size(); ++i) duc[i] -= w.uc_prev[stage][i];
+        if (!w.f_prev2[stage].empty())
+            for (size_t i = 0; i < dfp.size(); ++i) dfp[i] -= w.f_prev2[stage][i];
+        if (w.trained) f = ws_predict(c, w, duc, s.force_prev[stage], dfp, s.n);
+        ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
+        // samples from steps that have a previous force (the first step's
+        // "change" is the whole force and would set the target scale)
+        if (!w.trained && !w.uc_prev[stage].empty())
+        {
+            w.s_duc.push_back(duc);
+            w.s_fprev.push_back(s.force_prev[stage]);
+            w.s_dfp.push_back(dfp);
+            w.s_f.push_back(f);
+            if (stage == 3 && ++w.steps_seen >= w.train_steps) ws_train(c, w, s.n);
+        }
+        w.uc_prev[stage] = uc;
+        w.f_prev2[stage] = s.force_prev[stage];
+    }
+    else
+        ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
     s.force_prev[stage] = f;
     // LinSysSolver::pressure_correction (linsys.hpp:131-145)
     OpLists& ol = op_lists(c);

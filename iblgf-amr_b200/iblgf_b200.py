@@ -37,7 +37,8 @@ EXPORTS = [
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
-    "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_conv_block", "iblgf_conv_block_noalloc",
+    "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_warmstart", "iblgf_ib_warmstart_info",
+    "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
     "iblgf_fma_peak",
 ]
@@ -92,6 +93,9 @@ def lib():
     L.iblgf_ib_solve.argtypes = [vp, vp, cd, cd, ci, vp, vp]
     L.iblgf_ns_options.argtypes = [vp, vp, cd, ci]
     L.iblgf_ib_force.argtypes = [vp, ci, vp, vp]
+    L.iblgf_ib_warmstart.argtypes = [vp, ci, ci, ci, cd, ctypes.c_uint]
+    L.iblgf_ib_warmstart_info.argtypes = [vp, vp]
+    L.iblgf_ws_check.argtypes = [vp, ci, ci, vp, vp, vp, vp, vp, vp]
     L.iblgf_conv_block_noalloc.argtypes = [vp, vp, vp, vp, cd]
     L.iblgf_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_profile.argtypes = [vp, ci]
@@ -289,6 +293,27 @@ class Solver:
             self._check(lib().iblgf_ib_force(self.h, st, None, ctypes.byref(it)))
             out.append(it.value)
         return out
+
+    def ib_warmstart(self, mode, train_steps=0, epochs=0, lr=1e-3, seed=1):
+        self._check(lib().iblgf_ib_warmstart(self.h, int(mode), int(train_steps), int(epochs), float(lr), int(seed)))
+
+    def ib_warmstart_info(self):
+        out = np.zeros(6)
+        self._check(lib().iblgf_ib_warmstart_info(self.h, _p(out)))
+        return {"mode": int(out[0]), "trained": bool(out[1]), "samples": int(out[2]), "loss_first": out[3],
+                "loss_last": out[4], "params": int(out[5])}
+
+    def ws_check(self, params, x, t):
+        """One forward + backward pass of the warm-start network on the device."""
+        S, _, N = x.shape
+        p = np.ascontiguousarray(params, np.float32)
+        xx = np.ascontiguousarray(x, np.float32)
+        tt = np.ascontiguousarray(t, np.float32)
+        y = np.zeros((S, 3, N), np.float32)
+        g = np.zeros_like(p)
+        loss = ctypes.c_float()
+        self._check(lib().iblgf_ws_check(self.h, S, N, _p(p), _p(xx), _p(tt), _p(y), _p(g), ctypes.byref(loss)))
+        return y, g, loss.value
 
     def ib_set_points(self, X, Re):
         """IB points (n, 3) on the finest level (ib.hpp / server.hpp / client.hpp)."""

@@ -177,6 +177,27 @@ int iblgf_ib_flags(iblgf_ctx* ctx, int* flags);
 int iblgf_ib_solve(iblgf_ctx* ctx, const int* u_fields, double alpha, double threshold, int max_iter,
                    double* force, int* iters);
 
+/* ---- learned warm start of the IB force CG (no reference counterpart: the
+ * reference warm-starts from IB::force_prev, ifherk.hpp:1476) -------------
+ * mode 0: previous step's force of the stage (the reference). mode 1: the
+ * first IF-HERK step and the next train_steps steps run with mode 0; those
+ * train_steps steps record (change of the
+ * CG right-hand side since the previous step, previous force, its last
+ * change, solution) per stage; a 1-D convolutional network over the IB points
+ * in Morton order of their coordinates (9 -> 64 -> 64 -> 3 channels, kernel 5,
+ * 24 451 FP32 parameters,
+ * seeded initialisation) is then trained on them (full-batch Adam, `epochs`
+ * steps, learning rate lr, on the device) and from then on predicts the
+ * initial guess f_prev + correction; CG runs to the unchanged tolerance.
+ * iblgf_ib_warmstart_info: [mode, trained, samples, first loss, last loss,
+ * parameters]. iblgf_ws_check: one forward + backward pass of the network
+ * for given parameters (layout W1 b1 W2 b2 W3 b3), inputs [S][9][N] and
+ * targets [S][3][N]; outputs [S][3][N], gradients and the mean squared loss. */
+int iblgf_ib_warmstart(iblgf_ctx* ctx, int mode, int train_steps, int epochs, double lr, unsigned seed);
+int iblgf_ib_warmstart_info(iblgf_ctx* ctx, double* info);
+int iblgf_ws_check(iblgf_ctx* ctx, int n_samples, int n_points, const float* params, const float* inputs,
+                   const float* targets, float* outputs, float* grads, float* loss);
+
 /* ---- batches of independent problems -----------------------------------
  * Many unbounded Poisson problems of uneven size solved together: each is
  * PoissonSolver::apply_lgf (poisson.hpp:587-894) on its own octree
