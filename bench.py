@@ -364,17 +364,21 @@ def ib_bench(B, stream, device, steps, warmup):
     import torch
     case = S.SphereIB("c5")
     out = {"workload": "sphere D=1, Re=300, uniform stream, dx_finest=D/40, 16^3 blocks, 3 mesh levels, "
-                       "2009 IB points, CG threshold 1e-3, max 40"}
+                       "2009 IB points, CG threshold 1e-3, max 40; warm start: previous force per stage "
+                       "(reference) and the learned 1-D conv net (fp32_learned)"}
     dt = 0.35 * case.dx_base / 4 / 1.0
     res = {}
-    for name, prec in (("fp32", B.FP32), ("fp64", B.FP64)):
+    for name, prec, learned in (("fp32", B.FP32, False), ("fp64", B.FP64, False), ("fp32_learned", B.FP32, True)):
         g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                      n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=device,
                      stream=stream.cuda_stream)
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
         X = sphere_points(case.dx_base, g.depth - 1 - g.base_level, case.ibph)
         g.ib_set_points(X, case.Re)
         g.ns_options((-1.0, 0.0, 0.0))
+        if learned:
+            # the first step and `warmup` more run with the previous force and
+            # record samples; the network is trained before the timed steps
+            g.ib_warmstart(1, train_steps=max(warmup - 1, 1), epochs=1000, lr=2e-3, seed=7)
         u0 = case.velocity(g, U=(0.0, 0.0, 0.0))
         uf = [g.field(u0[k]) for k in range(3)]
         pf = g.field()
@@ -394,6 +398,9 @@ def ib_bench(B, stream, device, steps, warmup):
             its.append(sum(g.ib_iterations()))
         out["ms_per_step_" + name] = ms / steps
         out["cg_iterations_per_step_" + name] = float(np.mean(its))
+        if learned:
+            out["warm_start_training"] = g.ib_warmstart_info()
+            continue
         out["octants"], out["leaves"], out["ib_points"] = int(g.n), int(np.count_nonzero(g.leaf)), len(X)
         res[name] = np.stack([g.download(uf[k]) for k in range(3)])
         g.close()

@@ -162,3 +162,20 @@ def test_ns_step_oracle_projects_and_conserves_scale():
     du = float(np.abs(u1 - u0)[:, lf].max())
     assert 0.0 < du < 0.1 * float(np.abs(u0[:, lf]).max())
     assert np.isfinite(p).all()
+
+
+def test_ib_solve_oracle_converges_on_sphere():
+    """IB force solve (linsys.hpp:113-230) on the sphere: the CG reaches its
+    threshold well before the iteration limit, IB blocks sit at the finest
+    level, and the velocity at the points left after the solve is small."""
+    case = S.SphereIB("small")
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    X = O.sphere_points(case.dx_base, d.depth - 1 - d.base_level, case.ibph)
+    assert len(X) == 413
+    u = case.velocity(d)
+    f, flags, it = d.ib_solve(X, case.Re, u, 0.0, 1e-3, 40)
+    assert 0 < it < 40
+    fin = d.levels == d.depth - 1
+    assert (flags[fin] & 1).sum() > 0 and np.all((flags[~fin] & 2) == 0)
+    assert np.isfinite(f).all() and np.abs(f).max() > 0
