@@ -8,6 +8,8 @@
 // factor solves, the mimetic operators, buffer exchanges and level transfers
 // are the library's own kernels, with no host round trip inside a step.
 //
+// Steps without an immersed boundary replay a CUDA graph of one captured step
+// once a direct step with the same fields, dt and Re has run.
 // Scope: no immersed boundary (the Schur-complement solve, smearing and the
 // IB2xIB / IB2AMR pieces act on an empty point set and change none of the
 // fields the step reads), no adaptation, no body force, frame velocity 0.
@@ -58,7 +60,22 @@ struct NsState
     DevBuf<int> sm_list[2], sm_ptr[2], sm_dirs[2];
     int sm_n[2] = {0, 0};
     double T_last_vel_refresh = 0.0;  // ifherk.hpp:1980
+    // one captured time step (steps without an immersed boundary): replayed
+    // while the velocity / pressure fields, dt and Re stay the same
+    cudaGraphExec_t graph = nullptr;
+    int g_u[3] = {-1, -1, -1}, g_p = -1;
+    double g_dt = 0.0, g_Re = 0.0;
+    bool graph_failed = false;
+    int steps_done = 0;
+    long long graph_launches = 0;
+    // (u, p, dt, Re) of the last step run with direct launches: a capture
+    // needs one such step first, so that every plan, table and buffer the
+    // step uses exists before capturing
+    int w_u[3] = {-1, -1, -1}, w_p = -1;
+    double w_dt = 0.0, w_Re = 0.0;
 };
+
+long long st_launches(const NsState& s) { return s.graph_launches; }
 // per context: constant frame velocity and IB CG settings (set any time)
 struct NsOptions
 {
@@ -387,7 +404,66 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
     {
         if ((*T - s.T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
             throw Error(IBLGF_EINVAL, "velocity refresh (pad_velocity) branch is not supported");
-        st.time_step(uf, pf);
+        const bool graphable = !ib_active(c) && !c.profile && !s.graph_failed;
+        const bool same = s.graph && s.g_p == p && s.g_dt == dt && s.g_Re == Re && s.g_u[0] == u[0] &&
+                          s.g_u[1] == u[1] && s.g_u[2] == u[2];
+        if (graphable && same)
+        {
+            IBLGF_CUDA(cudaGraphLaunch(s.graph, c.stream));
+            c.launches += st_launches(s);
+        }
+        else if (graphable && s.w_p == p && s.w_dt == dt && s.w_Re == Re && s.w_u[0] == u[0] &&
+                 s.w_u[1] == u[1] && s.w_u[2] == u[2])
+        {
+            // capture after a first direct step has built every plan and sized
+            // every buffer, so the step makes no host synchronisation
+            if (s.graph)
+            {
+                cudaGraphExecDestroy(s.graph);
+                s.graph = nullptr;
+            }
+            const long long l0 = c.launches;
+            cudaGraph_t g = nullptr;
+            IBLGF_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+            bool ok = true;
+            try
+            {
+                st.time_step(uf, pf);
+            }
+            catch (const Error&)
+            {
+                ok = false;
+            }
+            const cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+            if (!ok || e != cudaSuccess || !g || cudaGraphInstantiate(&s.graph, g, 0) != cudaSuccess)
+            {
+                cudaGetLastError();
+                if (g) cudaGraphDestroy(g);
+                s.graph = nullptr;
+                s.graph_failed = true;
+                c.launches = l0;
+                st.time_step(uf, pf);  // nothing of the failed capture ran
+            }
+            else
+            {
+                cudaGraphDestroy(g);
+                s.graph_launches = c.launches - l0;
+                for (int k = 0; k < 3; ++k) s.g_u[k] = u[k];
+                s.g_p = p;
+                s.g_dt = dt;
+                s.g_Re = Re;
+                IBLGF_CUDA(cudaGraphLaunch(s.graph, c.stream));
+            }
+        }
+        else
+        {
+            st.time_step(uf, pf);
+            for (int k = 0; k < 3; ++k) s.w_u[k] = u[k];
+            s.w_p = p;
+            s.w_dt = dt;
+            s.w_Re = Re;
+        }
+        ++s.steps_done;
         *T += dt;
     }
     IBLGF_CUDA(cudaGetLastError());
@@ -404,6 +480,8 @@ void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max
 
 void ns_release(const Ctx* c)
 {
+    auto it = g_ns.find(c);
+    if (it != g_ns.end() && it->second->graph) cudaGraphExecDestroy(it->second->graph);
     g_ns.erase(c);
     g_nsopt.erase(c);
 }
