@@ -285,6 +285,11 @@ def main():
                 "frac": bytes_alg / t_k / 1e9 / hbm, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
     roof.update({"kernel": names[k], "traffic": None, "phase_ms_per_step": dict(zip(names, per_step.tolist())),
                  "algorithmic_flops": flops, "algorithmic_bytes": bytes_alg})
+    if k == 1:
+        # products the MAC kernels execute (whole sibling groups) vs the pair list
+        nexec = int(stats[8]) / args.steps
+        roof.update({"executed_products_per_step": nexec, "pair_share_of_executed": npairs / max(nexec, 1),
+                     "executed_tflops": 8.0 * nc * nexec / t_k / 1e12})
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -100,6 +100,7 @@ HostPlan merge_plans(const std::vector<std::pair<HostPlan, int>>& parts)
         m.pkey.insert(m.pkey.end(), h.pkey.begin(), h.pkey.end());
         m.all_keys.insert(m.all_keys.end(), h.all_keys.begin(), h.all_keys.end());
         m.n_pairs += h.n_pairs;
+        m.n_exec += h.n_exec;
     }
     m.n_csr_tgt = (int)m.tgt_list.size();
     for (size_t i = 0; i < parts.size(); ++i)
@@ -117,6 +118,7 @@ HostPlan merge_plans(const std::vector<std::pair<HostPlan, int>>& parts)
         append_off(m.ttab, h.ttab, tab_base);
         m.tcoarse.insert(m.tcoarse.end(), h.tcoarse.begin(), h.tcoarse.end());
         m.gsrc.insert(m.gsrc.end(), h.gsrc.begin(), h.gsrc.end());
+        m.gpm.insert(m.gpm.end(), h.gpm.begin(), h.gpm.end());
         for (int x : h.gtgt)
             m.gtgt.push_back(x < 0 ? -1 : (x < h.n_csr_tgt ? csrb[i] + x : grpb[i] + x - h.n_csr_tgt));
         m.n_groups += h.n_groups;

@@ -487,6 +487,14 @@ int iblgf_stats(iblgf_ctx* x, long long* out8)
     });
 }
 
+int iblgf_stats_n(iblgf_ctx* x, long long* out, int n)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!out || n < 1 || n > iblgf_b200::kNumStats) throw iblgf_b200::Error(IBLGF_EINVAL, "bad stats count");
+        for (int i = 0; i < n; ++i) out[i] = c.stats[i];
+    });
+}
+
 int iblgf_fma_peak(iblgf_ctx* x, int precision, double* tflops)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { *tflops = iblgf_b200::measure_fma_peak(c, precision); });

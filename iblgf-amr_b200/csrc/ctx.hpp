@@ -148,6 +148,8 @@ struct FmmPlan
     int n_tiles = 0, max_tile_src = 0, n_groups = 0;
     DevBuf<int> tile_gptr, tile_sptr, tile_src, tile_tab, tile_coarse, spec_u, grp_tgt;
     DevBuf<unsigned short> grp_src;
+    DevBuf<unsigned> grp_pm;     // per group: bit n set = neighbour parent n has a candidate
+    long long n_exec = 0;        // (target, source) products the MAC kernels execute
     bool empty() const { return n_tgt == 0; }
 };
 
@@ -171,15 +173,18 @@ struct HostPlan
     std::vector<std::array<int, 4>> all_keys;  // keys of every target's pairs: spectra to compute
     std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
     std::vector<unsigned short> gsrc;
+    std::vector<unsigned> gpm;
     std::vector<std::array<int, 4>> tab_keys;  // 343 per table
     int n_groups = 0, max_tile_src = 0, n_spec_unique = 0;
-    long long n_pairs = 0;
+    long long n_pairs = 0, n_exec = 0;
 };
 
 struct Field
 {
     DevBuf<double> d;
 };
+
+constexpr int kNumStats = 9;
 
 struct Ctx
 {
@@ -242,7 +247,9 @@ struct Ctx
     std::vector<std::array<cudaEvent_t, 5>> prof_events;
     // work counters since the last reset: sweeps, sources, targets, pairs,
     // unique spectra per sweep, anterpolation tasks, interpolation tasks
-    long long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // sweeps, sources, targets, pairs, unique spectra, anterp tasks, interp
+    // tasks, group-MAC targets, MAC products executed
+    long long stats[kNumStats] = {};
 
     // batch of independent problems (iblgf_batch_*): each problem's octree,
     // lists and masks live in a topology-only sub-context; fields, spectra and

@@ -199,69 +199,69 @@ __global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, c
 // k = (n, c')), and the offset of (child c, candidate (n, c')) is
 // u = c - c' - 2n in [-3,3]^3 (343 LGF spectra per tile).
 // For one neighbour parent n the 64 (c, c') pairs use only the 27 offsets
-// u = d - 2n, d = c - c' in [-1,1]^3, so the kernel walks n and, per z-slab
-// (c'z, cz), keeps the 9 spectra of that slab and the 4 sources with that c'z
-// in registers for 16 x M complex MACs.
+// u = d - 2n, d = c - c' in [-1,1]^3; the kernel walks n and, per dz = cz - c'z,
+// keeps the 9 spectra of that z-offset (shared by the slabs (c'z, cz) = (0, 0)
+// and (1, 1) at dz = 0) in registers for 16 or 32 complex MACs.
 // Adjacency filtering (coarse targets take only non-adjacent sources, the
 // integrating factor only adjacent ones) depends on u alone, so it is applied
 // once when the tile's spectra are staged: excluded offsets become zero rows.
-// One CTA = (tile of up to 32 sibling groups, chunk of F frequencies); the
-// tile's spectra (64-byte rows) and the groups' candidate rows live in shared
-// memory (~50 KB, four CTAs per SM); source spectra are read through L1/L2.
-// The 64 (c, c') sibling pairs of one neighbour parent n, z-slab by z-slab:
-// the 9 spectra of a slab stay in registers for 16 x M complex MACs. MASKED
-// skips the pairs a tile excludes (mode 1: adjacent ones, mode 2: all but the
-// adjacent ones); the conditions are uniform across the CTA.
-template<class R, int F, int M, bool MASKED>
-__device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&sv)[M][8], cx<R> (&acc)[M][8],
-                                                 int mode, int nx, int ny, int nz)
+// Tiles that take all or the non-adjacent pairs then run every pair (an
+// excluded pair adds exactly zero); tiles of adjacent pairs only (the
+// integrating factor, 27 of 216) skip the others.
+// One CTA = (tile of up to 32 sibling groups, chunk of F frequencies); each warp
+// takes one group at 32 consecutive frequencies, so a source load is one
+// contiguous 256-byte (FP32) or 512-byte (FP64) row segment. The tile's
+// spectra and the groups' candidate rows live in shared memory; source spectra
+// are read through L1/L2. Candidates that do not exist read a zero spectrum
+// row (zrow), and parents without any candidate are skipped via the group's
+// 27-bit mask (grp_pm).
+template<class R, int F, bool ADJ_ONLY>
+__device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&sv)[8], cx<R> (&acc)[8], int nx,
+                                                 int ny, int nz)
 {
 #pragma unroll
-    for (int cpz = 0; cpz < 2; ++cpz)
+    for (int dz = -1; dz <= 1; ++dz)
     {
+        if (ADJ_ONLY && abs(dz - 2 * nz) > 1) continue;
+        cx<R> gv[9];
 #pragma unroll
-        for (int cz = 0; cz < 2; ++cz)
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+                gv[(dy + 1) * 3 + dx + 1] = gn[(dx + 7 * dy + 49 * dz) * F];
+#pragma unroll
+        for (int cpz = 0; cpz < 2; ++cpz)
         {
-            const int dz = cz - cpz;
-            const bool adj_z = abs(dz - 2 * nz) <= 1;
-            if (MASKED && mode == 2 && !adj_z) continue;
-            cx<R> gv[9];
-#pragma unroll
-            for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-                for (int dx = -1; dx <= 1; ++dx)
-                    gv[(dy + 1) * 3 + dx + 1] = gn[(dx + 7 * dy + 49 * dz) * F];
+            const int cz = cpz + dz;
+            if (cz < 0 || cz > 1) continue;
 #pragma unroll
             for (int q = 0; q < 4; ++q)  // c' = 4 cpz + q
 #pragma unroll
                 for (int r = 0; r < 4; ++r)  // c = 4 cz + r
                 {
                     const int dx = (r & 1) - (q & 1), dy = (r >> 1) - (q >> 1);
-                    if (MASKED)
-                    {
-                        const bool adj = adj_z && abs(dx - 2 * nx) <= 1 && abs(dy - 2 * ny) <= 1;
-                        if (adj == (mode == 1)) continue;
-                    }
-                    const cx<R> g = gv[(dy + 1) * 3 + dx + 1];
-#pragma unroll
-                    for (int m = 0; m < M; ++m) cmac<R>(acc[m][4 * cz + r], g, sv[m][4 * cpz + q]);
+                    if (ADJ_ONLY && (abs(dx - 2 * nx) > 1 || abs(dy - 2 * ny) > 1)) continue;
+                    cmac<R>(acc[4 * cz + r], gv[(dy + 1) * 3 + dx + 1], sv[4 * cpz + q]);
                 }
         }
     }
 }
 
-template<class R, int F, int M>
-__global__ void __launch_bounds__(128, 4) group_mac_kernel(
-    const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, const int* __restrict__ tile_gptr,
-    const int* __restrict__ tile_sptr, const int* __restrict__ tile_src, const int* __restrict__ tile_tab,
-    const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
-    const unsigned short* __restrict__ grp_src, const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
+template<class R, int F, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
+    const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, int zrow,
+    const int* __restrict__ tile_gptr, const int* __restrict__ tile_sptr, const int* __restrict__ tile_src,
+    const int* __restrict__ tile_tab, const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
+    const unsigned short* __restrict__ grp_src, const unsigned* __restrict__ grp_pm,
+    const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
 {
-    static_assert(F * sizeof(cx<R>) == 64, "staged rows are 64 bytes");
-    constexpr int RW = 128 / F;
+    constexpr int RW = NT / F;      // thread rows, one group each per pass
+    constexpr int per = 16 / sizeof(cx<R>);
+    constexpr int parts = F / per;  // 16-byte pieces of a staged row
+    static_assert(F % 32 == 0 && NT % F == 0, "a warp covers one row");
     extern __shared__ __align__(16) unsigned char smraw[];
-    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);                              // [343][F]
-    int* Jr = reinterpret_cast<int*>(Gs + 343 * F);                          // [RW*M][216] source rows
+    cx<R>* Gs = reinterpret_cast<cx<R>*>(smraw);                      // [343][F]
+    int* Jr = reinterpret_cast<int*>(Gs + 343 * F);                  // [tile groups][216] source rows
     const int tile = blockIdx.x;
     const long long f0 = (long long)blockIdx.y * F;
     const int lane = threadIdx.x % F, row = threadIdx.x / F;
@@ -271,10 +271,9 @@ __global__ void __launch_bounds__(128, 4) group_mac_kernel(
     const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
     const cx<R> zero = mk<R>(0, 0);
     const bool full = f0 + F <= NC;
-    constexpr int per = 16 / sizeof(cx<R>);
-    for (int q = threadIdx.x; q < 343 * 4; q += blockDim.x)
+    for (int q = threadIdx.x; q < 343 * parts; q += blockDim.x)
     {
-        const int r = q >> 2, part = q & 3;
+        const int r = q / parts, part = q % parts;
         const int ux = r % 7 - 3, uy = (r / 7) % 7 - 3, uz = r / 49 - 3;
         const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
         const int slot = (mode == 1 && adj) || (mode == 2 && !adj) ? -1 : su[r];
@@ -286,67 +285,46 @@ __global__ void __launch_bounds__(128, 4) group_mac_kernel(
                 dst[e] = (src && f0 + part * per + e < NC) ? src[e] : zero;
     }
     __pipeline_commit();
-    for (int i = threadIdx.x; i < RW * M * 216; i += blockDim.x)
+    for (int i = threadIdx.x; i < kGroupTileCap * 216; i += blockDim.x)
     {
         const int g = g0 + i / 216;
         const unsigned short j = g < g1 ? grp_src[(size_t)g * 216 + (i % 216)] : (unsigned short)0xFFFF;
-        Jr[i] = j != 0xFFFF ? tile_src[s0 + j] : -1;
+        Jr[i] = j != 0xFFFF ? tile_src[s0 + j] : zrow;
     }
     __pipeline_wait_prior(0);
     __syncthreads();
     const long long f = f0 + lane;
     const long long fc = f < NC ? f : NC - 1;  // clamped column for the tail chunk
     const cx<R>* Sf = S + fc;
-    for (int gb = g0 + row * M; gb < g1; gb += RW * M)
+    for (int g = g0 + row; g < g1; g += RW)
     {
-        const int* jr = Jr + (gb - g0) * 216;
-        cx<R> acc[M][8];
+        const int* jr = Jr + (g - g0) * 216;
+        const unsigned pm = grp_pm[g];
+        cx<R> acc[8];
 #pragma unroll
-        for (int m = 0; m < M; ++m)
-#pragma unroll
-            for (int c = 0; c < 8; ++c) acc[m][c] = zero;
+        for (int c = 0; c < 8; ++c) acc[c] = zero;
         for (int n = 0; n < 27; ++n)
         {
-            int jj[M][8];
-            bool any = false;
+            if (!((pm >> n) & 1u)) continue;
+            const int4 ja = *reinterpret_cast<const int4*>(jr + 8 * n);
+            const int4 jb = *reinterpret_cast<const int4*>(jr + 8 * n + 4);
+            const int jj[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
+            cx<R> sv[8];
 #pragma unroll
-            for (int m = 0; m < M; ++m)
-#pragma unroll
-                for (int cp = 0; cp < 8; ++cp)
-                {
-                    jj[m][cp] = jr[m * 216 + n * 8 + cp];
-                    any = any || jj[m][cp] >= 0;
-                }
-            if (!any) continue;
+            for (int q = 0; q < 8; ++q) sv[q] = __ldg(Sf + (size_t)jj[q] * NC);
             // row of u = -2n; d = (dx, dy, dz) adds dx + 7 dy + 49 dz
             const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
             const cx<R>* gn = Gs + ((3 - 2 * nx) + 7 * (3 - 2 * ny) + 49 * (3 - 2 * nz)) * F + lane;
-            // all 8 x M source values of parent n in flight at once
-            cx<R> sv[M][8];
-#pragma unroll
-            for (int m = 0; m < M; ++m)
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                {
-                    const int j = jj[m][q];
-                    sv[m][q] = j >= 0 ? __ldg(Sf + (size_t)j * NC) : zero;
-                }
-            if (mode == 0) group_mac_parent<R, F, M, false>(gn, sv, acc, 0, nx, ny, nz);
-            else group_mac_parent<R, F, M, true>(gn, sv, acc, mode, nx, ny, nz);
+            if (mode == 2) group_mac_parent<R, F, true>(gn, sv, acc, nx, ny, nz);
+            else group_mac_parent<R, F, false>(gn, sv, acc, nx, ny, nz);
         }
         if (f < NC)
         {
 #pragma unroll
-            for (int m = 0; m < M; ++m)
+            for (int c = 0; c < 8; ++c)
             {
-                const int g = gb + m;
-                if (g >= g1) break;
-#pragma unroll
-                for (int c = 0; c < 8; ++c)
-                {
-                    const int t = grp_tgt[(size_t)g * 8 + c];
-                    if (t >= 0) ACC[(size_t)t * NC + f] = acc[m][c];
-                }
+                const int t = grp_tgt[(size_t)g * 8 + c];
+                if (t >= 0) ACC[(size_t)t * NC + f] = acc[c];
             }
         }
     }
@@ -494,21 +472,33 @@ struct Conv
         c.launches += 1;
     }
 
-    static constexpr int GF = std::is_same<R, float>::value ? 8 : 4;
-    static constexpr int GM = std::is_same<R, float>::value ? 2 : 1;  // rows x M = 32 groups per CTA
+#ifndef IBLGF_MAC_F32
+#define IBLGF_MAC_F32 64
+#define IBLGF_MAC_NT32 1024
+#define IBLGF_MAC_MINB32 1
+#endif
+#ifndef IBLGF_MAC_F64
+#define IBLGF_MAC_F64 32
+#define IBLGF_MAC_NT64 512
+#define IBLGF_MAC_MINB64 1
+#endif
+    static constexpr bool kF32 = std::is_same<R, float>::value;
+    static constexpr int GF = kF32 ? IBLGF_MAC_F32 : IBLGF_MAC_F64;
+    static constexpr int GNT = kF32 ? IBLGF_MAC_NT32 : IBLGF_MAC_NT64;
+    static constexpr int GMINB = kF32 ? IBLGF_MAC_MINB32 : IBLGF_MAC_MINB64;
 
+    // S holds p.n_src source spectra followed by one zero row
     static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc)
     {
         if (!p.n_tiles) return;
-        constexpr int RW = 128 / GF;
-        static_assert(RW * GM == kGroupTileCap, "one pass of thread rows covers a tile");
-        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)RW * GM * 216 * sizeof(int);
-        auto kfn = group_mac_kernel<R, GF, GM>;
+        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)kGroupTileCap * 216 * sizeof(int);
+        auto kfn = group_mac_kernel<R, GF, GNT, GMINB>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
-        kfn<<<grid, 128, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.tile_gptr.p,
-                                           p.tile_sptr.p, p.tile_src.p, p.tile_tab.p, p.tile_coarse.p,
-                                           p.spec_u.p, p.grp_src.p, p.grp_tgt.p, (cx<R>*)acc);
+        kfn<<<grid, GNT, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.n_src,
+                                            p.tile_gptr.p, p.tile_sptr.p, p.tile_src.p, p.tile_tab.p,
+                                            p.tile_coarse.p, p.spec_u.p, p.grp_src.p, p.grp_pm.p, p.grp_tgt.p,
+                                            (cx<R>*)acc);
         c.launches += 1;
     }
 

@@ -652,6 +652,7 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
     std::vector<int>& tcoarse = p.tcoarse;
     std::vector<int>& gtgt = p.gtgt;
     std::vector<unsigned short>& gsrc = p.gsrc;
+    std::vector<unsigned>& gpm = p.gpm;
     std::map<int, int> local;
     int cur_ld = -1, ngrp = 0, max_src = 0;
     auto close_tile = [&]() {
@@ -692,6 +693,20 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
             gsrc.push_back((unsigned short)j);
         }
         for (int cc = 0; cc < 8; ++cc) gtgt.push_back(gr.tgt[cc] >= 0 ? slot_of_tp[gr.tgt[cc]] : -1);
+        unsigned pm = 0;
+        for (int kk = 0; kk < 216; ++kk)
+            if (gr.used[kk]) pm |= 1u << (kk / 8);
+        gpm.push_back(pm);
+        // the kernel runs all 64 (c, c') products of a present parent, or
+        // only the adjacent ones when the plan is neighbour-only
+        for (int n = 0; n < 27; ++n)
+            if (pm >> n & 1u)
+            {
+                int cnt = 1;
+                for (int a = 0; a < 3; ++a)
+                    cnt *= (neighbor_only && (n / (a == 0 ? 1 : (a == 1 ? 3 : 9))) % 3 != 1) ? 1 : 4;
+                p.n_exec += cnt;
+            }
         ++ngrp;
     }
     close_tile();
@@ -699,6 +714,7 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
     p.max_tile_src = max_src;
     for (auto& x : tp) p.all_keys.insert(p.all_keys.end(), x.key.begin(), x.key.end());
     for (auto& x : tp) p.n_pairs += (long long)x.src.size();
+    p.n_exec += (long long)p.psrc.size();  // pair-list targets
     {
         std::vector<std::array<int, 4>> u;
         for (auto& x : tp) u.insert(u.end(), x.key.begin(), x.key.end());
@@ -761,7 +777,9 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
     p.tile_coarse.upload(h.tcoarse, c.stream);
     p.spec_u.upload(spec_u, c.stream);
     p.grp_src.upload(h.gsrc, c.stream);
+    p.grp_pm.upload(h.gpm, c.stream);
     p.grp_tgt.upload(h.gtgt, c.stream);
+    p.n_exec = h.n_exec;
     p.n_tgt = (int)h.tgt_list.size();
     p.n_pairs = h.n_pairs;
     p.n_spec_unique = h.n_spec_unique;
@@ -887,6 +905,7 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     for (auto& t : p.antrp) c.stats[5] += t.n_tasks;
     for (auto& t : p.intrp) c.stats[6] += t.n_tasks;
     c.stats[7] += p.n_tgt - p.n_csr_tgt;
+    c.stats[8] += p.n_exec;
     double* fs = c.field(c.f_fmm_s);
     double* ft = c.field(c.f_fmm_t);
     Timer tm(c);
@@ -899,7 +918,9 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     const size_t cb = c.cplx_bytes();
     if (!p.empty())
     {
-        ensure_bytes(c.d_src_spec, (size_t)p.n_src * c.NC * cb);
+        // the source spectra and one zero row after them (absent MAC candidates read it)
+        ensure_bytes(c.d_src_spec, (size_t)(p.n_src + 1) * c.NC * cb);
+        IBLGF_CUDA(cudaMemsetAsync(c.d_src_spec.p + (size_t)p.n_src * c.NC * cb, 0, c.NC * cb, c.stream));
         ensure_bytes(c.d_acc, (size_t)p.n_tgt * c.NC * cb);
         launch_forward_sources(c, fs, p.src_oct.p, p.n_src, c.d_src_spec.p);
     }

@@ -39,7 +39,7 @@ EXPORTS = [
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
     "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_warmstart", "iblgf_ib_warmstart_info",
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
-    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats",
+    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n",
     "iblgf_fma_peak",
 ]
 
@@ -101,6 +101,7 @@ def lib():
     L.iblgf_profile.argtypes = [vp, ci]
     L.iblgf_profile_read.argtypes = [vp, vp]
     L.iblgf_stats.argtypes = [vp, vp]
+    L.iblgf_stats_n.argtypes = [vp, vp, ci]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     _lib = L
     return L
@@ -347,8 +348,10 @@ class Solver:
         self._check(lib().iblgf_profile(self.h, 1 if enable else 0))
 
     def stats(self):
-        out = np.zeros(8, np.int64)
-        self._check(lib().iblgf_stats(self.h, _p(out)))
+        """[sweeps, sources, targets, pairs, unique spectra, anterp tasks,
+        interp tasks, group-MAC targets, MAC products executed]"""
+        out = np.zeros(9, np.int64)
+        self._check(lib().iblgf_stats_n(self.h, _p(out), 9))
         return out
 
     def fma_peak(self, precision):

@@ -257,6 +257,13 @@ int iblgf_profile_read(iblgf_ctx* ctx, double* out4);
  * block transfers, [6] interpolation block transfers, [7] targets handled by
  * the sibling-group MAC (the rest use the general pair-list MAC). */
 int iblgf_stats(iblgf_ctx* ctx, long long* out8);
+
+/* The first n (1 <= n <= 9) counters: [0]-[7] as iblgf_stats, then [8] the
+ * (target, source) spectral products the MAC kernels execute. A sibling group
+ * runs all 64 (child, candidate) products of every neighbour parent that has a
+ * candidate, so [8] >= [3]; [3] / [8] is the share of executed MAC work the
+ * reference's pair list also does. IBLGF_EINVAL for n outside [1, 9]. */
+int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the
  * roofline denominator of the CUDA-core kernels. */
