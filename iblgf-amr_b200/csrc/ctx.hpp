@@ -219,7 +219,6 @@ struct Ctx
     // LGF table (device), twiddles, transfer matrices
     DevBuf<double> d_lgf_table;
     DevBuf<double> d_tw64;  // 2P doubles: cos, -sin interleaved (forward)
-    DevBuf<float> d_tw32;
     // Nb*Nb matrices (child bit 0 / 1): [0,1] FMM Nli, cell-centred transfers with
     // relative position 1: [2,3] interpolation, [4,5] coarsification; relative
     // position 0: [6,7] interpolation, [8,9] coarsification (injection)

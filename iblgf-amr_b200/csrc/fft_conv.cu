@@ -6,23 +6,25 @@
 // block, scaled by dx^2 / P^3.
 //
 // B200 structure (one sweep = all blocks of all tree levels at once):
-//   fwd_xy   one CTA per (block, z-plane): pruned x (real, Nb -> Nb half
-//            frequencies) and y (Nb -> P) transforms in shared memory
-//   fwd_z    one thread per (ky,kx) pencil: z transform (Nb -> P)
-//            Each source block is transformed once per sweep; the reference
-//            transforms it once per (source, target) pair.
-//   mac      target-major spectral multiply-accumulate over the pair list,
-//            one thread per frequency, LGF spectra and source spectra read
-//            coalesced from L2/HBM (cached spectra stay resident across sweeps)
-//   inv_z    z inverse, only the Nb output planes of the extraction window
-//   inv_yx   y inverse (Nb outputs) and c2r along x (Nb outputs), scaled and
-//            added into the FP64 target block
+//   fwd_xy_rows  one CTA per source block: thread (z, y) transforms row y
+//                along x (real, Nb -> Nb half frequencies), thread (z, kx)
+//                then column kx along y (Nb -> P)
+//   fwd_z        one thread per (ky,kx) pencil: z transform (Nb -> P)
+//                Each source block is transformed once per sweep; the
+//                reference transforms it once per (source, target) pair.
+//   group_mac    sibling-group spectral multiply-accumulate (mac_kernel:
+//                general pair-list fallback)
+//   inv_fused    one CTA per (target, half of the output planes): z inverse,
+//                y inverse and c2r along x of the extraction window, in
+//                shared memory, added into the FP64 target block
 // The half spectrum is laid out [kz][ky][kx], kx < Nb (= P/2 + 1), as in the
-// reference's r2c output. Transforms are direct pruned DFTs: with half of the
-// inputs zero and half of the outputs discarded they cost about as much as a
-// mixed-radix FFT of length 35 and map onto regular loops.
+// reference's r2c output. Transforms are direct pruned DFTs (half of the
+// inputs zero, half of the outputs discarded). The forward loops are unrolled
+// over frequency and sample index so each twiddle is a compile-time constant
+// operand; the FP64 inverse reads a per-CTA twiddle table instead.
 #include <cmath>
 #include <mutex>
+#include <set>
 #include <type_traits>
 #include <vector>
 
@@ -36,7 +38,7 @@ namespace iblgf_b200
 {
 namespace
 {
-enum InMode { kFromField = 0, kFromLgf = 1, kFromDense = 2 };
+enum InMode { kFromLgf = 1, kFromDense = 2 };
 
 template<class R>
 __device__ __forceinline__ void load_tw(cx<R>* s_tw, const R* tw, int P)
@@ -44,8 +46,122 @@ __device__ __forceinline__ void load_tw(cx<R>* s_tw, const R* tw, int P)
     for (int j = threadIdx.x; j < P; j += blockDim.x) s_tw[j] = mk<R>(tw[2 * j], tw[2 * j + 1]);
 }
 
+// Twiddles e^{-2 pi i j / P} of every supported P (Nb = 6, 8, 10, 12, 16, 18)
+// in constant memory. The transform loops below are unrolled over both the
+// frequency and the sample index, so (k * j) mod P is a compile-time constant
+// and every twiddle is an immediate FMA operand: no shared-memory loads.
+constexpr int kTwTotal = 11 + 15 + 19 + 23 + 31 + 35;
+__host__ __device__ constexpr int tw_base(int P)
+{
+    return P == 11 ? 0 : P == 15 ? 11 : P == 19 ? 26 : P == 23 ? 45 : P == 31 ? 68 : 99;
+}
+__constant__ double c_tw64[2 * kTwTotal];
+__constant__ float c_tw32[2 * kTwTotal];
+
+template<class R, int P>
+__device__ __forceinline__ cx<R> ctw(int j)
+{
+    if constexpr (std::is_same<R, double>::value)
+        return mk<R>(c_tw64[2 * (tw_base(P) + j)], c_tw64[2 * (tw_base(P) + j) + 1]);
+    else
+        return mk<R>(c_tw32[2 * (tw_base(P) + j)], c_tw32[2 * (tw_base(P) + j) + 1]);
+}
+
+// Fully unrolled FP64 transforms at Nb = 18 exceed the register budget (the
+// scheduler hoists the loads of every term), so there the output loop stays
+// rolled and the twiddle index is carried in per-term counters; the twiddle
+// load is then one uniform constant-cache read.
+template<class R, int NB>
+constexpr bool kRollOutputs = std::is_same<R, double>::value && NB >= 18;
+
+// x and y transforms of a whole field block: thread (z, y) takes row y of
+// plane z along x (real NB -> NB half frequencies) into shared memory, then
+// thread (z, kx) takes column kx of plane z along y (NB -> P) and writes
+// W[item][z][ky][kx]. One CTA (NB^2 threads) per block; shared rows have an
+// odd stride (NB + 1 complex), so both passes are free of bank conflicts.
+template<class R, int NB>
+__global__ void __launch_bounds__(NB * NB) fwd_xy_rows_kernel(const double* __restrict__ field,
+                                                              const int* __restrict__ item_oct,
+                                                              cx<R>* __restrict__ W)
+{
+    constexpr int P = 2 * NB - 1, S = NB + 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<R>* s_x1 = reinterpret_cast<cx<R>*>(smraw);  // [z][y][kx]
+    const int item = blockIdx.x;
+    const int z = threadIdx.x / NB, r = threadIdx.x % NB;
+    {
+        const double* row = field + (size_t)item_oct[item] * (NB * NB * NB) + (size_t)threadIdx.x * NB;
+        R in[NB];
+#pragma unroll
+        for (int x = 0; x < NB; ++x) in[x] = (R)row[x];
+        cx<R>* dst = s_x1 + (size_t)threadIdx.x * S;
+        if constexpr (kRollOutputs<R, NB>)
+        {
+            int j[NB];  // j[x] = kx * x mod P
+#pragma unroll
+            for (int x = 0; x < NB; ++x) j[x] = 0;
+#pragma unroll 1
+            for (int kx = 0; kx < NB; ++kx)
+            {
+                cx<R> s = mk<R>(0, 0);
+#pragma unroll
+                for (int x = 0; x < NB; ++x)
+                {
+                    rmac<R>(s, in[x], ctw<R, P>(j[x]));
+                    j[x] = j[x] + x >= P ? j[x] + x - P : j[x] + x;
+                }
+                dst[kx] = s;
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int kx = 0; kx < NB; ++kx)
+            {
+                cx<R> s = mk<R>(0, 0);
+#pragma unroll
+                for (int x = 0; x < NB; ++x) rmac<R>(s, in[x], ctw<R, P>((kx * x) % P));
+                dst[kx] = s;
+            }
+        }
+    }
+    __syncthreads();
+    cx<R> v[NB];
+#pragma unroll
+    for (int y = 0; y < NB; ++y) v[y] = s_x1[(z * NB + y) * S + r];
+    cx<R>* out = W + ((size_t)item * NB + z) * (P * NB) + r;
+    if constexpr (kRollOutputs<R, NB>)
+    {
+        int j[NB];  // j[y] = ky * y mod P
+#pragma unroll
+        for (int y = 0; y < NB; ++y) j[y] = 0;
+#pragma unroll 1
+        for (int ky = 0; ky < P; ++ky)
+        {
+            cx<R> s = mk<R>(0, 0);
+#pragma unroll
+            for (int y = 0; y < NB; ++y)
+            {
+                cmac<R>(s, v[y], ctw<R, P>(j[y]));
+                j[y] = j[y] + y >= P ? j[y] + y - P : j[y] + y;
+            }
+            out[(size_t)ky * NB] = s;
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int ky = 0; ky < P; ++ky)
+        {
+            cx<R> s = mk<R>(0, 0);
+#pragma unroll
+            for (int y = 0; y < NB; ++y) cmac<R>(s, v[y], ctw<R, P>((ky * y) % P));
+            out[(size_t)ky * NB] = s;
+        }
+    }
+}
+
 // fwd_xy: x and y transforms of one z plane of one block.
-//   kFromField: block = field + item_oct[item] * NB^3 (NIN = NB)
 //   kFromLgf:   G((b + i) * 2^ld), desc[4*item] = {ld, bx, by, bz}  (NIN = P)
 //   kFromDense: dense[item * P^3]                                  (NIN = P)
 // W: [item][z < NIN][ky < P][kx < NB]
@@ -64,12 +180,7 @@ __global__ void __launch_bounds__(256) fwd_xy_kernel(const double* __restrict__ 
     const int item = blockIdx.x;
     const int z = blockIdx.y;
     load_tw<R>(s_tw, tw, P);
-    if (MODE == kFromField)
-    {
-        const double* blk = field + (size_t)item_oct[item] * (NB * NB * NB) + (size_t)z * NB * NB;
-        for (int i = threadIdx.x; i < NB * NB; i += blockDim.x) s_in[i] = (R)blk[i];
-    }
-    else if (MODE == kFromLgf)
+    if (MODE == kFromLgf)
     {
         // desc[0] >= 0: LGF_GL at stride 2^level_diff (lgf.hpp:222-262);
         // desc[0] < 0: LGF_GE table -desc[0]-1, E(n) = f[|n1|] f[|n2|] f[|n3|]
@@ -137,15 +248,11 @@ __global__ void __launch_bounds__(256) fwd_xy_kernel(const double* __restrict__ 
 
 // fwd_z: per (ky,kx) pencil, NIN -> P; spectrum slot = item_slot[item] (or item)
 template<class R, class RO, int NB, int NIN>
-__global__ void __launch_bounds__(128) fwd_z_kernel(const cx<R>* __restrict__ W, const R* __restrict__ tw,
-                                                    const int* __restrict__ item_slot,
+__global__ void __launch_bounds__(128) fwd_z_kernel(const cx<R>* __restrict__ W, const int* __restrict__ item_slot,
                                                     cx<RO>* __restrict__ spec)
 {
     constexpr int P = 2 * NB - 1;
     constexpr int NP = P * NB;
-    __shared__ cx<R> s_tw[P];
-    load_tw<R>(s_tw, tw, P);
-    __syncthreads();
     const int item = blockIdx.x;
     const int p = blockIdx.y * blockDim.x + threadIdx.x;
     if (p >= NP) return;
@@ -155,18 +262,34 @@ __global__ void __launch_bounds__(128) fwd_z_kernel(const cx<R>* __restrict__ W,
     for (int z = 0; z < NIN; ++z) v[z] = w[(size_t)z * NP];
     const int slot = item_slot ? item_slot[item] : item;
     cx<RO>* out = spec + (size_t)slot * P * NP + p;
-    for (int kz = 0; kz < P; ++kz)
+    if constexpr (NIN > NB)
     {
-        cx<R> s = mk<R>(0, 0);
-        int j = 0;
-#pragma unroll
-        for (int z = 0; z < NIN; ++z)
+        // dense P-point input (LGF spectra, cache fill only): kz rolled
+#pragma unroll 1
+        for (int kz = 0; kz < P; ++kz)
         {
-            cmac<R>(s, v[z], s_tw[j]);
-            j += kz;
-            if (j >= P) j -= P;
+            cx<R> s = mk<R>(0, 0);
+            int j = 0;
+#pragma unroll
+            for (int z = 0; z < NIN; ++z)
+            {
+                cmac<R>(s, v[z], ctw<R, P>(j));
+                j += kz;
+                if (j >= P) j -= P;
+            }
+            out[(size_t)kz * NP] = mk<RO>((RO)s.x, (RO)s.y);
         }
-        out[(size_t)kz * NP] = mk<RO>((RO)s.x, (RO)s.y);
+    }
+    else
+    {
+#pragma unroll
+        for (int kz = 0; kz < P; ++kz)
+        {
+            cx<R> s = mk<R>(0, 0);
+#pragma unroll
+            for (int z = 0; z < NIN; ++z) cmac<R>(s, v[z], ctw<R, P>((kz * z) % P));
+            out[(size_t)kz * NP] = mk<RO>((RO)s.x, (RO)s.y);
+        }
     }
 }
 
@@ -330,95 +453,89 @@ __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
     }
 }
 
-// inv_z: V[t][z'][p] = sum_kz ACC[t][kz][p] e^{+2 pi i kz (z'+NB-1)/P}, z' < NB.
-// The accumulators arrive in the working precision RA; the inverse transforms
-// run in RC = FP64 on both paths: cancellation in the c2r amplifies FP32
+// Fused inverse of one target block: z inverse, y inverse, c2r along x and
+// target[oct] += scale * window, with every intermediate in shared memory.
+// One CTA per (target, half of the NB output z-planes), NB^2 threads:
+//   z  thread per pencil (ky, kx): the P accumulators (working precision RA,
+//      widened to FP64) -> the NB/2 output planes of this half, into sV
+//   y  thread (kx, plane, half of yo): P -> NB/2 outputs yo
+//   x  thread (yo, plane, half of xo): c2r NB -> NB/2 outputs xo
+// All three passes use one FP64 table sT[k][o] = e^{-2 pi i k (o + NB - 1) / P}
+// (conjugated): each pass loops over its input index k and reads row k of
+// the table at compile-time offsets, a uniform broadcast read. The inverse
+// runs in FP64 on both paths: cancellation in the c2r amplifies FP32
 // rounding of the twiddled sums far more than in the forward transforms.
-template<class RA, class RC, int NB>
-__global__ void __launch_bounds__(128) inv_z_kernel(const cx<RA>* __restrict__ ACC, const RC* __restrict__ tw,
-                                                    cx<RC>* __restrict__ V)
+// The summation order per output is the reference order k = 0, 1, ...
+template<class RA, int NB>
+__global__ void __launch_bounds__(NB * NB, 2) inv_fused_kernel(const cx<RA>* __restrict__ ACC,
+                                                               const int* __restrict__ tgt_oct, double scale,
+                                                               double* __restrict__ target)
 {
-    constexpr int P = 2 * NB - 1;
-    constexpr int NP = P * NB;
-    __shared__ cx<RC> s_tw[P];
-    load_tw<RC>(s_tw, tw, P);
+    constexpr int P = 2 * NB - 1, NP = P * NB, ZH = NB / 2, S = NB + 1;
+    static_assert(NB % 2 == 0, "the block splits into two halves of output planes");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2* sT = reinterpret_cast<double2*>(smraw);  // [k < P][o < NB]
+    double2* sV = sT + P * NB;                        // [plane][ky][kx], then [plane][yo][kx] (stride S)
+    const int t = blockIdx.x, h = blockIdx.y;
+    for (int i = threadIdx.x; i < P * NB; i += blockDim.x)
+        sT[i] = ctw<double, P>(((i / NB) * (i % NB + NB - 1)) % P);
     __syncthreads();
-    const int t = blockIdx.x;
-    const int p = blockIdx.y * blockDim.x + threadIdx.x;
-    if (p >= NP) return;
-    const cx<RA>* a = ACC + (size_t)t * P * NP + p;
-    cx<RC> v[P];
-#pragma unroll
-    for (int kz = 0; kz < P; ++kz)
+    // z: P -> the ZH planes zo = h ZH + i
+    const cx<RA>* a = ACC + (size_t)t * P * NP;
+    for (int p = threadIdx.x; p < NP; p += blockDim.x)
     {
-        const cx<RA> x = a[(size_t)kz * NP];
-        v[kz] = mk<RC>((RC)x.x, (RC)x.y);
-    }
-    cx<RC>* out = V + (size_t)t * NB * NP + p;
-    for (int zo = 0; zo < NB; ++zo)
-    {
-        const int zz = zo + NB - 1;
-        cx<RC> s = mk<RC>(0, 0);
-        int j = 0;
+        double2 acc[ZH];
 #pragma unroll
+        for (int i = 0; i < ZH; ++i) acc[i] = mk<double>(0, 0);
+#pragma unroll 5
         for (int kz = 0; kz < P; ++kz)
         {
-            cmac_conj<RC>(s, v[kz], s_tw[j]);
-            j += zz;
-            if (j >= P) j -= P;
+            const cx<RA> x0 = a[(size_t)kz * NP + p];
+            const double2 x = mk<double>((double)x0.x, (double)x0.y);
+            const double2* tr = sT + kz * NB + h * ZH;
+#pragma unroll
+            for (int i = 0; i < ZH; ++i) cmac_conj<double>(acc[i], x, tr[i]);
         }
-        out[(size_t)zo * NP] = s;
+#pragma unroll
+        for (int i = 0; i < ZH; ++i) sV[i * NP + p] = acc[i];
     }
-}
-
-// inv_yx: y inverse (NB outputs) and c2r along x (NB outputs), then
-// target[oct] += scale * result over the whole Nb^3 block
-template<class R, int NB>
-__global__ void __launch_bounds__(256) inv_yx_kernel(const cx<R>* __restrict__ V, const R* __restrict__ tw,
-                                                     const int* __restrict__ tgt_oct, double scale,
-                                                     double* __restrict__ target)
-{
-    constexpr int P = 2 * NB - 1;
-    constexpr int NP = P * NB;
-    __shared__ cx<R> s_tw[P];
-    __shared__ cx<R> s_v[NP];
-    __shared__ cx<R> s_y[NB * NB];
-    const int t = blockIdx.x, zo = blockIdx.y;
-    load_tw<R>(s_tw, tw, P);
-    const cx<R>* vin = V + ((size_t)t * NB + zo) * NP;
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) s_v[i] = vin[i];
     __syncthreads();
-    for (int i = threadIdx.x; i < NB * NB; i += blockDim.x)
-    {
-        const int yo = i / NB, kx = i % NB, yy = yo + NB - 1;
-        cx<R> s = mk<R>(0, 0);
-        int j = 0;
+    // y: thread (kx, plane zl, half yh of the outputs yo)
+    const int kx = threadIdx.x % NB, rest = threadIdx.x / NB, zl = rest % ZH, yh = rest / ZH;
+    double2 acc[ZH];
+#pragma unroll
+    for (int i = 0; i < ZH; ++i) acc[i] = mk<double>(0, 0);
 #pragma unroll 5
-        for (int ky = 0; ky < P; ++ky)
-        {
-            cmac_conj<R>(s, s_v[ky * NB + kx], s_tw[j]);
-            j += yy;
-            if (j >= P) j -= P;
-        }
-        s_y[yo * NB + kx] = s;
+    for (int ky = 0; ky < P; ++ky)
+    {
+        const double2 x = sV[zl * NP + ky * NB + kx];
+        const double2* tr = sT + ky * NB + yh * ZH;
+#pragma unroll
+        for (int i = 0; i < ZH; ++i) cmac_conj<double>(acc[i], x, tr[i]);
     }
     __syncthreads();
-    double* out = target + (size_t)tgt_oct[t] * NB * NB * NB + (size_t)zo * NB * NB;
-    for (int i = threadIdx.x; i < NB * NB; i += blockDim.x)
+#pragma unroll
+    for (int i = 0; i < ZH; ++i) sV[(zl * NB + yh * ZH + i) * S + kx] = acc[i];
+    __syncthreads();
+    // x: thread (yo, plane zl2, half xh of the outputs xo); c2r of the half
+    // spectrum: v = Re y_0 + 2 sum_{k >= 1} Re(y_k e^{+2 pi i k (xo + NB - 1) / P})
+    const int xh = threadIdx.x / (ZH * NB), r2 = threadIdx.x % (ZH * NB), zl2 = r2 / NB, yo = r2 % NB;
+    const double2* yrow = sV + (size_t)(zl2 * NB + yo) * S;
+    double sx[ZH];
+#pragma unroll
+    for (int i = 0; i < ZH; ++i) sx[i] = 0;
+#pragma unroll 6
+    for (int k = 1; k < NB; ++k)
     {
-        const int yo = i / NB, xo = i % NB, xx = xo + NB - 1;
-        R acc = 0;
-        int j = xx;
-        for (int kx = 1; kx < NB; ++kx)
-        {
-            const cx<R> y = s_y[yo * NB + kx];
-            acc = fma(y.x, s_tw[j].x, fma(y.y, s_tw[j].y, acc));
-            j += xx;
-            if (j >= P) j -= P;
-        }
-        const double v = (double)s_y[yo * NB].x + 2.0 * (double)acc;
-        out[i] += scale * v;
+        const double2 y = yrow[k];
+        const double2* tr = sT + k * NB + xh * ZH;
+#pragma unroll
+        for (int i = 0; i < ZH; ++i) sx[i] = fma(y.x, tr[i].x, fma(y.y, tr[i].y, sx[i]));
     }
+    const double y0 = yrow[0].x;
+    double* out = target + (size_t)tgt_oct[t] * NB * NB * NB + ((size_t)(h * ZH + zl2) * NB + yo) * NB + xh * ZH;
+#pragma unroll
+    for (int i = 0; i < ZH; ++i) out[i] += scale * (y0 + 2.0 * sx[i]);
 }
 
 template<class R, int NB>
@@ -429,19 +546,28 @@ struct Conv
     static constexpr int P = 2 * NB - 1;
     static constexpr int NP = P * NB;
 
-    static const R* tw(Ctx& c)
+    static void launch_fwd_xy_rows(Ctx& c, const double* field, const int* d_item_oct, int n, cx<R>* W)
     {
-        return std::is_same<R, double>::value ? (const R*)c.d_tw64.p : (const R*)c.d_tw32.p;
+        const int smem = NB * NB * (NB + 1) * (int)sizeof(cx<R>);
+        auto kfn = fwd_xy_rows_kernel<R, NB>;
+        IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kfn<<<n, NB * NB, smem, c.stream>>>(field, d_item_oct, W);
+    }
+
+    static void launch_inverse(Ctx& c, const cx<R>* acc, const int* d_tgt_oct, int n, double scale, double* target)
+    {
+        const int smem = (P * NB + NB / 2 * NP) * (int)sizeof(double2);
+        auto kfn = inv_fused_kernel<R, NB>;
+        IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kfn<<<dim3(n, 2), NB * NB, smem, c.stream>>>(acc, d_tgt_oct, scale, target);
     }
 
     static void forward_field(Ctx& c, const double* field, const int* d_item_oct, int n, void* spec)
     {
         if (!n) return;
         cx<R>* W = (cx<R>*)c.d_w.p;
-        fwd_xy_kernel<R, NB, NB, kFromField><<<dim3(n, NB), 256, 0, c.stream>>>(field, d_item_oct, nullptr,
-                                                                              nullptr, tw(c), W, nullptr, 0);
-        fwd_z_kernel<R, R, NB, NB><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, tw(c), nullptr,
-                                                                                  (cx<R>*)spec);
+        launch_fwd_xy_rows(c, field, d_item_oct, n, W);
+        fwd_z_kernel<R, R, NB, NB><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, nullptr, (cx<R>*)spec);
         c.launches += 2;
     }
 
@@ -457,7 +583,7 @@ struct Conv
         else
             fwd_xy_kernel<double, NB, P, kFromLgf><<<dim3(n, P), 256, 0, c.stream>>>(
                 nullptr, nullptr, d_desc, c.d_lgf_table.p, c.d_tw64.p, W, c.d_ge.p, c.ge_stride);
-        fwd_z_kernel<double, R, NB, P><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, c.d_tw64.p, d_slot,
+        fwd_z_kernel<double, R, NB, P><<<dim3(n, (NP + 127) / 128), 128, 0, c.stream>>>(W, d_slot,
                                                                                       (cx<R>*)spec);
         c.launches += 2;
     }
@@ -505,11 +631,8 @@ struct Conv
     static void inverse(Ctx& c, const void* acc, const int* d_tgt_oct, int n_tgt, double scale, double* target)
     {
         if (!n_tgt) return;
-        double2* V = (double2*)c.d_w.p;
-        inv_z_kernel<R, double, NB><<<dim3(n_tgt, (NP + 127) / 128), 128, 0, c.stream>>>((const cx<R>*)acc,
-                                                                                        c.d_tw64.p, V);
-        inv_yx_kernel<double, NB><<<dim3(n_tgt, NB), 256, 0, c.stream>>>(V, c.d_tw64.p, d_tgt_oct, scale, target);
-        c.launches += 2;
+        launch_inverse(c, (const cx<R>*)acc, d_tgt_oct, n_tgt, scale, target);
+        c.launches += 1;
     }
 };
 
@@ -542,6 +665,29 @@ void ensure(DevBuf<char>& b, size_t bytes)
 }  // namespace
 
 bool nb_supported(int Nb) { return Nb == 6 || Nb == 8 || Nb == 10 || Nb == 12 || Nb == 16 || Nb == 18; }
+
+void init_twiddle_constants(int device)
+{
+    static std::mutex m;
+    static std::set<int> done;
+    std::lock_guard<std::mutex> lock(m);
+    if (done.count(device)) return;
+    std::vector<double> t64(2 * kTwTotal);
+    std::vector<float> t32(2 * kTwTotal);
+    for (int P : {11, 15, 19, 23, 31, 35})
+        for (int j = 0; j < P; ++j)
+        {
+            const double a = 2.0 * M_PI * j / P;
+            const int k = 2 * (tw_base(P) + j);
+            t64[k] = std::cos(a);
+            t64[k + 1] = -std::sin(a);
+            t32[k] = (float)t64[k];
+            t32[k + 1] = (float)t64[k + 1];
+        }
+    IBLGF_CUDA(cudaMemcpyToSymbol(c_tw64, t64.data(), t64.size() * sizeof(double)));
+    IBLGF_CUDA(cudaMemcpyToSymbol(c_tw32, t32.data(), t32.size() * sizeof(float)));
+    done.insert(device);
+}
 
 void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots)
 {
@@ -597,7 +743,6 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
 
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale)
 {
-    ensure(c.d_w, (size_t)p.n_tgt * c.Nb * c.P * c.Nb * 16);
     dispatch(c, [&](auto cv) {
         using CV = decltype(cv);
         CV::inverse(c, acc, p.tgt_oct.p, p.n_tgt, scale, fmm_t);
@@ -720,18 +865,14 @@ void launch_conv_block_noalloc(Ctx& c, const double* src, const double* kernel, 
         fwd_xy_kernel<double, NB, P, kFromDense><<<dim3(1, P), 256, 0, c.stream>>>(
             kernel, nullptr, nullptr, nullptr, c.d_tw64.p, (double2*)W, nullptr, 0);
         fwd_z_kernel<double, R, NB, P><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
-            (const double2*)W, c.d_tw64.p, nullptr, (cx<R>*)gspec);
-        fwd_xy_kernel<R, NB, NB, kFromField><<<dim3(1, NB), 256, 0, c.stream>>>(
-            src, d_zero, nullptr, nullptr, CV::tw(c), (cx<R>*)W, nullptr, 0);
+            (const double2*)W, nullptr, (cx<R>*)gspec);
+        CV::launch_fwd_xy_rows(c, src, d_zero, 1, (cx<R>*)W);
         fwd_z_kernel<R, R, NB, NB><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
-            (const cx<R>*)W, CV::tw(c), nullptr, (cx<R>*)sspec);
+            (const cx<R>*)W, nullptr, (cx<R>*)sspec);
         mac_kernel<R><<<dim3((unsigned)((c.NC + 127) / 128), 1), 128, 0, c.stream>>>(
             (const cx<R>*)gspec, (const cx<R>*)sspec, d_ptr, d_zero, d_zero, c.NC, (cx<R>*)acc);
-        inv_z_kernel<R, double, NB><<<dim3(1, (NP + 127) / 128), 128, 0, c.stream>>>(
-            (const cx<R>*)acc, c.d_tw64.p, (double2*)W);
-        inv_yx_kernel<double, NB><<<dim3(1, NB), 256, 0, c.stream>>>((const double2*)W, c.d_tw64.p, d_zero, s,
-                                                                       out);
-        c.launches += 7;
+        CV::launch_inverse(c, (const cx<R>*)acc, d_zero, 1, s, out);
+        c.launches += 6;
     });
     IBLGF_CUDA(cudaGetLastError());
 }

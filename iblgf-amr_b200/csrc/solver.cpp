@@ -20,6 +20,7 @@
 namespace iblgf_b200
 {
 bool nb_supported(int Nb);
+void init_twiddle_constants(int device);
 
 int mask_idx_gen(int type, int refinement_level, int nlas)
 {
@@ -108,19 +109,16 @@ void ctx_init(Ctx& c)
         c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
         return;
     }
+    init_twiddle_constants(c.cfg.device);
     // twiddles e^{-2 pi i j / P}
     std::vector<double> tw(2 * c.P);
-    std::vector<float> tw32(2 * c.P);
     for (int j = 0; j < c.P; ++j)
     {
         const double a = 2.0 * M_PI * j / c.P;
         tw[2 * j] = std::cos(a);
         tw[2 * j + 1] = -std::sin(a);
-        tw32[2 * j] = (float)tw[2 * j];
-        tw32[2 * j + 1] = (float)tw[2 * j + 1];
     }
     c.d_tw64.upload(tw, c.stream);
-    c.d_tw32.upload(tw32, c.stream);
     // [0,1] FMM Nli (pts_cap 10), [2,3] cell-centred interpolation (relpos 1),
     // [4,5] cell-centred coarsification (2-point average per axis)
     std::vector<double> mats;
