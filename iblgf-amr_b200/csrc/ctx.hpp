@@ -290,8 +290,11 @@ void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter
 void ib_flags(Ctx& c, int* flags);
 bool ib_active(const Ctx& c);
 const int* ib_face_aux2(Ctx& c);
+// write_prev = false (the velocity-refresh correction stages): the CG starts
+// from the stage's previous force but the result does not replace it, and the
+// learned warm start neither predicts nor records samples
 void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
-                 const std::function<void()>& gradient_d);
+                 const std::function<void()>& gradient_d, bool write_prev = true);
 void ib_force(Ctx& c, int stage, double* out, int* iters);
 void ib_release(const Ctx* c);
 void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const long long* at, const double* w,

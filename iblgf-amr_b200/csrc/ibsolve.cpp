@@ -552,12 +552,12 @@ const int* ib_face_aux2(Ctx& c) { return state(c).face_aux2; }
 // pressure correction of d, then face_aux = grad d + E f (the caller
 // subtracts it from r_i)
 void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
-                 const std::function<void()>& gradient_d)
+                 const std::function<void()>& gradient_d, bool write_prev)
 {
     IbState& s = state(c);
     WarmStart& w = s.ws;
     std::vector<double> f = s.force_prev[stage];
-    if (w.mode == 1)
+    if (w.mode == 1 && write_prev)
     {
         std::vector<double> uc, duc, dfp(s.force_prev[stage]);
         projection(c, s, s.face_aux2, uc);
@@ -583,7 +583,7 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
     }
     else
         ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
-    s.force_prev[stage] = f;
+    if (write_prev) s.force_prev[stage] = f;
     // LinSysSolver::pressure_correction (linsys.hpp:131-145)
     OpLists& ol = op_lists(c);
     const int l = c.tree.depth - 1;

@@ -10,11 +10,10 @@
 //
 // Steps without an immersed boundary replay a CUDA graph of one captured step
 // once a direct step with the same fields, dt and Re has run.
-// Scope: no immersed boundary (the Schur-complement solve, smearing and the
-// IB2xIB / IB2AMR pieces act on an empty point set and change none of the
-// fields the step reads), no adaptation, no body force, frame velocity 0.
-// The velocity-refresh branch (pad_velocity + adapt_corr_time_step, taken
-// once (T - T_last_refresh) 3.3 / (Re dx_base^2) > 7) is rejected.
+// Scope: optional immersed boundary (lin_sys_with_ib_solve), constant frame
+// velocity, no adaptation, no body force. The velocity refresh (pad_velocity
+// + adapt_corr_time_step, taken once (T - T_last_refresh) 3.3 / (Re dx_base^2)
+// > 7, ifherk.hpp:1093-1111) runs with direct launches.
 #include <cmath>
 #include <map>
 #include <memory>
@@ -54,8 +53,11 @@ void relpos(int mesh, int comp, int rp[3])
 struct NsState
 {
     VF q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
+    VF stream_f;                     // velocity refresh only, created on first use
     DevBuf<int> leaf;                // 1 for leaves, per octant
     std::vector<DevBuf<int>> corr;   // per level: correction blocks
+    std::vector<DevBuf<int>> nc;     // per level: blocks that are not correction blocks
+    std::vector<DevBuf<double>> nc_dx;
     // smooth2zero lists of the base level for leaf_only_boundary false / true
     DevBuf<int> sm_list[2], sm_ptr[2], sm_dirs[2];
     int sm_n[2] = {0, 0};
@@ -114,12 +116,17 @@ NsState& ns_state(Ctx& c)
     for (int i = 0; i < c.n_oct; ++i) leaf[i] = c.flags[i] & 1;
     s->leaf.upload(leaf, c.stream);
     s->corr.resize(c.level_octs.size());
+    s->nc.resize(c.level_octs.size());
+    s->nc_dx.resize(c.level_octs.size());
     for (size_t l = 0; l < c.level_octs.size(); ++l)
     {
-        std::vector<int> v;
+        std::vector<int> v, w;
         for (int o : c.level_octs[l])
-            if (c.flags[o] & 2) v.push_back(o);
+            (c.flags[o] & 2 ? v : w).push_back(o);
         s->corr[l].upload(v, c.stream);
+        s->nc[l].upload(w, c.stream);
+        s->nc_dx[l].upload(std::vector<double>(w.size(), c.cfg.dx_base / std::pow(2.0, (int)l - c.tree.base_level)),
+                           c.stream);
     }
     const int bl = c.tree.base_level;
     for (int lo = 0; lo < 2; ++lo)
@@ -161,9 +168,17 @@ class Step
         for (int k = 0; k < 3; ++k) alpha[k] = (cc[k + 1] - cc[k]) / tmp;
     }
 
-    void time_step(const VF& u, const VF& p)
+    // refresh: ifherk.hpp:1093-1111, the velocity refresh (pad_velocity and
+    // adapt_corr_time_step) takes the place of up_and_down(u)
+    void time_step(const VF& u, const VF& p, bool refresh)
     {
-        up_and_down(u);
+        if (refresh)
+        {
+            pad_velocity(u);
+            adapt_corr_time_step(u, p);
+        }
+        else
+            up_and_down(u);
         copy(u, s.q_i, 1.0);
         // stage 1
         clean(s.g_i, false);
@@ -209,6 +224,67 @@ class Step
         copy(s.d_i, p, 1.0 / coeff_a(3, 3) / dt);
     }
 
+    // pad_velocity<u, u>(true) (ifherk.hpp:1522-1573): u rebuilt from its
+    // vorticity through the stream function on the base level
+    void pad_velocity(const VF& u)
+    {
+        if (s.stream_f.id[0] < 0) s.stream_f = make_vf(c, kEdge);
+        clean(u, true);
+        up(u);
+        clean(s.edge_aux, false);
+        clean(s.stream_f, false);
+        for (int l = bl; l < depth; ++l)
+        {
+            exchange(u, l);
+            // curl on the blocks that are not correction blocks
+            const double* pin[3] = {F(u.id[0]), F(u.id[1]), F(u.id[2])};
+            double* pout[3] = {F(s.edge_aux.id[0]), F(s.edge_aux.id[1]), F(s.edge_aux.id[2])};
+            launch_op(c, 3, pin, 3, pout, 3, s.nc[l].p, s.nc_dx[l].p, (int)s.nc[l].n, 1.0);
+        }
+        clean_leaf_correction_boundary(s.edge_aux, bl, true);
+        for (int k = 0; k < 3; ++k) poisson_apply_lgf(c, s.edge_aux.id[k], s.stream_f.id[k], IBLGF_STREAM);
+        // refresh_correction_only: curl_transpose on the base level only
+        op(4, {&s.stream_f}, u, bl, -1.0);
+        down_to_correction(u);
+    }
+    // adapt_corr_time_step (ifherk.hpp:1206-1303): three projection stages
+    // with alpha = 0 and no nonlinear term; the IB solves read but do not
+    // replace the stages' previous forces
+    void adapt_corr_time_step(const VF& u, const VF& p)
+    {
+        up_and_down(u);
+        copy(u, s.q_i, 1.0);
+        write_prev = false;
+        // stage 1
+        clean(s.g_i, false);
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        clean(s.face_aux, false);
+        copy(s.q_i, s.r_i, 1.0);
+        stage = 1;
+        lin_sys(0.0);
+        // stage 2
+        clean(s.r_i, false);
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        add(s.q_i, s.r_i, 1.0);
+        up_and_down(s.u_i);
+        stage = 2;
+        lin_sys(0.0);
+        // stage 3
+        clean(s.d_i, false);
+        clean(s.cell_aux, false);
+        clean(s.w_2, false);
+        copy(s.q_i, s.r_i, 1.0);
+        apply_if(s.r_i, s.r_i, 0.0);
+        up_and_down(s.u_i);
+        stage = 3;
+        lin_sys(0.0);
+        write_prev = true;
+        copy(s.u_i, u, 1.0);
+        copy(s.d_i, p, 0.0);
+    }
+
   private:
     Ctx& c;
     NsState& s;
@@ -217,6 +293,7 @@ class Step
     double dt, Re;
     NsOptions opt;
     int bl = 0, depth = 0, stage = 0;
+    bool write_prev = true;
     // ifherk.hpp:2010-2011
     const double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
     const double cc[4] = {0.0, 1.0 / 3, 1.0, 1.0};
@@ -369,7 +446,7 @@ class Step
                     iblgf_b200::apply_if(c, fa2.id[k], fa2.id[k], alpha_k, IBLGF_IB2xIB, rp);
                 }
             ns_ib_stage(c, stage, alpha_k, opt.cg_threshold, opt.cg_max_iter, s.d_i.id[0], s.face_aux.id,
-                        [&]() { gradient(s.d_i, s.face_aux); });
+                        [&]() { gradient(s.d_i, s.face_aux); }, write_prev);
             add(s.face_aux, s.r_i, -1.0);
             if (std::fabs(alpha_k) > 1e-14) apply_if(s.r_i, s.u_i, alpha_k);
             else copy(s.r_i, s.u_i, 1.0);
@@ -403,7 +480,14 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
     for (int i = 0; i < n_steps; ++i)
     {
         if ((*T - s.T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
-            throw Error(IBLGF_EINVAL, "velocity refresh (pad_velocity) branch is not supported");
+        {
+            // velocity refresh step (ifherk.hpp:1093-1104): direct launches
+            s.T_last_vel_refresh = *T;
+            st.time_step(uf, pf, true);
+            ++s.steps_done;
+            *T += dt;
+            continue;
+        }
         const bool graphable = !ib_active(c) && !c.profile && !s.graph_failed;
         const bool same = s.graph && s.g_p == p && s.g_dt == dt && s.g_Re == Re && s.g_u[0] == u[0] &&
                           s.g_u[1] == u[1] && s.g_u[2] == u[2];
@@ -428,7 +512,7 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
             bool ok = true;
             try
             {
-                st.time_step(uf, pf);
+                st.time_step(uf, pf, false);
             }
             catch (const Error&)
             {
@@ -442,7 +526,7 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
                 s.graph = nullptr;
                 s.graph_failed = true;
                 c.launches = l0;
-                st.time_step(uf, pf);  // nothing of the failed capture ran
+                st.time_step(uf, pf, false);  // nothing of the failed capture ran
             }
             else
             {
@@ -457,7 +541,7 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
         }
         else
         {
-            st.time_step(uf, pf);
+            st.time_step(uf, pf, false);
             for (int k = 0; k < 3; ++k) s.w_u[k] = u[k];
             s.w_p = p;
             s.w_dt = dt;

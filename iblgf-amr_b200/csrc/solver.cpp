@@ -1073,11 +1073,22 @@ int ge_table(Ctx& c, double alpha)
 {
     auto it = c.ge_index.find(alpha);
     if (it != c.ge_index.end()) return it->second;
-    if (!(alpha > 0.0)) throw Error(IBLGF_EINVAL, "integrating-factor alpha must be positive");
+    if (!(alpha >= 0.0)) throw Error(IBLGF_EINVAL, "integrating-factor alpha must be non-negative");
     c.ge_stride = 4 * c.Nb + 9;
     const int nmax = c.ge_stride - 1;
     const double x = 2.0 * alpha;
     std::vector<double> f(c.ge_stride, 0.0);
+    if (alpha == 0.0)
+    {
+        // e^0 I_n(0) = [n == 0]: the identity (the recurrence divides by x)
+        f[0] = 1.0;
+        const int idx = (int)c.ge_index.size();
+        c.ge_index.emplace(alpha, idx);
+        c.ge_host.insert(c.ge_host.end(), f.begin(), f.end());
+        c.d_ge.upload(c.ge_host, c.stream);
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        return idx;
+    }
     const int m = nmax + 30 + (int)std::ceil(std::sqrt(90.0 * x));
     double a = 0.0, b = 1e-280, sum = 0.0;
     for (int k = m; k >= 1; --k)

@@ -145,9 +145,13 @@ int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out)
  * normal components) by n_steps steps of size dt at Reynolds number Re and
  * writes the pressure of the last step into p_field; *T is the simulation time
  * (in/out). The immersed boundary and the frame velocity come from
- * iblgf_ib_set_points / iblgf_ns_options. Not covered: adaptation, body
- * force, moving bodies (boundary velocity 0) and the velocity-refresh branch
- * (taken once (T - 0) 3.3 / (Re dx_base^2) > 7), which returns IBLGF_EINVAL. */
+ * iblgf_ib_set_points / iblgf_ns_options. A step whose time is far enough past
+ * the last velocity refresh ((T - T_last) 3.3 / (Re dx_base^2) > 7, T_last = 0
+ * initially, per context) first rebuilds u from its vorticity through the
+ * base-level stream function and runs the alpha = 0 correction step
+ * (pad_velocity + adapt_corr_time_step, ifherk.hpp:1093-1111, 1206-1303,
+ * 1522-1573). Not covered: adaptation, body force, moving bodies (boundary
+ * velocity 0). */
 int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, double Re, double* T,
                   int n_steps);
 /* Constant frame velocity (frame_vel[3], subtracted from the convecting

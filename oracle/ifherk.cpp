@@ -12,11 +12,11 @@
 //   include/iblgf/operators/operators.hpp:653-760 smooth2zero
 //   include/iblgf/interpolation/cell_center_nli_intrp.hpp:349-365 relative
 //     positions of cell / face / edge components.
-// Scope: no immersed boundary (the Schur-complement solve, smearing and the
-// IB2xIB / IB2AMR pieces act on an empty point set and leave every field the
-// time step reads unchanged), no adaptation, no body force, frame velocity 0.
-// The velocity-refresh branch (pad_velocity + adapt_corr_time_step, taken once
-// (T - T_last_refresh) 3.3 / (Re dx^2) > 7) is reported as unsupported.
+//     :1093-1111 velocity refresh once (T - T_last_refresh) 3.3 / (Re dx^2) > 7:
+//                pad_velocity (:1522-1573, refresh_correction_only) and
+//                adapt_corr_time_step (:1206-1303)
+// Scope: optional immersed boundary, constant frame velocity, no adaptation,
+// no body force.
 #include <cmath>
 #include <stdexcept>
 
@@ -54,6 +54,7 @@ Ifherk::Ifherk(Domain* d_, Solver* s_, double dt_, double Re_) : d(d_), s(s_), d
     mk(cell_aux, MESH_CELL, 1);
     mk(face_aux, MESH_FACE, 3);
     mk(edge_aux, MESH_EDGE, 3);
+    mk(stream_f, MESH_EDGE, 3);
     const double tmp = Re * d->dx_base * d->dx_base / dt;
     for (int k = 0; k < 3; ++k) alpha[k] = (c[k + 1] - c[k]) / tmp;
 }
@@ -270,7 +271,7 @@ void Ifherk::lin_sys(double alpha_k)
         std::vector<std::array<double, 3>> force = force_prev[stage_idx];
         const VField uin = fa2;
         ib->solve(uin, alpha_k, force, cg_threshold, cg_max_iter);
-        force_prev[stage_idx] = force;
+        if (write_prev_force) force_prev[stage_idx] = force;
         ib->pressure_correction(force, d_i);
         gradient(d_i, face_aux);
         ib->smearing(force, face_aux, false);
@@ -285,12 +286,78 @@ void Ifherk::lin_sys(double alpha_k)
     else copy(r_i, u_i, 1.0);
 }
 
+// pad_velocity<u, u>(true) (ifherk.hpp:1522-1573): the velocity is rebuilt
+// from its vorticity through the stream function on the base level
+void Ifherk::pad_velocity()
+{
+    const int bl = d->base_level;
+    clean(u, true);
+    up(u);
+    clean(edge_aux, false);
+    clean(stream_f, false);
+    for (int l = bl; l < d->depth; ++l)
+    {
+        exchange(u, l);
+        apply_op(*d, 3, {&u.c[0], &u.c[1], &u.c[2]}, {&edge_aux.c[0], &edge_aux.c[1], &edge_aux.c[2]}, l, 1.0,
+                 true);
+    }
+    clean_leaf_correction_boundary(edge_aux, bl, true);
+    for (int k = 0; k < 3; ++k) s->apply_lgf(edge_aux.c[k], stream_f.c[k], STREAM, true, false);
+    // refresh_correction_only: curl_transpose on the base level only
+    op_level(4, {&stream_f.c[0], &stream_f.c[1], &stream_f.c[2]}, {&u.c[0], &u.c[1], &u.c[2]}, bl, -1.0);
+    down_to_correction(u);
+}
+
+// adapt_corr_time_step (ifherk.hpp:1206-1303): three projection stages with
+// alpha = 0 and no nonlinear term; the IB solves start from the stage's
+// previous force without replacing it (write_prev_force = false)
+void Ifherk::adapt_corr_time_step()
+{
+    up_and_down(u);
+    copy(u, q_i, 1.0);
+    write_prev_force = false;
+    // stage 1
+    clean(g_i, false);
+    clean(d_i, false);
+    clean(cell_aux, false);
+    clean(face_aux, false);
+    copy(q_i, r_i, 1.0);
+    stage_idx = 1;
+    lin_sys(0.0);
+    // stage 2
+    clean(r_i, false);
+    clean(d_i, false);
+    clean(cell_aux, false);
+    add(q_i, r_i, 1.0);
+    up_and_down(u_i);
+    stage_idx = 2;
+    lin_sys(0.0);
+    // stage 3
+    clean(d_i, false);
+    clean(cell_aux, false);
+    clean(w_2, false);
+    copy(q_i, r_i, 1.0);
+    apply_if(r_i, r_i, 0.0);
+    up_and_down(u_i);
+    stage_idx = 3;
+    lin_sys(0.0);
+    write_prev_force = true;
+    copy(u_i, u, 1.0);
+    copy(d_i, p, 0.0);
+}
+
 void Ifherk::time_step()
 {
     const double dx = d->dx_base;
+    // ifherk.hpp:1093-1111: the velocity refresh replaces up_and_down(u)
     if ((T - T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
-        throw std::runtime_error("oracle: velocity refresh (pad_velocity) branch not supported");
-    up_and_down(u);
+    {
+        T_last_vel_refresh = T;
+        pad_velocity();
+        adapt_corr_time_step();
+    }
+    else
+        up_and_down(u);
     copy(u, q_i, 1.0);
     // stage 1
     clean(g_i, false);

@@ -136,6 +136,12 @@ void build_table()
 
 void bessel_ie_all(double x, int nmax, double* out)
 {
+    if (x == 0.0)
+    {
+        // e^0 I_n(0): 1 for n = 0, 0 otherwise (the recurrence divides by x)
+        for (int n = 0; n <= nmax; ++n) out[n] = n == 0 ? 1.0 : 0.0;
+        return;
+    }
     const int m = std::max(nmax, 0) + 30 + (int)std::ceil(std::sqrt(90.0 * x));
     double a = 0.0, b = 1e-280, sum = 0.0;
     for (int n = 0; n <= nmax; ++n) out[n] = 0.0;

@@ -59,11 +59,12 @@ void for_blocks(Domain& d, int level, F&& f)
 
 // op: 0 laplace, 1 gradient, 2 divergence, 3 curl, 4 curl_transpose, 5 nonlinear
 void apply_op(Domain& d, int op, const std::vector<const Field*>& in, const std::vector<Field*>& out,
-              int level, double scale)
+              int level, double scale, bool skip_correction)
 {
     const int Nb = d.Nb;
     const size_t B = (size_t)Nb * Nb * Nb;
     for_blocks(d, level, [&](Octant* o, double dx) {
+        if (skip_correction && o->correction) return;
         const size_t base = o->idx * B;
         auto at = [&](int c, int i, int j, int k) {
             return (*in[c])[base + i + (size_t)Nb * (j + (size_t)Nb * k)];

@@ -204,7 +204,8 @@ struct Ifherk
     double frame_vel[3] = {0.0, 0.0, 0.0};
     double c[4] = {0.0, 1.0 / 3, 1.0, 1.0};
     double alpha[3] = {0.0, 0.0, 0.0};
-    VField u, p, q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
+    VField u, p, q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux, stream_f;
+    bool write_prev_force = true;
 
     Ifherk(Domain* d, Solver* s, double dt, double Re);
     double coeff_a(int i, int j) const;
@@ -226,6 +227,8 @@ struct Ifherk
     void gradient(VField& src, VField& tgt);
     void apply_if(const VField& src, VField& tgt, double alpha_base);
     void lin_sys(double alpha_k);
+    void pad_velocity();
+    void adapt_corr_time_step();
 };
 
 // ---------------------------------------------------------------- IB
@@ -265,7 +268,7 @@ std::vector<std::array<double, 3>> sphere_points(double dx_base, int ib_level, d
 void nli_matrix(int Nb, int pts_cap, double* mat /* Nb x 2Nb, (p,c) at p*2Nb+c */);
 void buffer_exchange(Domain& d, Field& f, int level);
 void apply_op(Domain& d, int op, const std::vector<const Field*>& in, const std::vector<Field*>& out,
-              int level, double scale);
+              int level, double scale, bool skip_correction = false);
 void cc_matrix(int Nb, int pts_cap, int relpos, double* mat);
 
 }  // namespace orc

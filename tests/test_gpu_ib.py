@@ -73,3 +73,29 @@ def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
     assert rel_linf(g.download(pf), pr) < ptol, rel_linf(g.download(pf), pr)
     for st in range(3):
         assert rel_linf(g.ib_force(st + 1), fr[st]) < tol * 10, (st, rel_linf(g.ib_force(st + 1), fr[st]))
+
+
+def test_ns_step_with_ib_velocity_refresh_matches_oracle():
+    """Velocity refresh with the immersed boundary (FP64): the correction
+    stages solve the IB system from the stages' previous forces without
+    replacing them (write_prev_force = false, ifherk.hpp:1476-1478), so the
+    following plain step starts its CG from the same forces as the oracle."""
+    case = S.SphereIB("small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=B.FP64)
+    X = O.sphere_points(case.dx_base, o.depth - 1 - o.base_level, case.ibph)
+    u0 = case.velocity(o)
+    dt, fv, T0 = 0.01, (-1.0, 0.0, 0.0), 1.0e6
+    ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, T0, 2)
+    g.ib_set_points(X, case.Re)
+    g.ns_options(fv)
+    uf = [g.field(u0[k]) for k in range(3)]
+    pf = g.field()
+    g.ns_step(uf, pf, dt, case.Re, T0, 2)
+    for k in range(3):
+        assert rel_linf(g.download(uf[k]), ur[k]) < 1e-9, (k, rel_linf(g.download(uf[k]), ur[k]))
+    assert rel_linf(g.download(pf), pr) < 1e-9, rel_linf(g.download(pf), pr)
+    for st in range(3):
+        assert rel_linf(g.ib_force(st + 1), fr[st]) < 1e-8, (st, rel_linf(g.ib_force(st + 1), fr[st]))

@@ -164,6 +164,30 @@ def test_ns_step_oracle_projects_and_conserves_scale():
     assert np.isfinite(p).all()
 
 
+def test_ns_step_oracle_velocity_refresh():
+    """The velocity-refresh step (pad_velocity + adapt_corr_time_step,
+    ifherk.hpp:1093-1111, 1206-1303, 1522-1573) of a divergence-free flow:
+    rebuilding u from its vorticity through the base-level stream function
+    changes the leaves' velocity by a small fraction, the step stays finite,
+    and the projection keeps the velocity nearly divergence free."""
+    case = S.VortexRingNS("small")
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    u0 = case.initial_velocity(d)
+    u_plain, _ = d.ns_step(u0, case.dt(), case.Re, 0.0, 1)
+    u_ref, p = d.ns_step(u0, case.dt(), case.Re, 1.0e6, 1)
+    lf = d.leaf & ~d.correction
+
+    def div_max(u):
+        div = d.op(2, [u[0], u[1], u[2]], [d.zeros()])[0]
+        return float(np.abs(div[lf][:, 2:-2, 2:-2, 2:-2]).max())
+
+    assert np.isfinite(u_ref).all() and np.isfinite(p).all()
+    scale = float(np.abs(u0[:, lf]).max())
+    assert float(np.abs(u_ref - u_plain)[:, lf].max()) < 0.1 * scale
+    assert div_max(u_ref) < 0.05 * div_max(u0)
+
+
 def test_ib_solve_oracle_converges_on_sphere():
     """IB force solve (linsys.hpp:113-230) on the sphere: the CG reaches its
     threshold well before the iteration limit, IB blocks sit at the finest
