@@ -385,6 +385,20 @@ int iblgf_ns_options(iblgf_ctx* x, const double* frame_vel, double cg_threshold,
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ns_options(c, frame_vel, cg_threshold, cg_max_iter); });
 }
 
+int iblgf_adapt(iblgf_ctx* x, int n_attempts, const uint64_t* keys, const int* level_change, int n_interp,
+                const int* interp_fields, const int* interp_mesh, int* base_mesh_update)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::domain_adapt(c, n_attempts, reinterpret_cast<const iblgf_b200::u64*>(keys), level_change,
+                                 n_interp, interp_fields, interp_mesh, base_mesh_update);
+    });
+}
+
+int iblgf_block_norms(iblgf_ctx* x, const int* fields, int n_comp, double* max_out, double* rms_out)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::block_norms(c, fields, n_comp, max_out, rms_out); });
+}
+
 int iblgf_ib_force(iblgf_ctx* x, int stage, double* out, int* iters)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_force(c, stage, out, iters); });

@@ -106,7 +106,16 @@ struct HostTree
     bool try_2to1(u64 k, std::map<u64, bool>& checklist) const;
     void refine(int i, bool ratio_2to1);
     void init_refine(int n_ref, int level_up_max, iblgf_refine_fn pred, void* user);
-    void mark_correction();
+    // aim_del (per tree position, may be null): deletion marks of an adaptation
+    void mark_correction(std::vector<char>* aim_del = nullptr);
+    bool leaf_search(int i, bool require_data) const;
+    void delete_oct(int i);
+    // one adaptation (server side of Domain::adapt): attempts (key, level
+    // change) of leaves, ib per tree position (bit 0 is_ib, bit 1 extended);
+    // returns the tree positions of the parents whose children take
+    // interpolated data, in (level, key) order
+    std::vector<int> adapt(const std::vector<std::pair<u64, int>>& attempts, const std::vector<char>& ib,
+                           bool& base_mesh_update);
     void import_octants(int n, const u64* keys, const int* flags);
     std::vector<int> canonical() const;  // has_data octants, (level, key) order
 };
@@ -340,6 +349,20 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
 // constant frame velocity and IB CG settings of the IF-HERK step
 void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter);
 void ns_release(const Ctx* c);
+// after an adaptation: the time step's per-tree lists are rebuilt, its graph
+// dropped; base_mesh_update forces a velocity refresh at the next step
+void ns_on_adapt(Ctx& c, bool base_mesh_update);
+void ib_on_adapt(Ctx& c);
+// per-octant IB flags (bit 0 is_ib, bit 1 is_extended_ib); empty without IB
+std::vector<int> ib_octant_flags(Ctx& c);
+// octree rebuild after the host tree changed (lists, masks; no fields)
+void domain_rebuild(Ctx& c);
+// Ifherk::adapt + Domain::adapt for one process: attempts (key, level change),
+// then every field remapped to the new octants, the listed fields
+// interpolated into the children of the interpolation parents
+void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_interp, const int* interp_fields,
+                  const int* interp_mesh, int* base_mesh_update);
+void block_norms(Ctx& c, const int* fields, int n_comp, double* host_max, double* host_rms);
 OpLists& op_lists(Ctx& c);
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);
 int mask_idx_gen(int type, int refinement_level, int nlas);
@@ -354,6 +377,8 @@ void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, i
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale);
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
+void launch_remap_blocks(Ctx& c, const double* old, double* nw, const int* d_src, int n_new);
+void launch_block_norms(Ctx& c, const double* const* comps, int n_comp, double* d_max, double* d_rms);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
 void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
                         bool assign);

@@ -61,6 +61,7 @@ struct WarmStart
 struct IbState
 {
     int n = 0;
+    double Re = 0.0;
     std::vector<double> X;
     std::vector<int> flags;  // per octant: bit0 is_ib (parents of IB blocks included), bit1 is_extended_ib
     // projection: per point CSR over entries (field offset, 3 weights)
@@ -116,6 +117,7 @@ void ib_set_points(Ctx& c, int n, const double* X, double Re)
     if (!(Re > 0)) throw Error(IBLGF_EINVAL, "Re must be positive");
     auto s = std::make_unique<IbState>();
     s->n = n;
+    s->Re = Re;
     s->X.assign(X, X + 3 * (size_t)n);
     const int l_max = c.tree.depth - 1, bl = c.tree.base_level;
     const int ib_level = l_max - bl;
@@ -654,5 +656,30 @@ void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter
 }
 
 void ib_release(const Ctx* c) { g_ib.erase(c); }
+
+std::vector<int> ib_octant_flags(Ctx& c)
+{
+    auto it = g_ib.find(&c);
+    if (it == g_ib.end()) return {};
+    return it->second->flags;
+}
+
+// After an adaptation the point set is re-attached to the new tree (flags,
+// masks, influence lists, cleaning lists); the stage forces and the warm-start
+// network carry over
+void ib_on_adapt(Ctx& c)
+{
+    auto it = g_ib.find(&c);
+    if (it == g_ib.end()) return;
+    std::vector<double> fp[4];
+    for (int k = 0; k < 4; ++k) fp[k] = it->second->force_prev[k];
+    WarmStart ws = std::move(it->second->ws);
+    const std::vector<double> X = it->second->X;
+    const double Re = it->second->Re;
+    ib_set_points(c, (int)(X.size() / 3), X.data(), Re);
+    IbState& s = state(c);
+    for (int k = 0; k < 4; ++k) s.force_prev[k] = fp[k];
+    s.ws = std::move(ws);
+}
 
 }  // namespace iblgf_b200

@@ -62,6 +62,7 @@ struct NsState
     DevBuf<int> sm_list[2], sm_ptr[2], sm_dirs[2];
     int sm_n[2] = {0, 0};
     double T_last_vel_refresh = 0.0;  // ifherk.hpp:1980
+    bool force_refresh = false;       // base_mesh_update of the last adaptation
     // one captured time step (steps without an immersed boundary): replayed
     // while the velocity / pressure fields, dt and Re stay the same
     cudaGraphExec_t graph = nullptr;
@@ -97,6 +98,8 @@ VF make_vf(Ctx& c, int mesh)
     return f;
 }
 
+void ns_build_lists(Ctx& c, NsState& st);
+
 NsState& ns_state(Ctx& c)
 {
     auto it = g_ns.find(&c);
@@ -112,6 +115,17 @@ NsState& ns_state(Ctx& c)
     s->cell_aux = make_vf(c, kCell);
     s->face_aux = make_vf(c, kFace);
     s->edge_aux = make_vf(c, kEdge);
+    ns_build_lists(c, *s);
+    auto& ref = *s;
+    g_ns.emplace(&c, std::move(s));
+    return ref;
+}
+
+// the step's per-tree lists: leaves, correction / other blocks per level,
+// smooth2zero directions of the base level
+void ns_build_lists(Ctx& c, NsState& st)
+{
+    NsState* s = &st;
     std::vector<int> leaf(c.n_oct);
     for (int i = 0; i < c.n_oct; ++i) leaf[i] = c.flags[i] & 1;
     s->leaf.upload(leaf, c.stream);
@@ -150,9 +164,6 @@ NsState& ns_state(Ctx& c)
         s->sm_dirs[lo].upload(dirs, c.stream);
     }
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
-    auto& ref = *s;
-    g_ns.emplace(&c, std::move(s));
-    return ref;
 }
 
 class Step
@@ -479,8 +490,9 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
     const double dx = c.cfg.dx_base;
     for (int i = 0; i < n_steps; ++i)
     {
-        if ((*T - s.T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
+        if (s.force_refresh || (*T - s.T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
         {
+            s.force_refresh = false;
             // velocity refresh step (ifherk.hpp:1093-1104): direct launches
             s.T_last_vel_refresh = *T;
             st.time_step(uf, pf, true);
@@ -560,6 +572,21 @@ void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max
     for (int k = 0; k < 3; ++k) o.frame_vel[k] = frame_vel ? frame_vel[k] : 0.0;
     o.cg_threshold = cg_threshold;
     o.cg_max_iter = cg_max_iter;
+}
+
+void ns_on_adapt(Ctx& c, bool base_mesh_update)
+{
+    auto it = g_ns.find(&c);
+    if (it == g_ns.end()) return;
+    NsState& s = *it->second;
+    if (s.graph) cudaGraphExecDestroy(s.graph);
+    s.graph = nullptr;
+    s.graph_failed = false;
+    s.g_p = s.w_p = -1;
+    for (int k = 0; k < 3; ++k) s.g_u[k] = s.w_u[k] = -1;
+    ns_build_lists(c, s);
+    // ifherk.hpp:1093-1096: a grown base mesh refreshes the velocity
+    s.force_refresh = s.force_refresh || base_mesh_update;
 }
 
 void ns_release(const Ctx* c)

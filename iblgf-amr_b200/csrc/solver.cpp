@@ -310,8 +310,20 @@ int field_create(Ctx& c)
 
 void domain_finalize(Ctx& c)
 {
+    domain_rebuild(c);
+    if (c.topology_only) return;
+    c.f_source_tmp = field_create(c);
+    c.f_target_tmp = field_create(c);
+    c.f_correction_tmp = field_create(c);
+    c.f_fmm_s = field_create(c);
+    c.f_fmm_t = field_create(c);
+}
+
+void domain_rebuild(Ctx& c)
+{
     HostTree& t = c.tree;
     const std::vector<int> canon = t.canonical();
+    c.key_index.clear();
     c.n_oct = (int)canon.size();
     for (int i = 0; i < c.n_oct; ++i) t.o[canon[i]].idx = i;
     const int n = c.n_oct;
@@ -360,13 +372,6 @@ void domain_finalize(Ctx& c)
     c.d_bbase.upload(c.bbase, c.stream);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     build_masks(c);
-    c.finalized = true;
-    if (c.topology_only) return;
-    c.f_source_tmp = field_create(c);
-    c.f_target_tmp = field_create(c);
-    c.f_correction_tmp = field_create(c);
-    c.f_fmm_s = field_create(c);
-    c.f_fmm_t = field_create(c);
     c.finalized = true;
 }
 

@@ -286,4 +286,80 @@ void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list,
     IBLGF_CUDA(cudaGetLastError());
 }
 
+// Adaptation: new block b takes old block src[b] (or zeros when src[b] < 0)
+__global__ void remap_blocks_kernel(const double2* __restrict__ old, double2* __restrict__ nw,
+                                    const int* __restrict__ src, int half_block)
+{
+    const int b = blockIdx.x;
+    const int s = src[b];
+    double2* d = nw + (size_t)b * half_block;
+    if (s < 0)
+        for (int i = threadIdx.x; i < half_block; i += blockDim.x) d[i] = make_double2(0.0, 0.0);
+    else
+    {
+        const double2* o = old + (size_t)s * half_block;
+        for (int i = threadIdx.x; i < half_block; i += blockDim.x) d[i] = o[i];
+    }
+}
+
+void launch_remap_blocks(Ctx& c, const double* old, double* nw, const int* d_src, int n_new)
+{
+    if (!n_new) return;
+    const int half = (int)(c.block_elems() / 2);  // Nb even: Nb^3 / 2 double2
+    remap_blocks_kernel<<<n_new, 256, 0, c.stream>>>(reinterpret_cast<const double2*>(old),
+                                                     reinterpret_cast<double2*>(nw), d_src, half);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+// Operator::maxnorm / blockRootMeanSquare (operators.hpp:1149-1211) over the
+// block's interior nodes: max over nodes of sqrt(sum_c v_c^2) and
+// sqrt(sum_nodes sum_c v_c^2 / nodes)
+__global__ void block_norms_kernel(const double* __restrict__ f0, const double* __restrict__ f1,
+                                   const double* __restrict__ f2, int n_comp, int NB, double* __restrict__ out_max,
+                                   double* __restrict__ out_rms)
+{
+    const int b = blockIdx.x;
+    const int e = NB - 2;
+    const size_t base = (size_t)b * NB * NB * NB;
+    double mx = 0.0, sum = 0.0;
+    for (int i = threadIdx.x; i < e * e * e; i += blockDim.x)
+    {
+        const int x = i % e + 1, y = (i / e) % e + 1, z = i / (e * e) + 1;
+        const size_t at = base + x + (size_t)NB * (y + (size_t)NB * z);
+        double v = f0[at] * f0[at];
+        if (n_comp > 1) v += f1[at] * f1[at];
+        if (n_comp > 2) v += f2[at] * f2[at];
+        sum += v;
+        mx = fmax(mx, sqrt(v));
+    }
+    __shared__ double smx[256], ssum[256];
+    smx[threadIdx.x] = mx;
+    ssum[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1)
+    {
+        if ((int)threadIdx.x < o)
+        {
+            smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + o]);
+            ssum[threadIdx.x] += ssum[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        out_max[b] = smx[0];
+        out_rms[b] = sqrt(ssum[0] / ((double)e * e * e));
+    }
+}
+
+void launch_block_norms(Ctx& c, const double* const* comps, int n_comp, double* d_max, double* d_rms)
+{
+    if (!c.n_oct) return;
+    block_norms_kernel<<<c.n_oct, 256, 0, c.stream>>>(comps[0], n_comp > 1 ? comps[1] : comps[0],
+                                                      n_comp > 2 ? comps[2] : comps[0], n_comp, c.Nb, d_max, d_rms);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 }  // namespace iblgf_b200

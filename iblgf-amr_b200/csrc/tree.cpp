@@ -13,6 +13,8 @@
 // always true.
 #include <algorithm>
 #include <cmath>
+#include <functional>
+#include <set>
 #include <stack>
 
 #include "ctx.hpp"
@@ -241,14 +243,20 @@ void HostTree::init_refine(int n_ref, int level_up_max, iblgf_refine_fn pred, vo
     mark_correction();
 }
 
-void HostTree::mark_correction()
+void HostTree::mark_correction(std::vector<char>* aim_del)
 {
+    auto del = [&](int i) { return aim_del && i < (int)aim_del->size() && (*aim_del)[i]; };
+    auto keep = [&](int i) {
+        if (!aim_del) return;
+        if ((int)aim_del->size() <= i) aim_del->resize(o.size(), 0);
+        (*aim_del)[i] = 0;
+    };
     for (auto& x : o) x.physical = false;
     for (int l = depth - 1; l >= base_level; --l)
         for (int i = 0; i < (int)o.size(); ++i)
         {
             if (!o[i].has_data || o[i].level != l) continue;
-            o[i].physical = o[i].leaf;
+            o[i].physical = o[i].leaf && !del(i);
             if (!o[i].physical)
                 for (int c : o[i].child)
                     if (c >= 0 && o[c].has_data) o[i].physical = o[i].physical || o[c].physical;
@@ -288,6 +296,7 @@ void HostTree::mark_correction()
             for (int n : nb)
             {
                 if (n < 0 || o[n].physical) continue;
+                keep(n);
                 o[n].correction = true;
             }
         }
@@ -305,7 +314,211 @@ void HostTree::mark_correction()
         }
         else
             o[i].correction = false;
+        keep(i);
     }
+}
+
+bool HostTree::leaf_search(int i, bool require_data) const
+{
+    for (int c : o[i].child)
+        if (c >= 0 && (!require_data || o[c].has_data)) return false;
+    return true;
+}
+
+// Tree::delete_oct (tree.hpp:455-466): the octant loses its data and, without
+// children, its place in the parent
+void HostTree::delete_oct(int i)
+{
+    o[i].has_data = false;
+    o[i].leaf = false;
+    o[i].correction = false;
+    o[i].idx = -1;
+    if (leaf_search(i, false) && o[i].parent >= 0)
+    {
+        HOct& p = o[o[i].parent];
+        for (int& c : p.child)
+            if (c == i) c = -1;
+    }
+}
+
+// Domain::adapt / Decomposition::adapt_decoposition, server part
+// (domain/decomposition/decomposition.hpp:182-470) for one process, with
+// Tree::deletionReset_2to1 (octree/tree.hpp:304-327) and
+// Domain::delete_all_children (domain.hpp:512-569); baseBlockBufferNumber_ = 2
+std::vector<int> HostTree::adapt(const std::vector<std::pair<u64, int>>& attempts, const std::vector<char>& ib,
+                                 bool& base_mesh_update)
+{
+    base_mesh_update = false;
+    std::vector<char> del(o.size(), 0);
+    std::vector<int> lchange(o.size(), 0);
+    auto grow = [&]() {
+        if (del.size() < o.size()) del.resize(o.size(), 0);
+        if (lchange.size() < o.size()) lchange.resize(o.size(), 0);
+    };
+    auto is_ib = [&](int i) { return i < (int)ib.size() && (ib[i] & 1); };
+    auto is_ext = [&](int i) { return i < (int)ib.size() && (ib[i] & 2); };
+    auto by_level_key = [&](std::vector<int> v) {
+        std::sort(v.begin(), v.end(), [&](int a, int b) {
+            return o[a].level != o[b].level ? o[a].level < o[b].level : o[a].key < o[b].key;
+        });
+        return v;
+    };
+    auto leaves = [&]() {
+        std::vector<int> v;
+        for (int i = 0; i < (int)o.size(); ++i)
+            if (o[i].has_data && o[i].leaf) v.push_back(i);
+        return by_level_key(v);
+    };
+    auto level_list = [&](int l) {
+        std::vector<int> v;
+        for (int i = 0; i < (int)o.size(); ++i)
+            if (o[i].has_data && o[i].level == l) v.push_back(i);
+        return by_level_key(v);
+    };
+    std::set<u64> old_leaves;
+    for (int i = 0; i < (int)o.size(); ++i)
+    {
+        if (o[i].has_data && o[i].leaf) old_leaves.insert(o[i].key);
+        del[i] = o[i].correction && !is_ib(i);
+    }
+    for (auto& a : attempts)
+    {
+        if (a.second == 0) continue;
+        const int i = find(a.first);
+        if (i < 0 || !o[i].has_data) throw Error(IBLGF_EINVAL, "adaptation attempt for an octant without data");
+        lchange[i] = a.second;
+    }
+    std::map<u64, bool> checklist;
+    std::vector<int> refine_list;
+    for (int i : leaves())
+    {
+        if (lchange[i] == 0) continue;
+        if (lchange[i] < 0) del[i] = 1;
+        else if (is_ib(i) || try_2to1(o[i].key, checklist))
+            refine_list.push_back(i);
+    }
+    for (int i : leaves())
+        if (is_ib(i) || is_ext(i)) del[i] = 0;
+    // base-level blocks within two blocks of a kept base block
+    std::set<u64> away;
+    for (int i : level_list(base_level))
+    {
+        if (del[i] || o[i].correction) continue;
+        int c[3];
+        key_coord(o[i].key, c);
+        const int lim = 1 << o[i].level;
+        for (int dz = -2; dz <= 2; ++dz)
+            for (int dy = -2; dy <= 2; ++dy)
+                for (int dx = -2; dx <= 2; ++dx)
+                {
+                    const int x = c[0] + dx, y = c[1] + dy, z = c[2] + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) continue;
+                    away.insert(key_make(x, y, z, o[i].level));
+                }
+    }
+    for (u64 nk : away)
+    {
+        int c[3];
+        key_coord(nk, c);
+        bool inside = true;
+        for (int d = 0; d < 3; ++d)
+            if (c[d] < 0 || c[d] > key_bd_extent[d] - 1) inside = false;
+        if (!inside) continue;
+        int n = find(nk);
+        if (n < 0 || !o[n].has_data)
+        {
+            n = insert(nk);
+            alloc(n, o[n].level - base_level);
+            o[n].leaf = true;
+            o[n].correction = false;
+            base_mesh_update = true;
+            grow();
+        }
+        del[n] = 0;
+    }
+    for (int i : refine_list)
+    {
+        if (!o[i].leaf) continue;
+        refine(i, true);
+        grow();
+    }
+    // deletionReset_2to1 from the parents of refined leaves
+    std::set<int> reset_done;
+    std::function<void(int)> reset = [&](int l) {
+        if (reset_done.count(l)) return;
+        if (o[l].level - base_level < 0) return;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx)
+                {
+                    const u64 nk = key_neighbor(o[l].key, dx, dy, dz);
+                    if (key_is_end(nk)) continue;
+                    const int n = find(nk);
+                    if (n < 0 || !o[n].has_data) continue;
+                    del[n] = 0;
+                    reset(o[n].parent);
+                }
+        reset_done.insert(l);
+    };
+    for (int i : leaves())
+        if (o[i].level - base_level > 0) reset(o[i].parent);
+    // base-level deletions, then collapse of fully deleted sibling groups
+    for (int i : level_list(base_level))
+        if (del[i] && o[i].leaf) delete_oct(i);
+    for (int l = depth - 2; l >= base_level; --l)
+        for (int i : level_list(l))
+        {
+            if (leaf_search(i, true)) continue;
+            bool all = true;
+            for (int ch : o[i].child)
+            {
+                if (ch < 0 || !o[ch].has_data) continue;
+                if (!del[ch] || (!o[ch].leaf && !o[ch].correction))
+                {
+                    all = false;
+                    break;
+                }
+            }
+            if (all)
+            {
+                for (int ch : o[i].child)
+                {
+                    if (ch < 0) continue;
+                    o[ch].leaf = false;
+                    o[ch].correction = false;
+                    del[ch] = 1;
+                }
+                o[i].leaf = true;
+                o[i].correction = false;
+                del[i] = 0;
+            }
+            else
+                for (int ch : o[i].child)
+                    if (ch >= 0) del[ch] = 0;
+        }
+    mark_correction(&del);
+    grow();
+    for (int i = 0; i < (int)o.size(); ++i)
+        if (o[i].has_data && del[i] && o[i].level - base_level > 0) delete_oct(i);
+    for (int l = base_level - 1; l > 0; --l)
+        for (int i = 0; i < (int)o.size(); ++i)
+            if (o[i].level == l && leaf_search(i, false)) delete_oct(i);
+    // new octants' ancestors get data
+    for (int i = 0; i < (int)o.size(); ++i)
+    {
+        if (!o[i].has_data || o[i].idx >= 0) continue;
+        for (int pa = o[i].parent; pa >= 0 && !o[pa].has_data; pa = o[pa].parent) alloc(pa, o[pa].level - base_level);
+    }
+    depth = 0;
+    for (auto& x : o)
+        if (x.has_data) depth = std::max(depth, x.level + 1);
+    // parents of new leaves above the base level
+    std::vector<int> parents;
+    for (int i : leaves())
+        if (o[i].level - base_level > 0 && !old_leaves.count(o[i].key)) parents.push_back(o[i].parent);
+    parents = by_level_key(parents);
+    parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
+    return parents;
 }
 
 void HostTree::import_octants(int n, const u64* keys, const int* flags)

@@ -39,7 +39,7 @@ EXPORTS = [
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
     "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_warmstart", "iblgf_ib_warmstart_info",
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
-    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n",
+    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms",
     "iblgf_fma_peak",
 ]
 
@@ -102,6 +102,8 @@ def lib():
     L.iblgf_profile_read.argtypes = [vp, vp]
     L.iblgf_stats.argtypes = [vp, vp]
     L.iblgf_stats_n.argtypes = [vp, vp, ci]
+    L.iblgf_adapt.argtypes = [vp, ci, vp, vp, ci, vp, vp, vp]
+    L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     _lib = L
     return L
@@ -160,6 +162,10 @@ class Solver:
             self._check(L.iblgf_domain_init_refine(self.h, int(n_levels), int(global_refinement), self._cb, None))
         self._check(L.iblgf_domain_finalize(self.h, 1 if subtract_non_leaf else 0))
         self._check(L.iblgf_poisson_options(self.h, 1 if use_correction else 0, 1 if subtract_non_leaf else 0))
+        self._load_octants()
+
+    def _load_octants(self):
+        L = lib()
         bl, dp, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(L.iblgf_domain_info(self.h, ctypes.byref(bl), ctypes.byref(dp), ctypes.byref(n)))
         self.base_level, self.depth, self.n = bl.value, dp.value, n.value
@@ -168,6 +174,39 @@ class Solver:
         self.flags = np.zeros(self.n, np.int32)
         self.bbase = np.zeros((self.n, 3), np.int32)
         self._check(L.iblgf_domain_octants(self.h, _p(self.keys), _p(self.levels), _p(self.flags), _p(self.bbase)))
+
+    # ------------------------------------------------------------ adaptation
+    def block_norms(self, fields):
+        """(max |v|, rms |v|) per octant over the interior nodes of the vector
+        whose component fields are `fields` (Operator::maxnorm /
+        blockRootMeanSquare, operators.hpp:1149-1211)."""
+        f = np.ascontiguousarray(fields, dtype=np.int32).ravel()
+        mx = np.zeros(self.n)
+        rms = np.zeros(self.n)
+        self._check(lib().iblgf_block_norms(self.h, _p(f), len(f), _p(mx), _p(rms)))
+        return mx, rms
+
+    def adapt(self, keys, level_change, interpolate=()):
+        """One adaptation (Ifherk::adapt, ifherk.hpp:1018-1076): `keys` /
+        `level_change` are the adapt condition's attempts (+1 refine, -1
+        delete); `interpolate` lists (mesh, [field ids]) with mesh 0 cell (one
+        id), 1 face, 2 edge (three ids) whose values are interpolated into the
+        children of each new leaf's parent. Returns base_mesh_update; octant
+        arrays (keys, levels, flags, bbase, n) are reloaded."""
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        lc = np.ascontiguousarray(level_change, dtype=np.int32)
+        if len(k) != len(lc):
+            raise ValueError("keys and level_change differ in length")
+        fids = np.full((max(len(interpolate), 1), 3), -1, np.int32)
+        mesh = np.zeros(max(len(interpolate), 1), np.int32)
+        for i, (m, ids) in enumerate(interpolate):
+            mesh[i] = m
+            fids[i, :len(ids)] = ids
+        bmu = ctypes.c_int()
+        self._check(lib().iblgf_adapt(self.h, len(k), _p(k), _p(lc), len(interpolate), _p(fids), _p(mesh),
+                                      ctypes.byref(bmu)))
+        self._load_octants()
+        return bool(bmu.value)
 
     # ------------------------------------------------------------ basics
     def _check(self, rc):

@@ -451,3 +451,87 @@ class SphereIB:
                 X, Y, Z = x[0][None, None, :], x[1][None, :, None], x[2][:, None, None]
                 u[c, o] = U[c] + 0.1 * np.sin(k[c, 0] * X) * np.cos(k[c, 1] * Y) * np.cos(k[c, 2] * Z)
         return u
+
+
+# ----------------------------------------------------------------- adaptation
+def key_parent(k):
+    """Parent Morton key (octree/key.hpp parent(): coordinate bits of level
+    l - 1, level field l - 1)."""
+    k = int(k)
+    lv = (k >> 2) & 31
+    if lv == 0:
+        return k
+    m = 0 if lv - 1 <= 0 else ((1 << (3 * (lv - 1))) - 1) << (64 - 3 * (lv - 1))
+    return ((m & k) | ((lv - 1) << 2)) + 1
+
+
+def update_source_max(source_max, block_rms, all_time_max=False):
+    """Ifherk::update_source_max (ifherk.hpp:401-426): the largest block RMS
+    of the field, blended with (or maxed against) the previous value, at least
+    1e-2."""
+    new = float(np.max(block_rms)) if len(block_rms) else 0.0
+    out = max(source_max, new) if all_time_max else 0.5 * (source_max + new)
+    return max(out, 1e-2)
+
+
+def adapt_level_change(keys, levels, flags, base_level, cell_aux_max, correction_max, edge_aux_max, source_max,
+                       n_level_refinement, refinement_factor=0.125, base_threshold=1e-4, hard_max_level=None,
+                       ib_flags=None, n_ib_add_level=0):
+    """The adapt condition of the reference's NS setup
+    (tests/ns_amr_lgf/ns_amr_lgf.hpp:402-489): per-octant block max-norms
+    (iblgf_block_norms) of cell_aux, correction_tmp and edge_aux against
+    source_max = (cell, vorticity); returns the attempts (keys, level change)
+    for iblgf_adapt. Leaves ask for refinement when the field is within the
+    refinement_factor^k band of source_max for a deeper level, for deletion
+    when it falls below the band by the deletion factor 0.7; correction blocks
+    (non-leaf) ask through their parent's key."""
+    hard = n_level_refinement if hard_max_level is None else hard_max_level
+    ib = np.zeros(len(keys), np.int32) if ib_flags is None else np.asarray(ib_flags)
+    out_k, out_l = [], []
+
+    def field_change(o, field_max, smax, base_thr):
+        rl = int(levels[o]) - base_level
+        if (ib[o] & 1) and (flags[o] & 1):
+            return 1 if rl < n_level_refinement + n_ib_add_level else 0
+        smax *= 1.05
+        if field_max < 1e-10:
+            return -1
+        deletion_factor = 0.7
+        lr = np.log(field_max / smax)
+        l_aim = int(np.ceil(n_level_refinement - lr / np.log(refinement_factor)))
+        l_del = int(np.ceil(n_level_refinement - ((lr - np.log(deletion_factor)) / np.log(refinement_factor))))
+        l_aim = min(l_aim, hard)
+        if rl == 0 and base_thr:
+            if field_max > smax * base_threshold:
+                l_aim = max(l_aim, 0)
+            if field_max > smax * base_threshold * deletion_factor:
+                l_del = max(l_del, 0)
+        if ib[o] & 1:
+            return 0
+        if l_aim - rl > 0:
+            return 1
+        if l_del - rl < 0:
+            return -1
+        return 0
+
+    for o in range(len(keys)):
+        leaf, corr = bool(flags[o] & 1), bool(flags[o] & 2)
+        if not leaf and not corr:
+            continue
+        if leaf and corr:
+            continue
+        l1 = l2 = l3 = -1
+        if leaf and not corr:
+            l1 = field_change(o, cell_aux_max[o], source_max[0], True)
+            l3 = field_change(o, edge_aux_max[o], source_max[1], False)
+        if corr and not leaf:
+            l2 = field_change(o, correction_max[o], source_max[0], False)
+        lv = max(l1, l2, l3)
+        if lv != 0:
+            if leaf and not corr:
+                out_k.append(int(keys[o]))
+                out_l.append(lv)
+            elif corr and not leaf and l2 > 0:
+                out_k.append(key_parent(keys[o]))
+                out_l.append(l2)
+    return np.array(out_k, np.uint64), np.array(out_l, np.int32)

@@ -161,6 +161,28 @@ int iblgf_ns_step(iblgf_ctx* ctx, const int* u_fields, int p_field, double dt, d
  * each stage of iblgf_ns_step runs lin_sys_with_ib_solve with the IB
  * (ifherk.hpp:1451-1517), warm-started from that stage's previous force. */
 int iblgf_ns_options(iblgf_ctx* ctx, const double* frame_vel, double cg_threshold, int cg_max_iter);
+/* ---- Mesh adaptation (Ifherk::adapt, ifherk.hpp:1018-1076, with the server
+ * side of Domain::adapt, decomposition.hpp:182-470) ------------------------
+ * attempts: n_attempts (key, level change) pairs for octants with data, the
+ * output of an adapt condition (for example the one of tests/ns_amr_lgf,
+ * ns_amr_lgf.hpp:402-489, built on iblgf_block_norms): +1 refine (if the 2:1
+ * balance allows it, or the octant is an IB block), -1 delete; correction
+ * blocks that no physical block needs are deleted, base blocks within two
+ * blocks of a kept base block are added (*base_mesh_update = 1 then, and the
+ * next iblgf_ns_step refreshes the velocity). Every field keeps its values on
+ * the octants that stay and is zero on new ones; the n_interp listed fields
+ * (interp_fields: 3 ids per entry, the first used for mesh 0 = cell, all
+ * three for 1 = face / 2 = edge) are interpolated from each parent of a new
+ * leaf above the base level into all its children (nli_intrp_node,
+ * cell_center_nli_intrp.hpp:310-420). Octant indices change: query keys,
+ * levels and flags again (iblgf_domain_info, iblgf_domain_octants). IB points stay attached. */
+int iblgf_adapt(iblgf_ctx* ctx, int n_attempts, const uint64_t* keys, const int* level_change, int n_interp,
+                const int* interp_fields, const int* interp_mesh, int* base_mesh_update);
+/* Operator::maxnorm and blockRootMeanSquare (operators.hpp:1149-1211) of the
+ * vector (n_comp = 1..3 component fields) over each octant's interior nodes:
+ * max_out[o] = max |v|, rms_out[o] = sqrt(mean |v|^2), n_octants each. */
+int iblgf_block_norms(iblgf_ctx* ctx, const int* fields, int n_comp, double* max_out, double* rms_out);
+
 /* IB force (IB::force_prev, n x 3) and CG iteration count of the last
  * step's stage 1, 2 or 3; either output may be NULL */
 int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out, int* iters);

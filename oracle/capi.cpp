@@ -16,6 +16,10 @@ struct Handle
 {
     std::unique_ptr<Domain> d;
     std::unique_ptr<Solver> s;
+    // last adaptation: old canonical index per new octant (-1: new), the
+    // interpolation parents (new canonical indices, in order)
+    std::vector<int> adapt_src, adapt_parents;
+    int adapt_old_n = 0;
 };
 template<class F>
 int guard(F&& f)
@@ -85,6 +89,69 @@ int orc_domain_finalize(void* hp, int subtract_non_leaf)
         h->d->finalize();
         fmm_lgf_mask_build(*h->d, subtract_non_leaf != 0);
         fmm_stream_mask_build(*h->d);
+    });
+}
+
+// Domain::adapt (one process): tree change, new canonical order and masks.
+// *n_octants gets the new octant count; fields follow with orc_adapt_field.
+int orc_adapt(void* hp, int n_att, const unsigned long long* keys, const int* lchange, int subtract_non_leaf,
+              int* base_mesh_update, int* n_octants)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        std::vector<std::pair<u64, int>> att(n_att);
+        for (int i = 0; i < n_att; ++i) att[i] = {(u64)keys[i], lchange[i]};
+        h->adapt_old_n = (int)h->d->octs.size();
+        bool bmu = false;
+        const std::vector<Octant*> parents = h->d->adapt(att, bmu);
+        std::map<Octant*, int> old;
+        h->d->construct_level_maps();
+        for (auto& lm : h->d->level_maps)
+            for (auto& kv : lm) old[kv.second] = kv.second->idx;
+        h->d->construct_lists();
+        h->d->finalize();
+        h->adapt_src.assign(h->d->octs.size(), -1);
+        for (Octant* o : h->d->octs) h->adapt_src[o->idx] = old[o];
+        h->adapt_parents.clear();
+        for (Octant* p : parents) h->adapt_parents.push_back(p->idx);
+        for (Octant* o : h->d->octs)
+            for (auto& m : o->mask) m = {false, false};
+        fmm_lgf_mask_build(*h->d, subtract_non_leaf != 0);
+        fmm_stream_mask_build(*h->d);
+        *base_mesh_update = bmu ? 1 : 0;
+        *n_octants = (int)h->d->octs.size();
+    });
+}
+
+// one component field through the last adaptation: old (old octant count x
+// Nb^3) -> out (new count x Nb^3); mesh >= 0 (0 cell, 1 face, 2 edge, with
+// component comp) also interpolates each parent into all its children
+// (cell_center_nli_intrp.hpp:310-420)
+int orc_adapt_field(void* hp, const double* old, int mesh, int comp, double* out)
+{
+    auto* h = static_cast<Handle*>(hp);
+    return guard([&] {
+        const size_t B = (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
+        const size_t n = h->d->octs.size();
+        Field f(n * B, 0.0);
+        for (size_t i = 0; i < n; ++i)
+            if (h->adapt_src[i] >= 0) std::copy(old + h->adapt_src[i] * B, old + (h->adapt_src[i] + 1) * B, &f[i * B]);
+        if (mesh >= 0)
+        {
+            int rp[3];
+            mesh_relpos(mesh, comp, rp);
+            for (int pi : h->adapt_parents)
+            {
+                Octant* p = h->d->octs[pi];
+                for (int c = 0; c < 8; ++c)
+                {
+                    Octant* ch = p->child[c].get();
+                    if (!ch || !ch->has_data) continue;
+                    h->s->cc_intrp_child(f, p, c, rp);
+                }
+            }
+        }
+        std::copy(f.begin(), f.end(), out);
     });
 }
 

@@ -9,6 +9,8 @@
 //     :617-736 (mark_correction), :878-939 (init_refine), :1092-1106 (refine).
 // Single process: every octant is "locally owned".
 #include <algorithm>
+#include <functional>
+#include <set>
 #include <cmath>
 #include <stack>
 #include <stdexcept>
@@ -466,6 +468,200 @@ void Domain::mark_correction()
     }
     construct_level_maps();
     construct_lists();
+}
+
+bool Domain::leaf_search(const Octant* o, bool require_data) const
+{
+    for (auto& c : o->child)
+        if (c && (!require_data || c->has_data)) return false;
+    return true;
+}
+
+// octree/tree.hpp:455-466: data dropped; an octant without children leaves
+// its parent (and is freed)
+void Domain::delete_oct(Octant* o)
+{
+    o->has_data = false;
+    o->leaf = o->correction = false;
+    o->idx = -1;
+    if (leaf_search(o, false) && o->parent)
+    {
+        Octant* p = o->parent;
+        for (auto& c : p->child)
+            if (c.get() == o) c.reset();
+    }
+}
+
+// Decomposition::adapt_decoposition, server part (domain/decomposition/
+// decomposition.hpp:182-470) for one client; Tree::deletionReset_2to1
+// (octree/tree.hpp:304-327); Domain::delete_all_children (domain.hpp:512-569);
+// baseBlockBufferNumber_ = 2 (domain.hpp:1336)
+std::vector<Octant*> Domain::adapt(const std::vector<std::pair<u64, int>>& attempts, bool& base_mesh_update)
+{
+    base_mesh_update = false;
+    auto all_octants = [&]() {
+        std::vector<Octant*> v{root.get()};
+        dfs(root.get(), [&](Octant* o) { v.push_back(o); });
+        return v;
+    };
+    auto ordered = [](std::vector<Octant*> v) {
+        std::sort(v.begin(), v.end(), [](const Octant* a, const Octant* b) {
+            return a->level != b->level ? a->level < b->level : a->key < b->key;
+        });
+        return v;
+    };
+    auto leaves = [&]() {
+        std::vector<Octant*> v;
+        for (Octant* o : all_octants())
+            if (o->has_data && o->leaf) v.push_back(o);
+        return ordered(v);
+    };
+    auto at_level = [&](int l) {
+        std::vector<Octant*> v;
+        for (Octant* o : all_octants())
+            if (o->has_data && o->level == l) v.push_back(o);
+        return ordered(v);
+    };
+    std::set<u64> old_leaves;
+    for (Octant* o : all_octants())
+    {
+        if (o->has_data && o->leaf) old_leaves.insert(o->key);
+        o->aim_deletion = o->correction && !o->ib;
+    }
+    std::map<Octant*, int> change;
+    for (auto& a : attempts)
+    {
+        if (!a.second) continue;
+        Octant* o = find(a.first);
+        if (!o || !o->has_data) throw std::runtime_error("oracle: adaptation attempt for an octant without data");
+        change[o] = a.second;
+    }
+    std::map<u64, bool> checklist;
+    std::vector<Octant*> to_refine;
+    for (Octant* o : leaves())
+    {
+        auto it = change.find(o);
+        if (it == change.end()) continue;
+        if (it->second < 0) o->aim_deletion = true;
+        else if (o->ib || try_2to1(o->key, checklist))
+            to_refine.push_back(o);
+    }
+    for (Octant* o : leaves())
+        if (o->ib || o->ext_ib) o->aim_deletion = false;
+    // base blocks within two blocks of every kept base block
+    std::set<u64> away;
+    for (Octant* o : at_level(base_level))
+    {
+        if (o->aim_deletion || o->correction) continue;
+        const auto c = key_coord(o->key);
+        for (int dz = -2; dz <= 2; ++dz)
+            for (int dy = -2; dy <= 2; ++dy)
+                for (int dx = -2; dx <= 2; ++dx)
+                {
+                    const int x = c[0] + dx, y = c[1] + dy, z = c[2] + dz;
+                    const int lim = 1 << o->level;
+                    if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) continue;
+                    away.insert(key_make(x, y, z, o->level));
+                }
+    }
+    for (u64 nk : away)
+    {
+        const auto c = key_coord(nk);
+        bool inside = true;
+        for (int d = 0; d < 3; ++d)
+            if (c[d] < 0 || c[d] > key_bd_extent[d] - 1) inside = false;
+        if (!inside) continue;
+        Octant* n = find(nk);
+        if (!n || !n->has_data)
+        {
+            n = insert(nk);
+            alloc(n, n->level - base_level);
+            n->leaf = true;
+            n->correction = false;
+            base_mesh_update = true;
+        }
+        n->aim_deletion = false;
+    }
+    construct_level_maps();
+    for (Octant* o : to_refine)
+        if (o->leaf) refine(o, true);
+    // deletionReset_2to1 from the parents of refined leaves
+    std::set<Octant*> done;
+    std::function<void(Octant*)> reset = [&](Octant* l) {
+        if (done.count(l)) return;
+        if (l->level - base_level < 0) return;
+        for (u64 nk : key_neighbor_keys(l->key))
+        {
+            if (key_is_end(nk)) continue;
+            Octant* n = find(nk);
+            if (!n || !n->has_data) continue;
+            n->aim_deletion = false;
+            reset(n->parent);
+        }
+        done.insert(l);
+    };
+    for (Octant* o : leaves())
+        if (o->level - base_level > 0) reset(o->parent);
+    for (Octant* o : at_level(base_level))
+        if (o->aim_deletion && o->leaf) delete_oct(o);
+    construct_level_maps();
+    // sibling groups whose children all go: the parent becomes the leaf
+    for (int l = depth - 2; l >= base_level; --l)
+        for (Octant* o : at_level(l))
+        {
+            if (leaf_search(o, true)) continue;
+            bool all = true;
+            for (auto& c : o->child)
+            {
+                if (!c || !c->has_data) continue;
+                if (!c->aim_deletion || (!c->leaf && !c->correction))
+                {
+                    all = false;
+                    break;
+                }
+            }
+            for (auto& c : o->child)
+            {
+                if (!c) continue;
+                if (all)
+                {
+                    c->leaf = c->correction = false;
+                    c->aim_deletion = true;
+                }
+                else
+                    c->aim_deletion = false;
+            }
+            if (all)
+            {
+                o->leaf = true;
+                o->correction = false;
+                o->aim_deletion = false;
+            }
+        }
+    construct_level_maps();
+    mark_correction();
+    for (Octant* o : all_octants())
+        if (o->has_data && o->aim_deletion && o->level - base_level > 0) delete_oct(o);
+    for (int l = base_level - 1; l > 0; --l)
+        for (Octant* o : all_octants())
+            if (o->level == l && leaf_search(o, false)) delete_oct(o);
+    // ancestors of new octants get data
+    for (Octant* o : all_octants())
+    {
+        if (!o->has_data || o->idx >= 0) continue;
+        for (Octant* p = o->parent; p && !p->has_data; p = p->parent) alloc(p, p->level - base_level);
+    }
+    depth = 0;
+    for (Octant* o : all_octants())
+        if (o->has_data) depth = std::max(depth, o->level + 1);
+    construct_level_maps();
+    construct_lists();
+    std::vector<Octant*> parents;
+    for (Octant* o : leaves())
+        if (o->level - base_level > 0 && !old_leaves.count(o->key)) parents.push_back(o->parent);
+    parents = ordered(parents);
+    parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
+    return parents;
 }
 
 void Domain::finalize()

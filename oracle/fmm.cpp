@@ -998,6 +998,14 @@ void Solver::cc_intrp_level(Field& from, Field& to, int level, bool correction_o
     }
 }
 
+void Solver::cc_intrp_child(Field& f, Octant* p, int c, const int* rp)
+{
+    const size_t B = (size_t)Nb * Nb * Nb;
+    Octant* ch = p->child[c].get();
+    tp_interp(Nb, cc_intrp[2 * rp[0] + (c & 1)].data(), cc_intrp[2 * rp[1] + ((c >> 1) & 1)].data(),
+              cc_intrp[2 * rp[2] + ((c >> 2) & 1)].data(), &f[p->idx * B], &f[ch->idx * B], false);
+}
+
 // PoissonSolver::apply_if (poisson.hpp:436-494) for AMR2AMR; rp: relative
 // positions of the field's mesh object (cell {1,1,1} when null)
 void Solver::apply_if(const Field& src, Field& tgt, double alpha_base, bool subtract_non_leaf, const int* rp,

@@ -116,6 +116,13 @@ struct Domain
     void refine(Octant* o, bool ratio_2to1);
     void init_refine(int nRef, int level_up_max, RefinePred pred, void* user);
     void mark_correction();
+    // adaptation (server side of Domain::adapt): attempts (key, level change);
+    // returns the parents of new leaves above the base level, (level, key)
+    // order. Octants keep their idx of the previous canonical order until
+    // finalize(); new ones have idx -1.
+    std::vector<Octant*> adapt(const std::vector<std::pair<u64, int>>& attempts, bool& base_mesh_update);
+    bool leaf_search(const Octant* o, bool require_data) const;
+    void delete_oct(Octant* o);
 };
 
 std::unique_ptr<Domain> domain_create(const int* bd_base, const int* bd_extent,
@@ -171,6 +178,8 @@ struct Solver
     // cell_center_nli transfers; rp = relative position per axis (0: node
     // coincides with the child's, 1: half a cell off), cell {1,1,1} when null
     void cc_intrp_level(Field& from, Field& to, int level, bool correction_only, const int* rp = nullptr);
+    // nli_intrp_node of one child: f[child c of p] = interpolation of f[p]
+    void cc_intrp_child(Field& f, Octant* p, int c, const int* rp);
     void coarsify_all(Field& f, const int* rp = nullptr);
     void copy_level_interior(const Field& src, Field& dst, int l) const;
 };

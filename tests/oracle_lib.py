@@ -38,6 +38,8 @@ def lib():
         L.orc_nli_matrix.argtypes = [ci, ci, vp]
         L.orc_cc_matrix.argtypes = [ci, ci, ci, vp]
         L.orc_domain_create.restype = vp
+        L.orc_adapt.argtypes = [vp, ci, vp, vp, ci, vp, vp]
+        L.orc_adapt_field.argtypes = [vp, vp, ci, ci, vp]
         L.orc_domain_create.argtypes = [vp, vp, ci, cd, ci, vp, vp]
         L.orc_domain_destroy.argtypes = [vp]
         L.orc_domain_init_refine.argtypes = [vp, ci, ci, PRED_T, vp]
@@ -127,6 +129,12 @@ class Domain:
             self._cb = PRED_T(lambda *a: 0)
             _check(L.orc_domain_init_refine(self.h, 0, 0, self._cb, None))
         _check(L.orc_domain_finalize(self.h, 1 if subtract_non_leaf else 0))
+        self._subtract_non_leaf = subtract_non_leaf
+        self._load_octants()
+        _check(L.orc_solver_create(self.h, intrp_order))
+
+    def _load_octants(self):
+        L = lib()
         bl, dp, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         L.orc_domain_info(self.h, ctypes.byref(bl), ctypes.byref(dp), ctypes.byref(n))
         self.base_level, self.depth, self.n = bl.value, dp.value, n.value
@@ -135,7 +143,26 @@ class Domain:
         self.flags = np.zeros(self.n, np.int32)
         self.bbase = np.zeros((self.n, 3), np.int32)
         L.orc_domain_octants(self.h, _p(self.keys), _p(self.levels), _p(self.flags), _p(self.bbase))
-        _check(L.orc_solver_create(self.h, intrp_order))
+
+    def adapt(self, keys, level_change, fields=()):
+        """Domain::adapt (decomposition.hpp:182-470, one process) with the
+        attempts (keys, level_change); `fields` lists (array (n, Nb, Nb, Nb),
+        mesh, comp) with mesh -1 (remap only) or 0 cell / 1 face / 2 edge
+        (remap, then interpolation into the children of each new leaf's
+        parent). Returns (base_mesh_update, remapped fields)."""
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        lc = np.ascontiguousarray(level_change, dtype=np.int32)
+        bmu, n = ctypes.c_int(), ctypes.c_int()
+        _check(lib().orc_adapt(self.h, len(k), _p(k), _p(lc), 1 if self._subtract_non_leaf else 0,
+                               ctypes.byref(bmu), ctypes.byref(n)))
+        self._load_octants()
+        out = []
+        for f, mesh, comp in fields:
+            old = np.ascontiguousarray(f, dtype=np.float64)
+            new = np.zeros((self.n, self.Nb, self.Nb, self.Nb))
+            _check(lib().orc_adapt_field(self.h, _p(old), int(mesh), int(comp), _p(new)))
+            out.append(new)
+        return bool(bmu.value), out
 
     def __del__(self):
         if getattr(self, "h", None):

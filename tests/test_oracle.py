@@ -188,6 +188,57 @@ def test_ns_step_oracle_velocity_refresh():
     assert div_max(u_ref) < 0.05 * div_max(u0)
 
 
+def test_adapt_oracle_refines_balanced_and_keeps_data():
+    """Domain::adapt (decomposition.hpp:182-470): refinement attempts near the
+    vortex ring add a level, the refined tree stays 2:1 balanced (every
+    neighbour key of a refined leaf's parent exists with data), octants that
+    stay keep their values, a constant face field interpolates exactly into
+    the new children, and the base mesh grows to two blocks around its kept
+    blocks (base_mesh_update)."""
+    import adapt_cases as A
+    case = S.VortexRingNS("small")
+    d = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    att_k, att_l = A.ring_attempts(d.keys, d.levels, d.flags, d.bbase, d.base_level, d.block_extent,
+                                   case.bd_base, case.bd_extent)
+    assert (att_l > 0).sum() > 0
+    old_keys, old_depth, old_n = d.keys.copy(), d.depth, d.n
+    rnd = np.random.default_rng(3).standard_normal((d.n, d.Nb, d.Nb, d.Nb))
+    ones = np.ones((d.n, d.Nb, d.Nb, d.Nb))
+    bmu, (r2, o2) = d.adapt(att_k, att_l, [(rnd, -1, 0), (ones, 1, 0)])
+    assert d.depth == old_depth + 1 and d.n > old_n and bmu
+    pos = {int(k): i for i, k in enumerate(d.keys)}
+    old_pos = {int(k): i for i, k in enumerate(old_keys)}
+    for k, i in old_pos.items():
+        if k in pos:
+            assert np.array_equal(r2[pos[k]], rnd[i])
+    # 2:1 balance: the parent of every leaf above the base level has all
+    # existing-in-domain neighbour keys present
+    leaf = (d.flags & 1) != 0
+    new_leaves = [i for i in range(d.n) if leaf[i] and int(d.keys[i]) not in old_pos
+                  and d.levels[i] > d.base_level]
+    assert new_leaves
+    for i in new_leaves:
+        p = S.key_parent(d.keys[i])
+        assert p in pos, hex(p)
+        assert np.abs(o2[i, 1:-1, 1:-1, 1:-1] - 1.0).max() < 1e-12
+    for i in range(d.n):
+        if not leaf[i] or d.levels[i] <= d.base_level:
+            continue
+        pl = d.levels[i] - 1
+        pc = (d.bbase[i] // 2) // d.block_extent  # parent block coordinate at its level
+        for off in np.ndindex(3, 3, 3):
+            q = pc + np.array(off) - 1
+            if (q < 0).any():
+                continue
+            hit = [j for j in range(d.n) if d.levels[j] == pl and
+                   np.array_equal(d.bbase[j] // d.block_extent, q)]
+            lo = np.array(case.bd_base) // d.block_extent * 2 ** (pl - d.base_level)
+            hi = lo + np.array(case.bd_extent) // d.block_extent * 2 ** (pl - d.base_level)
+            if ((q >= lo) & (q < hi)).all():
+                assert hit, (i, q)
+
+
 def test_ib_solve_oracle_converges_on_sphere():
     """IB force solve (linsys.hpp:113-230) on the sphere: the CG reaches its
     threshold well before the iteration limit, IB blocks sit at the finest
