@@ -12,6 +12,7 @@
 // Also the per-block norms of the adaptation criterion: Operator::maxnorm and
 // blockRootMeanSquare (operators/operators.hpp:1149-1211).
 #include <algorithm>
+#include <set>
 
 #include "ctx.hpp"
 
@@ -60,6 +61,10 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
         if (t.o[i].has_data && t.o[i].idx >= 0 && !of.empty()) ib[i] = (char)of[t.o[i].idx];
     std::vector<std::pair<u64, int>> att(n_att);
     for (int i = 0; i < n_att; ++i) att[i] = {keys[i], lchange[i]};
+    // base-level correction blocks before the change (Octant::old_correction)
+    std::set<u64> old_corr_keys;
+    for (int o = 0; o < c.n_oct; ++o)
+        if (c.levels[o] == t.base_level && (c.flags[o] & 2)) old_corr_keys.insert(c.keys[o]);
     bool bmu = false;
     const std::vector<int> parents = t.adapt(att, ib, bmu);
     // old canonical index of every tree position that keeps its data
@@ -124,7 +129,9 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
             IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // tt goes out of scope
         }
     }
-    ns_on_adapt(c, bmu);
+    std::vector<char> old_corr(c.n_oct, 0);
+    for (int o = 0; o < c.n_oct; ++o) old_corr[o] = c.levels[o] == t.base_level && old_corr_keys.count(c.keys[o]);
+    ns_on_adapt(c, bmu, old_corr);
     ib_on_adapt(c);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     if (base_mesh_update) *base_mesh_update = bmu ? 1 : 0;

@@ -394,6 +394,23 @@ int iblgf_adapt(iblgf_ctx* x, int n_attempts, const uint64_t* keys, const int* l
     });
 }
 
+int iblgf_ns_fields(iblgf_ctx* x, int* ids)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ns_fields(c, ids); });
+}
+
+int iblgf_ns_clean(iblgf_ctx* x, int field, int non_leaf_only, int width)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ns_clean(c, field, non_leaf_only != 0, width); });
+}
+
+int iblgf_ns_clean_leaf_correction_boundary(iblgf_ctx* x, const int* fields, int n, int level, int leaf_only_boundary)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::ns_clean_leaf_correction_boundary(c, fields, n, level, leaf_only_boundary != 0);
+    });
+}
+
 int iblgf_block_norms(iblgf_ctx* x, const int* fields, int n_comp, double* max_out, double* rms_out)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::block_norms(c, fields, n_comp, max_out, rms_out); });

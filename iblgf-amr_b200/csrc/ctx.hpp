@@ -351,7 +351,12 @@ void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max
 void ns_release(const Ctx* c);
 // after an adaptation: the time step's per-tree lists are rebuilt, its graph
 // dropped; base_mesh_update forces a velocity refresh at the next step
-void ns_on_adapt(Ctx& c, bool base_mesh_update);
+void ns_on_adapt(Ctx& c, bool base_mesh_update, const std::vector<char>& old_corr);
+// Ifherk's scratch fields read by the adapt condition: cell_aux, edge_aux[3],
+// correction_tmp of the Poisson solver
+void ns_fields(Ctx& c, int* ids);
+void ns_clean(Ctx& c, int field, bool non_leaf_only, int width);
+void ns_clean_leaf_correction_boundary(Ctx& c, const int* fields, int n, int level, bool leaf_only_boundary);
 void ib_on_adapt(Ctx& c);
 // per-octant IB flags (bit 0 is_ib, bit 1 is_extended_ib); empty without IB
 std::vector<int> ib_octant_flags(Ctx& c);

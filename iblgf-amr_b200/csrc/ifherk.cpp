@@ -14,6 +14,7 @@
 // velocity, no adaptation, no body force. The velocity refresh (pad_velocity
 // + adapt_corr_time_step, taken once (T - T_last_refresh) 3.3 / (Re dx_base^2)
 // > 7, ifherk.hpp:1093-1111) runs with direct launches.
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -22,7 +23,7 @@
 
 namespace iblgf_b200
 {
-void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only);
+void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only, int width = 1);
 void launch_axpby(Ctx& c, double* to, const double* from, double a, int mode);
 void launch_smooth(Ctx& c, double* f, const int* list, const int* ptr, const int* dirs, int n, int reps);
 
@@ -58,6 +59,9 @@ struct NsState
     std::vector<DevBuf<int>> corr;   // per level: correction blocks
     std::vector<DevBuf<int>> nc;     // per level: blocks that are not correction blocks
     std::vector<DevBuf<double>> nc_dx;
+    // Octant::old_correction (ifherk.hpp:247-258): base-level correction flags
+    // from before the last adaptation, in force for the step that follows it
+    std::vector<char> old_corr;
     // smooth2zero lists of the base level for leaf_only_boundary false / true
     DevBuf<int> sm_list[2], sm_ptr[2], sm_dirs[2];
     int sm_n[2] = {0, 0};
@@ -88,6 +92,9 @@ struct NsOptions
 };
 std::map<const Ctx*, NsOptions> g_nsopt;
 std::map<const Ctx*, std::unique_ptr<NsState>> g_ns;
+// an adaptation before the context's first time step: its old-correction
+// flags and base-mesh update wait for the time step's state
+std::map<const Ctx*, std::pair<std::vector<char>, bool>> g_ns_pending;
 
 VF make_vf(Ctx& c, int mesh)
 {
@@ -99,6 +106,15 @@ VF make_vf(Ctx& c, int mesh)
 }
 
 void ns_build_lists(Ctx& c, NsState& st);
+
+// the loop's next iteration copies the correction flags into the old ones
+// (ifherk.hpp:247-258): without an adaptation in between they add nothing
+void drop_old_correction(Ctx& c, NsState& s)
+{
+    if (s.old_corr.empty()) return;
+    s.old_corr.clear();
+    ns_build_lists(c, s);
+}
 
 NsState& ns_state(Ctx& c)
 {
@@ -115,6 +131,13 @@ NsState& ns_state(Ctx& c)
     s->cell_aux = make_vf(c, kCell);
     s->face_aux = make_vf(c, kFace);
     s->edge_aux = make_vf(c, kEdge);
+    auto pend = g_ns_pending.find(&c);
+    if (pend != g_ns_pending.end())
+    {
+        s->old_corr = pend->second.first;
+        s->force_refresh = pend->second.second;
+        g_ns_pending.erase(pend);
+    }
     ns_build_lists(c, *s);
     auto& ref = *s;
     g_ns.emplace(&c, std::move(s));
@@ -132,12 +155,18 @@ void ns_build_lists(Ctx& c, NsState& st)
     s->corr.resize(c.level_octs.size());
     s->nc.resize(c.level_octs.size());
     s->nc_dx.resize(c.level_octs.size());
+    auto old = [&](int o) { return o < (int)s->old_corr.size() && s->old_corr[o]; };
     for (size_t l = 0; l < c.level_octs.size(); ++l)
     {
         std::vector<int> v, w;
         for (int o : c.level_octs[l])
             (c.flags[o] & 2 ? v : w).push_back(o);
-        s->corr[l].upload(v, c.stream);
+        // clean_leaf_correction_boundary zeroes correction or old-correction blocks
+        std::vector<int> vz = v;
+        for (int o : w)
+            if (old(o)) vz.push_back(o);
+        std::sort(vz.begin(), vz.end());
+        s->corr[l].upload(vz, c.stream);
         s->nc[l].upload(w, c.stream);
         s->nc_dx[l].upload(std::vector<double>(w.size(), c.cfg.dx_base / std::pow(2.0, (int)l - c.tree.base_level)),
                            c.stream);
@@ -152,7 +181,7 @@ void ns_build_lists(Ctx& c, NsState& st)
             for (int i = 0; i < 27; ++i)
             {
                 const int q = c.nbr[27 * (size_t)o + i];
-                if (q < 0 || (lo && (c.flags[q] & 2))) dirs.push_back(i);
+                if (q < 0 || (lo && ((c.flags[q] & 2) || old(q)))) dirs.push_back(i);
             }
             if (dirs.size() == d0) continue;
             list.push_back(o);
@@ -498,6 +527,7 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
             st.time_step(uf, pf, true);
             ++s.steps_done;
             *T += dt;
+            drop_old_correction(c, s);
             continue;
         }
         const bool graphable = !ib_active(c) && !c.profile && !s.graph_failed;
@@ -561,8 +591,45 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
         }
         ++s.steps_done;
         *T += dt;
+        drop_old_correction(c, s);
     }
     IBLGF_CUDA(cudaGetLastError());
+}
+
+void ns_fields(Ctx& c, int* ids)
+{
+    need_single(c);
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    NsState& s = ns_state(c);
+    ids[0] = s.cell_aux.id[0];
+    for (int k = 0; k < 3; ++k) ids[1 + k] = s.edge_aux.id[k];
+    ids[4] = c.f_correction_tmp;
+}
+
+void ns_clean(Ctx& c, int field, bool non_leaf_only, int width)
+{
+    need_single(c);
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (field < 0 || field >= (int)c.fields.size() || width < 1 || width > c.Nb / 2)
+        throw Error(IBLGF_EINVAL, "bad clean arguments");
+    NsState& s = ns_state(c);
+    launch_clean(c, c.field(field), s.leaf.p, non_leaf_only, width);
+}
+
+void ns_clean_leaf_correction_boundary(Ctx& c, const int* fields, int n, int level, bool leaf_only_boundary)
+{
+    need_single(c);
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (n < 1 || n > 3 || level < 0 || level > kMaxLevel) throw Error(IBLGF_EINVAL, "bad arguments");
+    for (int k = 0; k < n; ++k)
+        if (fields[k] < 0 || fields[k] >= (int)c.fields.size()) throw Error(IBLGF_EINVAL, "bad field id");
+    NsState& s = ns_state(c);
+    if (leaf_only_boundary && level < (int)s.corr.size())
+        for (int k = 0; k < n; ++k) launch_zero_blocks(c, c.field(fields[k]), s.corr[level].p, (int)s.corr[level].n);
+    if (level != c.tree.base_level) return;
+    const int v = leaf_only_boundary ? 1 : 0;
+    for (int k = 0; k < n; ++k)
+        launch_smooth(c, c.field(fields[k]), s.sm_list[v].p, s.sm_ptr[v].p, s.sm_dirs[v].p, s.sm_n[v], n);
 }
 
 void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter)
@@ -574,11 +641,18 @@ void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max
     o.cg_max_iter = cg_max_iter;
 }
 
-void ns_on_adapt(Ctx& c, bool base_mesh_update)
+void ns_on_adapt(Ctx& c, bool base_mesh_update, const std::vector<char>& old_corr)
 {
     auto it = g_ns.find(&c);
-    if (it == g_ns.end()) return;
+    if (it == g_ns.end())
+    {
+        auto& pend = g_ns_pending[&c];
+        pend.first = old_corr;
+        pend.second = pend.second || base_mesh_update;
+        return;
+    }
     NsState& s = *it->second;
+    s.old_corr = old_corr;
     if (s.graph) cudaGraphExecDestroy(s.graph);
     s.graph = nullptr;
     s.graph_failed = false;
@@ -595,6 +669,7 @@ void ns_release(const Ctx* c)
     if (it != g_ns.end() && it->second->graph) cudaGraphExecDestroy(it->second->graph);
     g_ns.erase(c);
     g_nsopt.erase(c);
+    g_ns_pending.erase(c);
 }
 
 }  // namespace iblgf_b200

@@ -1,6 +1,6 @@
 // Field kernels of the IF-HERK time step (FP64, whole component fields):
 //   clean_kernel     Ifherk::clean (ifherk.hpp:1309-1352): zero whole blocks,
-//                    or with non_leaf_only only the one-cell buffer shell of
+//                    or with non_leaf_only only the outer `width` planes of
 //                    leaves and all of every other block
 //   axpby_kernel     Ifherk::copy / add (ifherk.hpp:1878-1960) and in-place
 //                    scaling, over every node including buffers
@@ -18,7 +18,7 @@ namespace iblgf_b200
 namespace
 {
 template<int NB>
-__global__ void clean_kernel(double* __restrict__ f, const int* __restrict__ leaf, int non_leaf_only)
+__global__ void clean_kernel(double* __restrict__ f, const int* __restrict__ leaf, int non_leaf_only, int w)
 {
     constexpr int N3 = NB * NB * NB;
     const int o = blockIdx.x;
@@ -29,7 +29,7 @@ __global__ void clean_kernel(double* __restrict__ f, const int* __restrict__ lea
         if (shell)
         {
             const int x = i % NB, y = (i / NB) % NB, z = i / (NB * NB);
-            if (x != 0 && y != 0 && z != 0 && x != NB - 1 && y != NB - 1 && z != NB - 1) continue;
+            if (x >= w && y >= w && z >= w && x < NB - w && y < NB - w && z < NB - w) continue;
         }
         b[i] = 0.0;
     }
@@ -102,12 +102,12 @@ void nb_switch(int Nb, F&& f)
 }
 }  // namespace
 
-void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only)
+void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only, int width)
 {
     if (!c.n_oct) return;
     nb_switch(c.Nb, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
-        clean_kernel<NB><<<c.n_oct, 256, 0, c.stream>>>(f, d_leaf, non_leaf_only ? 1 : 0);
+        clean_kernel<NB><<<c.n_oct, 256, 0, c.stream>>>(f, d_leaf, non_leaf_only ? 1 : 0, width);
     });
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());

@@ -39,7 +39,8 @@ EXPORTS = [
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
     "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_warmstart", "iblgf_ib_warmstart_info",
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
-    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms",
+    "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
+    "iblgf_ns_clean_leaf_correction_boundary",
     "iblgf_fma_peak",
 ]
 
@@ -103,6 +104,9 @@ def lib():
     L.iblgf_stats.argtypes = [vp, vp]
     L.iblgf_stats_n.argtypes = [vp, vp, ci]
     L.iblgf_adapt.argtypes = [vp, ci, vp, vp, ci, vp, vp, vp]
+    L.iblgf_ns_fields.argtypes = [vp, vp]
+    L.iblgf_ns_clean.argtypes = [vp, ci, ci, ci]
+    L.iblgf_ns_clean_leaf_correction_boundary.argtypes = [vp, vp, ci, ci, ci]
     L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     _lib = L
@@ -185,6 +189,61 @@ class Solver:
         rms = np.zeros(self.n)
         self._check(lib().iblgf_block_norms(self.h, _p(f), len(f), _p(mx), _p(rms)))
         return mx, rms
+
+    def ns_fields(self):
+        """Ids of the IF-HERK scratch fields the adapt condition reads:
+        (cell_aux, [edge_aux x, y, z], correction_tmp)."""
+        ids = np.zeros(5, np.int32)
+        self._check(lib().iblgf_ns_fields(self.h, _p(ids)))
+        return int(ids[0]), [int(x) for x in ids[1:4]], int(ids[4])
+
+    def ns_clean(self, field, non_leaf_only=False, width=1):
+        """Ifherk::clean (ifherk.hpp:1309-1352)."""
+        self._check(lib().iblgf_ns_clean(self.h, int(field), 1 if non_leaf_only else 0, int(width)))
+
+    def ns_clean_leaf_correction_boundary(self, fields, level, leaf_only_boundary=False):
+        """Ifherk::clean_leaf_correction_boundary (ifherk.hpp:1355-1411) of a
+        1- or 3-component field."""
+        f = np.ascontiguousarray(fields, dtype=np.int32).ravel()
+        self._check(lib().iblgf_ns_clean_leaf_correction_boundary(self.h, _p(f), len(f), int(level),
+                                                                  1 if leaf_only_boundary else 0))
+
+    def ns_march(self, u, p, dt, Re, T, n_steps, adapt_freq=0, adapt_condition=None, source_max=(1.0, 1.0),
+                 updating_source_max=True, all_time_max=False):
+        """Ifherk::time_march (ifherk.hpp:176-400) without output or restart.
+        Per iteration: the non-leaf cleaning of cell_aux (width 2), edge_aux
+        (1) and correction_tmp (2); every adapt_freq-th iteration but the
+        first, source_max updated from the block RMS of cell_aux / edge_aux
+        (update_source_max, :401-426) and one adaptation (Ifherk::adapt with
+        coarsify_field = false, :1018-1076): cell_aux and edge_aux tapered at
+        the base level, adapt_condition(solver, max cell_aux, max
+        correction_tmp, max edge_aux, source_max) -> (keys, level_change),
+        iblgf_adapt with the velocity interpolated; then one time step. (The
+        loop's clean<u>(true) before the balance step repeats the step's own
+        first clean and is left out.) Returns (T, source_max, attempts of each
+        adaptation)."""
+        import iblgf_setups as S
+        sm = [float(source_max[0]), float(source_max[1])]
+        history = []
+        for it in range(int(n_steps)):
+            cell, edge, corr = self.ns_fields()
+            self.ns_clean(cell, True, 2)
+            for e in edge:
+                self.ns_clean(e, True, 1)
+            self.ns_clean(corr, True, 2)
+            if adapt_freq and it % adapt_freq == 0 and it != 0 and adapt_condition is not None:
+                if updating_source_max:
+                    sm[0] = S.update_source_max(sm[0], self.block_norms([cell])[1], all_time_max)
+                    sm[1] = S.update_source_max(sm[1], self.block_norms(edge)[1], all_time_max)
+                if sm[0] >= 1e-10 and sm[1] >= 1e-10:
+                    self.ns_clean_leaf_correction_boundary([cell], self.base_level, True)
+                    self.ns_clean_leaf_correction_boundary(edge, self.base_level, True)
+                    keys, lc = adapt_condition(self, self.block_norms([cell])[0], self.block_norms([corr])[0],
+                                               self.block_norms(edge)[0], sm)
+                    self.adapt(keys, lc, interpolate=[(1, list(u))])
+                    history.append((np.array(keys, np.uint64), np.array(lc, np.int32)))
+            T = self.ns_step(u, p, dt, Re, T, 1)
+        return T, sm, history
 
     def adapt(self, keys, level_change, interpolate=()):
         """One adaptation (Ifherk::adapt, ifherk.hpp:1018-1076): `keys` /

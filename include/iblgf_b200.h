@@ -178,6 +178,20 @@ int iblgf_ns_options(iblgf_ctx* ctx, const double* frame_vel, double cg_threshol
  * levels and flags again (iblgf_domain_info, iblgf_domain_octants). IB points stay attached. */
 int iblgf_adapt(iblgf_ctx* ctx, int n_attempts, const uint64_t* keys, const int* level_change, int n_interp,
                 const int* interp_fields, const int* interp_mesh, int* base_mesh_update);
+/* The IF-HERK step's scratch fields that the adapt condition reads: ids[0]
+ * cell_aux, ids[1..3] edge_aux (vorticity components), ids[4] the Poisson
+ * solver's correction_tmp. Their values are those of the last step. */
+int iblgf_ns_fields(iblgf_ctx* ctx, int* ids);
+/* Ifherk::clean (ifherk.hpp:1309-1352): zero the field, or with
+ * non_leaf_only every non-leaf block and the outer `width` planes of leaves. */
+int iblgf_ns_clean(iblgf_ctx* ctx, int field, int non_leaf_only, int width);
+/* Ifherk::clean_leaf_correction_boundary (ifherk.hpp:1355-1411) of a field of
+ * n = 1..3 components at `level`: with leaf_only_boundary, correction (and, for
+ * the step after an adaptation, former base-level correction) blocks are
+ * zeroed; at the base level every block next to a missing (or correction)
+ * neighbour is tapered towards it (smooth2zero, once per component). */
+int iblgf_ns_clean_leaf_correction_boundary(iblgf_ctx* ctx, const int* fields, int n, int level,
+                                            int leaf_only_boundary);
 /* Operator::maxnorm and blockRootMeanSquare (operators.hpp:1149-1211) of the
  * vector (n_comp = 1..3 component fields) over each octant's interior nodes:
  * max_out[o] = max |v|, rms_out[o] = sqrt(mean |v|^2), n_octants each. */

@@ -20,6 +20,9 @@ struct Handle
     // interpolation parents (new canonical indices, in order)
     std::vector<int> adapt_src, adapt_parents;
     int adapt_old_n = 0;
+    // IF-HERK state kept across orc_ns_step calls (the device keeps it per context)
+    double ns_T_last = 0.0;
+    bool ns_force_refresh = false;
 };
 template<class F>
 int guard(F&& f)
@@ -120,6 +123,7 @@ int orc_adapt(void* hp, int n_att, const unsigned long long* keys, const int* lc
         fmm_stream_mask_build(*h->d);
         *base_mesh_update = bmu ? 1 : 0;
         *n_octants = (int)h->d->octs.size();
+        h->ns_force_refresh = h->ns_force_refresh || bmu;
     });
 }
 
@@ -303,8 +307,12 @@ int orc_ns_step(void* hp, double dt, double Re, double T0, double* u, double* p,
         const size_t n = h->d->octs.size() * (size_t)h->d->Nb * h->d->Nb * h->d->Nb;
         Ifherk ns(h->d.get(), h->s.get(), dt, Re);
         ns.T = T0;
+        ns.T_last_vel_refresh = h->ns_T_last;
+        ns.force_refresh = h->ns_force_refresh;
         for (int k = 0; k < 3; ++k) ns.u.c[k].assign(u + k * n, u + (k + 1) * n);
         for (int st = 0; st < n_steps; ++st) ns.time_step();
+        h->ns_T_last = ns.T_last_vel_refresh;
+        h->ns_force_refresh = ns.force_refresh;
         for (int k = 0; k < 3; ++k) std::memcpy(u + k * n, ns.u.c[k].data(), n * sizeof(double));
         std::memcpy(p, ns.p.c[0].data(), n * sizeof(double));
     });
@@ -325,6 +333,8 @@ int orc_ns_step_ib(void* hp, double dt, double Re, double T0, double* u, double*
         IbSystem ib(h->d.get(), h->s.get(), pts, Re);
         Ifherk ns(h->d.get(), h->s.get(), dt, Re);
         ns.T = T0;
+        ns.T_last_vel_refresh = h->ns_T_last;
+        ns.force_refresh = h->ns_force_refresh;
         ns.ib = &ib;
         ns.cg_threshold = threshold;
         ns.cg_max_iter = max_iter;
@@ -332,6 +342,8 @@ int orc_ns_step_ib(void* hp, double dt, double Re, double T0, double* u, double*
         for (auto& fp : ns.force_prev) fp.assign(n_pts, {0.0, 0.0, 0.0});
         for (int k = 0; k < 3; ++k) ns.u.c[k].assign(u + k * n, u + (k + 1) * n);
         for (int st = 0; st < n_steps; ++st) ns.time_step();
+        h->ns_T_last = ns.T_last_vel_refresh;
+        h->ns_force_refresh = ns.force_refresh;
         for (int k = 0; k < 3; ++k) std::memcpy(u + k * n, ns.u.c[k].data(), n * sizeof(double));
         std::memcpy(p, ns.p.c[0].data(), n * sizeof(double));
         for (int sidx = 1; sidx <= 3; ++sidx)

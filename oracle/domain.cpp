@@ -527,6 +527,8 @@ std::vector<Octant*> Domain::adapt(const std::vector<std::pair<u64, int>>& attem
     {
         if (o->has_data && o->leaf) old_leaves.insert(o->key);
         o->aim_deletion = o->correction && !o->ib;
+        // time_march (ifherk.hpp:247-258): old_correction = correction on the base level
+        o->old_correction = o->has_data && o->level == base_level && o->correction;
     }
     std::map<Octant*, int> change;
     for (auto& a : attempts)

@@ -149,7 +149,7 @@ void Ifherk::clean_leaf_correction_boundary(VField& f, int l, bool leaf_only_bou
     for (auto& kv : d->level_maps[l])
     {
         Octant* o = kv.second;
-        if (leaf_only_boundary && o->correction)
+        if (leaf_only_boundary && (o->correction || o->old_correction))
             for (auto& comp : f.c) std::fill(&comp[o->idx * B], &comp[o->idx * B] + B, 0.0);
     }
     if (l != d->base_level) return;
@@ -159,7 +159,7 @@ void Ifherk::clean_leaf_correction_boundary(VField& f, int l, bool leaf_only_bou
         for (int i = 0; i < 27; ++i)
         {
             Octant* n = o->neighbor[i];
-            if (!n || !n->has_data || (leaf_only_boundary && n->correction))
+            if (!n || !n->has_data || (leaf_only_boundary && (n->correction || n->old_correction)))
                 // the reference calls smooth2zero (which scales every
                 // component) once per component of the field
                 for (size_t rep = 0; rep < f.c.size(); ++rep) smooth2zero(f, o, i);
@@ -350,8 +350,9 @@ void Ifherk::time_step()
 {
     const double dx = d->dx_base;
     // ifherk.hpp:1093-1111: the velocity refresh replaces up_and_down(u)
-    if ((T - T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
+    if (force_refresh || (T - T_last_vel_refresh) / (Re * dx * dx) * 3.3 > 7)
     {
+        force_refresh = false;
         T_last_vel_refresh = T;
         pad_velocity();
         adapt_corr_time_step();
@@ -402,5 +403,7 @@ void Ifherk::time_step()
     copy(u_i, u, 1.0);
     copy(d_i, p, 1.0 / coeff_a(3, 3) / dt);
     T += dt;
+    // the next loop iteration resets old_correction to the correction flags
+    for (Octant* o : d->octs) o->old_correction = false;
 }
 }  // namespace orc

@@ -78,6 +78,7 @@ struct Octant
     int bbase[3] = {0, 0, 0};  // block base (level cell units, no buffer)
     int data_level = 0;        // refinement level given at allocation
     bool leaf = false, correction = false, physical = false, aim_deletion = false;
+    bool old_correction = false;  // base-level correction flag before the last adaptation
     bool ib = false, ext_ib = false;  // immersed-boundary blocks (server.hpp:544-576)
     std::array<Octant*, 27> neighbor{};
     std::array<Octant*, 189> influence{};
@@ -203,6 +204,7 @@ struct Ifherk
     Solver* s;
     double dt, Re;
     double T = 0.0, T_last_vel_refresh = 0.0;
+    bool force_refresh = false;  // base_mesh_update of the last adaptation
     double a[6] = {1.0 / 3, -1.0, 2.0, 0.0, 0.75, 0.25};
     // immersed boundary (optional): force of the previous step per stage
     // (IB::force_prev, the CG warm start), CG settings, frame velocity

@@ -83,3 +83,35 @@ def test_block_norms_match_numpy():
     assert np.allclose(rms, np.sqrt(mag2.mean(1)), rtol=1e-13, atol=0)
     with pytest.raises(B.IblgfError):
         g.block_norms([uf[0], uf[1], uf[2], uf[0]])
+
+
+def test_ns_march_with_adaptation_matches_oracle_replay():
+    """Ifherk::time_march with adaptation (adapt_frequency 2): three
+    iterations, the third preceded by an adaptation whose attempts come from
+    the NS setup's adapt condition (ns_amr_lgf.hpp:402-489) on the device's
+    block norms; the oracle replays the same sequence (two steps, the same
+    attempts with the velocity interpolated, one step, a grown base mesh
+    refreshing the velocity and the former correction blocks cleaned as such
+    for that step). Velocity and pressure, FP64, <= 1e-10."""
+    case = S.VortexRingNS("small")
+    o, g = make(case)
+    u0 = case.initial_velocity(o)
+    dt = case.dt()
+
+    def cond(sv, mc, mk, me, sm):
+        return S.adapt_level_change(sv.keys, sv.levels, sv.flags, sv.base_level, mc, mk, me, sm,
+                                    n_level_refinement=sv.depth - sv.base_level)
+
+    uf = [g.field(u0[k]) for k in range(3)]
+    pf = g.field()
+    n0 = g.n
+    T, sm, hist = g.ns_march(uf, pf, dt, case.Re, 0.0, 3, adapt_freq=2, adapt_condition=cond)
+    assert len(hist) == 1 and len(hist[0][0]) > 0 and g.n != n0
+    assert abs(T - 3 * dt) < 1e-14
+    uo, _ = o.ns_step(u0, dt, case.Re, 0.0, 2)
+    _, (ux, uy, uz) = o.adapt(hist[0][0], hist[0][1], [(uo[0], 1, 0), (uo[1], 1, 1), (uo[2], 1, 2)])
+    assert np.array_equal(g.keys, o.keys) and np.array_equal(g.flags, o.flags)
+    ur, pr = o.ns_step(np.stack([ux, uy, uz]), dt, case.Re, 2 * dt, 1)
+    for k in range(3):
+        assert rel_linf(g.download(uf[k]), ur[k]) < 1e-10, (k, rel_linf(g.download(uf[k]), ur[k]))
+    assert rel_linf(g.download(pf), pr) < 1e-10, rel_linf(g.download(pf), pr)
