@@ -54,31 +54,40 @@ __device__ __forceinline__ double taper(double x)
     return (0.5 + 0.5 * tanh(fac * (x - shift))) + c;
 }
 
-// entries [ptr[b], ptr[b+1]) of block list[b]: neighbour directions (0..26)
+// entries [ptr[b], ptr[b+1]) of block list[b]: neighbour directions (0..26).
+// The taper takes 2 NB distinct values (node index i from the low or the high
+// side); the CTA evaluates them once into shared memory.
 template<int NB>
 __global__ void smooth_kernel(double* __restrict__ f, const int* __restrict__ list, const int* __restrict__ ptr,
                               const int* __restrict__ dirs, int reps)
 {
     constexpr int N3 = NB * NB * NB;
+    __shared__ double tlo[NB], thi[NB];  // taper(i / (NB-1)), taper(1 - i / (NB-1))
+    if (threadIdx.x < NB)
+    {
+        // local_pct over the block with its buffer (node.hpp:121-124)
+        const double pc = (double)threadIdx.x / (NB - 1);
+        tlo[threadIdx.x] = taper(pc);
+        thi[threadIdx.x] = taper(1.0 - pc);
+    }
+    __syncthreads();
     double* b = f + (size_t)list[blockIdx.x] * N3;
     const int e0 = ptr[blockIdx.x], e1 = ptr[blockIdx.x + 1];
     for (int i = threadIdx.x; i < N3; i += blockDim.x)
     {
         const int ix = i % NB, iy = (i / NB) % NB, iz = i / (NB * NB);
-        // local_pct over the block with its buffer (node.hpp:121-124)
-        const double px = (double)ix / (NB - 1), py = (double)iy / (NB - 1), pz = (double)iz / (NB - 1);
         double v = b[i];
         for (int e = e0; e < e1; ++e)
         {
             const int d = dirs[e], x = d % 3, y = (d / 3) % 3, z = d / 9;
             double sq = 0.0;
             int cnt = 0;
-            if (z == 0) sq = fmax(sq, taper(pz)), ++cnt;
-            else if (z == 2) sq = fmax(sq, taper(1.0 - pz)), ++cnt;
-            if (y == 0) sq = fmax(sq, taper(py)), ++cnt;
-            else if (y == 2) sq = fmax(sq, taper(1.0 - py)), ++cnt;
-            if (x == 0) sq = fmax(sq, taper(px)), ++cnt;
-            else if (x == 2) sq = fmax(sq, taper(1.0 - px)), ++cnt;
+            if (z == 0) sq = fmax(sq, tlo[iz]), ++cnt;
+            else if (z == 2) sq = fmax(sq, thi[iz]), ++cnt;
+            if (y == 0) sq = fmax(sq, tlo[iy]), ++cnt;
+            else if (y == 2) sq = fmax(sq, thi[iy]), ++cnt;
+            if (x == 0) sq = fmax(sq, tlo[ix]), ++cnt;
+            else if (x == 2) sq = fmax(sq, thi[ix]), ++cnt;
             if (cnt > 0)
                 for (int r = 0; r < reps; ++r) v *= sq;
         }

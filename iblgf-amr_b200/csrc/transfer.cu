@@ -112,20 +112,45 @@ __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
     for (int m = 0; m < NB; ++m) d[m * NB * NB] = acc[m];
 }
 
+// threads walk the buffer shell only: the two z = 0, NB-1 planes, then per
+// inner z plane its ring (rows y = 0, NB-1, columns x = 0, NB-1)
 template<int NB>
 __global__ void halo_kernel(double* __restrict__ f, const int* __restrict__ list, const int* __restrict__ nbr,
                             const int* __restrict__ bbase, int e)
 {
     constexpr int N3 = NB * NB * NB;
+    constexpr int P2 = NB * NB, RING = 4 * NB - 4, SHELL = 2 * P2 + (NB - 2) * RING;
     const int o = list[blockIdx.x];
     double* blk = f + (size_t)o * N3;
-    for (int i = threadIdx.x; i < N3; i += blockDim.x)
+    for (int t = threadIdx.x; t < SHELL; t += blockDim.x)
     {
-        const int x = i % NB, y = (i / NB) % NB, z = i / (NB * NB);
+        int x, y, z;
+        if (t < 2 * P2)
+        {
+            z = t < P2 ? 0 : NB - 1;
+            x = (t % P2) % NB;
+            y = (t % P2) / NB;
+        }
+        else
+        {
+            const int u = t - 2 * P2, r = u % RING;
+            z = 1 + u / RING;
+            if (r < 2 * NB)
+            {
+                y = r < NB ? 0 : NB - 1;
+                x = r % NB;
+            }
+            else
+            {
+                const int w = r - 2 * NB;
+                x = (w & 1) ? NB - 1 : 0;
+                y = 1 + w / 2;
+            }
+        }
+        const int i = x + NB * (y + NB * z);
         const int dx = x == 0 ? -1 : (x == NB - 1 ? 1 : 0);
         const int dy = y == 0 ? -1 : (y == NB - 1 ? 1 : 0);
         const int dz = z == 0 ? -1 : (z == NB - 1 ? 1 : 0);
-        if (!dx && !dy && !dz) continue;
         const int q = nbr[27 * o + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
         if (q < 0) continue;
         // global cell of this buffer node and its position in q's interior
