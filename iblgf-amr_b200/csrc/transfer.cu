@@ -14,6 +14,7 @@
 //   correction    add_source_correction (cell_center_nli_intrp.hpp:171-238)
 //   zero / copy_interior / axpy over block lists (fmm.hpp:1029-1106,
 //                 poisson.hpp:921-1013)
+#include <algorithm>
 #include <cstring>
 
 #include "ctx.hpp"
@@ -26,10 +27,13 @@ namespace
 // value: they sit in the constant bank, and with the passes fully unrolled
 // every matrix entry is an FMA operand at a fixed offset (no shared-memory
 // loads). Face and edge components use different matrices per axis.
+// lo: for the banded passes (W > 0), first column of row m's band of width W
+// in summation order (the row's nonzeros all lie in [lo, lo + W))
 template<int NB>
 struct TpMats
 {
     double m[3][2][NB * NB];
+    unsigned char lo[3][2][NB];
 };
 
 template<int NB>
@@ -45,30 +49,54 @@ constexpr int tp_threads()
 // the fastest one, so all three passes read contiguous pencils; after three
 // passes the layout is back to [z][y][x]. The last pass adds into the
 // thread's accumulators instead of writing shared memory.
-template<int NB, int A, int K, bool TR, bool LAST>
+// W > 0: only the W entries of row m's band [lo, lo + W) are summed, in
+// the same order; the skipped entries are zeros, whose FMAs leave the running
+// sum unchanged, so the result equals the full row's
+template<int NB, int A, int K, bool TR, bool LAST, int W>
 __device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* __restrict__ out,
                                         const TpMats<NB>& mt, int p, double* acc)
 {
-    double v[NB];
-#pragma unroll
-    for (int n = 0; n < NB; ++n) v[n] = in[p * NB + n];
-#pragma unroll
-    for (int m = 0; m < NB; ++m)
+    if constexpr (W == 0)
     {
-        double s = 0.0;
+        double v[NB];
 #pragma unroll
-        for (int n = 0; n < NB; ++n) s = fma(TR ? mt.m[A][K][n * NB + m] : mt.m[A][K][m * NB + n], v[n], s);
-        if (LAST) acc[m] += s;
-        else out[m * NB * NB + p] = s;
+        for (int n = 0; n < NB; ++n) v[n] = in[p * NB + n];
+#pragma unroll
+        for (int m = 0; m < NB; ++m)
+        {
+            double s = 0.0;
+#pragma unroll
+            for (int n = 0; n < NB; ++n) s = fma(TR ? mt.m[A][K][n * NB + m] : mt.m[A][K][m * NB + n], v[n], s);
+            if (LAST) acc[m] += s;
+            else out[m * NB * NB + p] = s;
+        }
+    }
+    else
+    {
+        const double* row = in + p * NB;
+#pragma unroll
+        for (int m = 0; m < NB; ++m)
+        {
+            const int lo = mt.lo[A][K][m];
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < W; ++j)
+            {
+                const int n = lo + j;
+                s = fma(TR ? mt.m[A][K][n * NB + m] : mt.m[A][K][m * NB + n], row[n], s);
+            }
+            if (LAST) acc[m] += s;
+            else out[m * NB * NB + p] = s;
+        }
     }
 }
 
-template<int NB, int A, bool TR, bool LAST>
+template<int NB, int A, bool TR, bool LAST, int W>
 __device__ __forceinline__ void tp_pass_bit(int bit, const double* in, double* out, const TpMats<NB>& mt, int p,
                                             double* acc)
 {
-    if (bit) tp_pass<NB, A, 1, TR, LAST>(in, out, mt, p, acc);
-    else tp_pass<NB, A, 0, TR, LAST>(in, out, mt, p, acc);
+    if (bit) tp_pass<NB, A, 1, TR, LAST, W>(in, out, mt, p, acc);
+    else tp_pass<NB, A, 0, TR, LAST, W>(in, out, mt, p, acc);
 }
 
 // mode 0: dst[group] += sum_tasks A(src)        (anterpolation / coarsify)
@@ -76,7 +104,7 @@ __device__ __forceinline__ void tp_pass_bit(int bit, const double* in, double* o
 // mode 2: dst[group]  = I(src)                  (cell-centred interpolation)
 // One CTA per receiving block, one thread per pencil; the sending blocks of
 // a group are applied in child order into per-thread accumulators.
-template<int NB, bool TR>
+template<int NB, bool TR, int W>
 __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
     const int* __restrict__ gptr, const int* __restrict__ gdst, const int* __restrict__ tsrc,
     const int* __restrict__ tcid, const double* __restrict__ src, double* __restrict__ dst,
@@ -100,11 +128,11 @@ __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
         const int cid = tcid[t];
         for (int i = threadIdx.x; i < N3 / 2; i += blockDim.x) reinterpret_cast<double2*>(a)[i] = s2[i];
         __syncthreads();
-        if (active) tp_pass_bit<NB, 0, TR, false>(cid & 1, a, b, mt, p, acc);
+        if (active) tp_pass_bit<NB, 0, TR, false, W>(cid & 1, a, b, mt, p, acc);
         __syncthreads();
-        if (active) tp_pass_bit<NB, 1, TR, false>((cid >> 1) & 1, b, a, mt, p, acc);
+        if (active) tp_pass_bit<NB, 1, TR, false, W>((cid >> 1) & 1, b, a, mt, p, acc);
         __syncthreads();
-        if (active) tp_pass_bit<NB, 2, TR, true>((cid >> 2) & 1, a, nullptr, mt, p, acc);
+        if (active) tp_pass_bit<NB, 2, TR, true, W>((cid >> 2) & 1, a, nullptr, mt, p, acc);
         __syncthreads();
     }
     if (!active) return;
@@ -245,20 +273,50 @@ void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, co
         constexpr int NB = decltype(nbc)::value;
         static_assert((NB * NB * NB) % 2 == 0, "blocks are copied as double2");
         TpMats<NB> mt;
+        const bool tr = mode != 0;
+        int width = 0;  // widest band of any row, in summation order
         for (int a = 0; a < 3; ++a)
         {
             const size_t off = (size_t)mat_base[a] * NB * NB;
             if (c.h_mats.size() < off + 2 * NB * NB) throw Error(IBLGF_EINTERNAL, "transfer matrices missing");
             std::memcpy(mt.m[a], c.h_mats.data() + off, sizeof(mt.m[a]));
+            for (int k = 0; k < 2; ++k)
+                for (int m = 0; m < NB; ++m)
+                {
+                    int lo = NB, hi = 0;
+                    for (int n = 0; n < NB; ++n)
+                        if ((tr ? mt.m[a][k][n * NB + m] : mt.m[a][k][m * NB + n]) != 0.0)
+                        {
+                            lo = std::min(lo, n);
+                            hi = n + 1;
+                        }
+                    mt.lo[a][k][m] = (unsigned char)(lo < hi ? lo : 0);
+                    width = std::max(width, lo < hi ? hi - lo : 0);
+                }
         }
+        const int W = width <= 2 ? 2 : (width <= 5 ? 5 : 0);
+        if (W)
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 2; ++k)
+                    for (int m = 0; m < NB; ++m) mt.lo[a][k][m] = (unsigned char)std::min<int>(mt.lo[a][k][m], NB - W);
         const size_t smem = 2 * (size_t)NB * NB * NB * sizeof(double);
         auto launch = [&](auto kfn) {
             IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             kfn<<<t.n_groups, tp_threads<NB>(), smem, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
                                                                   t.task_cid.p, src, dst, mt, mode);
         };
-        if (mode == 0) launch(tp_kernel<NB, false>);
-        else launch(tp_kernel<NB, true>);
+        if (mode == 0)
+        {
+            if (W == 2) launch(tp_kernel<NB, false, 2>);
+            else if (W == 5) launch(tp_kernel<NB, false, 5>);
+            else launch(tp_kernel<NB, false, 0>);
+        }
+        else
+        {
+            if (W == 2) launch(tp_kernel<NB, true, 2>);
+            else if (W == 5) launch(tp_kernel<NB, true, 5>);
+            else launch(tp_kernel<NB, true, 0>);
+        }
     });
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
