@@ -54,8 +54,10 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            # the timed region starts once sampling has started
+            self.first = self.proc.stdout.readline()
         except OSError:
             self.proc = None
         return self
@@ -70,7 +72,7 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        for line in out.splitlines():
+        for line in [self.first] + out.splitlines():
             f = [x.strip() for x in line.split(",")]
             if len(f) >= 9:
                 self.rows.append(f)
@@ -163,7 +165,9 @@ def main():
     stream = torch.cuda.Stream()
     if args.ns_only:
         if rank == 0:
-            print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
+            print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup),
+                              "ns_step_adaptive": ns_adapt_bench(B, stream, local, args.steps, args.warmup)}),
+                  flush=True)
         return
     if args.ib_only:
         if rank == 0:
@@ -296,6 +300,7 @@ def main():
         cpu = cpu_baseline(case)
     if rank == 0 and not args.no_ns:
         extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
+        extra["ns_step_adaptive"] = ns_adapt_bench(B, stream, local, args.steps, args.warmup)
     if rank == 0 and not args.no_ib:
         extra["ns_step_ib"] = ib_bench(B, stream, local, args.steps, args.warmup)
     if rank == 0 and not args.no_batch:
@@ -358,6 +363,45 @@ def ns_bench(B, stream, device, steps, warmup):
                 "dt": dt, "Re": case.Re, "steps": steps, "warmup": warmup,
                 "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
                 "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
+    return out
+
+
+def ns_adapt_bench(B, stream, device, steps, warmup, adapt_freq=5):
+    """IF-HERK time loop with adaptation on the vortex-ring configuration
+    (FP32): Solver.ns_march with the NS setup's adapt condition every
+    adapt_freq iterations against the same number of plain steps; wall time
+    per iteration (host tree update, field remap and plan rebuild included)."""
+    import time
+    case = S.VortexRingNS("c4")
+    dt = case.dt()
+    out = {"workload": "vortex ring (as ns_step), adapt condition of the NS setup (refinement_factor 1/8, "
+                       "base_level_threshold 1e-4), adapt_frequency %d" % adapt_freq}
+
+    def cond(sv, mc, mk, me, sm):
+        return S.adapt_level_change(sv.keys, sv.levels, sv.flags, sv.base_level, mc, mk, me, sm,
+                                    n_level_refinement=case.n_levels)
+
+    for name, freq in (("plain", 0), ("adaptive", adapt_freq)):
+        g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                     n_levels=case.n_levels, predicate=case.predicate, precision=B.FP32, device=device,
+                     stream=stream.cuda_stream)
+        u0 = case.initial_velocity(g)
+        uf = [g.field(u0[k]) for k in range(3)]
+        pf = g.field()
+        T = g.ns_step(uf, pf, dt, case.Re, 0.0, warmup)
+        g.synchronize()
+        n0 = g.n
+        t0 = time.perf_counter()
+        T, sm, hist = g.ns_march(uf, pf, dt, case.Re, T, steps, adapt_freq=freq, adapt_condition=cond)
+        g.synchronize()
+        out["ms_per_iteration_" + name] = (time.perf_counter() - t0) * 1e3 / steps
+        if freq:
+            out["adaptations"] = len(hist)
+            out["attempts"] = [int(len(h[0])) for h in hist]
+            out["octants_before_after"] = [int(n0), int(g.n)]
+        g.close()
+    out["adapt_overhead_ms_per_adaptation"] = (
+        (out["ms_per_iteration_adaptive"] - out["ms_per_iteration_plain"]) * steps / max(out.get("adaptations", 0), 1))
     return out
 
 

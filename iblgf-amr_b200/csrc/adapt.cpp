@@ -82,12 +82,12 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
     d_src.upload(src, c.stream);
     for (auto& f : c.fields)
     {
-        DevBuf<double> nw;
-        nw.alloc(c.field_elems());
+        PoolBuf nw;
+        nw.alloc(c.field_elems(), c.cfg.device, c.stream);
         launch_remap_blocks(c, f->d.p, nw.p, d_src.p, c.n_oct);
-        IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // the old buffer is freed on swap
-        f->d = std::move(nw);
+        f->d = std::move(nw);  // the old buffer is freed in stream order after the remap
     }
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     // interpolation parents -> all their children with data, one level at a time
     if (n_interp && !parents.empty())
     {

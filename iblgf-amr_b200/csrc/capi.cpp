@@ -85,6 +85,8 @@ int iblgf_destroy(iblgf_ctx* x)
     iblgf_b200::ns_release(&x->c);
     iblgf_b200::batch_release(&x->c);
     iblgf_b200::ib_release(&x->c);
+    x->c.fields.clear();  // stream-ordered frees on the context stream
+    cudaStreamSynchronize(x->c.stream);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
     return IBLGF_OK;

@@ -188,9 +188,47 @@ struct HostPlan
     long long n_pairs = 0, n_exec = 0;
 };
 
+// Field storage comes from a per-device stream-ordered memory pool that keeps
+// freed memory mapped: an adaptation reallocates every field, and plain
+// cudaMalloc / cudaFree of that many large buffers costs up to seconds once
+// the device has seen other large allocations come and go.
+cudaMemPool_t field_pool(int device);
+struct PoolBuf
+{
+    double* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    PoolBuf() = default;
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    PoolBuf& operator=(PoolBuf&& o) noexcept
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        std::swap(s, o.s);
+        return *this;
+    }
+    ~PoolBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, int device, cudaStream_t stream)
+    {
+        release();
+        s = stream;
+        if (count == 0) return;
+        IBLGF_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(double),
+                                           field_pool(device), stream));
+        n = count;
+    }
+};
+
 struct Field
 {
-    DevBuf<double> d;
+    PoolBuf d;
 };
 
 constexpr int kNumStats = 9;

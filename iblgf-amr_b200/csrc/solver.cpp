@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "ctx.hpp"
 
@@ -299,10 +300,29 @@ void build_ib_masks(Ctx& c, std::vector<int>& ib)
     }
 }
 
+cudaMemPool_t field_pool(int device)
+{
+    static std::mutex m;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(m);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool;
+    IBLGF_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ull;  // never hand freed memory back while the process runs
+    IBLGF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools.emplace(device, pool);
+    return pool;
+}
+
 int field_create(Ctx& c)
 {
     auto f = std::make_unique<Field>();
-    f->d.alloc(c.field_elems());
+    f->d.alloc(c.field_elems(), c.cfg.device, c.stream);
     IBLGF_CUDA(cudaMemsetAsync(f->d.p, 0, c.field_elems() * sizeof(double), c.stream));
     c.fields.push_back(std::move(f));
     return (int)c.fields.size() - 1;
