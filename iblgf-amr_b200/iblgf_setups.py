@@ -535,3 +535,80 @@ def adapt_level_change(keys, levels, flags, base_level, cell_aux_max, correction
                 out_k.append(key_parent(keys[o]))
                 out_l.append(l2)
     return np.array(out_k, np.uint64), np.array(out_l, np.int32)
+
+
+class NsAmrLgfTest:
+    """The reference's NS test (tests/ns_amr_lgf/configs): one fat vortex ring
+    R = 0.5 in the z = 0 plane (vortex_ring_vor_fat_ic, ns_amr_lgf.hpp:588-612),
+    Re = 1000, domain (-24..23)^3 base cells in blocks of 6^3, cfl 0.35, to
+    T = 0.35:
+      config 0: dx_base 0.25, no refinement, dt = dx_base cfl = 0.0875, 4 steps
+      config 1: dx_base 0.5, one refinement level where the vorticity on the
+                block grown by 2 cells exceeds w_max (1/8)^diff_level
+                (refinement, :759-818), dt = 0.0875 on the fine level, 4 steps
+    The velocity starts from the vorticity through the stream function
+    (initialize, :491-575): vorticity on the edges, a Poisson solve per
+    component, curl_transpose with scale -1. The test's pass marks (EXP_LInf)
+    are 1e-2 and 3e-4 on the finest level's largest |u_x - u_ref,x|."""
+
+    def __init__(self, config=1):
+        self.config = config
+        self.bd_base, self.bd_extent = (-24,) * 3, (48,) * 3
+        self.block_extent = 6
+        self.blocks = [((-24,) * 3, (48,) * 3)]
+        self.R, self.Re, self.cfl = 0.5, 1000.0, 0.35
+        self.refinement_factor = 0.125
+        if config == 0:
+            self.dx_base, self.n_levels, self.base_steps, self.exp_linf = 0.25, 0, 4, 1e-2
+        else:
+            self.dx_base, self.n_levels, self.base_steps, self.exp_linf = 0.5, 1, 2, 3e-4
+        dt_base = self.dx_base * self.cfl
+        self.dt = dt_base / 2 ** self.n_levels
+        self.steps = self.base_steps * 2 ** self.n_levels
+        self.T_end = self.base_steps * dt_base
+
+    def predicate(self, base, extent, rl, diff_level):
+        e = extent[0]
+        dxl = self.dx_base / 2 ** rl
+        w_max = abs(float(self.vorticity(np.array(self.R), np.array(0.0), np.array(0.0), 1)))
+        thr = w_max * self.refinement_factor ** diff_level
+        i = np.arange(-2, e + 2)
+        c = [base[a] + i for a in range(3)]
+        for comp in range(3):
+            pos = [(c[a] + (0.5 if a == comp else 0.0)) * dxl for a in range(3)]
+            w = self.vorticity(pos[0][:, None, None], pos[1][None, :, None], pos[2][None, None, :], comp)
+            if (np.abs(w) > thr).any():
+                return True
+        return False
+
+    def vorticity(self, x, y, z, comp):
+        alpha = 0.54857674
+        R2 = self.R * self.R
+        r = np.sqrt(x * x + y * y)
+        s2 = z * z + (r - self.R) ** 2
+        theta = np.arctan2(y, x)
+        with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+            w = alpha / R2 * np.exp(-4.0 * s2 / (R2 - s2))
+        w = np.where(s2 >= R2, 0.0, w)
+        if comp == 0:
+            return -w * np.sin(theta)
+        if comp == 1:
+            return w * np.cos(theta)
+        return np.zeros_like(w)
+
+    def initial_vorticity(self, octs):
+        """(3, n, Nb, Nb, Nb) edge vorticity on every node: edge component d at
+        ((i + 1/2 [d = x]) dx, (j + 1/2 [d = y]) dx, (k + 1/2 [d = z]) dx), i, j,
+        k global cell indices of the octant's level (the domain centre is the
+        origin, ns_amr_lgf.hpp:500-540)."""
+        Nb = self.block_extent + 2
+        w = np.zeros((3, octs.n, Nb, Nb, Nb))
+        i = np.arange(Nb) - 1.0
+        for o in range(octs.n):
+            rl = int(octs.levels[o]) - octs.base_level
+            dxl = self.dx_base / 2 ** max(rl, 0)
+            b = octs.bbase[o]
+            for comp in range(3):
+                c = [(b[a] + i + (0.5 if a == comp else 0.0)) * dxl for a in range(3)]
+                w[comp, o] = self.vorticity(c[0][None, None, :], c[1][None, :, None], c[2][:, None, None], comp)
+        return w
