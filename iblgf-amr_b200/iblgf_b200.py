@@ -141,6 +141,7 @@ class Solver:
         rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
             raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+        self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
         self.Nb = block_extent + 2
         self.block_extent = block_extent
@@ -274,7 +275,7 @@ class Solver:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().iblgf_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -502,6 +503,7 @@ class BatchSolver(Solver):
         rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
             raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+        self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
         self.Nb = block_extent + 2
         self.block_extent = block_extent
