@@ -119,6 +119,17 @@ int iblgf_domain_import(iblgf_ctx* x, int n, const uint64_t* keys, const int* fl
     });
 }
 
+int iblgf_domain_restart(iblgf_ctx* x, int n, const uint64_t* keys, const unsigned char* leaf)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::need_single(c);
+        if (c.finalized) throw iblgf_b200::Error(IBLGF_EINVAL, "domain already finalized");
+        if (n <= 0 || !keys || !leaf) throw iblgf_b200::Error(IBLGF_EINVAL, "bad restart arguments");
+        c.tree.restart(n, keys, leaf);
+        c.has_blocks = true;
+    });
+}
+
 int iblgf_domain_init_refine(iblgf_ctx* x, int n_ref, int global_refinement, iblgf_refine_fn pred, void* user)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {

@@ -117,6 +117,7 @@ struct HostTree
     std::vector<int> adapt(const std::vector<std::pair<u64, int>>& attempts, const std::vector<char>& ib,
                            bool& base_mesh_update);
     void import_octants(int n, const u64* keys, const int* flags);
+    void restart(int n, const u64* keys, const unsigned char* leaf);
     std::vector<int> canonical() const;  // has_data octants, (level, key) order
 };
 

@@ -536,6 +536,21 @@ void HostTree::import_octants(int n, const u64* keys, const int* flags)
     }
 }
 
+// Domain restart (domain.hpp:235-290 with restart_list_construct, :839-849):
+// the keys Tree::write stored (every octant with data but the root) with
+// their leaf flags; ancestors get data as in the run that wrote them, then
+// mark_correction derives the correction flags.
+void HostTree::restart(int n, const u64* keys, const unsigned char* leaf)
+{
+    std::vector<int> flags(n);
+    for (int i = 0; i < n; ++i) flags[i] = leaf[i] ? 1 : 0;
+    import_octants(n, keys, flags.data());
+    for (int i = 0; i < (int)o.size(); ++i)
+        if (o[i].has_data)
+            for (int pa = o[i].parent; pa >= 0 && !o[pa].has_data; pa = o[pa].parent) alloc(pa, o[pa].level - base_level);
+    mark_correction();
+}
+
 std::vector<int> HostTree::canonical() const
 {
     std::vector<std::pair<std::pair<int, u64>, int>> v;

@@ -30,7 +30,7 @@ class Config(ctypes.Structure):
 
 EXPORTS = [
     "iblgf_create", "iblgf_destroy", "iblgf_last_error", "iblgf_synchronize",
-    "iblgf_domain_add_blocks", "iblgf_domain_import", "iblgf_domain_init_refine", "iblgf_domain_finalize",
+    "iblgf_domain_add_blocks", "iblgf_domain_import", "iblgf_domain_restart", "iblgf_domain_init_refine", "iblgf_domain_finalize",
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
@@ -64,6 +64,7 @@ def lib():
     L.iblgf_domain_add_blocks.argtypes = [vp, ci, vp, vp]
     L.iblgf_domain_init_refine.argtypes = [vp, ci, ci, REFINE_FN, vp]
     L.iblgf_domain_import.argtypes = [vp, ci, vp, vp]
+    L.iblgf_domain_restart.argtypes = [vp, ci, vp, vp]
     L.iblgf_domain_finalize.argtypes = [vp, ci]
     L.iblgf_domain_info.argtypes = [vp, vp, vp, vp]
     L.iblgf_domain_octants.argtypes = [vp, vp, vp, vp, vp]
@@ -121,6 +122,39 @@ class IblgfError(RuntimeError):
     pass
 
 
+def write_tree(path, keys, levels, flags):
+    """Tree::write (tree.hpp:832-855): the key of every octant with data but
+    the root (level 0) in depth-first order, 8 bytes each, then their leaf
+    flags, one byte each. Depth-first order with children 0..7 is ascending
+    key order: the coordinate bits sit above the level bits."""
+    keys = np.asarray(keys, np.uint64)
+    sel = np.nonzero(np.asarray(levels) > 0)[0]
+    order = sel[np.argsort(keys[sel], kind="stable")]
+    with open(path, "wb") as f:
+        f.write(keys[order].astype("<u8").tobytes())
+        f.write(((np.asarray(flags)[order] & 1) != 0).astype(np.uint8).tobytes())
+
+
+def read_tree(path):
+    """Tree::read (tree.hpp:857-885): (keys, leaf flags) of a tree file."""
+    b = open(path, "rb").read()
+    n = len(b) // 9
+    keys = np.frombuffer(b, "<u8", n).astype(np.uint64)
+    leaf = np.frombuffer(b, np.uint8, n, 8 * n).copy()
+    return keys, leaf
+
+
+def read_restart_info(path):
+    """The `key = value;` lines of Ifherk::write_info (ifherk.hpp:961-983)."""
+    out = {}
+    for line in open(path):
+        line = line.strip().rstrip(";")
+        if "=" in line:
+            k, v = (x.strip() for x in line.split("=", 1))
+            out[k] = float(v)
+    return out
+
+
 class Solver:
     """Domain + LGF-FMM Poisson solver on one GPU.
 
@@ -132,7 +166,8 @@ class Solver:
 
     def __init__(self, bd_base, bd_extent, block_extent, dx_base, blocks, n_levels=0,
                  global_refinement=0, predicate=None, precision=FP64, subtract_non_leaf=False,
-                 intrp_order=5, device=0, stream=None, use_correction=True, import_octants=None):
+                 intrp_order=5, device=0, stream=None, use_correction=True, import_octants=None,
+                 restart_tree=None):
         L = lib()
         cfg = Config(block_extent, (ctypes.c_int * 3)(*bd_base), (ctypes.c_int * 3)(*bd_extent),
                      float(dx_base), int(precision), int(device), int(intrp_order),
@@ -146,7 +181,15 @@ class Solver:
         self.Nb = block_extent + 2
         self.block_extent = block_extent
         self.precision = precision
-        if import_octants is not None:
+        self.dx_base = float(dx_base)
+        if restart_tree is not None:
+            keys, leaf = read_tree(restart_tree) if isinstance(restart_tree, str) else restart_tree
+            keys = np.ascontiguousarray(keys, dtype=np.uint64)
+            leaf = np.ascontiguousarray(leaf, dtype=np.uint8)
+            self._check(L.iblgf_domain_restart(self.h, len(keys), _p(keys), _p(leaf)))
+            n_levels, global_refinement, predicate = 0, 0, None
+            self._imported = True
+        elif import_octants is not None:
             keys = np.ascontiguousarray(import_octants[0], dtype=np.uint64)
             flags = np.ascontiguousarray(import_octants[1], dtype=np.int32)
             self._check(L.iblgf_domain_import(self.h, len(keys), _p(keys), _p(flags)))
@@ -208,6 +251,64 @@ class Solver:
         f = np.ascontiguousarray(fields, dtype=np.int32).ravel()
         self._check(lib().iblgf_ns_clean_leaf_correction_boundary(self.h, _p(f), len(f), int(level),
                                                                   1 if leaf_only_boundary else 0))
+
+    def write_chombo(self, path, fields, time=0.0, dt=1, include_correction=True, base_correction_only=True):
+        """Writes fields as a Chombo-HDF5 file in the reference's layout
+        (Simulation::write, simulation.hpp:99-121, through
+        io::H5_io::write_h5 / write_h5_withTime, IO/chombo/h5_io.hpp:161-200;
+        by default with the base-level correction blocks, as Simulation::write):
+        `fields` lists (name, field id) for a scalar and (name, [3 ids]) for a
+        vector, whose components are named name_0, name_1, name_2."""
+        import chombo_h5
+        names, ids = [], []
+        for name, fid in fields:
+            if np.ndim(fid) == 0:
+                names.append(name)
+                ids.append(int(fid))
+            else:
+                for k, f in enumerate(fid):
+                    names.append("%s_%d" % (name, k))
+                    ids.append(int(f))
+        vals = np.stack([self.download(f) for f in ids], 1)
+        levels = chombo_h5.chombo_levels(self.keys, self.levels, self.bbase, self.block_extent, self.base_level,
+                                         vals, self.flags, include_correction, base_correction_only)
+        chombo_h5.write_chombo(path, names, levels, self.dx_base, time, dt)
+
+    def read_chombo_field(self, path, name, fields, mesh):
+        """Simulation::read_h5<Field> (simulation.hpp:200-204, Chombo::read_u,
+        chombo_impl.hpp:216-520): the field `name` (scalar: one id; vector:
+        three ids, components name_0..name_2) read from a Chombo file into the
+        leaves; mesh 0 cell, 1 face, 2 edge, 3 vertex."""
+        import chombo_h5
+        ids = [int(fields)] if np.ndim(fields) == 0 else [int(f) for f in fields]
+        vals = np.stack([self.download(f) for f in ids], 1)
+        rl = self.levels - self.base_level
+        corr = self.correction
+        listed = (rl >= 0) & (~corr | (rl == 0))
+        chombo_h5.read_field_into_blocks(chombo_h5.read_chombo(path), name, len(ids), mesh, self.dx_base, rl,
+                                         self.bbase, self.block_extent, self.leaf, listed, vals)
+        for k, f in enumerate(ids):
+            self.upload(f, vals[:, k])
+            self.synchronize()
+
+    def write_tree(self, path):
+        """Tree::write (tree.hpp:832-855) of this octree."""
+        write_tree(path, self.keys, self.levels, self.flags)
+
+    def write_restart(self, directory, fields, T, adapt_count=0, source_max=(0.0, 0.0), restart_n_last=0,
+                      T_last_vel_refresh=0.0):
+        """Ifherk::write_restart (ifherk.hpp:428-444): restart_field.hdf5
+        (the fields, with base-level correction blocks, Simulation::write
+        with restart_file, simulation.hpp:99-106), tree_info.bin and
+        restart_info (Ifherk::write_info, :961-983)."""
+        os.makedirs(directory, exist_ok=True)
+        self.write_chombo(os.path.join(directory, "restart_field.hdf5"), fields)
+        self.write_tree(os.path.join(directory, "tree_info.bin"))
+        with open(os.path.join(directory, "restart_info"), "w") as f:
+            for k, v in (("T", T), ("adapt_count", adapt_count), ("cell_aux_max", source_max[0]),
+                         ("u_max", source_max[1]), ("restart_n_last", restart_n_last),
+                         ("T_last_vel_refresh", T_last_vel_refresh)):
+                f.write("%s = %s;\n" % (k, repr(float(v)) if isinstance(v, float) else v))
 
     def ns_march(self, u, p, dt, Re, T, n_steps, adapt_freq=0, adapt_condition=None, source_max=(1.0, 1.0),
                  updating_source_max=True, all_time_max=False):

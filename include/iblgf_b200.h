@@ -80,6 +80,13 @@ int iblgf_domain_init_refine(iblgf_ctx* ctx, int n_ref, int global_refinement,
  * Tree::octant_to_level_coordinate (domain.hpp:196-201). Call once, before
  * iblgf_domain_finalize. */
 int iblgf_domain_import(iblgf_ctx* ctx, int n, const uint64_t* keys, const int* flags);
+/* Rebuilds the octree of a restart (Domain::Domain from restart files,
+ * domain.hpp:235-290, then restart_list_construct :839-849): `keys` and
+ * `leaf` (one byte each) as Tree::write stores them (tree.hpp:832-855:
+ * every octant with data except the root); ancestors receive data and
+ * mark_correction recomputes the correction flags. Replaces add_blocks +
+ * init_refine; call once, before iblgf_domain_finalize. */
+int iblgf_domain_restart(iblgf_ctx* ctx, int n, const uint64_t* keys, const unsigned char* leaf);
 /* Builds the neighbour / influence lists on the device, the FMM masks
  * (FmmMaskBuilder::fmm_lgf_mask_build, fmm_vortex_streamfun_mask) and
  * allocates the working fields. subtract_non_leaf as in the reference. */

@@ -1,0 +1,25 @@
+"""Generates tests/golden/chombo_layout_ref.json: the group / attribute /
+dataset structure (names and value kinds, no data) of the reference's stored
+NS solution, tests/ns_amr_lgf/configs/ref.hdf5 in the reference tree, as the
+package's Chombo-HDF5 reader describes it. The writer's test compares the
+files it writes against this structure."""
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "iblgf-amr_b200"))
+import chombo_h5  # noqa: E402
+
+SRC = "/root/reference/tests/ns_amr_lgf/configs/ref.hdf5"
+
+
+def main():
+    d = chombo_h5.describe(SRC)
+    with open(os.path.join(HERE, "chombo_layout_ref.json"), "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    print(json.dumps(d, sort_keys=True)[:400])
+
+
+if __name__ == "__main__":
+    main()
