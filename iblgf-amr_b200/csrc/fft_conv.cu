@@ -370,15 +370,17 @@ __device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&
     }
 }
 
-template<class R, int F, int NT, int MINB>
+template<class R, int F, int NT, int MINB, int NB>
 __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
-    const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, long long NC, int zrow,
+    const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, int zrow,
     const int* __restrict__ tile_gptr, const int* __restrict__ tile_sptr, const int* __restrict__ tile_src,
     const int* __restrict__ tile_tab, const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
     const unsigned short* __restrict__ grp_src, const unsigned* __restrict__ grp_pm,
     const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
 {
     constexpr int RW = NT / F;      // thread rows, one group each per pass
+    constexpr int P = 2 * NB - 1;
+    constexpr long long NC = (long long)(P / 2 + 1) * P * P;  // spectrum row length
     constexpr int per = 16 / sizeof(cx<R>);
     constexpr int parts = F / per;  // 16-byte pieces of a staged row
     static_assert(F % 32 == 0 && NT % F == 0, "a warp covers one row");
@@ -426,20 +428,28 @@ __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
         cx<R> acc[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) acc[c] = zero;
-        for (int n = 0; n < 27; ++n)
+        // neighbour parents n = (nx, ny, nz): the x-offset unrolled, so that the
+        // LGF row of u = -2n (d = (dx, dy, dz) adds dx + 7 dy + 49 dz) sits at
+        // a compile-time offset from the (ny, nz) base
+        for (int nzy = 0; nzy < 9; ++nzy)
         {
-            if (!((pm >> n) & 1u)) continue;
-            const int4 ja = *reinterpret_cast<const int4*>(jr + 8 * n);
-            const int4 jb = *reinterpret_cast<const int4*>(jr + 8 * n + 4);
-            const int jj[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
-            cx<R> sv[8];
+            const int ny = nzy % 3 - 1, nz = nzy / 3 - 1;
+            const cx<R>* gzy = Gs + (7 * (3 - 2 * ny) + 49 * (3 - 2 * nz)) * F + lane;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) sv[q] = __ldg(Sf + (size_t)jj[q] * NC);
-            // row of u = -2n; d = (dx, dy, dz) adds dx + 7 dy + 49 dz
-            const int nx = n % 3 - 1, ny = (n / 3) % 3 - 1, nz = n / 9 - 1;
-            const cx<R>* gn = Gs + ((3 - 2 * nx) + 7 * (3 - 2 * ny) + 49 * (3 - 2 * nz)) * F + lane;
-            if (mode == 2) group_mac_parent<R, F, true>(gn, sv, acc, nx, ny, nz);
-            else group_mac_parent<R, F, false>(gn, sv, acc, nx, ny, nz);
+            for (int nxi = 0; nxi < 3; ++nxi)
+            {
+                const int n = 3 * nzy + nxi, nx = nxi - 1;
+                if (!((pm >> n) & 1u)) continue;
+                const int4 ja = *reinterpret_cast<const int4*>(jr + 8 * n);
+                const int4 jb = *reinterpret_cast<const int4*>(jr + 8 * n + 4);
+                const int jj[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
+                cx<R> sv[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) sv[q] = __ldg(Sf + (size_t)jj[q] * NC);
+                const cx<R>* gn = gzy + (3 - 2 * nx) * F;
+                if (mode == 2) group_mac_parent<R, F, true>(gn, sv, acc, nx, ny, nz);
+                else group_mac_parent<R, F, false>(gn, sv, acc, nx, ny, nz);
+            }
         }
         if (f < NC)
         {
@@ -600,7 +610,7 @@ struct Conv
 
 #ifndef IBLGF_MAC_F32
 #define IBLGF_MAC_F32 64
-#define IBLGF_MAC_NT32 1024
+#define IBLGF_MAC_NT32 768
 #define IBLGF_MAC_MINB32 1
 #endif
 #ifndef IBLGF_MAC_F64
@@ -617,11 +627,13 @@ struct Conv
     static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc)
     {
         if (!p.n_tiles) return;
+        if (c.NC != (long long)NB * (2 * NB - 1) * (2 * NB - 1))
+            throw Error(IBLGF_EINTERNAL, "spectrum row length differs from the kernel's");
         const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)kGroupTileCap * 216 * sizeof(int);
-        auto kfn = group_mac_kernel<R, GF, GNT, GMINB>;
+        auto kfn = group_mac_kernel<R, GF, GNT, GMINB, NB>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
-        kfn<<<grid, GNT, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, c.NC, p.n_src,
+        kfn<<<grid, GNT, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, p.n_src,
                                             p.tile_gptr.p, p.tile_sptr.p, p.tile_src.p, p.tile_tab.p,
                                             p.tile_coarse.p, p.spec_u.p, p.grp_src.p, p.grp_pm.p, p.grp_tgt.p,
                                             (cx<R>*)acc);
