@@ -156,8 +156,9 @@ struct FmmPlan
     // candidate sources (216, local index into the tile's staged list, 0xFFFF
     // for none) and targets (8 child slots), LGF spectrum slot per offset
     int n_tiles = 0, max_tile_src = 0, n_groups = 0;
-    DevBuf<int> tile_gptr, tile_sptr, tile_src, tile_tab, tile_coarse, spec_u, grp_tgt;
-    DevBuf<unsigned short> grp_src;
+    // tile_jr: per tile kGroupTileCap x 216 source rows of its groups'
+    // candidates (the zero row for absent ones)
+    DevBuf<int> tile_gptr, tile_jr, tile_tab, tile_coarse, spec_u, grp_tgt;
     DevBuf<unsigned> grp_pm;     // per group: bit n set = neighbour parent n has a candidate
     long long n_exec = 0;        // (target, source) products the MAC kernels execute
     bool empty() const { return n_tgt == 0; }

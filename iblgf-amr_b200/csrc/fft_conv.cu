@@ -373,9 +373,9 @@ __device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&
 template<class R, int F, int NT, int MINB, int NB>
 __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
     const cx<R>* __restrict__ G, const cx<R>* __restrict__ S, int zrow,
-    const int* __restrict__ tile_gptr, const int* __restrict__ tile_sptr, const int* __restrict__ tile_src,
+    const int* __restrict__ tile_gptr, const int* __restrict__ tile_jr,
     const int* __restrict__ tile_tab, const int* __restrict__ tile_coarse, const int* __restrict__ spec_u,
-    const unsigned short* __restrict__ grp_src, const unsigned* __restrict__ grp_pm,
+    const unsigned* __restrict__ grp_pm,
     const int* __restrict__ grp_tgt, cx<R>* __restrict__ ACC)
 {
     constexpr int RW = NT / F;      // thread rows, one group each per pass
@@ -392,16 +392,29 @@ __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
     const int lane = threadIdx.x % F, row = threadIdx.x / F;
     const int mode = tile_coarse[tile];  // 0 all, 1 non-adjacent only, 2 adjacent only
     const int* su = spec_u + 343 * tile_tab[tile];
-    const int s0 = tile_sptr[tile];
     const int g0 = tile_gptr[tile], g1 = tile_gptr[tile + 1];
     const cx<R> zero = mk<R>(0, 0);
     const bool full = f0 + F <= NC;
+    {
+        // the tile's candidate rows, one 16-byte copy per 4 entries
+        const int* jsrc = tile_jr + (size_t)tile * kGroupTileCap * 216;
+        for (int i = threadIdx.x; i < kGroupTileCap * 216 / 4; i += blockDim.x)
+            __pipeline_memcpy_async(Jr + 4 * i, jsrc + 4 * i, 16);
+    }
+    // spectrum slot of each offset row (-1: excluded by the tile's mode),
+    // evaluated once per row
+    int* Sl = Jr + kGroupTileCap * 216;
+    for (int r = threadIdx.x; r < 343; r += blockDim.x)
+    {
+        const int ux = r % 7 - 3, uy = (r / 7) % 7 - 3, uz = r / 49 - 3;
+        const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
+        Sl[r] = (mode == 1 && adj) || (mode == 2 && !adj) ? -1 : su[r];
+    }
+    __syncthreads();
     for (int q = threadIdx.x; q < 343 * parts; q += blockDim.x)
     {
         const int r = q / parts, part = q % parts;
-        const int ux = r % 7 - 3, uy = (r / 7) % 7 - 3, uz = r / 49 - 3;
-        const bool adj = ux >= -1 && ux <= 1 && uy >= -1 && uy <= 1 && uz >= -1 && uz <= 1;
-        const int slot = (mode == 1 && adj) || (mode == 2 && !adj) ? -1 : su[r];
+        const int slot = Sl[r];
         cx<R>* dst = Gs + r * F + part * per;
         const cx<R>* src = slot >= 0 ? G + (size_t)slot * NC + f0 + part * per : nullptr;
         if (src && full) __pipeline_memcpy_async(dst, src, 16);
@@ -410,12 +423,6 @@ __global__ void __launch_bounds__(NT, MINB) group_mac_kernel(
                 dst[e] = (src && f0 + part * per + e < NC) ? src[e] : zero;
     }
     __pipeline_commit();
-    for (int i = threadIdx.x; i < kGroupTileCap * 216; i += blockDim.x)
-    {
-        const int g = g0 + i / 216;
-        const unsigned short j = g < g1 ? grp_src[(size_t)g * 216 + (i % 216)] : (unsigned short)0xFFFF;
-        Jr[i] = j != 0xFFFF ? tile_src[s0 + j] : zrow;
-    }
     __pipeline_wait_prior(0);
     __syncthreads();
     const long long f = f0 + lane;
@@ -629,13 +636,13 @@ struct Conv
         if (!p.n_tiles) return;
         if (c.NC != (long long)NB * (2 * NB - 1) * (2 * NB - 1))
             throw Error(IBLGF_EINTERNAL, "spectrum row length differs from the kernel's");
-        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)kGroupTileCap * 216 * sizeof(int);
+        const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)(kGroupTileCap * 216 + 344) * sizeof(int);
         auto kfn = group_mac_kernel<R, GF, GNT, GMINB, NB>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
         kfn<<<grid, GNT, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, p.n_src,
-                                            p.tile_gptr.p, p.tile_sptr.p, p.tile_src.p, p.tile_tab.p,
-                                            p.tile_coarse.p, p.spec_u.p, p.grp_src.p, p.grp_pm.p, p.grp_tgt.p,
+                                            p.tile_gptr.p, p.tile_jr.p, p.tile_tab.p,
+                                            p.tile_coarse.p, p.spec_u.p, p.grp_pm.p, p.grp_tgt.p,
                                             (cx<R>*)acc);
         c.launches += 1;
     }

@@ -794,12 +794,24 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
     p.n_tiles = (int)h.ttab.size();
     p.max_tile_src = h.max_tile_src;
     p.tile_gptr.upload(h.tgptr, c.stream);
-    p.tile_sptr.upload(h.tsptr, c.stream);
-    p.tile_src.upload(h.tsrc, c.stream);
+    {
+        // candidate source rows per tile: group g's candidate kk reads row
+        // tsrc[tsptr[t] + gsrc[g][kk]], absent ones (and unused group slots)
+        // the zero row n_src
+        std::vector<int> jr((size_t)p.n_tiles * kGroupTileCap * 216, p.n_src);
+        for (int t = 0; t < p.n_tiles; ++t)
+            for (int g = h.tgptr[t]; g < h.tgptr[t + 1]; ++g)
+                for (int kk = 0; kk < 216; ++kk)
+                {
+                    const unsigned short j = h.gsrc[(size_t)g * 216 + kk];
+                    if (j != 0xFFFF)
+                        jr[((size_t)t * kGroupTileCap + (g - h.tgptr[t])) * 216 + kk] = h.tsrc[h.tsptr[t] + j];
+                }
+        p.tile_jr.upload(jr, c.stream);
+    }
     p.tile_tab.upload(h.ttab, c.stream);
     p.tile_coarse.upload(h.tcoarse, c.stream);
     p.spec_u.upload(spec_u, c.stream);
-    p.grp_src.upload(h.gsrc, c.stream);
     p.grp_pm.upload(h.gpm, c.stream);
     p.grp_tgt.upload(h.gtgt, c.stream);
     p.n_exec = h.n_exec;
