@@ -6,7 +6,8 @@ every level, the level transfers and the correction, as the reference's
 "Rate" (tests/poisson/vortexrings.hpp:292-298) times it. `value` is cells per
 second with the source already in HBM (device-timed, CUDA events on the
 library's stream, max over ranks); `e2e` adds the pinned host->device copy of
-the source and the device->host copy of the solution through the C ABI.
+the source and the device->host copy of the solution through the C ABI, both as
+the leaf blocks' interiors (iblgf_field_upload_leaves / download_leaves).
 
 --gpus N runs N independent replicas (one process per GPU); the solve has no
 data-path collective.
@@ -215,8 +216,10 @@ def main():
     ms_step = ms / args.steps
     value = world * cells / (ms_step * 1e-3)
 
-    # ---- end to end through the C ABI with pinned host buffers
-    hsrc = torch.from_numpy(np.ascontiguousarray(src_host)).pin_memory()
+    # ---- end to end through the C ABI with pinned host buffers: the leaf
+    # interiors (the cells the metric counts) in, the solution on them out
+    leaf = (g.flags & 1) != 0
+    hsrc = torch.from_numpy(np.ascontiguousarray(src_host[leaf][:, 1:-1, 1:-1, 1:-1])).pin_memory()
     hout = torch.empty(hsrc.shape, dtype=torch.float64).pin_memory()
     nbytes = hsrc.numel() * 8
     L = B.lib()
@@ -224,9 +227,9 @@ def main():
     g.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
-        g._check(L.iblgf_field_upload(g.h, fs, hsrc.data_ptr(), hsrc.numel()))
+        g._check(L.iblgf_field_upload_leaves(g.h, fs, hsrc.data_ptr(), hsrc.numel()))
         g.apply_lgf(fs, ft)
-        g._check(L.iblgf_field_download(g.h, ft, hout.data_ptr(), hout.numel()))
+        g._check(L.iblgf_field_download_leaves(g.h, ft, hout.data_ptr(), hout.numel()))
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps

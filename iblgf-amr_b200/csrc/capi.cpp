@@ -86,6 +86,7 @@ int iblgf_destroy(iblgf_ctx* x)
     iblgf_b200::batch_release(&x->c);
     iblgf_b200::ib_release(&x->c);
     x->c.fields.clear();  // stream-ordered frees on the context stream
+    x->c.leaf_stage.release();
     cudaStreamSynchronize(x->c.stream);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
@@ -231,6 +232,22 @@ int iblgf_field_download(iblgf_ctx* x, int f, double* host, size_t count)
         if (count != c.field_elems() || !host) throw iblgf_b200::Error(IBLGF_EINVAL, "field size mismatch");
         IBLGF_CUDA(cudaMemcpyAsync(host, c.field(f), count * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_field_upload_leaves(iblgf_ctx* x, int f, const double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        iblgf_b200::field_upload_leaves(c, f, host, count);
+    });
+}
+
+int iblgf_field_download_leaves(iblgf_ctx* x, int f, double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        iblgf_b200::field_download_leaves(c, f, host, count);
     });
 }
 

@@ -260,6 +260,11 @@ struct Ctx
 
     // device octant data
     DevBuf<int> d_bbase, d_nbr;
+    // leaf blocks in canonical order and the device staging of their
+    // interiors (leaf-interior field transfers); rebuilt with the domain
+    DevBuf<int> d_leaf_blocks;
+    int n_leaf_blocks = -1;
+    PoolBuf leaf_stage;
 
     // fields
     std::vector<std::unique_ptr<Field>> fields;
@@ -424,6 +429,11 @@ void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
 void launch_remap_blocks(Ctx& c, const double* old, double* nw, const int* d_src, int n_new);
 void launch_block_norms(Ctx& c, const double* const* comps, int n_comp, double* d_max, double* d_rms);
+// leaf-interior transfers: staging [leaf][e^3] (x fastest) <-> field blocks
+void launch_leaves_scatter(Ctx& c, const double* stage, double* field, const int* list, int n);
+void launch_leaves_gather(Ctx& c, const double* field, double* stage, const int* list, int n);
+void field_upload_leaves(Ctx& c, int f, const double* host, size_t count);
+void field_download_leaves(Ctx& c, int f, double* host, size_t count);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
 void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
                         bool assign);

@@ -344,6 +344,7 @@ void domain_rebuild(Ctx& c)
     HostTree& t = c.tree;
     const std::vector<int> canon = t.canonical();
     c.key_index.clear();
+    c.n_leaf_blocks = -1;
     c.n_oct = (int)canon.size();
     for (int i = 0; i < c.n_oct; ++i) t.o[canon[i]].idx = i;
     const int n = c.n_oct;

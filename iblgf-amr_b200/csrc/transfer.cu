@@ -353,6 +353,94 @@ void launch_zero_blocks(Ctx& c, double* f, const int* list, int n)
     IBLGF_CUDA(cudaGetLastError());
 }
 
+// one CTA per leaf; host order: leaf i's interior e^3 values, x fastest
+__global__ void leaves_scatter_kernel(const double* __restrict__ stage, double* __restrict__ f,
+                                      const int* __restrict__ list, int e, int NB)
+{
+    const int e3 = e * e * e;
+    const double* s = stage + (size_t)blockIdx.x * e3;
+    double* b = f + (size_t)list[blockIdx.x] * NB * NB * NB;
+    for (int i = threadIdx.x; i < e3; i += blockDim.x)
+    {
+        const int x = i % e, y = (i / e) % e, z = i / (e * e);
+        b[((z + 1) * NB + y + 1) * NB + x + 1] = s[i];
+    }
+}
+
+__global__ void leaves_gather_kernel(const double* __restrict__ f, double* __restrict__ stage,
+                                     const int* __restrict__ list, int e, int NB)
+{
+    const int e3 = e * e * e;
+    double* s = stage + (size_t)blockIdx.x * e3;
+    const double* b = f + (size_t)list[blockIdx.x] * NB * NB * NB;
+    for (int i = threadIdx.x; i < e3; i += blockDim.x)
+    {
+        const int x = i % e, y = (i / e) % e, z = i / (e * e);
+        s[i] = b[((z + 1) * NB + y + 1) * NB + x + 1];
+    }
+}
+
+void launch_leaves_scatter(Ctx& c, const double* stage, double* field, const int* list, int n)
+{
+    if (!n) return;
+    leaves_scatter_kernel<<<n, 256, 0, c.stream>>>(stage, field, list, c.Nb - 2, c.Nb);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_leaves_gather(Ctx& c, const double* field, double* stage, const int* list, int n)
+{
+    if (!n) return;
+    leaves_gather_kernel<<<n, 256, 0, c.stream>>>(field, stage, list, c.Nb - 2, c.Nb);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+namespace
+{
+// the leaf blocks (flag bit 0) in canonical order and a staging buffer for
+// their interiors, built on first use after each domain (re)build
+int leaf_blocks(Ctx& c)
+{
+    if (c.n_leaf_blocks < 0)
+    {
+        std::vector<int> l;
+        for (int o = 0; o < c.n_oct; ++o)
+            if (c.flags[o] & 1) l.push_back(o);
+        c.d_leaf_blocks.upload(l, c.stream);
+        c.n_leaf_blocks = (int)l.size();
+        const size_t e = (size_t)c.Nb - 2;
+        c.leaf_stage.alloc(std::max<size_t>(1, l.size() * e * e * e), c.cfg.device, c.stream);
+    }
+    return c.n_leaf_blocks;
+}
+}  // namespace
+
+// DataField::update_device / update_host (datafield.hpp:211-226) restricted to
+// the values a solve reads and produces: the interiors of the leaf blocks.
+// The upload zeroes the whole field first (buffers and non-leaf blocks).
+void field_upload_leaves(Ctx& c, int f, const double* host, size_t count)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    const int n = leaf_blocks(c);
+    const size_t e = (size_t)c.Nb - 2;
+    if (!host || count != (size_t)n * e * e * e) throw Error(IBLGF_EINVAL, "leaf field size mismatch");
+    IBLGF_CUDA(cudaMemcpyAsync(c.leaf_stage.p, host, count * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    IBLGF_CUDA(cudaMemsetAsync(c.field(f), 0, c.field_elems() * sizeof(double), c.stream));
+    launch_leaves_scatter(c, c.leaf_stage.p, c.field(f), c.d_leaf_blocks.p, n);
+}
+
+void field_download_leaves(Ctx& c, int f, double* host, size_t count)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    const int n = leaf_blocks(c);
+    const size_t e = (size_t)c.Nb - 2;
+    if (!host || count != (size_t)n * e * e * e) throw Error(IBLGF_EINVAL, "leaf field size mismatch");
+    launch_leaves_gather(c, c.field(f), c.leaf_stage.p, c.d_leaf_blocks.p, n);
+    IBLGF_CUDA(cudaMemcpyAsync(host, c.leaf_stage.p, count * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n)
 {
     if (!n) return;

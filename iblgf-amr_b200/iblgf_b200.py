@@ -33,6 +33,7 @@ EXPORTS = [
     "iblgf_domain_add_blocks", "iblgf_domain_import", "iblgf_domain_restart", "iblgf_domain_init_refine", "iblgf_domain_finalize",
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
+    "iblgf_field_upload_leaves", "iblgf_field_download_leaves",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
@@ -74,6 +75,8 @@ def lib():
     L.iblgf_field_zero.argtypes = [vp, ci]
     L.iblgf_field_upload.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_download.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_upload_leaves.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_download_leaves.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_device_ptr.argtypes = [vp, ci, pp]
     L.iblgf_fmm_apply.argtypes = [vp, ci, ci, ci, ci, cd, ci]
     L.iblgf_poisson_apply_lgf.argtypes = [vp, ci, ci, ci]
@@ -421,6 +424,23 @@ class Solver:
     def download(self, fid, out=None):
         a = self.zeros() if out is None else out
         self._check(lib().iblgf_field_download(self.h, fid, _p(a), a.size))
+        return a
+
+    @property
+    def n_leaves(self):
+        return int((self.flags & 1).sum())
+
+    def upload_leaves(self, fid, values):
+        """Leaf interiors (n_leaves, e, e, e) in canonical octant order into
+        field `fid`; buffers and non-leaf blocks become zero."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(lib().iblgf_field_upload_leaves(self.h, fid, _p(a), a.size))
+        self._keep = a
+
+    def download_leaves(self, fid, out=None):
+        e = self.block_extent
+        a = np.zeros((self.n_leaves, e, e, e)) if out is None else out
+        self._check(lib().iblgf_field_download_leaves(self.h, fid, _p(a), a.size))
         return a
 
     def zero(self, fid):

@@ -103,6 +103,15 @@ int iblgf_field_create(iblgf_ctx* ctx, int* field);
 int iblgf_field_zero(iblgf_ctx* ctx, int field);
 int iblgf_field_upload(iblgf_ctx* ctx, int field, const double* host, size_t count);
 int iblgf_field_download(iblgf_ctx* ctx, int field, double* host, size_t count);
+/* Leaf-interior transfers (DataField::update_device / update_host,
+ * datafield.hpp:211-226, for the values a solve reads and writes): `host`
+ * holds, for every leaf octant (flag bit 0) in canonical order, its
+ * block_extent^3 interior values, x fastest; count = n_leaves *
+ * block_extent^3. The upload zeroes the field (buffers, non-leaf blocks)
+ * and scatters the interiors; the download gathers them and returns after
+ * the copy. */
+int iblgf_field_upload_leaves(iblgf_ctx* ctx, int field, const double* host, size_t count);
+int iblgf_field_download_leaves(iblgf_ctx* ctx, int field, double* host, size_t count);
 int iblgf_field_device_ptr(iblgf_ctx* ctx, int field, double** dptr);
 
 /* ---- solver ----------------------------------------------------------- */
