@@ -334,10 +334,11 @@ __global__ void __launch_bounds__(128) mac_kernel(const cx<R>* __restrict__ G, c
 // One CTA = (tile of up to 32 sibling groups, chunk of F frequencies); each warp
 // takes one group at 32 consecutive frequencies, so a source load is one
 // contiguous 256-byte (FP32) or 512-byte (FP64) row segment. The tile's
-// spectra and the groups' candidate rows live in shared memory; source spectra
-// are read through L1/L2. Candidates that do not exist read a zero spectrum
-// row (zrow), and parents without any candidate are skipped via the group's
-// 27-bit mask (grp_pm).
+// spectra and the groups' candidate rows (precomputed with the plan, tile_jr)
+// are copied asynchronously into shared memory; source spectra are read
+// through L1/L2. Candidates that do not exist read a zero spectrum row (zrow),
+// and parents without any candidate are skipped via the group's 27-bit mask
+// (grp_pm).
 template<class R, int F, bool ADJ_ONLY>
 __device__ __forceinline__ void group_mac_parent(const cx<R>* gn, const cx<R> (&sv)[8], cx<R> (&acc)[8], int nx,
                                                  int ny, int nz)
