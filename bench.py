@@ -29,8 +29,7 @@ sys.path.insert(0, os.path.join(ROOT, "iblgf-amr_b200"))
 
 import iblgf_setups as S  # noqa: E402
 
-METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.path.exists(
-    os.path.join(ROOT, "BASELINE.json")) else "LGF-FMM cells/s"
+METRIC = "LGF-FMM cells/s, NS step ms: FP32-batched vs FP64 plain, 1 B200, rel err\u22641e-5"
 
 
 def peaks():
