@@ -7,7 +7,9 @@ every level, the level transfers and the correction, as the reference's
 second with the source already in HBM (device-timed, CUDA events on the
 library's stream, max over ranks); `e2e` adds the pinned host->device copy of
 the source and the device->host copy of the solution through the C ABI, both as
-the leaf blocks' interiors (iblgf_field_upload_leaves / download_leaves).
+the leaf blocks' interiors (iblgf_field_upload_leaves /
+download_leaves_async: a step's solution copy overlaps the next step's upload
+and solve; every copy completes inside the timed region).
 
 --gpus N runs N independent replicas (one process per GPU); the solve has no
 data-path collective.
@@ -225,10 +227,13 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g.synchronize()
     e0.record(stream)
+    # each step's solution copy runs on the library's copy stream, under the
+    # next step's upload and solve; all copies end before e1
     for _ in range(args.steps):
         g._check(L.iblgf_field_upload_leaves(g.h, fs, hsrc.data_ptr(), hsrc.numel()))
         g.apply_lgf(fs, ft)
-        g._check(L.iblgf_field_download_leaves(g.h, ft, hout.data_ptr(), hout.numel()))
+        g._check(L.iblgf_field_download_leaves_async(g.h, ft, hout.data_ptr(), hout.numel()))
+    g.synchronize()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps

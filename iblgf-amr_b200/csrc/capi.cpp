@@ -85,6 +85,7 @@ int iblgf_destroy(iblgf_ctx* x)
     iblgf_b200::ns_release(&x->c);
     iblgf_b200::batch_release(&x->c);
     iblgf_b200::ib_release(&x->c);
+    iblgf_b200::copy_stream_release(x->c);
     x->c.fields.clear();  // stream-ordered frees on the context stream
     x->c.leaf_stage.release();
     cudaStreamSynchronize(x->c.stream);
@@ -97,7 +98,10 @@ const char* iblgf_last_error(iblgf_ctx* x) { return x ? x->c.err.c_str() : g_cre
 
 int iblgf_synchronize(iblgf_ctx* x)
 {
-    return guard(x, [](iblgf_b200::Ctx& c) { IBLGF_CUDA(cudaStreamSynchronize(c.stream)); });
+    return guard(x, [](iblgf_b200::Ctx& c) {
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        if (c.copy_stream) IBLGF_CUDA(cudaStreamSynchronize(c.copy_stream));
+    });
 }
 
 int iblgf_domain_add_blocks(iblgf_ctx* x, int n, const int* base, const int* extent)
@@ -248,6 +252,14 @@ int iblgf_field_download_leaves(iblgf_ctx* x, int f, double* host, size_t count)
     return guard(x, [&](iblgf_b200::Ctx& c) {
         need_field(c, f);
         iblgf_b200::field_download_leaves(c, f, host, count);
+    });
+}
+
+int iblgf_field_download_leaves_async(iblgf_ctx* x, int f, double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        iblgf_b200::field_download_leaves_async(c, f, host, count);
     });
 }
 

@@ -265,6 +265,11 @@ struct Ctx
     DevBuf<int> d_leaf_blocks;
     int n_leaf_blocks = -1;
     PoolBuf leaf_stage;
+    // asynchronous leaf downloads: gathered into leaf_out on `stream`, copied
+    // to the host on copy_stream (created on first use)
+    PoolBuf leaf_out;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_gathered = nullptr, ev_copied = nullptr;
 
     // fields
     std::vector<std::unique_ptr<Field>> fields;
@@ -434,6 +439,8 @@ void launch_leaves_scatter(Ctx& c, const double* stage, double* field, const int
 void launch_leaves_gather(Ctx& c, const double* field, double* stage, const int* list, int n);
 void field_upload_leaves(Ctx& c, int f, const double* host, size_t count);
 void field_download_leaves(Ctx& c, int f, double* host, size_t count);
+void field_download_leaves_async(Ctx& c, int f, double* host, size_t count);
+void copy_stream_release(Ctx& c);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
 void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
                         bool assign);

@@ -441,6 +441,44 @@ void field_download_leaves(Ctx& c, int f, double* host, size_t count)
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+// Gather on the context stream, host copy on a second stream, so that the
+// copy overlaps whatever the context stream runs next (the next upload, the
+// next solve). The gather waits for the previous asynchronous copy out of
+// leaf_out; iblgf_synchronize waits for both streams.
+void field_download_leaves_async(Ctx& c, int f, double* host, size_t count)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    const int n = leaf_blocks(c);
+    const size_t e = (size_t)c.Nb - 2, vals = (size_t)n * e * e * e;
+    if (!host || count != vals) throw Error(IBLGF_EINVAL, "leaf field size mismatch");
+    if (!c.copy_stream)
+    {
+        IBLGF_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+        IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_gathered, cudaEventDisableTiming));
+        IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_copied, cudaEventDisableTiming));
+        IBLGF_CUDA(cudaEventRecord(c.ev_copied, c.copy_stream));
+    }
+    IBLGF_CUDA(cudaStreamWaitEvent(c.stream, c.ev_copied, 0));
+    if (c.leaf_out.n != std::max<size_t>(1, vals)) c.leaf_out.alloc(std::max<size_t>(1, vals), c.cfg.device, c.stream);
+    launch_leaves_gather(c, c.field(f), c.leaf_out.p, c.d_leaf_blocks.p, n);
+    IBLGF_CUDA(cudaEventRecord(c.ev_gathered, c.stream));
+    IBLGF_CUDA(cudaStreamWaitEvent(c.copy_stream, c.ev_gathered, 0));
+    IBLGF_CUDA(cudaMemcpyAsync(host, c.leaf_out.p, vals * sizeof(double), cudaMemcpyDeviceToHost, c.copy_stream));
+    IBLGF_CUDA(cudaEventRecord(c.ev_copied, c.copy_stream));
+}
+
+void copy_stream_release(Ctx& c)
+{
+    if (!c.copy_stream) return;
+    cudaStreamSynchronize(c.copy_stream);
+    c.leaf_out.release();
+    cudaEventDestroy(c.ev_gathered);
+    cudaEventDestroy(c.ev_copied);
+    cudaStreamDestroy(c.copy_stream);
+    c.copy_stream = nullptr;
+    c.ev_gathered = c.ev_copied = nullptr;
+}
+
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n)
 {
     if (!n) return;

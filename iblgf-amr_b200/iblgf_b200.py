@@ -33,7 +33,7 @@ EXPORTS = [
     "iblgf_domain_add_blocks", "iblgf_domain_import", "iblgf_domain_restart", "iblgf_domain_init_refine", "iblgf_domain_finalize",
     "iblgf_domain_info", "iblgf_domain_octants", "iblgf_domain_lists", "iblgf_domain_masks",
     "iblgf_field_create", "iblgf_field_zero", "iblgf_field_upload", "iblgf_field_download",
-    "iblgf_field_upload_leaves", "iblgf_field_download_leaves",
+    "iblgf_field_upload_leaves", "iblgf_field_download_leaves", "iblgf_field_download_leaves_async",
     "iblgf_field_device_ptr", "iblgf_fmm_apply", "iblgf_poisson_apply_lgf", "iblgf_poisson_apply_if",
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
@@ -77,6 +77,7 @@ def lib():
     L.iblgf_field_download.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_upload_leaves.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_download_leaves.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_download_leaves_async.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_device_ptr.argtypes = [vp, ci, pp]
     L.iblgf_fmm_apply.argtypes = [vp, ci, ci, ci, ci, cd, ci]
     L.iblgf_poisson_apply_lgf.argtypes = [vp, ci, ci, ci]
@@ -442,6 +443,14 @@ class Solver:
         a = np.zeros((self.n_leaves, e, e, e)) if out is None else out
         self._check(lib().iblgf_field_download_leaves(self.h, fid, _p(a), a.size))
         return a
+
+    def download_leaves_async(self, fid, out):
+        """Starts the copy of the leaf interiors into `out` (pinned, (n_leaves,
+        e, e, e) float64 or a pointer-bearing tensor) and returns; the copy
+        is complete after synchronize()."""
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        n = out.numel() if hasattr(out, "numel") else out.size
+        self._check(lib().iblgf_field_download_leaves_async(self.h, fid, ctypes.c_void_p(ptr), n))
 
     def zero(self, fid):
         self._check(lib().iblgf_field_zero(self.h, fid))

@@ -112,6 +112,11 @@ int iblgf_field_download(iblgf_ctx* ctx, int field, double* host, size_t count);
  * the copy. */
 int iblgf_field_upload_leaves(iblgf_ctx* ctx, int field, const double* host, size_t count);
 int iblgf_field_download_leaves(iblgf_ctx* ctx, int field, double* host, size_t count);
+/* As iblgf_field_download_leaves, but returns at once: the gather is ordered
+ * on the context stream, the copy to `host` runs on a second stream of the
+ * context (overlapping the context stream's next work, e.g. the next upload
+ * and solve; `host` should be pinned). iblgf_synchronize waits for it. */
+int iblgf_field_download_leaves_async(iblgf_ctx* ctx, int field, double* host, size_t count);
 int iblgf_field_device_ptr(iblgf_ctx* ctx, int field, double** dptr);
 
 /* ---- solver ----------------------------------------------------------- */

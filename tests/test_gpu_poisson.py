@@ -51,3 +51,28 @@ def test_solve_from_leaf_upload_matches_block_upload(precision):
     g.apply_lgf(fs, ft)
     out = g.download_leaves(ft)
     np.testing.assert_array_equal(out, ref)
+
+
+def test_async_leaf_download_pipeline():
+    """Solves of two sources, each solution downloaded asynchronously while
+    the next upload and solve run: both equal the synchronous downloads."""
+    import torch
+    case = S.GaussianPoisson("amr_small")
+    g = solver(case, B.FP64)
+    e = g.block_extent
+    rng = np.random.default_rng(5)
+    srcs = [rng.standard_normal((g.n_leaves, e, e, e)) for _ in range(2)]
+    fs, ft = g.field(), g.field()
+    ref = []
+    for x in srcs:
+        g.upload_leaves(fs, x)
+        g.apply_lgf(fs, ft)
+        ref.append(g.download_leaves(ft))
+    outs = [torch.empty((g.n_leaves, e, e, e), dtype=torch.float64).pin_memory() for _ in srcs]
+    for x, o in zip(srcs, outs):
+        g.upload_leaves(fs, x)
+        g.apply_lgf(fs, ft)
+        g.download_leaves_async(ft, o)
+    g.synchronize()
+    for r, o in zip(ref, outs):
+        np.testing.assert_array_equal(o.numpy(), r)
