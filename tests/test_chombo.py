@@ -258,3 +258,26 @@ def test_restart_info_round_trip(tmp_path):
     d = B.read_restart_info(str(p))
     assert d == {"T": 0.35000000000000003, "adapt_count": 3, "cell_aux_max": 1.5, "u_max": 2,
                  "restart_n_last": 7, "T_last_vel_refresh": 0.25}
+
+
+def test_read_field_factor_four_window(tmp_path):
+    """A file two levels finer than the runtime base (dx_base / 4): read_u's
+    window per axis is fine offsets (4-1)/2 .. 4/2 = 1..2 of each coarse
+    cell, so a cell field reads the mean of the central 2x2x2 of its 4x4x4
+    fine cells."""
+    rng = np.random.default_rng(21)
+    fine = rng.standard_normal((1, 16, 16, 16))
+    path = str(tmp_path / "f.hdf5")
+    C.write_chombo(path, ["q"], [{"boxes": np.array([[[0, 15], [0, 15], [0, 15]]]), "data": [fine]}],
+                   dx_base=0.25)
+    e = 4
+    got = np.zeros((1, 1, e + 2, e + 2, e + 2))
+    one = np.ones(1, bool)
+    C.read_field_into_blocks(C.read_chombo(path), "q", 1, 0, 1.0, np.zeros(1, int), np.zeros((1, 3), int), e, one,
+                             one, got)
+    exp = np.zeros((e, e, e))
+    for sz in (1, 2):
+        for sy in (1, 2):
+            for sx in (1, 2):
+                exp += fine[0, sz::4, sy::4, sx::4]
+    np.testing.assert_allclose(got[0, 0, 1:-1, 1:-1, 1:-1], exp / 8, rtol=0, atol=1e-15)
