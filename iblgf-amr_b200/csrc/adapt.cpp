@@ -18,7 +18,7 @@
 
 namespace iblgf_b200
 {
-void poisson_release(const Ctx* c);
+void poisson_release(Ctx& c);
 
 namespace
 {
@@ -72,7 +72,7 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
     for (size_t i = 0; i < t.o.size(); ++i)
         if (t.o[i].has_data) old_idx[i] = t.o[i].idx;
     c.plans.clear();
-    poisson_release(&c);
+    poisson_release(c);
     domain_rebuild(c);
     // gather every field into the new order
     std::vector<int> src(c.n_oct, -1);

@@ -40,7 +40,6 @@ struct BatchState
     std::vector<TpTasks> coarsify, cc_intrp, corr_intrp;
     std::map<std::pair<int, int>, std::unique_ptr<FmmPlan>> plans;  // (r, non_leaf_as_source)
 };
-std::map<const Ctx*, std::unique_ptr<BatchState>> g_batch;
 
 int no_refine(void*, const int*, const int*, int, int) { return 0; }
 
@@ -132,8 +131,7 @@ HostPlan merge_plans(const std::vector<std::pair<HostPlan, int>>& parts)
 
 BatchState& batch_state(Ctx& c)
 {
-    auto it = g_batch.find(&c);
-    if (it != g_batch.end()) return *it->second;
+    if (auto* have = c.ext_get<BatchState>(Ctx::kExtBatch)) return *have;
     auto b = std::make_unique<BatchState>();
     const int np = (int)c.sub.size();
     b->depth_rel.resize(np);
@@ -218,7 +216,7 @@ BatchState& batch_state(Ctx& c)
     }
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     auto& ref = *b;
-    g_batch.emplace(&c, std::move(b));
+    c.ext[Ctx::kExtBatch] = std::shared_ptr<BatchState>(std::move(b));
     return ref;
 }
 
@@ -315,9 +313,9 @@ void batch_apply_lgf(Ctx& c, int src, int tgt)
     double* tt = c.field(c.f_target_tmp);
     double* ct = c.field(c.f_correction_tmp);
     const size_t bytes = c.field_elems() * sizeof(double);
-    IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
-    IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
-    IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    launch_fill_zero(c, st, bytes / sizeof(double));
+    launch_fill_zero(c, tt, bytes / sizeof(double));
+    launch_fill_zero(c, ct, bytes / sizeof(double));
     launch_axpy_blocks(c, c.field(src), st, b.leaves.p, (int)b.leaves.n, 1.0, true);
     for (int r = b.rmax - 2; r >= 0; --r) launch_tp(c, b.coarsify[r], st, st, 4, 0);
     for (int r = 0; r < b.rmax; ++r)
@@ -339,6 +337,6 @@ void batch_apply_lgf(Ctx& c, int src, int tgt)
     }
 }
 
-void batch_release(const Ctx* c) { g_batch.erase(c); }
+void batch_release(Ctx& c) { c.ext[Ctx::kExtBatch].reset(); }
 
 }  // namespace iblgf_b200

@@ -52,7 +52,7 @@ void need_field(iblgf_b200::Ctx& c, int f)
 namespace iblgf_b200
 {
 void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
-void poisson_release(const Ctx* c);
+void poisson_release(Ctx& c);
 double measure_fma_peak(Ctx& c, int precision);
 }  // namespace iblgf_b200
 
@@ -81,10 +81,10 @@ int iblgf_destroy(iblgf_ctx* x)
 {
     if (!x) return IBLGF_EINVAL;
     cudaStreamSynchronize(x->c.stream);
-    iblgf_b200::poisson_release(&x->c);
-    iblgf_b200::ns_release(&x->c);
-    iblgf_b200::batch_release(&x->c);
-    iblgf_b200::ib_release(&x->c);
+    iblgf_b200::poisson_release(x->c);
+    iblgf_b200::ns_release(x->c);
+    iblgf_b200::batch_release(x->c);
+    iblgf_b200::ib_release(x->c);
     iblgf_b200::copy_stream_release(x->c);
     x->c.fields.clear();  // stream-ordered frees on the context stream
     x->c.leaf_stage.release();
@@ -101,6 +101,7 @@ int iblgf_synchronize(iblgf_ctx* x)
     return guard(x, [](iblgf_b200::Ctx& c) {
         IBLGF_CUDA(cudaStreamSynchronize(c.stream));
         if (c.copy_stream) IBLGF_CUDA(cudaStreamSynchronize(c.copy_stream));
+        iblgf_b200::check_status(c);
     });
 }
 
@@ -235,7 +236,7 @@ int iblgf_field_download(iblgf_ctx* x, int f, double* host, size_t count)
         need_field(c, f);
         if (count != c.field_elems() || !host) throw iblgf_b200::Error(IBLGF_EINVAL, "field size mismatch");
         IBLGF_CUDA(cudaMemcpyAsync(host, c.field(f), count * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        iblgf_b200::check_status(c);  // synchronises the stream
     });
 }
 
@@ -463,6 +464,15 @@ int iblgf_ib_force(iblgf_ctx* x, int stage, double* out, int* iters)
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_force(c, stage, out, iters); });
 }
 
+int iblgf_ib_stage_status(iblgf_ctx* x, int stage, int* iters, int* converged)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        int nc = 0;
+        iblgf_b200::ib_force(c, stage, nullptr, iters, &nc);
+        if (converged) *converged = nc ? 0 : 1;
+    });
+}
+
 int iblgf_ib_warmstart(iblgf_ctx* x, int mode, int train_steps, int epochs, double lr, unsigned seed)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::ib_warmstart(c, mode, train_steps, epochs, lr, seed); });
@@ -505,7 +515,9 @@ int iblgf_ib_solve(iblgf_ctx* x, const int* u_fields, double alpha, double thres
     return guard(x, [&](iblgf_b200::Ctx& c) {
         if (!u_fields || !force) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
         if (max_iter < 0) throw iblgf_b200::Error(IBLGF_EINVAL, "negative iteration limit");
-        iblgf_b200::ib_solve(c, u_fields, alpha, threshold, max_iter, force, iters);
+        if (!iblgf_b200::ib_solve(c, u_fields, alpha, threshold, max_iter, force, iters))
+            throw iblgf_b200::Error(IBLGF_ENOTCONVERGED, "IB force CG reached max_iter without converging "
+                                                         "(force and iteration count written)");
     });
 }
 

@@ -161,6 +161,8 @@ struct FmmPlan
     DevBuf<int> tile_gptr, tile_jr, tile_tab, tile_coarse, spec_u, grp_tgt;
     DevBuf<unsigned> grp_pm;     // per group: bit n set = neighbour parent n has a candidate
     long long n_exec = 0;        // (target, source) products the MAC kernels execute
+    long long mac_flops = 0;     // floating-point operations of the MAC kernels per frequency
+    bool adj_only = false;       // every tile takes adjacent pairs only (integrating factor)
     bool empty() const { return n_tgt == 0; }
 };
 
@@ -233,7 +235,7 @@ struct Field
     PoolBuf d;
 };
 
-constexpr int kNumStats = 9;
+constexpr int kNumStats = 10;
 
 struct Ctx
 {
@@ -301,6 +303,9 @@ struct Ctx
     DevBuf<double> d_ge;
     int ge_stride = 0;
     long long launches = 0;
+    // device status word: bounded waits in kernels that run out set bits
+    // (kStatusTimeout); read and cleared by check_status()
+    DevBuf<int> d_status;
     bool profile = false;
     std::vector<std::array<cudaEvent_t, 5>> prof_events;
     // work counters since the last reset: sweeps, sources, targets, pairs,
@@ -315,6 +320,18 @@ struct Ctx
     bool batch = false, topology_only = false, has_blocks = false;
     std::vector<std::unique_ptr<Ctx>> sub;
     std::vector<int> sub_off;
+
+    // per-context state of the other modules (batch lists and plans,
+    // immersed boundary, time stepping, level lists), created on first use
+    // and owned here, so that contexts driven from different host threads
+    // share no mutable state
+    enum { kExtBatch, kExtIb, kExtNsOpt, kExtNs, kExtNsPending, kExtPLists, kExtOpLists, kNumExt };
+    std::shared_ptr<void> ext[kNumExt];
+    template<class T>
+    T* ext_get(int i) const
+    {
+        return static_cast<T*>(ext[i].get());
+    }
 
     size_t block_elems() const { return (size_t)Nb * Nb * Nb; }
     size_t field_elems() const { return (size_t)n_oct * block_elems(); }
@@ -341,11 +358,15 @@ int batch_add_problem(Ctx& c, const int* bd_base, const int* bd_extent, int n, c
                       int n_ref, iblgf_refine_fn pred, void* user);
 void batch_finalize(Ctx& c);
 void batch_apply_lgf(Ctx& c, int src, int tgt);
-void batch_release(const Ctx* c);
+void batch_release(Ctx& c);
 // immersed boundary (ibsolve.cpp)
 void build_ib_masks(Ctx& c, std::vector<int>& ib);
 void ib_set_points(Ctx& c, int n, const double* X, double Re);
-void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters);
+// false when the solve stopped at max_iter without converging (f and iters
+// are written either way)
+bool ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters);
+// IB steps can be captured in a graph (the learned warm start reads the host)
+bool ib_graphable(const Ctx& c);
 void ib_flags(Ctx& c, int* flags);
 bool ib_active(const Ctx& c);
 const int* ib_face_aux2(Ctx& c);
@@ -354,13 +375,25 @@ const int* ib_face_aux2(Ctx& c);
 // learned warm start neither predicts nor records samples
 void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
                  const std::function<void()>& gradient_d, bool write_prev = true);
-void ib_force(Ctx& c, int stage, double* out, int* iters);
-void ib_release(const Ctx* c);
+void ib_force(Ctx& c, int stage, double* out, int* iters, int* not_converged = nullptr);
+void ib_release(Ctx& c);
 void launch_ib_projection(Ctx& c, const double* const* u, const int* ptr, const long long* at, const double* w,
                           int n, double* f);
 void launch_ib_smearing(Ctx& c, double* const* u, const long long* node_at, const int* nptr, const int* npt,
                         const int* nent, const double* w, int n_nodes, const double* f);
 void launch_face_planes(Ctx& c, double* f, const int* list, const unsigned char* faces, int n, int width);
+// device force CG (ib.cu): FP64 dot products by one CTA in a fixed order;
+// ctl = [done, iterations, not converged], sc = [rsold, p.Ap, rsnew, f.f]
+void launch_cg_dot(Ctx& c, const double* a, const double* b, const double* a2, const double* b2, int n,
+                   double* out0, double* out1, const int* ctl);
+void launch_cg_init(Ctx& c, const double* uc, const double* Ax, double* r, double* p, int n, int* ctl, int max_iter);
+void launch_cg_update(Ctx& c, double* f, double* r, const double* p, const double* Ap, int n, const double* sc,
+                      int* ctl);
+void launch_cg_direction(Ctx& c, double* p, const double* r, int n, const double* sc, const int* ctl,
+                         double threshold);
+void launch_cg_advance(Ctx& c, double* sc, int* ctl, double threshold, int max_iter, unsigned long long cond,
+                       bool set_cond);
+void launch_cg_record(Ctx& c, const int* ctl, int* rec);
 // learned warm start network (warmstart.cu)
 constexpr int kWsChannels = 64, kWsInputs = 9;
 void ws_offsets(int* off);  // 7 offsets: W1 b1 W2 b2 W3 b3 end
@@ -398,7 +431,7 @@ PoissonLists& poisson_lists(Ctx& c);
 void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n_steps);
 // constant frame velocity and IB CG settings of the IF-HERK step
 void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter);
-void ns_release(const Ctx* c);
+void ns_release(Ctx& c);
 // after an adaptation: the time step's per-tree lists are rebuilt, its graph
 // dropped; base_mesh_update forces a velocity refresh at the next step
 void ns_on_adapt(Ctx& c, bool base_mesh_update, const std::vector<char>& old_corr);
@@ -430,8 +463,21 @@ void launch_build_lists(Ctx& c, const u64* d_sorted_keys, const int* d_sorted_id
 void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots);
 void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, int n_src, void* src_spec);
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
+// sibling-group MAC with the fast block-Toeplitz product (group_mac.cu);
+// false when the plan's tiles need the direct kernel (adjacent pairs only)
+bool toeplitz_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
+// waits for the context stream and throws IBLGF_ETIMEOUT if a kernel's
+// bounded wait ran out since the last check
+void check_status(Ctx& c);
 void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t, double scale);
+// prime-factor inverse (inverse.cu); false when the block size has no
+// prime-factor split (the direct inverse runs instead)
+bool inverse_pfa(Ctx& c, const void* acc, const int* d_tgt_oct, int n, double scale, double* target,
+                 bool fp32_passes);
+void init_pfa_constants(int device);
+bool inverse_fp32_passes(const Ctx& c);
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
+void launch_fill_zero(Ctx& c, double* p, size_t n);
 void launch_remap_blocks(Ctx& c, const double* old, double* nw, const int* d_src, int n_new);
 void launch_block_norms(Ctx& c, const double* const* comps, int n_comp, double* d_max, double* d_rms);
 // leaf-interior transfers: staging [leaf][e^3] (x fastest) <-> field blocks

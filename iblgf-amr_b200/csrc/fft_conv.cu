@@ -651,6 +651,7 @@ struct Conv
     static void inverse(Ctx& c, const void* acc, const int* d_tgt_oct, int n_tgt, double scale, double* target)
     {
         if (!n_tgt) return;
+        if (inverse_pfa(c, acc, d_tgt_oct, n_tgt, scale, target, inverse_fp32_passes(c))) return;
         launch_inverse(c, (const cx<R>*)acc, d_tgt_oct, n_tgt, scale, target);
         c.launches += 1;
     }
@@ -756,7 +757,7 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
         using CV = decltype(cv);
         // targets outside sibling groups: general pair-list MAC
         CV::mac(c, c.d_spec.p, src_spec, p.pair_ptr.p, p.pair_src.p, p.pair_spec.p, p.n_csr_tgt, acc);
-        CV::group_mac(c, p, src_spec, acc);
+        if (!toeplitz_mac(c, p, src_spec, acc)) CV::group_mac(c, p, src_spec, acc);
     });
     IBLGF_CUDA(cudaGetLastError());
 }
@@ -838,11 +839,28 @@ __global__ void noalloc_index_kernel(int* idx)
 
 size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 
+// Makes the context's device current for the scope of a call and restores
+// the caller's current device on every way out (return or exception).
+struct DeviceScope
+{
+    int prev = -1;
+    explicit DeviceScope(int device)
+    {
+        IBLGF_CUDA(cudaGetDevice(&prev));
+        if (prev != device) IBLGF_CUDA(cudaSetDevice(device));
+    }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// the static scratch's device address on the current device (set up once
+// per device); the caller holds a DeviceScope for the context's device
 unsigned char* noalloc_scratch(Ctx& c)
 {
     int dev = -1;
-    IBLGF_CUDA(cudaGetDevice(&dev));
-    if (dev != c.cfg.device) IBLGF_CUDA(cudaSetDevice(c.cfg.device));
     IBLGF_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error(IBLGF_EINVAL, "device ordinal beyond the scratch table");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -870,6 +888,7 @@ void launch_conv_block_noalloc(Ctx& c, const double* src, const double* kernel, 
         throw Error(IBLGF_EINVAL, "block too large for the static convolution scratch (needs " +
                                       std::to_string(need) + " bytes, limit " +
                                       std::to_string(kNoAllocScratchBytes) + ")");
+    DeviceScope on_device(c.cfg.device);
     unsigned char* base = noalloc_scratch(c);
     const int* d_zero = reinterpret_cast<const int*>(base);
     const int* d_ptr = d_zero + 1;

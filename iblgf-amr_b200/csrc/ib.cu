@@ -104,4 +104,182 @@ void launch_face_planes(Ctx& c, double* f, const int* list, const unsigned char*
     IBLGF_CUDA(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------
+// Force CG of LinSysSolver::CG_solve (linsys.hpp:171-230) on the device. The
+// iterates and residuals stay in device memory; the scalars (FP64 dot
+// products, linsys.hpp:501-517) are reduced by one CTA in a fixed order, so a
+// solve is bit-reproducible. sc: [0] rsold, [1] p.Ap, [2] rsnew, [3] f.f;
+// ctl: [0] done, [1] iterations, [2] stopped at max_iter without converging.
+namespace
+{
+constexpr int kDotThreads = 1024;
+
+// sum over i < n of a[i] * b[i] (and of c[i] * d[i] when c is given): each
+// thread sums its strided elements in order, then a fixed tree over threads
+__global__ void __launch_bounds__(kDotThreads) cg_dot_kernel(const double* __restrict__ a,
+                                                             const double* __restrict__ b,
+                                                             const double* __restrict__ c,
+                                                             const double* __restrict__ d, int n,
+                                                             double* __restrict__ out0, double* __restrict__ out1,
+                                                             const int* __restrict__ ctl)
+{
+    __shared__ double s0[kDotThreads], s1[kDotThreads];
+    if (ctl && ctl[0]) return;
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < n; i += kDotThreads)
+    {
+        t0 = fma(a[i], b[i], t0);
+        if (c) t1 = fma(c[i], d[i], t1);
+    }
+    s0[threadIdx.x] = t0;
+    s1[threadIdx.x] = t1;
+    __syncthreads();
+    for (int h = kDotThreads / 2; h > 0; h >>= 1)
+    {
+        if ((int)threadIdx.x < h)
+        {
+            s0[threadIdx.x] += s0[threadIdx.x + h];
+            s1[threadIdx.x] += s1[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        *out0 = s0[0];
+        if (c) *out1 = s1[0];
+    }
+}
+
+// r = uc - Ax, p = r; the controls reset (done when max_iter <= 0)
+__global__ void cg_init_kernel(const double* __restrict__ uc, const double* __restrict__ Ax, double* __restrict__ r,
+                               double* __restrict__ p, int n, int* __restrict__ ctl, int max_iter)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        const double v = uc[i] - Ax[i];
+        r[i] = v;
+        p[i] = v;
+    }
+    if (i == 0)
+    {
+        ctl[0] = max_iter <= 0 ? 1 : 0;
+        ctl[1] = 0;
+        ctl[2] = 0;
+    }
+}
+
+// after Ap and p.Ap: one more iteration counted; p.Ap = 0 stops the solve;
+// otherwise f += a p, r -= a Ap with a = rsold / p.Ap
+__global__ void cg_update_kernel(double* __restrict__ f, double* __restrict__ r, const double* __restrict__ p,
+                                 const double* __restrict__ Ap, int n, const double* __restrict__ sc,
+                                 int* __restrict__ ctl)
+{
+    if (ctl[0]) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double pAp = sc[1];
+    if (pAp == 0.0) return;
+    const double a = sc[0] / pAp;
+    if (i < n)
+    {
+        f[i] = f[i] + p[i] * a;
+        r[i] = r[i] + Ap[i] * -a;
+    }
+}
+
+// direction update p = r + (rsnew / rsold) p unless this iteration stops
+// the solve (p.Ap = 0, or sqrt(rsnew / f.f) < threshold)
+__global__ void cg_direction_kernel(double* __restrict__ p, const double* __restrict__ r, int n,
+                                    const double* __restrict__ sc, const int* __restrict__ ctl, double threshold)
+{
+    if (ctl[0]) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sc[1] == 0.0 || sqrt(sc[2] / sc[3]) < threshold) return;
+    if (i < n) p[i] = r[i] + p[i] * (sc[2] / sc[0]);
+}
+
+// the scalar side of the iteration (one thread, after the direction update
+// has read rsold): iteration count, stop decision, rsold = rsnew; inside a
+// graph the loop's condition is set from it
+__global__ void cg_advance_kernel(double* __restrict__ sc, int* __restrict__ ctl, double threshold, int max_iter,
+                                  cudaGraphConditionalHandle cond, int set_cond)
+{
+    if (!ctl[0])
+    {
+        const int it = ctl[1] + 1;
+        ctl[1] = it;
+        const bool stop_zero = sc[1] == 0.0;
+        const bool conv = !stop_zero && sqrt(sc[2] / sc[3]) < threshold;
+        if (stop_zero || conv) ctl[0] = 1;
+        else
+        {
+            sc[0] = sc[2];
+            if (it >= max_iter)
+            {
+                ctl[0] = 1;
+                ctl[2] = 1;
+            }
+        }
+    }
+    if (set_cond) cudaGraphSetConditional(cond, ctl[0] ? 0u : 1u);
+}
+
+// per-stage record of a finished solve: [iterations, not converged]
+__global__ void cg_record_kernel(const int* __restrict__ ctl, int* __restrict__ rec)
+{
+    rec[0] = ctl[1];
+    rec[1] = ctl[2];
+}
+}  // namespace
+
+void launch_cg_dot(Ctx& c, const double* a, const double* b, const double* a2, const double* b2, int n,
+                   double* out0, double* out1, const int* ctl)
+{
+    cg_dot_kernel<<<1, kDotThreads, 0, c.stream>>>(a, b, a2, b2, n, out0, out1, ctl);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_cg_init(Ctx& c, const double* uc, const double* Ax, double* r, double* p, int n, int* ctl, int max_iter)
+{
+    cg_init_kernel<<<(n + 255) / 256 + (n == 0), 256, 0, c.stream>>>(uc, Ax, r, p, n, ctl, max_iter);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_cg_update(Ctx& c, double* f, double* r, const double* p, const double* Ap, int n, const double* sc,
+                      int* ctl)
+{
+    if (!n) return;
+    cg_update_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(f, r, p, Ap, n, sc, ctl);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_cg_direction(Ctx& c, double* p, const double* r, int n, const double* sc, const int* ctl,
+                         double threshold)
+{
+    if (!n) return;
+    cg_direction_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(p, r, n, sc, ctl, threshold);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_cg_advance(Ctx& c, double* sc, int* ctl, double threshold, int max_iter,
+                       unsigned long long cond, bool set_cond)
+{
+    cg_advance_kernel<<<1, 1, 0, c.stream>>>(sc, ctl, threshold, max_iter, (cudaGraphConditionalHandle)cond,
+                                             set_cond ? 1 : 0);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_cg_record(Ctx& c, const int* ctl, int* rec)
+{
+    cg_record_kernel<<<1, 1, 0, c.stream>>>(ctl, rec);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 }  // namespace iblgf_b200

@@ -79,12 +79,25 @@ struct IbState
     int n_ibc = 0, n_cb = 0, n_corr = 0;
     bool clean_base = false;
     int face_aux[3] = {-1, -1, -1}, face_aux2[3] = {-1, -1, -1}, cell_aux2 = -1;
-    DevBuf<double> d_f;  // 3 n forces (smearing input / projection output)
-    std::vector<double> force_prev[4];  // IB::force_prev per IF-HERK stage (CG warm start)
-    int iters[4] = {0, 0, 0, 0};        // CG iterations of the last step's stages
+    // force CG of LinSysSolver::CG_solve on the device: iterate, residual,
+    // direction, Schur product, projected velocity (3 n each), the scalars
+    // [rsold, p.Ap, rsnew, f.f] and controls [done, iterations, not converged]
+    DevBuf<double> cg_f, cg_r, cg_p, cg_Ap, cg_uc, cg_sc;
+    DevBuf<int> cg_ctl;
+    DevBuf<int> cg_rec;                 // per stage 0..3: [iterations, not converged] of its last solve
+    DevBuf<double> fprev[4];            // IB::force_prev per IF-HERK stage (CG warm start), on the device
+    int* done_host = nullptr;           // pinned: the done flag, read once per iteration of a direct solve
+    cudaStream_t body_stream = nullptr; // captures the loop body of a solve inside a graph
     WarmStart ws;
+    IbState() = default;
+    IbState(const IbState&) = delete;
+    IbState& operator=(const IbState&) = delete;
+    ~IbState()
+    {
+        if (done_host) cudaFreeHost(done_host);
+        if (body_stream) cudaStreamDestroy(body_stream);
+    }
 };
-std::map<const Ctx*, std::unique_ptr<IbState>> g_ib;
 
 // face neighbour direction -> face bit (0 z-, 1 y-, 2 x-, 3 x+, 4 y+, 5 z+)
 int face_bit(int i)
@@ -103,9 +116,9 @@ int face_bit(int i)
 
 IbState& state(Ctx& c)
 {
-    auto it = g_ib.find(&c);
-    if (it == g_ib.end()) throw Error(IBLGF_EINVAL, "no immersed-boundary points set");
-    return *it->second;
+    auto* s = c.ext_get<IbState>(Ctx::kExtIb);
+    if (!s) throw Error(IBLGF_EINVAL, "no immersed-boundary points set");
+    return *s;
 }
 }  // namespace
 
@@ -243,15 +256,14 @@ void ib_set_points(Ctx& c, int n, const double* X, double Re)
     s->n_ibc = (int)ibc_list.size();
     s->n_cb = (int)cb_list.size();
     s->n_corr = (int)corr.size();
-    auto old = g_ib.find(&c);
-    if (old != g_ib.end())
+    if (const IbState* old = c.ext_get<IbState>(Ctx::kExtIb))
     {
         for (int k = 0; k < 3; ++k)
         {
-            s->face_aux[k] = old->second->face_aux[k];
-            s->face_aux2[k] = old->second->face_aux2[k];
+            s->face_aux[k] = old->face_aux[k];
+            s->face_aux2[k] = old->face_aux2[k];
         }
-        s->cell_aux2 = old->second->cell_aux2;
+        s->cell_aux2 = old->cell_aux2;
     }
     else
     {
@@ -262,10 +274,19 @@ void ib_set_points(Ctx& c, int n, const double* X, double Re)
         }
         s->cell_aux2 = field_create(c);
     }
-    s->d_f.alloc(3 * (size_t)n);
-    for (auto& fp : s->force_prev) fp.assign(3 * (size_t)n, 0.0);
+    for (DevBuf<double>* b : {&s->cg_f, &s->cg_r, &s->cg_p, &s->cg_Ap, &s->cg_uc}) b->alloc(3 * (size_t)n);
+    for (auto& fp : s->fprev)
+    {
+        fp.alloc(3 * (size_t)n);
+        launch_fill_zero(c, fp.p, fp.n);
+    }
+    s->cg_sc.upload(std::vector<double>(4, 0.0), c.stream);
+    s->cg_ctl.upload(std::vector<int>(3, 0), c.stream);
+    s->cg_rec.upload(std::vector<int>(8, 0), c.stream);
+    IBLGF_CUDA(cudaMallocHost(&s->done_host, sizeof(int)));
+    IBLGF_CUDA(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
-    g_ib[&c] = std::move(s);
+    c.ext[Ctx::kExtIb] = std::shared_ptr<IbState>(std::move(s));
 }
 
 void ib_flags(Ctx& c, int* flags)
@@ -276,22 +297,28 @@ void ib_flags(Ctx& c, int* flags)
 
 namespace
 {
-void projection(Ctx& c, IbState& s, const int* u, std::vector<double>& f)
+// Operator::ib_projection into the device vector out (3 n)
+void projection(Ctx& c, IbState& s, const int* u, double* out)
 {
     const double* pu[3] = {c.field(u[0]), c.field(u[1]), c.field(u[2])};
-    launch_ib_projection(c, pu, s.ptr.p, s.at.p, s.w.p, s.n, s.d_f.p);
-    f.resize(3 * (size_t)s.n);
-    IBLGF_CUDA(cudaMemcpyAsync(f.data(), s.d_f.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    launch_ib_projection(c, pu, s.ptr.p, s.at.p, s.w.p, s.n, out);
 }
 
-void smearing(Ctx& c, IbState& s, const std::vector<double>& f, const int* u, bool cleaning = true)
+std::vector<double> download(Ctx& c, const double* d, size_t n)
 {
-    IBLGF_CUDA(cudaMemcpyAsync(s.d_f.p, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    std::vector<double> h(n);
+    IBLGF_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    return h;
+}
+
+// Operator::ib_smearing of the device forces f (3 n)
+void smearing(Ctx& c, IbState& s, const double* f, const int* u, bool cleaning = true)
+{
     double* pu[3] = {c.field(u[0]), c.field(u[1]), c.field(u[2])};
     if (cleaning)
-        for (int k = 0; k < 3; ++k) IBLGF_CUDA(cudaMemsetAsync(pu[k], 0, c.field_elems() * sizeof(double), c.stream));
-    launch_ib_smearing(c, pu, s.node_at.p, s.nptr.p, s.npt.p, s.nent.p, s.w.p, s.n_nodes, s.d_f.p);
+        for (int k = 0; k < 3; ++k) launch_fill_zero(c, pu[k], c.field_elems());
+    launch_ib_smearing(c, pu, s.node_at.p, s.nptr.p, s.npt.p, s.nent.p, s.w.p, s.n_nodes, f);
 }
 
 // apply_Schur<Source, Target>(xIB2IB), linsys.hpp:299-330
@@ -318,10 +345,11 @@ void apply_schur(Ctx& c, IbState& s, const int* src, const int* tgt)
     }
 }
 
-void et_h_s_e(Ctx& c, IbState& s, const std::vector<double>& fin, std::vector<double>& fout, double alpha)
+// LinSysSolver::ET_H_S_E (linsys.hpp:260-297): device forces in, device
+// projection out
+void et_h_s_e(Ctx& c, IbState& s, const double* fin, double* fout, double alpha)
 {
-    for (int k = 0; k < 3; ++k)
-        IBLGF_CUDA(cudaMemsetAsync(c.field(s.face_aux[k]), 0, c.field_elems() * sizeof(double), c.stream));
+    for (int k = 0; k < 3; ++k) launch_fill_zero(c, c.field(s.face_aux[k]), c.field_elems());
     smearing(c, s, fin, s.face_aux2);
     if (std::fabs(alpha) > 1e-14)
         for (int k = 0; k < 3; ++k)
@@ -336,7 +364,7 @@ void et_h_s_e(Ctx& c, IbState& s, const std::vector<double>& fin, std::vector<do
 }
 }  // namespace
 
-bool ib_active(const Ctx& c) { return g_ib.count(&c) != 0; }
+bool ib_active(const Ctx& c) { return c.ext[Ctx::kExtIb] != nullptr; }
 
 namespace
 {
@@ -549,48 +577,145 @@ void ws_check(Ctx& c, int S, int N, const float* params, const float* x, const f
 
 const int* ib_face_aux2(Ctx& c) { return state(c).face_aux2; }
 
+namespace
+{
+// One iteration of CG_solve (linsys.hpp:202-229) on the device: Ap = S p,
+// p.Ap, the update of f and r, r.r and f.f, the next direction and the
+// scalar step; inside a graph's loop the last launch sets the loop condition
+void cg_iteration(Ctx& c, IbState& s, double alpha, double threshold, int max_iter, unsigned long long cond,
+                  bool set_cond)
+{
+    const int m = 3 * s.n;
+    et_h_s_e(c, s, s.cg_p.p, s.cg_Ap.p, alpha);
+    launch_cg_dot(c, s.cg_p.p, s.cg_Ap.p, nullptr, nullptr, m, s.cg_sc.p + 1, nullptr, s.cg_ctl.p);
+    launch_cg_update(c, s.cg_f.p, s.cg_r.p, s.cg_p.p, s.cg_Ap.p, m, s.cg_sc.p, s.cg_ctl.p);
+    launch_cg_dot(c, s.cg_r.p, s.cg_r.p, s.cg_f.p, s.cg_f.p, m, s.cg_sc.p + 2, s.cg_sc.p + 3, s.cg_ctl.p);
+    launch_cg_direction(c, s.cg_p.p, s.cg_r.p, m, s.cg_sc.p, s.cg_ctl.p, threshold);
+    launch_cg_advance(c, s.cg_sc.p, s.cg_ctl.p, threshold, max_iter, cond, set_cond);
+}
+
+// LinSysSolver::ib_solve + CG_solve (linsys.hpp:113-230) from the iterate
+// already in cg_f; rec (device, 2 ints) receives [iterations, not converged].
+// Outside a stream capture the host reads the done flag once per iteration;
+// inside one the loop is a conditional while-node of the graph, its body one
+// iteration, so a captured time step runs the whole solve on the device.
+void cg_solve(Ctx& c, IbState& s, const int* u, double alpha, double threshold, int max_iter, int* rec)
+{
+    const int m = 3 * s.n;
+    projection(c, s, u, s.cg_uc.p);
+    for (int k = 0; k < 3; ++k) launch_fill_zero(c, c.field(s.face_aux2[k]), c.field_elems());
+    et_h_s_e(c, s, s.cg_f.p, s.cg_Ap.p, alpha);
+    launch_cg_init(c, s.cg_uc.p, s.cg_Ap.p, s.cg_r.p, s.cg_p.p, m, s.cg_ctl.p, max_iter);
+    launch_cg_dot(c, s.cg_r.p, s.cg_r.p, nullptr, nullptr, m, s.cg_sc.p, nullptr, nullptr);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    IBLGF_CUDA(cudaStreamGetCaptureInfo(c.stream, &cs, nullptr, &g, &deps, &nd));
+    if (cs == cudaStreamCaptureStatusActive)
+    {
+        cudaGraphConditionalHandle h;
+        IBLGF_CUDA(cudaGraphConditionalHandleCreate(&h, g, max_iter > 0 ? 1u : 0u, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        IBLGF_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        IBLGF_CUDA(cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies));
+        IBLGF_CUDA(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeRelaxed));
+        cudaStream_t outer = c.stream;
+        c.stream = s.body_stream;
+        try
+        {
+            cg_iteration(c, s, alpha, threshold, max_iter, (unsigned long long)h, true);
+        }
+        catch (...)
+        {
+            c.stream = outer;
+            cudaGraph_t dummy = nullptr;
+            cudaStreamEndCapture(s.body_stream, &dummy);
+            throw;
+        }
+        c.stream = outer;
+        cudaGraph_t captured = nullptr;
+        IBLGF_CUDA(cudaStreamEndCapture(s.body_stream, &captured));
+    }
+    else
+    {
+        for (int k = 0; k < max_iter; ++k)
+        {
+            cg_iteration(c, s, alpha, threshold, max_iter, 0, false);
+            IBLGF_CUDA(cudaMemcpyAsync(s.done_host, s.cg_ctl.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+            IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+            if (*s.done_host) break;
+        }
+    }
+    launch_cg_record(c, s.cg_ctl.p, rec);
+}
+}  // namespace
+
+bool ib_graphable(const Ctx& c)
+{
+    const IbState* s = c.ext_get<IbState>(Ctx::kExtIb);
+    return !s || s->ws.mode != 1;
+}
+
 // lin_sys_with_ib_solve's IB part (ifherk.hpp:1474-1494) after face_aux2 =
 // r_i - grad d_i (+ IF): CG warm-started from the stage's previous force,
 // pressure correction of d, then face_aux = grad d + E f (the caller
-// subtracts it from r_i)
+// subtracts it from r_i). With the reference warm start everything stays on
+// the device; the learned warm start assembles its inputs on the host.
 void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter, int d_field, const int* face_aux,
                  const std::function<void()>& gradient_d, bool write_prev)
 {
     IbState& s = state(c);
     WarmStart& w = s.ws;
-    std::vector<double> f = s.force_prev[stage];
+    const size_t m = 3 * (size_t)s.n;
+    int* rec = s.cg_rec.p + 2 * stage;
     if (w.mode == 1 && write_prev)
     {
-        std::vector<double> uc, duc, dfp(s.force_prev[stage]);
-        projection(c, s, s.face_aux2, uc);
-        duc = uc;
+        projection(c, s, s.face_aux2, s.cg_uc.p);
+        std::vector<double> uc = download(c, s.cg_uc.p, m), fp = download(c, s.fprev[stage].p, m);
+        std::vector<double> duc(uc), dfp(fp);
         if (!w.uc_prev[stage].empty())
             for (size_t i = 0; i < duc.size(); ++i) duc[i] -= w.uc_prev[stage][i];
         if (!w.f_prev2[stage].empty())
             for (size_t i = 0; i < dfp.size(); ++i) dfp[i] -= w.f_prev2[stage][i];
-        if (w.trained) f = ws_predict(c, w, duc, s.force_prev[stage], dfp, s.n);
-        ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
+        std::vector<double> f = w.trained ? ws_predict(c, w, duc, fp, dfp, s.n) : fp;
+        IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, f.data(), m * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
+        f = download(c, s.cg_f.p, m);
         // samples from steps that have a previous force (the first step's
         // "change" is the whole force and would set the target scale)
         if (!w.trained && !w.uc_prev[stage].empty())
         {
             w.s_duc.push_back(duc);
-            w.s_fprev.push_back(s.force_prev[stage]);
+            w.s_fprev.push_back(fp);
             w.s_dfp.push_back(dfp);
             w.s_f.push_back(f);
             if (stage == 3 && ++w.steps_seen >= w.train_steps) ws_train(c, w, s.n);
         }
         w.uc_prev[stage] = uc;
-        w.f_prev2[stage] = s.force_prev[stage];
+        w.f_prev2[stage] = fp;
     }
     else
-        ib_solve(c, s.face_aux2, alpha, threshold, max_iter, f.data(), &s.iters[stage]);
-    if (write_prev) s.force_prev[stage] = f;
+    {
+        IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, s.fprev[stage].p, m * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   c.stream));
+        cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
+    }
+    if (write_prev)
+        IBLGF_CUDA(cudaMemcpyAsync(s.fprev[stage].p, s.cg_f.p, m * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   c.stream));
     // LinSysSolver::pressure_correction (linsys.hpp:131-145)
     OpLists& ol = op_lists(c);
     const int l = c.tree.depth - 1;
-    IBLGF_CUDA(cudaMemsetAsync(c.field(s.cell_aux2), 0, c.field_elems() * sizeof(double), c.stream));
-    smearing(c, s, f, s.face_aux2);
+    launch_fill_zero(c, c.field(s.cell_aux2), c.field_elems());
+    smearing(c, s, s.cg_f.p, s.face_aux2);
     for (int k = 0; k < 3; ++k) launch_halo(c, c.field(s.face_aux2[k]), ol.list[l].p, (int)ol.list[l].n);
     const double* pin[3] = {c.field(s.face_aux2[0]), c.field(s.face_aux2[1]), c.field(s.face_aux2[2])};
     double* pc[1] = {c.field(s.cell_aux2)};
@@ -600,68 +725,49 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
     poisson_apply_lgf(c, s.cell_aux2, s.cell_aux2, IBLGF_IB2AMR);
     launch_axpby(c, c.field(d_field), c.field(s.cell_aux2), -1.0, 1);
     gradient_d();
-    smearing(c, s, f, face_aux, false);
+    smearing(c, s, s.cg_f.p, face_aux, false);
 }
 
-void ib_force(Ctx& c, int stage, double* out, int* iters)
+void ib_force(Ctx& c, int stage, double* out, int* iters, int* not_converged)
 {
     IbState& s = state(c);
     if (stage < 1 || stage > 3) throw Error(IBLGF_EINVAL, "stage must be 1, 2 or 3");
     if (out)
-        for (size_t i = 0; i < s.force_prev[stage].size(); ++i) out[i] = s.force_prev[stage][i];
-    if (iters) *iters = s.iters[stage];
+    {
+        const std::vector<double> f = download(c, s.fprev[stage].p, 3 * (size_t)s.n);
+        std::copy(f.begin(), f.end(), out);
+    }
+    int rec[2] = {0, 0};
+    IBLGF_CUDA(cudaMemcpyAsync(rec, s.cg_rec.p + 2 * stage, sizeof(rec), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    if (iters) *iters = rec[0];
+    if (not_converged) *not_converged = rec[1];
 }
 
-void ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters)
+bool ib_solve(Ctx& c, const int* u, double alpha, double threshold, int max_iter, double* f, int* iters)
 {
     IbState& s = state(c);
     const int nf = (int)c.fields.size();
     for (int k = 0; k < 3; ++k)
         if (u[k] < 0 || u[k] >= nf) throw Error(IBLGF_EINVAL, "bad velocity field id");
     const size_t m = 3 * (size_t)s.n;
-    std::vector<double> uc, Ax, r(m), p, Ap, fv(f, f + m);
-    projection(c, s, u, uc);
-    for (int k = 0; k < 3; ++k)
-        IBLGF_CUDA(cudaMemsetAsync(c.field(s.face_aux2[k]), 0, c.field_elems() * sizeof(double), c.stream));
-    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
-        double t = 0.0;
-        for (size_t i = 0; i < m; ++i) t += a[i] * b[i];
-        return t;
-    };
-    et_h_s_e(c, s, fv, Ax, alpha);
-    for (size_t i = 0; i < m; ++i) r[i] = uc[i] - Ax[i];
-    p = r;
-    double rsold = dot(r, r);
-    int it = 0;
-    for (int k = 0; k < max_iter; ++k)
-    {
-        et_h_s_e(c, s, p, Ap, alpha);
-        ++it;
-        const double pAp = dot(p, Ap);
-        if (pAp == 0.0) break;
-        const double a = rsold / pAp;
-        for (size_t i = 0; i < m; ++i)
-        {
-            fv[i] = fv[i] + p[i] * a;
-            r[i] = r[i] + Ap[i] * -a;
-        }
-        const double rsnew = dot(r, r);
-        const double f2 = dot(fv, fv);
-        if (std::sqrt(rsnew / f2) < threshold) break;
-        for (size_t i = 0; i < m; ++i) p[i] = r[i] + p[i] * (rsnew / rsold);
-        rsold = rsnew;
-    }
-    for (size_t i = 0; i < m; ++i) f[i] = fv[i];
-    if (iters) *iters = it;
+    IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, f, m * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    cg_solve(c, s, u, alpha, threshold, max_iter, s.cg_rec.p);  // record slot 0: direct solves
+    IBLGF_CUDA(cudaMemcpyAsync(f, s.cg_f.p, m * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    int rec[2] = {0, 0};
+    IBLGF_CUDA(cudaMemcpyAsync(rec, s.cg_rec.p, sizeof(rec), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    if (iters) *iters = rec[0];
+    return rec[1] == 0;
 }
 
-void ib_release(const Ctx* c) { g_ib.erase(c); }
+void ib_release(Ctx& c) { c.ext[Ctx::kExtIb].reset(); }
 
 std::vector<int> ib_octant_flags(Ctx& c)
 {
-    auto it = g_ib.find(&c);
-    if (it == g_ib.end()) return {};
-    return it->second->flags;
+    const IbState* s = c.ext_get<IbState>(Ctx::kExtIb);
+    if (!s) return {};
+    return s->flags;
 }
 
 // After an adaptation the point set is re-attached to the new tree (flags,
@@ -669,16 +775,17 @@ std::vector<int> ib_octant_flags(Ctx& c)
 // network carry over
 void ib_on_adapt(Ctx& c)
 {
-    auto it = g_ib.find(&c);
-    if (it == g_ib.end()) return;
+    IbState* old = c.ext_get<IbState>(Ctx::kExtIb);
+    if (!old) return;
     std::vector<double> fp[4];
-    for (int k = 0; k < 4; ++k) fp[k] = it->second->force_prev[k];
-    WarmStart ws = std::move(it->second->ws);
-    const std::vector<double> X = it->second->X;
-    const double Re = it->second->Re;
+    for (int k = 0; k < 4; ++k) fp[k] = download(c, old->fprev[k].p, old->fprev[k].n);
+    WarmStart ws = std::move(old->ws);
+    const std::vector<double> X = old->X;
+    const double Re = old->Re;
     ib_set_points(c, (int)(X.size() / 3), X.data(), Re);
     IbState& s = state(c);
-    for (int k = 0; k < 4; ++k) s.force_prev[k] = fp[k];
+    for (int k = 0; k < 4; ++k) s.fprev[k].upload(fp[k], c.stream);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     s.ws = std::move(ws);
 }
 

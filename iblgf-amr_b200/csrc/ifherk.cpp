@@ -51,6 +51,22 @@ void relpos(int mesh, int comp, int rp[3])
     }
 }
 
+// What a captured time step depends on besides the device data: the field
+// ids, dt, Re, the frame velocity (a launch argument, and whether the
+// frame-velocity update launches at all) and the Poisson solver's switches
+// (which launches a solve makes)
+struct StepKey
+{
+    int u[3] = {-1, -1, -1}, p = -1;
+    double dt = 0.0, Re = 0.0, fv[3] = {0.0, 0.0, 0.0};
+    bool corr = true, snl = false;
+    bool operator==(const StepKey& o) const
+    {
+        return u[0] == o.u[0] && u[1] == o.u[1] && u[2] == o.u[2] && p == o.p && dt == o.dt && Re == o.Re &&
+               fv[0] == o.fv[0] && fv[1] == o.fv[1] && fv[2] == o.fv[2] && corr == o.corr && snl == o.snl;
+    }
+};
+
 struct NsState
 {
     VF q_i, g_i, d_i, r_i, u_i, w_1, w_2, cell_aux, face_aux, edge_aux;
@@ -68,18 +84,16 @@ struct NsState
     double T_last_vel_refresh = 0.0;  // ifherk.hpp:1980
     bool force_refresh = false;       // base_mesh_update of the last adaptation
     // one captured time step (steps without an immersed boundary): replayed
-    // while the velocity / pressure fields, dt and Re stay the same
+    // while everything the capture baked in stays the same (g_key)
     cudaGraphExec_t graph = nullptr;
-    int g_u[3] = {-1, -1, -1}, g_p = -1;
-    double g_dt = 0.0, g_Re = 0.0;
+    StepKey g_key;
     bool graph_failed = false;
     int steps_done = 0;
     long long graph_launches = 0;
-    // (u, p, dt, Re) of the last step run with direct launches: a capture
-    // needs one such step first, so that every plan, table and buffer the
-    // step uses exists before capturing
-    int w_u[3] = {-1, -1, -1}, w_p = -1;
-    double w_dt = 0.0, w_Re = 0.0;
+    // the key of the last step run with direct launches: a capture needs one
+    // such step first, so that every plan, table and buffer the step uses
+    // exists before capturing
+    StepKey w_key;
 };
 
 long long st_launches(const NsState& s) { return s.graph_launches; }
@@ -90,11 +104,19 @@ struct NsOptions
     double cg_threshold = 1e-3;
     int cg_max_iter = 40;
 };
-std::map<const Ctx*, NsOptions> g_nsopt;
-std::map<const Ctx*, std::unique_ptr<NsState>> g_ns;
 // an adaptation before the context's first time step: its old-correction
 // flags and base-mesh update wait for the time step's state
-std::map<const Ctx*, std::pair<std::vector<char>, bool>> g_ns_pending;
+struct NsPending
+{
+    std::vector<char> old_corr;
+    bool base_mesh_update = false;
+};
+
+NsOptions& ns_opt(Ctx& c)
+{
+    if (!c.ext[Ctx::kExtNsOpt]) c.ext[Ctx::kExtNsOpt] = std::make_shared<NsOptions>();
+    return *c.ext_get<NsOptions>(Ctx::kExtNsOpt);
+}
 
 VF make_vf(Ctx& c, int mesh)
 {
@@ -118,8 +140,7 @@ void drop_old_correction(Ctx& c, NsState& s)
 
 NsState& ns_state(Ctx& c)
 {
-    auto it = g_ns.find(&c);
-    if (it != g_ns.end()) return *it->second;
+    if (auto* have = c.ext_get<NsState>(Ctx::kExtNs)) return *have;
     auto s = std::make_unique<NsState>();
     s->q_i = make_vf(c, kFace);
     s->g_i = make_vf(c, kFace);
@@ -131,16 +152,18 @@ NsState& ns_state(Ctx& c)
     s->cell_aux = make_vf(c, kCell);
     s->face_aux = make_vf(c, kFace);
     s->edge_aux = make_vf(c, kEdge);
-    auto pend = g_ns_pending.find(&c);
-    if (pend != g_ns_pending.end())
+    if (const NsPending* pend = c.ext_get<NsPending>(Ctx::kExtNsPending))
     {
-        s->old_corr = pend->second.first;
-        s->force_refresh = pend->second.second;
-        g_ns_pending.erase(pend);
+        s->old_corr = pend->old_corr;
+        s->force_refresh = pend->base_mesh_update;
+        c.ext[Ctx::kExtNsPending].reset();
     }
     ns_build_lists(c, *s);
     auto& ref = *s;
-    g_ns.emplace(&c, std::move(s));
+    c.ext[Ctx::kExtNs] = std::shared_ptr<NsState>(s.release(), [](NsState* p) {
+        if (p->graph) cudaGraphExecDestroy(p->graph);
+        delete p;
+    });
     return ref;
 }
 
@@ -199,7 +222,7 @@ class Step
 {
   public:
     Step(Ctx& c_, NsState& s_, double dt_, double Re_)
-    : c(c_), s(s_), pl(poisson_lists(c_)), ol(op_lists(c_)), dt(dt_), Re(Re_), opt(g_nsopt[&c_])
+    : c(c_), s(s_), pl(poisson_lists(c_)), ol(op_lists(c_)), dt(dt_), Re(Re_), opt(ns_opt(c_))
     {
         bl = c.tree.base_level;
         depth = c.tree.depth;
@@ -530,16 +553,26 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
             drop_old_correction(c, s);
             continue;
         }
-        const bool graphable = !ib_active(c) && !c.profile && !s.graph_failed;
-        const bool same = s.graph && s.g_p == p && s.g_dt == dt && s.g_Re == Re && s.g_u[0] == u[0] &&
-                          s.g_u[1] == u[1] && s.g_u[2] == u[2];
+        // steps with the immersed boundary are captured too: their force CG
+        // is a conditional while-node of the graph (not with the learned
+        // warm start, which assembles its inputs on the host)
+        const bool graphable = (!ib_active(c) || ib_graphable(c)) && !c.profile && !s.graph_failed;
+        StepKey key;
+        for (int k = 0; k < 3; ++k) key.u[k] = u[k];
+        key.p = p;
+        key.dt = dt;
+        key.Re = Re;
+        const NsOptions& opt = ns_opt(c);
+        for (int k = 0; k < 3; ++k) key.fv[k] = opt.frame_vel[k];
+        key.corr = c.use_correction;
+        key.snl = c.subtract_non_leaf;
+        const bool same = s.graph && s.g_key == key;
         if (graphable && same)
         {
             IBLGF_CUDA(cudaGraphLaunch(s.graph, c.stream));
             c.launches += st_launches(s);
         }
-        else if (graphable && s.w_p == p && s.w_dt == dt && s.w_Re == Re && s.w_u[0] == u[0] &&
-                 s.w_u[1] == u[1] && s.w_u[2] == u[2])
+        else if (graphable && s.w_key == key)
         {
             // capture after a first direct step has built every plan and sized
             // every buffer, so the step makes no host synchronisation
@@ -574,20 +607,14 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
             {
                 cudaGraphDestroy(g);
                 s.graph_launches = c.launches - l0;
-                for (int k = 0; k < 3; ++k) s.g_u[k] = u[k];
-                s.g_p = p;
-                s.g_dt = dt;
-                s.g_Re = Re;
+                s.g_key = key;
                 IBLGF_CUDA(cudaGraphLaunch(s.graph, c.stream));
             }
         }
         else
         {
             st.time_step(uf, pf, false);
-            for (int k = 0; k < 3; ++k) s.w_u[k] = u[k];
-            s.w_p = p;
-            s.w_dt = dt;
-            s.w_Re = Re;
+            s.w_key = key;
         }
         ++s.steps_done;
         *T += dt;
@@ -635,7 +662,7 @@ void ns_clean_leaf_correction_boundary(Ctx& c, const int* fields, int n, int lev
 void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max_iter)
 {
     if (!(cg_threshold > 0) || cg_max_iter < 0) throw Error(IBLGF_EINVAL, "bad CG settings");
-    NsOptions& o = g_nsopt[&c];
+    NsOptions& o = ns_opt(c);
     for (int k = 0; k < 3; ++k) o.frame_vel[k] = frame_vel ? frame_vel[k] : 0.0;
     o.cg_threshold = cg_threshold;
     o.cg_max_iter = cg_max_iter;
@@ -643,33 +670,31 @@ void ns_options(Ctx& c, const double* frame_vel, double cg_threshold, int cg_max
 
 void ns_on_adapt(Ctx& c, bool base_mesh_update, const std::vector<char>& old_corr)
 {
-    auto it = g_ns.find(&c);
-    if (it == g_ns.end())
+    NsState* sp = c.ext_get<NsState>(Ctx::kExtNs);
+    if (!sp)
     {
-        auto& pend = g_ns_pending[&c];
-        pend.first = old_corr;
-        pend.second = pend.second || base_mesh_update;
+        if (!c.ext[Ctx::kExtNsPending]) c.ext[Ctx::kExtNsPending] = std::make_shared<NsPending>();
+        NsPending& pend = *c.ext_get<NsPending>(Ctx::kExtNsPending);
+        pend.old_corr = old_corr;
+        pend.base_mesh_update = pend.base_mesh_update || base_mesh_update;
         return;
     }
-    NsState& s = *it->second;
+    NsState& s = *sp;
     s.old_corr = old_corr;
     if (s.graph) cudaGraphExecDestroy(s.graph);
     s.graph = nullptr;
     s.graph_failed = false;
-    s.g_p = s.w_p = -1;
-    for (int k = 0; k < 3; ++k) s.g_u[k] = s.w_u[k] = -1;
+    s.g_key = s.w_key = StepKey{};
     ns_build_lists(c, s);
     // ifherk.hpp:1093-1096: a grown base mesh refreshes the velocity
     s.force_refresh = s.force_refresh || base_mesh_update;
 }
 
-void ns_release(const Ctx* c)
+void ns_release(Ctx& c)
 {
-    auto it = g_ns.find(c);
-    if (it != g_ns.end() && it->second->graph) cudaGraphExecDestroy(it->second->graph);
-    g_ns.erase(c);
-    g_nsopt.erase(c);
-    g_ns_pending.erase(c);
+    c.ext[Ctx::kExtNs].reset();
+    c.ext[Ctx::kExtNsOpt].reset();
+    c.ext[Ctx::kExtNsPending].reset();
 }
 
 }  // namespace iblgf_b200

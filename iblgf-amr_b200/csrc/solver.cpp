@@ -110,7 +110,10 @@ void ctx_init(Ctx& c)
         c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
         return;
     }
+    c.d_status.alloc(1);
+    IBLGF_CUDA(cudaMemsetAsync(c.d_status.p, 0, sizeof(int), c.stream));
     init_twiddle_constants(c.cfg.device);
+    init_pfa_constants(c.cfg.device);
     // twiddles e^{-2 pi i j / P}
     std::vector<double> tw(2 * c.P);
     for (int j = 0; j < c.P; ++j)
@@ -148,6 +151,27 @@ void ctx_init(Ctx& c)
     c.h_mats = mats;
     c.tree.init(e, c.cfg.bd_base, c.cfg.bd_extent);
     launch_lgf_table(c);
+}
+
+bool inverse_fp32_passes(const Ctx& c)
+{
+    static const bool on = [] {
+        const char* e = std::getenv("IBLGF_INV_FP32");
+        return e && e[0] == '1';
+    }();
+    return c.cfg.precision == IBLGF_FP32 && on;
+}
+
+void check_status(Ctx& c)
+{
+    if (!c.d_status.p) return;
+    int h = 0;
+    IBLGF_CUDA(cudaMemcpyAsync(&h, c.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    if (!h) return;
+    IBLGF_CUDA(cudaMemsetAsync(c.d_status.p, 0, sizeof(int), c.stream));
+    if (h & 1) throw Error(IBLGF_ETIMEOUT, "a bounded device wait ran out (results of the affected launches are void)");
+    throw Error(IBLGF_EINTERNAL, "device status " + std::to_string(h));
 }
 
 // --------------------------------------------------------------- domain
@@ -816,6 +840,22 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
     p.grp_pm.upload(h.gpm, c.stream);
     p.grp_tgt.upload(h.gtgt, c.stream);
     p.n_exec = h.n_exec;
+    p.adj_only = !h.tcoarse.empty();
+    for (int m : h.tcoarse) p.adj_only = p.adj_only && m == 2;
+    // MAC work per frequency: 8 flops per complex multiply-add of the direct
+    // kernels; the block-Toeplitz kernel per (group, present parent) 27
+    // complex multiply-adds and 19 complex additions, per group the 38
+    // additions of the final combination, and per CTA (16 groups) the 3375
+    // real-times-complex terms of its coefficient rows
+    p.mac_flops = (long long)h.psrc.size() * 8;
+    if (p.adj_only || h.ttab.empty())
+        p.mac_flops += (h.n_exec - (long long)h.psrc.size()) * 8;
+    else
+    {
+        for (unsigned pm : h.gpm) p.mac_flops += (long long)__builtin_popcount(pm) * (27 * 8 + 19 * 2) + 38 * 2;
+        for (size_t t = 0; t + 1 < h.tgptr.size(); ++t)
+            p.mac_flops += (long long)((h.tgptr[t + 1] - h.tgptr[t] + 15) / 16) * 3375 * 4;
+    }
     p.n_tgt = (int)h.tgt_list.size();
     p.n_pairs = h.n_pairs;
     p.n_spec_unique = h.n_spec_unique;
@@ -941,6 +981,7 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     for (auto& t : p.antrp) c.stats[5] += t.n_tasks;
     for (auto& t : p.intrp) c.stats[6] += t.n_tasks;
     c.stats[7] += p.n_tgt - p.n_csr_tgt;
+    c.stats[9] += p.mac_flops;
     c.stats[8] += p.n_exec;
     double* fs = c.field(c.f_fmm_s);
     double* ft = c.field(c.f_fmm_t);
@@ -956,7 +997,8 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     {
         // the source spectra and one zero row after them (absent MAC candidates read it)
         ensure_bytes(c.d_src_spec, (size_t)(p.n_src + 1) * c.NC * cb);
-        IBLGF_CUDA(cudaMemsetAsync(c.d_src_spec.p + (size_t)p.n_src * c.NC * cb, 0, c.NC * cb, c.stream));
+        launch_fill_zero(c, reinterpret_cast<double*>(c.d_src_spec.p + (size_t)p.n_src * c.NC * cb),
+                         c.NC * cb / sizeof(double));
         ensure_bytes(c.d_acc, (size_t)p.n_tgt * c.NC * cb);
         launch_forward_sources(c, fs, p.src_oct.p, p.n_src, c.d_src_spec.p);
     }
@@ -975,15 +1017,9 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
 }
 
 // --------------------------------------------------------------- Poisson
-namespace
-{
-std::map<const Ctx*, std::unique_ptr<PoissonLists>> g_plists;
-}  // namespace
-
 PoissonLists& poisson_lists(Ctx& c)
 {
-    auto it = g_plists.find(&c);
-    if (it != g_plists.end()) return *it->second;
+    if (auto* have = c.ext_get<PoissonLists>(Ctx::kExtPLists)) return *have;
     auto pl = std::make_unique<PoissonLists>();
     std::vector<int> all, leaves;
     for (int i = 0; i < c.n_oct; ++i)
@@ -1035,20 +1071,14 @@ PoissonLists& poisson_lists(Ctx& c)
     }
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     auto& ref = *pl;
-    g_plists.emplace(&c, std::move(pl));
+    c.ext[Ctx::kExtPLists] = std::shared_ptr<PoissonLists>(std::move(pl));
     return ref;
 }
 
-namespace
-{
 // per level (and "all levels" at index kMaxLevel+1): block list and dx per block
-std::map<const Ctx*, std::unique_ptr<OpLists>> g_oplists;
-}  // namespace
-
 OpLists& op_lists(Ctx& c)
 {
-    auto it = g_oplists.find(&c);
-    if (it != g_oplists.end()) return *it->second;
+    if (auto* have = c.ext_get<OpLists>(Ctx::kExtOpLists)) return *have;
     auto ol = std::make_unique<OpLists>();
     const int L = kMaxLevel + 2;
     ol->list.resize(L);
@@ -1072,7 +1102,7 @@ OpLists& op_lists(Ctx& c)
     ol->dx[L - 1].upload(alldx, c.stream);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     auto& ref = *ol;
-    g_oplists.emplace(&c, std::move(ol));
+    c.ext[Ctx::kExtOpLists] = std::shared_ptr<OpLists>(std::move(ol));
     return ref;
 }
 
@@ -1173,8 +1203,8 @@ void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const i
     double* st = c.field(c.f_source_tmp);
     double* tt = c.field(c.f_target_tmp);
     const size_t bytes = c.field_elems() * sizeof(double);
-    IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
-    IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
+    launch_fill_zero(c, st, bytes / sizeof(double));
+    launch_fill_zero(c, tt, bytes / sizeof(double));
     const int bl = c.tree.base_level, depth = c.tree.depth;
     if (fmm_type == IBLGF_IB2xIB)
     {
@@ -1205,10 +1235,10 @@ void apply_if(Ctx& c, int src, int tgt, double alpha_base, int fmm_type, const i
     }
 }
 
-void poisson_release(const Ctx* c)
+void poisson_release(Ctx& c)
 {
-    g_plists.erase(c);
-    g_oplists.erase(c);
+    c.ext[Ctx::kExtPLists].reset();
+    c.ext[Ctx::kExtOpLists].reset();
 }
 
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
@@ -1221,9 +1251,9 @@ void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type)
     double* tt = c.field(c.f_target_tmp);
     double* ct = c.field(c.f_correction_tmp);
     const size_t bytes = c.field_elems() * sizeof(double);
-    IBLGF_CUDA(cudaMemsetAsync(st, 0, bytes, c.stream));
-    IBLGF_CUDA(cudaMemsetAsync(tt, 0, bytes, c.stream));
-    IBLGF_CUDA(cudaMemsetAsync(ct, 0, bytes, c.stream));
+    launch_fill_zero(c, st, bytes / sizeof(double));
+    launch_fill_zero(c, tt, bytes / sizeof(double));
+    launch_fill_zero(c, ct, bytes / sizeof(double));
     if (fmm_type == IBLGF_IB2AMR)
     {
         // finest-level interior copy, coarsified (cell mesh), one sweep per

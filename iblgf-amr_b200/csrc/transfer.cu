@@ -345,6 +345,36 @@ void launch_source_correction(Ctx& c, const double* target_tmp, double* corr, co
     IBLGF_CUDA(cudaGetLastError());
 }
 
+namespace
+{
+// n doubles from p set to zero (16-byte stores where p is aligned)
+__global__ void fill_zero_kernel(double* __restrict__ p, size_t n)
+{
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0)
+    {
+        double2* q = reinterpret_cast<double2*>(p);
+        const double2 z = make_double2(0.0, 0.0);
+        for (size_t j = i; j < n / 2; j += stride) q[j] = z;
+        if (i == 0 && (n & 1)) p[n - 1] = 0.0;
+    }
+    else
+        for (size_t j = i; j < n; j += stride) p[j] = 0.0;
+}
+}  // namespace
+
+// a plain kernel (not cudaMemsetAsync), so that the zeroing can sit in the
+// body of a conditional graph node
+void launch_fill_zero(Ctx& c, double* p, size_t n)
+{
+    if (!n) return;
+    const size_t blocks = std::min<size_t>((n / 2 + 255) / 256, 148 * 8);
+    fill_zero_kernel<<<(unsigned)std::max<size_t>(blocks, 1), 256, 0, c.stream>>>(p, n);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n)
 {
     if (!n) return;

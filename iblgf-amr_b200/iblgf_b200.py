@@ -38,7 +38,8 @@ EXPORTS = [
     "iblgf_poisson_options", "iblgf_op_apply", "iblgf_buffer_exchange", "iblgf_lgf_table", "iblgf_lgf_get",
     "iblgf_ns_step", "iblgf_batch_add_problem", "iblgf_batch_finalize", "iblgf_batch_problem_info",
     "iblgf_batch_problem_octants", "iblgf_batch_apply_lgf", "iblgf_ib_set_points", "iblgf_ib_flags",
-    "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_warmstart", "iblgf_ib_warmstart_info",
+    "iblgf_ib_solve", "iblgf_ns_options", "iblgf_ib_force", "iblgf_ib_stage_status", "iblgf_ib_warmstart",
+    "iblgf_ib_warmstart_info",
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
@@ -99,6 +100,7 @@ def lib():
     L.iblgf_ib_solve.argtypes = [vp, vp, cd, cd, ci, vp, vp]
     L.iblgf_ns_options.argtypes = [vp, vp, cd, ci]
     L.iblgf_ib_force.argtypes = [vp, ci, vp, vp]
+    L.iblgf_ib_stage_status.argtypes = [vp, ci, vp, vp]
     L.iblgf_ib_warmstart.argtypes = [vp, ci, ci, ci, cd, ctypes.c_uint]
     L.iblgf_ib_warmstart_info.argtypes = [vp, vp]
     L.iblgf_ws_check.argtypes = [vp, ci, ci, vp, vp, vp, vp, vp, vp]
@@ -122,8 +124,16 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+ENOTCONVERGED = 6
+
+
 class IblgfError(RuntimeError):
     pass
+
+
+class IblgfNotConverged(IblgfError):
+    """An iterative solve stopped at its iteration limit; the outputs
+    (force, iterations) are attached."""
 
 
 def write_tree(path, keys, levels, flags):
@@ -182,6 +192,7 @@ class Solver:
             raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
         self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
+        self._async_out = []  # host buffers of asynchronous downloads in flight
         self.Nb = block_extent + 2
         self.block_extent = block_extent
         self.precision = precision
@@ -380,8 +391,9 @@ class Solver:
 
     def close(self):
         if getattr(self, "h", None):
-            self._destroy(self.h)
+            self._destroy(self.h)  # waits for the context's copies
             self.h = None
+        self._async_out = []
 
     def __del__(self):
         self.close()
@@ -445,12 +457,26 @@ class Solver:
         return a
 
     def download_leaves_async(self, fid, out):
-        """Starts the copy of the leaf interiors into `out` (pinned, (n_leaves,
-        e, e, e) float64 or a pointer-bearing tensor) and returns; the copy
-        is complete after synchronize()."""
-        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
-        n = out.numel() if hasattr(out, "numel") else out.size
+        """Starts the copy of the leaf interiors into `out` and returns; the
+        copy is complete after synchronize(). `out` is a C-contiguous float64
+        array or tensor of shape (n_leaves, e, e, e), pinned for the copy to
+        overlap; it is kept alive here until synchronize() or close()."""
+        e = self.block_extent
+        shape = (self.n_leaves, e, e, e)
+        if hasattr(out, "data_ptr"):  # torch tensor
+            import torch
+            ok = (out.dtype == torch.float64 and out.is_contiguous() and tuple(out.shape) == shape
+                  and out.device.type == "cpu")
+            ptr, n = out.data_ptr(), out.numel()
+        else:
+            ok = (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                  and out.shape == shape)
+            ptr, n = (out.ctypes.data, out.size) if ok else (0, 0)
+        if not ok:
+            raise IblgfError("download_leaves_async: out must be a C-contiguous float64 host array of shape %s"
+                             % (shape,))
         self._check(lib().iblgf_field_download_leaves_async(self.h, fid, ctypes.c_void_p(ptr), n))
+        self._async_out.append(out)
 
     def zero(self, fid):
         self._check(lib().iblgf_field_zero(self.h, fid))
@@ -462,6 +488,7 @@ class Solver:
 
     def synchronize(self):
         self._check(lib().iblgf_synchronize(self.h))
+        self._async_out = []
 
     # ------------------------------------------------------------ solver
     def fmm_apply(self, src, tgt, level, non_leaf_as_source, scale=1.0, fmm_type=AMR2AMR):
@@ -524,6 +551,16 @@ class Solver:
             out.append(it.value)
         return out
 
+    def ib_converged(self):
+        """Whether each of stages 1..3 of the last step converged before
+        cg_max_iter (the reference stops there silently)."""
+        out = []
+        for st in (1, 2, 3):
+            it, ok = ctypes.c_int(), ctypes.c_int()
+            self._check(lib().iblgf_ib_stage_status(self.h, st, ctypes.byref(it), ctypes.byref(ok)))
+            out.append(bool(ok.value))
+        return out
+
     def ib_warmstart(self, mode, train_steps=0, epochs=0, lr=1e-3, seed=1):
         self._check(lib().iblgf_ib_warmstart(self.h, int(mode), int(train_steps), int(epochs), float(lr), int(seed)))
 
@@ -560,8 +597,13 @@ class Solver:
         uf = np.ascontiguousarray(np.asarray(u_fields, dtype=np.int32))
         f = np.zeros((len(self._ib_X), 3)) if f0 is None else np.ascontiguousarray(f0, dtype=np.float64).copy()
         it = ctypes.c_int()
-        self._check(lib().iblgf_ib_solve(self.h, _p(uf), float(alpha), float(threshold), int(max_iter), _p(f),
-                                         ctypes.byref(it)))
+        rc = lib().iblgf_ib_solve(self.h, _p(uf), float(alpha), float(threshold), int(max_iter), _p(f),
+                                  ctypes.byref(it))
+        if rc == ENOTCONVERGED:
+            err = IblgfNotConverged("IB force CG stopped at max_iter = %d without converging" % max_iter)
+            err.force, err.iterations = f, it.value
+            raise err
+        self._check(rc)
         return f, it.value
 
     def conv_block(self, src_dptr, kernel_dptr, out_dptr, scale=1.0):
@@ -578,9 +620,10 @@ class Solver:
 
     def stats(self):
         """[sweeps, sources, targets, pairs, unique spectra, anterp tasks,
-        interp tasks, group-MAC targets, MAC products executed]"""
-        out = np.zeros(9, np.int64)
-        self._check(lib().iblgf_stats_n(self.h, _p(out), 9))
+        interp tasks, group-MAC targets, MAC products covered, MAC flops per
+        frequency]"""
+        out = np.zeros(10, np.int64)
+        self._check(lib().iblgf_stats_n(self.h, _p(out), 10))
         return out
 
     def fma_peak(self, precision):
@@ -635,6 +678,7 @@ class BatchSolver(Solver):
             raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
         self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
+        self._async_out = []  # host buffers of asynchronous downloads in flight
         self.Nb = block_extent + 2
         self.block_extent = block_extent
         self.precision = precision

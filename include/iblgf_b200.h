@@ -31,7 +31,8 @@ enum
     IBLGF_ECUDA = 2,    /* CUDA runtime error */
     IBLGF_ENOMEM = 3,   /* device allocation failed */
     IBLGF_ETIMEOUT = 4, /* a bounded device wait gave up */
-    IBLGF_EINTERNAL = 5
+    IBLGF_EINTERNAL = 5,
+    IBLGF_ENOTCONVERGED = 6 /* an iterative solve stopped at its iteration limit; outputs written */
 };
 
 enum { IBLGF_FP64 = 0, IBLGF_FP32 = 1 };
@@ -221,6 +222,11 @@ int iblgf_block_norms(iblgf_ctx* ctx, const int* fields, int n_comp, double* max
 /* IB force (IB::force_prev, n x 3) and CG iteration count of the last
  * step's stage 1, 2 or 3; either output may be NULL */
 int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out, int* iters);
+/* CG iteration count of the last solve of stage 1, 2 or 3 and whether it
+ * converged (0: it stopped at cg_max_iter, where the reference's CG_solve,
+ * linsys.hpp:202-229, stops silently); no counterpart in the reference.
+ * Synchronises the context stream. Either output may be NULL. */
+int iblgf_ib_stage_status(iblgf_ctx* ctx, int stage, int* iters, int* converged);
 
 /* ---- immersed boundary (ib.hpp, linsys.hpp) ------------------------------
  * iblgf_ib_set_points: the IB points (n x 3 coordinates, the reference's
@@ -232,7 +238,9 @@ int iblgf_ib_force(iblgf_ctx* ctx, int stage, double* out, int* iters);
  * is_ib, bit1 is_extended_ib. iblgf_ib_solve: LinSysSolver::ib_solve +
  * CG_solve (linsys.hpp:113-230) for the face velocity u_fields[0..2] (a body
  * at rest in the frame); force (n x 3) is the initial guess in and the IB
- * force out, iters the CG iteration count. */
+ * force out, iters the CG iteration count. The CG runs on the device (FP64
+ * iterates and dot products); a solve that stops at max_iter without
+ * converging writes force and iters and returns IBLGF_ENOTCONVERGED. */
 int iblgf_ib_set_points(iblgf_ctx* ctx, int n, const double* coords, double Re);
 int iblgf_ib_flags(iblgf_ctx* ctx, int* flags);
 int iblgf_ib_solve(iblgf_ctx* ctx, const int* u_fields, double alpha, double threshold, int max_iter,
@@ -319,11 +327,13 @@ int iblgf_profile_read(iblgf_ctx* ctx, double* out4);
  * the sibling-group MAC (the rest use the general pair-list MAC). */
 int iblgf_stats(iblgf_ctx* ctx, long long* out8);
 
-/* The first n (1 <= n <= 9) counters: [0]-[7] as iblgf_stats, then [8] the
- * (target, source) spectral products the MAC kernels execute. A sibling group
- * runs all 64 (child, candidate) products of every neighbour parent that has a
- * candidate, so [8] >= [3]; [3] / [8] is the share of executed MAC work the
- * reference's pair list also does. IBLGF_EINVAL for n outside [1, 9]. */
+/* The first n (1 <= n <= 10) counters: [0]-[7] as iblgf_stats, then [8] the
+ * (target, source) spectral products the sibling-group MAC covers: a group
+ * covers all 64 (child, candidate) products of every neighbour parent that
+ * has a candidate, so [8] >= [3]; and [9] the floating-point operations the
+ * MAC kernels execute per spectrum frequency (the block-Toeplitz group
+ * kernel forms the 64 products of a parent with 27 complex multiplies).
+ * IBLGF_EINVAL for n outside [1, 10]. */
 int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the

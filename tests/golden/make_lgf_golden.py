@@ -16,7 +16,9 @@ import warnings
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IBLGF_REFERENCE")
+    if not ref:
+        sys.exit("usage: %s <reference tree> (or set IBLGF_REFERENCE)" % sys.argv[0])
     sys.path.insert(0, os.path.join(ref, "include/iblgf/lgf/lgf_table_gen"))
     import lgf_integrator  # noqa: E402
 

@@ -13,11 +13,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "iblgf-amr_b200"))
 import chombo_h5  # noqa: E402
 
-SRC = "/root/reference/tests/ns_amr_lgf/configs/ref.hdf5"
+
+def source_path():
+    """ref.hdf5 inside the reference tree, whose root is the first command-line
+    argument or the IBLGF_REFERENCE environment variable."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IBLGF_REFERENCE")
+    if not root:
+        sys.exit("usage: %s <reference tree> (or set IBLGF_REFERENCE)" % sys.argv[0])
+    return os.path.join(root, "tests", "ns_amr_lgf", "configs", "ref.hdf5")
 
 
 def main():
-    r = chombo_h5.read_chombo(SRC)
+    r = chombo_h5.read_chombo(source_path())
     lev = r["levels"][0]
     comps = r["components"]
     idx = [comps.index(n) for n in ("u_0", "u_1", "u_2", "p")]

@@ -1,0 +1,146 @@
+"""GPU parity at the benchmarked configurations (not shrunken cases): the
+device path through the C ABI against the FP64 oracle on the same seeded
+inputs.
+
+* amr_3level (8^3 base blocks of 16^3 cells, 3 mesh levels, 9596 octants):
+  PoissonSolver::apply_lgf (poisson.hpp:587-894), FP64 <= 1e-12 and FP32
+  FFT/MAC path <= 1e-5 relative L-inf over every node of every block.
+* The batch of 256 independent problems (1..64 blocks of 16^3 cells): every
+  problem against the oracle's solve of that problem alone, same tolerances.
+* The vortex ring (dx = R/32, 1362 octants) and the flow past the sphere
+  (2009 IB points, wake refinement): two IF-HERK steps (ifherk.hpp:1078-1200,
+  with LinSysSolver::ib_solve, linsys.hpp:113-230, for the sphere), velocity
+  and pressure against the oracle: FP64 <= 1e-10 (no IB) / 1e-9 (IB), FP32
+  <= 1e-5 for velocity.
+
+The oracle needs tens of seconds per case on the host cores; these tests are
+marked slow as well as gpu."""
+import numpy as np
+import pytest
+
+import iblgf_b200 as B
+import iblgf_setups as S
+import oracle_lib as O
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def rel_linf(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def amr_3level_oracle():
+    case = S.GaussianPoisson("amr_3level")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(o)
+    return case, o, src, o.apply_lgf(src)
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_poisson_amr_3level_matches_oracle(amr_3level_oracle, precision, tol):
+    case, o, src, ref = amr_3level_oracle
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=precision)
+    assert g.n == o.n == 9596
+    assert np.array_equal(g.keys, o.keys) and np.array_equal(g.flags, o.flags)
+    fs, ft = g.field(src), g.field()
+    for call in range(2):  # the second solve runs on cached plans and spectra
+        g.apply_lgf(fs, ft)
+        err = rel_linf(g.download(ft), ref)
+        print("amr_3level precision %d call %d: rel L-inf %.3e" % (precision, call, err))
+        assert err < tol, (call, err)
+    g.close()
+
+
+@pytest.fixture(scope="module")
+def batch_c3_oracle():
+    case = S.BatchPoisson("c3")
+    doms, refs = [], []
+    for i, p in enumerate(case.problems):
+        o = O.Domain(p["bd_base"], p["bd_extent"], case.block_extent, case.dx_base, p["blocks"])
+        doms.append((o.keys, o.flags))
+        refs.append(o.apply_lgf(case.fields(o, i)))
+    return case, doms, refs
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_batch_256_problems_match_oracle(batch_c3_oracle, precision, tol):
+    case, doms, refs = batch_c3_oracle
+    assert len(case.problems) == 256
+    g = B.BatchSolver(case.block_extent, case.dx_base, case.problems, precision=precision)
+    src = g.zeros()
+    for i in range(len(case.problems)):
+        v = g.problem(i)
+        assert np.array_equal(doms[i][0], v.keys) and np.array_equal(doms[i][1], v.flags)
+        src[v.offset:v.offset + v.n] = case.fields(v, i)
+    fs, ft = g.field(src), g.field()
+    g.apply_lgf(fs, ft)
+    out = g.split(g.download(ft))
+    errs = [rel_linf(out[i], ref) for i, ref in enumerate(refs)]
+    print("batch of 256, precision %d: worst rel L-inf %.3e (problem %d)"
+          % (precision, max(errs), int(np.argmax(errs))))
+    assert max(errs) < tol
+    g.close()
+
+
+@pytest.fixture(scope="module")
+def c4_oracle():
+    case = S.VortexRingNS("c4")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    u0 = case.initial_velocity(o)
+    ur, pr = o.ns_step(u0, case.dt(), case.Re, 0.0, 2)
+    return case, o, u0, ur, pr
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-10), (B.FP32, 1e-5)])
+def test_ns_vortex_ring_c4_two_steps_match_oracle(c4_oracle, precision, tol):
+    case, o, u0, ur, pr = c4_oracle
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=precision)
+    assert np.array_equal(o.keys, g.keys) and np.array_equal(o.flags, g.flags)
+    uf = [g.field(u0[k]) for k in range(3)]
+    pf = g.field()
+    g.ns_step(uf, pf, case.dt(), case.Re, 0.0, 2)
+    errs = [rel_linf(g.download(uf[k]), ur[k]) for k in range(3)]
+    perr = rel_linf(g.download(pf), pr)
+    print("vortex ring c4, precision %d: u %s, p %.3e" % (precision, ["%.2e" % e for e in errs], perr))
+    assert max(errs) < tol and perr < tol * 10
+    g.close()
+
+
+@pytest.fixture(scope="module")
+def c5_oracle():
+    case = S.SphereIB("c5")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    X = O.sphere_points(case.dx_base, o.depth - 1 - o.base_level, case.ibph)
+    u0 = case.velocity(o, U=(0.0, 0.0, 0.0))
+    dt, fv = 0.35 * case.dx_base / 4, (-1.0, 0.0, 0.0)
+    ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, 0.0, 2)
+    return case, o, X, u0, dt, fv, ur, pr, fr
+
+
+@pytest.mark.parametrize("precision,tol,ptol", [(B.FP64, 1e-9, 1e-9), (B.FP32, 1e-4, 5e-4)])
+def test_ns_sphere_c5_two_steps_match_oracle(c5_oracle, precision, tol, ptol):
+    """Tolerances as the small sphere case: in FP32 the pressure carries the
+    FP32 perturbation of the IB CG iterates divided by a33 dt."""
+    case, o, X, u0, dt, fv, ur, pr, fr = c5_oracle
+    assert len(X) == 2009
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate, precision=precision)
+    g.ib_set_points(X, case.Re)
+    g.ns_options(fv)
+    uf = [g.field(u0[k]) for k in range(3)]
+    pf = g.field()
+    g.ns_step(uf, pf, dt, case.Re, 0.0, 2)
+    errs = [rel_linf(g.download(uf[k]), ur[k]) for k in range(3)]
+    perr = rel_linf(g.download(pf), pr)
+    ferr = [rel_linf(g.ib_force(st + 1), fr[st]) for st in range(3)]
+    print("sphere c5, precision %d: u %s, p %.3e, forces %s"
+          % (precision, ["%.2e" % e for e in errs], perr, ["%.2e" % e for e in ferr]))
+    assert max(errs) < tol and perr < ptol
+    assert max(ferr) < tol * 10
+    g.close()
