@@ -192,6 +192,8 @@ def main():
     for _ in range(args.warmup):
         g.apply_lgf(fs, ft)
     g.synchronize()
+    # the group-MAC autotuner's measurements (first warm-up solve, per plan)
+    tuning = g.mac_tuning()
 
     # ---- device-timed region: inputs resident in HBM (> L2: fields and spectra)
     g.profile(True)
@@ -342,6 +344,9 @@ def main():
                 "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s",
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
                 "gpu_launches": int(launches),
+                "mac_autotune": {"variants": "0, 1: direct sibling-group kernel (64 x 768, 32 x 512 FP32); "
+                                             "2: block-Toeplitz kernel (TMA-staged coefficients)",
+                                 "plans": tuning},
                 "roofline": roof,
                 "clocks": ck.summary(),
                 "cpu_baseline": cpu}

@@ -521,6 +521,25 @@ int iblgf_ib_solve(iblgf_ctx* x, const int* u_fields, double alpha, double thres
     });
 }
 
+int iblgf_mac_variant(iblgf_ctx* x, int variant)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (variant < -1 || variant > 2) throw iblgf_b200::Error(IBLGF_EINVAL, "MAC variant must be -1, 0, 1 or 2");
+        c.mac_variant_forced = variant;
+    });
+}
+
+int iblgf_mac_tuning(iblgf_ctx* x, double* out, int max_rows, int* n_rows)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!n_rows || (max_rows > 0 && !out)) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        const int n = (int)c.mac_tuning.size();
+        *n_rows = n;
+        for (int i = 0; i < n && i < max_rows; ++i)
+            for (int j = 0; j < 7; ++j) out[7 * i + j] = c.mac_tuning[i][j];
+    });
+}
+
 int iblgf_conv_block_noalloc(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {

@@ -135,6 +135,8 @@ struct TpTasks  // tensor-product transfer tasks of one tree level
 // sibling groups per group-MAC tile; the kernel's thread rows x groups per
 // row cover exactly this many
 constexpr int kGroupTileCap = 32;
+// sibling groups per work item of the block-Toeplitz MAC (a tile has up to 3)
+constexpr int kToeplitzPart = 14;
 
 struct FmmPlan
 {
@@ -160,9 +162,13 @@ struct FmmPlan
     // candidates (the zero row for absent ones)
     DevBuf<int> tile_gptr, tile_jr, tile_tab, tile_coarse, spec_u, grp_tgt;
     DevBuf<unsigned> grp_pm;     // per group: bit n set = neighbour parent n has a candidate
+    DevBuf<int> tile_combo;      // per tile: coefficient table of the block-Toeplitz MAC (its level difference)
+    DevBuf<int> tile_parts;      // block-Toeplitz work: tile << 2 | part for the non-empty parts of 14 groups
+    int n_parts = 0;
     long long n_exec = 0;        // (target, source) products the MAC kernels execute
     long long mac_flops = 0;     // floating-point operations of the MAC kernels per frequency
     bool adj_only = false;       // every tile takes adjacent pairs only (integrating factor)
+    mutable int mac_variant = -1;  // group-MAC variant chosen by the autotuner (-1: not tuned yet)
     bool empty() const { return n_tgt == 0; }
 };
 
@@ -295,6 +301,14 @@ struct Ctx
     // per-sweep work buffers (sized on demand)
     DevBuf<char> d_src_spec, d_acc, d_w;
 
+    // coefficient tables of the block-Toeplitz group MAC, one per level
+    // difference: 729 rows of NC complex (working precision) each, and the
+    // TMA tensor map (CUtensorMap, 128 bytes) over all of them
+    std::map<int, int> combo_of_ld;
+    int combo_tables = 0, combo_cap = 0;
+    DevBuf<char> d_combo;
+    alignas(64) unsigned char combo_map[128] = {};
+
     std::map<std::tuple<int, int, int>, std::unique_ptr<FmmPlan>> plans;
     // integrating-factor kernels: e^{-2 alpha} I_n(2 alpha), n < ge_stride, one
     // table per alpha (LGF_GE::build_lt / compute_lgf)
@@ -303,6 +317,11 @@ struct Ctx
     DevBuf<double> d_ge;
     int ge_stride = 0;
     long long launches = 0;
+    // group-MAC autotuning: a variant pinned by the caller (-1: tune per
+    // plan) and one record per tuned plan: level, mask index, targets, ms of
+    // variants 0, 1, 2 (-1: not applicable), chosen variant
+    int mac_variant_forced = -1;
+    std::vector<std::array<double, 7>> mac_tuning;
     // device status word: bounded waits in kernels that run out set bits
     // (kStatusTimeout); read and cleared by check_status()
     DevBuf<int> d_status;
@@ -466,6 +485,9 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
 // sibling-group MAC with the fast block-Toeplitz product (group_mac.cu);
 // false when the plan's tiles need the direct kernel (adjacent pairs only)
 bool toeplitz_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
+// the coefficient table of level difference ld from the 343 spectrum slots
+// of its offsets (created once per context)
+int combo_table(Ctx& c, int ld, const std::vector<int>& slots);
 // waits for the context stream and throws IBLGF_ETIMEOUT if a kernel's
 // bounded wait ran out since the last check
 void check_status(Ctx& c);

@@ -616,29 +616,17 @@ struct Conv
         c.launches += 1;
     }
 
-#ifndef IBLGF_MAC_F32
-#define IBLGF_MAC_F32 64
-#define IBLGF_MAC_NT32 768
-#define IBLGF_MAC_MINB32 1
-#endif
-#ifndef IBLGF_MAC_F64
-#define IBLGF_MAC_F64 32
-#define IBLGF_MAC_NT64 512
-#define IBLGF_MAC_MINB64 1
-#endif
     static constexpr bool kF32 = std::is_same<R, float>::value;
-    static constexpr int GF = kF32 ? IBLGF_MAC_F32 : IBLGF_MAC_F64;
-    static constexpr int GNT = kF32 ? IBLGF_MAC_NT32 : IBLGF_MAC_NT64;
-    static constexpr int GMINB = kF32 ? IBLGF_MAC_MINB32 : IBLGF_MAC_MINB64;
 
-    // S holds p.n_src source spectra followed by one zero row
-    static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc)
+    // S holds p.n_src source spectra followed by one zero row. Two tile
+    // shapes per precision (frequencies per CTA GF, threads GNT), chosen per
+    // plan by the MAC autotuner: variant 0 = (64, 768) FP32 / (32, 512)
+    // FP64, variant 1 = (32, 512) / (32, 256)
+    template<int GF, int GNT>
+    static void group_mac_shape(Ctx& c, const FmmPlan& p, const void* S, void* acc)
     {
-        if (!p.n_tiles) return;
-        if (c.NC != (long long)NB * (2 * NB - 1) * (2 * NB - 1))
-            throw Error(IBLGF_EINTERNAL, "spectrum row length differs from the kernel's");
         const size_t smem = (size_t)343 * GF * sizeof(cx<R>) + (size_t)(kGroupTileCap * 216 + 344) * sizeof(int);
-        auto kfn = group_mac_kernel<R, GF, GNT, GMINB, NB>;
+        auto kfn = group_mac_kernel<R, GF, GNT, 1, NB>;
         IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid(p.n_tiles, (unsigned)((c.NC + GF - 1) / GF));
         kfn<<<grid, GNT, smem, c.stream>>>((const cx<R>*)c.d_spec.p, (const cx<R>*)S, p.n_src,
@@ -646,6 +634,23 @@ struct Conv
                                             p.tile_coarse.p, p.spec_u.p, p.grp_pm.p, p.grp_tgt.p,
                                             (cx<R>*)acc);
         c.launches += 1;
+    }
+
+    static void group_mac(Ctx& c, const FmmPlan& p, const void* S, void* acc, int variant)
+    {
+        if (!p.n_tiles) return;
+        if (c.NC != (long long)NB * (2 * NB - 1) * (2 * NB - 1))
+            throw Error(IBLGF_EINTERNAL, "spectrum row length differs from the kernel's");
+        if (variant == 1)
+        {
+            if constexpr (kF32) group_mac_shape<32, 512>(c, p, S, acc);
+            else group_mac_shape<32, 256>(c, p, S, acc);
+        }
+        else
+        {
+            if constexpr (kF32) group_mac_shape<64, 768>(c, p, S, acc);
+            else group_mac_shape<32, 512>(c, p, S, acc);
+        }
     }
 
     static void inverse(Ctx& c, const void* acc, const int* d_tgt_oct, int n_tgt, double scale, double* target)
@@ -751,14 +756,68 @@ void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, i
     IBLGF_CUDA(cudaGetLastError());
 }
 
+// one run of the sibling-group MAC in the given variant: 0, 1 the direct
+// kernel in its two tile shapes, 2 the block-Toeplitz kernel
+void group_mac_variant(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc, int variant)
+{
+    if (variant == 2 && toeplitz_mac(c, p, src_spec, acc)) return;
+    dispatch(c, [&](auto cv) {
+        using CV = decltype(cv);
+        CV::group_mac(c, p, src_spec, acc, variant);
+    });
+}
+
+// The MAC autotuner: on a plan's first sweep (outside stream capture) every
+// applicable group-MAC variant runs twice on the sweep's real data, the
+// second run timed with CUDA events on the context stream; the fastest one
+// is kept for the plan (and run last, so that the accumulators hold its
+// result). iblgf_mac_variant() can pin a variant instead.
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
 {
     dispatch(c, [&](auto cv) {
         using CV = decltype(cv);
         // targets outside sibling groups: general pair-list MAC
         CV::mac(c, c.d_spec.p, src_spec, p.pair_ptr.p, p.pair_src.p, p.pair_spec.p, p.n_csr_tgt, acc);
-        if (!toeplitz_mac(c, p, src_spec, acc)) CV::group_mac(c, p, src_spec, acc);
     });
+    if (p.n_tiles)
+    {
+        const bool toep_ok = !p.adj_only && p.tile_combo.p && c.cfg.precision == IBLGF_FP32;
+        int v = c.mac_variant_forced;
+        if (v == 2 && !toep_ok) v = 0;
+        if (v < 0) v = p.mac_variant;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        IBLGF_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+        if (v < 0 && cs != cudaStreamCaptureStatusNone) v = 0;
+        if (v < 0)
+        {
+            const int nv = toep_ok ? 3 : 2;
+            double ms[3] = {-1.0, -1.0, -1.0};
+            cudaEvent_t e0, e1;
+            IBLGF_CUDA(cudaEventCreate(&e0));
+            IBLGF_CUDA(cudaEventCreate(&e1));
+            for (int k = 0; k < nv; ++k)
+            {
+                group_mac_variant(c, p, src_spec, acc, k);
+                IBLGF_CUDA(cudaEventRecord(e0, c.stream));
+                group_mac_variant(c, p, src_spec, acc, k);
+                IBLGF_CUDA(cudaEventRecord(e1, c.stream));
+                IBLGF_CUDA(cudaEventSynchronize(e1));
+                float t = 0.0f;
+                IBLGF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                ms[k] = t;
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            int best = 0;
+            for (int k = 1; k < nv; ++k)
+                if (ms[k] < ms[best]) best = k;
+            p.mac_variant = best;
+            c.mac_tuning.push_back({(double)p.level, (double)p.mask_idx, (double)p.n_tgt, ms[0], ms[1], ms[2],
+                                    (double)best});
+            v = best;
+        }
+        group_mac_variant(c, p, src_spec, acc, v);
+    }
     IBLGF_CUDA(cudaGetLastError());
 }
 

@@ -806,6 +806,11 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
         return slot;
     };
     for (auto& k : h.all_keys) slot_of(k);
+    // the block-Toeplitz MAC reads all 343 offsets of a table (absent
+    // sources multiply zero rows): every offset gets its spectrum
+    const bool toeplitz = !h.ttab.empty() && h.ge < 0 && c.cfg.precision == IBLGF_FP32;
+    if (toeplitz)
+        for (auto& k : h.tab_keys) slot_of(k);
     std::vector<int> pspec(h.pkey.size());
     for (size_t i = 0; i < h.pkey.size(); ++i) pspec[i] = slot_of(h.pkey[i]);
     std::vector<int> spec_u(h.tab_keys.size());
@@ -823,7 +828,10 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
         // candidate source rows per tile: group g's candidate kk reads row
         // tsrc[tsptr[t] + gsrc[g][kk]], absent ones (and unused group slots)
         // the zero row n_src
-        std::vector<int> jr((size_t)p.n_tiles * kGroupTileCap * 216, p.n_src);
+        // padded so that the block-Toeplitz MAC's copy of a tile's last part
+        // (3 parts of kToeplitzPart rows) stays inside the buffer
+        const size_t pad = (size_t)(3 * kToeplitzPart - kGroupTileCap) * 216;
+        std::vector<int> jr((size_t)p.n_tiles * kGroupTileCap * 216 + pad, p.n_src);
         for (int t = 0; t < p.n_tiles; ++t)
             for (int g = h.tgptr[t]; g < h.tgptr[t + 1]; ++g)
                 for (int kk = 0; kk < 216; ++kk)
@@ -844,18 +852,13 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
     for (int m : h.tcoarse) p.adj_only = p.adj_only && m == 2;
     // MAC work per frequency: 8 flops per complex multiply-add of the direct
     // kernels; the block-Toeplitz kernel per (group, present parent) 27
-    // complex multiply-adds and 19 complex additions, per group the 38
-    // additions of the final combination, and per CTA (16 groups) the 3375
-    // real-times-complex terms of its coefficient rows
+    // complex multiply-adds and 19 complex additions, and per group the 38
+    // additions of the final combination
     p.mac_flops = (long long)h.psrc.size() * 8;
-    if (p.adj_only || h.ttab.empty())
+    if (p.adj_only || !toeplitz)
         p.mac_flops += (h.n_exec - (long long)h.psrc.size()) * 8;
     else
-    {
         for (unsigned pm : h.gpm) p.mac_flops += (long long)__builtin_popcount(pm) * (27 * 8 + 19 * 2) + 38 * 2;
-        for (size_t t = 0; t + 1 < h.tgptr.size(); ++t)
-            p.mac_flops += (long long)((h.tgptr[t + 1] - h.tgptr[t] + 15) / 16) * 3375 * 4;
-    }
     p.n_tgt = (int)h.tgt_list.size();
     p.n_pairs = h.n_pairs;
     p.n_spec_unique = h.n_spec_unique;
@@ -881,6 +884,23 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
         }
         launch_spectra(c, new_slots);
         c.spec_used = need;
+    }
+    if (toeplitz && !p.adj_only)
+    {
+        std::vector<int> tcombo(h.ttab.size());
+        std::vector<int> of_tab(h.tab_keys.size() / 343, -1);
+        for (size_t t = 0; t < of_tab.size(); ++t)
+        {
+            const std::vector<int> slots(spec_u.begin() + 343 * t, spec_u.begin() + 343 * (t + 1));
+            of_tab[t] = combo_table(c, h.tab_keys[343 * t][0], slots);
+        }
+        for (size_t i = 0; i < h.ttab.size(); ++i) tcombo[i] = of_tab[h.ttab[i]];
+        p.tile_combo.upload(tcombo, c.stream);
+        std::vector<int> parts;
+        for (size_t t = 0; t + 1 < h.tgptr.size(); ++t)
+            for (int q = 0; q * kToeplitzPart < h.tgptr[t + 1] - h.tgptr[t]; ++q) parts.push_back((int)(t << 2) | q);
+        p.n_parts = (int)parts.size();
+        p.tile_parts.upload(parts, c.stream);
     }
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     return plan;

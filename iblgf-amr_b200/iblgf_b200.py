@@ -43,7 +43,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak",
+    "iblgf_fma_peak", "iblgf_mac_variant", "iblgf_mac_tuning",
 ]
 
 _lib = None
@@ -101,6 +101,8 @@ def lib():
     L.iblgf_ns_options.argtypes = [vp, vp, cd, ci]
     L.iblgf_ib_force.argtypes = [vp, ci, vp, vp]
     L.iblgf_ib_stage_status.argtypes = [vp, ci, vp, vp]
+    L.iblgf_mac_variant.argtypes = [vp, ci]
+    L.iblgf_mac_tuning.argtypes = [vp, vp, ci, vp]
     L.iblgf_ib_warmstart.argtypes = [vp, ci, ci, ci, cd, ctypes.c_uint]
     L.iblgf_ib_warmstart_info.argtypes = [vp, vp]
     L.iblgf_ws_check.argtypes = [vp, ci, ci, vp, vp, vp, vp, vp, vp]
@@ -550,6 +552,21 @@ class Solver:
             self._check(lib().iblgf_ib_force(self.h, st, None, ctypes.byref(it)))
             out.append(it.value)
         return out
+
+    def mac_variant(self, variant):
+        """Pin the sibling-group MAC variant (0, 1 direct tile shapes, 2
+        block-Toeplitz; -1 autotunes per plan)."""
+        self._check(lib().iblgf_mac_variant(self.h, int(variant)))
+
+    def mac_tuning(self):
+        """Autotuner records: dicts with level, mask, targets, ms per variant
+        (None if not applicable) and the chosen variant."""
+        n = ctypes.c_int()
+        self._check(lib().iblgf_mac_tuning(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros((max(n.value, 1), 7))
+        self._check(lib().iblgf_mac_tuning(self.h, _p(out), n.value, ctypes.byref(n)))
+        return [{"level": int(r[0]), "mask": int(r[1]), "targets": int(r[2]),
+                 "ms": [None if v < 0 else float(v) for v in r[3:6]], "choice": int(r[6])} for r in out[:n.value]]
 
     def ib_converged(self):
         """Whether each of stages 1..3 of the last step converged before

@@ -335,6 +335,18 @@ int iblgf_stats(iblgf_ctx* ctx, long long* out8);
  * kernel forms the 64 products of a parent with 27 complex multiplies).
  * IBLGF_EINVAL for n outside [1, 10]. */
 int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
+
+/* Sibling-group MAC autotuning (no reference counterpart). On the first
+ * sweep of each plan the library times every applicable variant of the
+ * group MAC on that sweep's data (0: direct kernel, 64 frequencies x 768
+ * threads in FP32 / 32 x 512 in FP64; 1: direct kernel, 32 x 512 / 32 x 256;
+ * 2: block-Toeplitz kernel with TMA-staged coefficients, FP32 only) and keeps
+ * the fastest. iblgf_mac_variant pins a variant for later plans and sweeps
+ * (-1: autotune). iblgf_mac_tuning returns one row of 7 doubles per tuned
+ * plan: level, mask index, targets, ms of variants 0, 1, 2 (-1: not
+ * applicable), chosen variant; n_rows receives the number of rows. */
+int iblgf_mac_variant(iblgf_ctx* ctx, int variant);
+int iblgf_mac_tuning(iblgf_ctx* ctx, double* out, int max_rows, int* n_rows);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the
  * roofline denominator of the CUDA-core kernels. */

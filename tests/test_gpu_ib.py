@@ -49,10 +49,12 @@ def test_ib_solve_needs_points():
 
 @pytest.mark.parametrize("precision,tol,ptol", [(B.FP64, 1e-9, 1e-9), (B.FP32, 1e-4, 5e-4)])
 def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
-    """Two IF-HERK steps past the sphere in a uniform stream (frame velocity
+    """Three IF-HERK steps past the sphere in a uniform stream (frame velocity
     (-1, 0, 0): the body at rest, the fluid moving at +1): velocity, pressure
-    and the three stage forces of the last step against the oracle. In FP32
-    the pressure (d_i / (a33 dt), a factor 400 here) carries the FP32
+    and the three stage forces of the last step against the oracle. The first
+    step runs direct, the second is captured as a CUDA graph (its force CG a
+    conditional while-node) and the third replays that graph. In FP32 the
+    pressure (d_i / (a33 dt), a factor 400 here) carries the FP32
     perturbation of the IB CG iterates: 5e-4 for it, 1e-4 for velocity."""
     case = S.SphereIB("small")
     o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
@@ -62,17 +64,38 @@ def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
     X = O.sphere_points(case.dx_base, o.depth - 1 - o.base_level, case.ibph)
     u0 = case.velocity(o)
     dt, fv = 0.01, (-1.0, 0.0, 0.0)
-    ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, 0.0, 2)
+    ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, 0.0, 3)
     g.ib_set_points(X, case.Re)
     g.ns_options(fv)
     uf = [g.field(u0[k]) for k in range(3)]
     pf = g.field()
-    g.ns_step(uf, pf, dt, case.Re, 0.0, 2)
+    T = 0.0
+    for _ in range(3):
+        T = g.ns_step(uf, pf, dt, case.Re, T, 1)
     for k in range(3):
         assert rel_linf(g.download(uf[k]), ur[k]) < tol, (k, rel_linf(g.download(uf[k]), ur[k]))
     assert rel_linf(g.download(pf), pr) < ptol, rel_linf(g.download(pf), pr)
     for st in range(3):
         assert rel_linf(g.ib_force(st + 1), fr[st]) < tol * 10, (st, rel_linf(g.ib_force(st + 1), fr[st]))
+    assert g.ib_converged() == [True, True, True]
+
+
+def test_ib_solve_reports_not_converged():
+    """A solve that reaches max_iter without meeting the threshold returns
+    IBLGF_ENOTCONVERGED with the force and iteration count written (the
+    reference's CG_solve stops there silently, linsys.hpp:202-229)."""
+    case = S.SphereIB("small")
+    g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    X = O.sphere_points(case.dx_base, g.depth - 1 - g.base_level, case.ibph)
+    g.ib_set_points(X, case.Re)
+    u = case.velocity(g)
+    uf = [g.field(u[k]) for k in range(3)]
+    with pytest.raises(B.IblgfNotConverged) as e:
+        g.ib_solve(uf, 0.0, threshold=1e-15, max_iter=2)
+    assert e.value.iterations == 2 and np.abs(e.value.force).max() > 0
+    f, it = g.ib_solve(uf, 0.0, threshold=1e-3, max_iter=40)
+    assert it < 40
 
 
 def test_ns_step_with_ib_velocity_refresh_matches_oracle():

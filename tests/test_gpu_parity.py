@@ -118,11 +118,16 @@ def test_fmm_impulse(precision, tol):
         assert np.abs(out[blk, 1:-1, 1:-1, 1:-1] - ex).max() < 5e-8 + tol
 
 
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2])
 @pytest.mark.parametrize("nlas", [0, 1])
 @pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
-def test_fmm_apply_random_amr(nlas, precision, tol):
+def test_fmm_apply_random_amr(nlas, precision, tol, variant):
+    """Every sibling-group MAC variant (0, 1: direct kernel tile shapes; 2:
+    block-Toeplitz, FP32 only, the FP64 path runs variant 0 instead; -1: the
+    autotuner's choice) against the oracle."""
     case = S.GaussianPoisson("amr_small")
     o, g = pair(case, precision)
+    g.mac_variant(variant)
     rng = np.random.default_rng(7)
     src = rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb))
     tgt0 = rng.standard_normal((o.n, o.Nb, o.Nb, o.Nb))
@@ -133,6 +138,10 @@ def test_fmm_apply_random_amr(nlas, precision, tol):
         g.fmm_apply(fs, ft, level, nlas, 0.75, B.AMR2AMR)
         out = g.download(ft)
         assert rel_linf(out - tgt0, ref - tgt0) < tol, (level, rel_linf(out - tgt0, ref - tgt0))
+    if variant < 0:
+        rec = g.mac_tuning()
+        assert rec and all(r["choice"] in (0, 1, 2) for r in rec)
+        assert all((r["ms"][2] is None) == (precision == B.FP64) for r in rec)
 
 
 @pytest.mark.parametrize("n_levels", [0, 1])

@@ -76,3 +76,19 @@ def test_async_leaf_download_pipeline():
     g.synchronize()
     for r, o in zip(ref, outs):
         np.testing.assert_array_equal(o.numpy(), r)
+
+
+def test_async_leaf_download_checks_its_buffer():
+    """The asynchronous download takes only a C-contiguous float64 host
+    buffer of the leaf shape (the copy writes n_leaves e^3 doubles)."""
+    case = S.GaussianPoisson("amr_small")
+    g = solver(case, B.FP64)
+    e = g.block_extent
+    f = g.field()
+    for bad in (np.zeros((g.n_leaves, e, e, e), np.float32), np.zeros((g.n_leaves, e, e, e + 1)),
+                np.zeros((g.n_leaves, e, e, 2 * e))[:, :, :, ::2]):
+        with pytest.raises(B.IblgfError):
+            g.download_leaves_async(f, bad)
+    out = np.zeros((g.n_leaves, e, e, e))
+    g.download_leaves_async(f, out)
+    g.synchronize()
