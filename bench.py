@@ -442,27 +442,33 @@ def ib_bench(B, stream, device, steps, warmup):
     case = S.SphereIB("c5")
     out = {"workload": "sphere D=1, Re=300, uniform stream, dx_finest=D/40, 16^3 blocks, 3 mesh levels, "
                        "2009 IB points, CG threshold 1e-3, max 40; warm start: previous force per stage "
-                       "(reference) and the learned 1-D conv net (fp32_learned)"}
+                       "(reference), its linear extrapolation (fp32_extrapolated) and the learned 1-D conv net "
+                       "correcting the extrapolation (fp32_learned, trained on 8 steps x 3 stages)"}
     dt = 0.35 * case.dx_base / 4 / 1.0
     res = {}
-    for name, prec, learned in (("fp32", B.FP32, False), ("fp64", B.FP64, False), ("fp32_learned", B.FP32, True)):
+    train_steps = 8
+    for name, prec, mode in (("fp32", B.FP32, 0), ("fp64", B.FP64, 0), ("fp32_extrapolated", B.FP32, 2),
+                             ("fp32_learned", B.FP32, 1)):
+        learned = mode == 1
         g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                      n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=device,
                      stream=stream.cuda_stream)
         X = sphere_points(case.dx_base, g.depth - 1 - g.base_level, case.ibph)
         g.ib_set_points(X, case.Re)
         g.ns_options((-1.0, 0.0, 0.0))
-        if learned:
-            # the first step and `warmup` more run with the previous force and
-            # record samples; the network is trained before the timed steps
-            g.ib_warmstart(1, train_steps=max(warmup - 1, 1), epochs=1000, lr=2e-3, seed=7)
+        if mode == 1:
+            # steps 3 .. train_steps + 2 record samples (the extrapolation
+            # needs two forces); the network is trained before the timed steps
+            g.ib_warmstart(1, train_steps=train_steps, epochs=1000, lr=2e-3, seed=7)
+        elif mode == 2:
+            g.ib_warmstart(2)
         u0 = case.velocity(g, U=(0.0, 0.0, 0.0))
         uf = [g.field(u0[k]) for k in range(3)]
         pf = g.field()
         T = 0.0
-        # the learned leg trains at the end of the warm-up; one more untimed
+        # the learned leg trains at the end of its warm-up; one more untimed
         # step runs the first prediction, which pays a one-time set-up cost
-        for _ in range(warmup + (1 if learned else 0)):
+        for _ in range(max(warmup, train_steps + 2) + 1 if learned else warmup):
             T = g.ns_step(uf, pf, dt, case.Re, T, 1)
         torch.cuda.synchronize()
         its = []
@@ -477,8 +483,9 @@ def ib_bench(B, stream, device, steps, warmup):
             its.append(sum(g.ib_iterations()))
         out["ms_per_step_" + name] = ms / steps
         out["cg_iterations_per_step_" + name] = float(np.mean(its))
-        if learned:
-            out["warm_start_training"] = g.ib_warmstart_info()
+        if mode:
+            if learned:
+                out["warm_start_training"] = g.ib_warmstart_info()
             g.close()
             continue
         out["octants"], out["leaves"], out["ib_points"] = int(g.n), int(np.count_nonzero(g.leaf)), len(X)

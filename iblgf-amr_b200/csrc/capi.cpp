@@ -353,6 +353,86 @@ int iblgf_lgf_get(iblgf_ctx* x, const int* coords, size_t n, double* host_out)
     });
 }
 
+int iblgf_lgf_ge_get(iblgf_ctx* x, double alpha, const int* coords, size_t n, double* host_out)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!n) return;
+        if (!coords || !host_out) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        const int ge = iblgf_b200::ge_table(c, alpha);
+        iblgf_b200::DevBuf<int> dc;
+        iblgf_b200::DevBuf<double> dout;
+        dc.alloc(3 * n);
+        dout.alloc(n);
+        IBLGF_CUDA(cudaMemcpyAsync(dc.p, coords, 3 * n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        iblgf_b200::launch_lgf_ge_eval(c, ge, dc.p, n, dout.p);
+        IBLGF_CUDA(cudaMemcpyAsync(host_out, dout.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_fmm_apply_kernel(iblgf_ctx* x, int source, int target, int level, int nlas, double scale, int fmm_type,
+                           int kernel, double alpha)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, source);
+        need_field(c, target);
+        if (kernel == IBLGF_KERNEL_GL)
+            iblgf_b200::fmm_apply(c, source, target, level, nlas != 0, scale, fmm_type);
+        else if (kernel == IBLGF_KERNEL_GE)
+        {
+            if (fmm_type != IBLGF_AMR2AMR && fmm_type != IBLGF_IB2xIB)
+                throw iblgf_b200::Error(IBLGF_EINVAL, "the LGF_GE kernel sweeps with AMR2AMR or IB2xIB masks");
+            const int ge = iblgf_b200::ge_table(c, alpha);
+            iblgf_b200::fmm_apply(c, source, target, level, nlas != 0, scale, fmm_type, ge);
+        }
+        else
+            throw iblgf_b200::Error(IBLGF_EINVAL, "kernel must be IBLGF_KERNEL_GL or IBLGF_KERNEL_GE");
+    });
+}
+
+int iblgf_op_apply_octants(iblgf_ctx* x, int op, const int* in, int n_in, const int* out, int n_out,
+                           const int* octants, int n, double scale)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!in || !out || (n > 0 && !octants)) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        for (int i = 0; i < n_in; ++i) need_field(c, in[i]);
+        for (int i = 0; i < n_out; ++i) need_field(c, out[i]);
+        iblgf_b200::apply_op_octants(c, op, in, n_in, out, n_out, octants, n, scale);
+    });
+}
+
+int iblgf_field_upload_octants(iblgf_ctx* x, int field, const int* octants, int n, const double* host)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, field);
+        if (n > 0 && (!octants || !host)) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        const size_t B = c.block_elems();
+        for (int i = 0; i < n; ++i)
+        {
+            if (octants[i] < 0 || octants[i] >= c.n_oct) throw iblgf_b200::Error(IBLGF_EINVAL, "octant out of range");
+            IBLGF_CUDA(cudaMemcpyAsync(c.field(field) + (size_t)octants[i] * B, host + (size_t)i * B,
+                                       B * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        }
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int iblgf_field_download_octants(iblgf_ctx* x, int field, const int* octants, int n, double* host)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, field);
+        if (n > 0 && (!octants || !host)) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        const size_t B = c.block_elems();
+        for (int i = 0; i < n; ++i)
+        {
+            if (octants[i] < 0 || octants[i] >= c.n_oct) throw iblgf_b200::Error(IBLGF_EINVAL, "octant out of range");
+            IBLGF_CUDA(cudaMemcpyAsync(host + (size_t)i * B, c.field(field) + (size_t)octants[i] * B,
+                                       B * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        }
+        iblgf_b200::check_status(c);  // synchronises the stream
+    });
+}
+
 int iblgf_conv_block(iblgf_ctx* x, const double* src, const double* kernel, double* out, double scale)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
@@ -519,6 +599,20 @@ int iblgf_ib_solve(iblgf_ctx* x, const int* u_fields, double alpha, double thres
             throw iblgf_b200::Error(IBLGF_ENOTCONVERGED, "IB force CG reached max_iter without converging "
                                                          "(force and iteration count written)");
     });
+}
+
+int iblgf_domain_partition(iblgf_ctx* x, int n_ranks, int* owner)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!owner) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        const std::vector<int> w = iblgf_b200::domain_partition(c, n_ranks);
+        std::copy(w.begin(), w.end(), owner);
+    });
+}
+
+int iblgf_domain_set_owner(iblgf_ctx* x, const int* owner, int rank, iblgf_exchange_fn exchange, void* user)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) { iblgf_b200::domain_set_owner(c, owner, rank, exchange, user); });
 }
 
 int iblgf_mac_variant(iblgf_ctx* x, int variant)

@@ -333,6 +333,16 @@ struct Ctx
     // tasks, group-MAC targets, MAC products executed
     long long stats[kNumStats] = {};
 
+    // sharded sweeps (one rank of several): owner rank per canonical octant
+    // (empty: not sharded); a sweep computes the targets this rank owns (and
+    // the coarser targets their values are interpolated from), then the
+    // exchange callback sums the sweep's level targets over the ranks
+    std::vector<int> owner;
+    int rank = 0;
+    iblgf_exchange_fn exchange_fn = nullptr;
+    void* exchange_user = nullptr;
+    PoolBuf exchange_buf;
+
     // batch of independent problems (iblgf_batch_*): each problem's octree,
     // lists and masks live in a topology-only sub-context; fields, spectra and
     // work buffers live here, the problems' octants back to back
@@ -413,6 +423,10 @@ void launch_cg_direction(Ctx& c, double* p, const double* r, int n, const double
 void launch_cg_advance(Ctx& c, double* sc, int* ctl, double threshold, int max_iter, unsigned long long cond,
                        bool set_cond);
 void launch_cg_record(Ctx& c, const int* ctl, int* rec);
+// CG warm start (ib.cu): f0 = f_prev, or 2 f_prev - f_prev2 once count >= 2
+// when extrapolating; record shifts the stage's force history
+void launch_ws_base(Ctx& c, double* f0, const double* fp, const double* fp2, int n, const int* count, bool extrapolate);
+void launch_ws_record(Ctx& c, double* fp2, double* fp, const double* f, int n, int* count);
 // learned warm start network (warmstart.cu)
 constexpr int kWsChannels = 64, kWsInputs = 9;
 void ws_offsets(int* off);  // 7 offsets: W1 b1 W2 b2 W3 b3 end
@@ -471,12 +485,15 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
                   const int* interp_mesh, int* base_mesh_update);
 void block_norms(Ctx& c, const int* fields, int n_comp, double* host_max, double* host_rms);
 OpLists& op_lists(Ctx& c);
+void apply_op_octants(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, const int* octants, int n,
+                      double scale);
 void poisson_apply_lgf(Ctx& c, int src, int tgt, int fmm_type);
 int mask_idx_gen(int type, int refinement_level, int nlas);
 
 // -------------------------------------------------------------- kernels (.cu)
 void launch_lgf_table(Ctx& c);
 void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
+void launch_lgf_ge_eval(Ctx& c, int ge, const int* d_coords, size_t n, double* d_out);
 void launch_build_lists(Ctx& c, const u64* d_sorted_keys, const int* d_sorted_idx, int n_sorted,
                         const u64* d_keys, int n, int* d_nbr, int* d_infl, int* d_ninfl);
 void launch_spectra(Ctx& c, const std::vector<std::array<int, 5>>& new_slots);
@@ -497,6 +514,11 @@ void launch_inverse_add(Ctx& c, const FmmPlan& p, const void* acc, double* fmm_t
 bool inverse_pfa(Ctx& c, const void* acc, const int* d_tgt_oct, int n, double scale, double* target,
                  bool fp32_passes);
 void init_pfa_constants(int device);
+// sharding (solver.cpp): the reference server's load-balanced partition and
+// this context's share of it
+std::vector<int> domain_partition(const Ctx& c, int n);
+void domain_set_owner(Ctx& c, const int* owner, int rank, iblgf_exchange_fn fn, void* user);
+// whether the prime-factor inverse runs its z and y passes in FP32
 bool inverse_fp32_passes(const Ctx& c);
 void launch_zero_blocks(Ctx& c, double* f, const int* list, int n);
 void launch_fill_zero(Ctx& c, double* p, size_t n);
@@ -505,6 +527,9 @@ void launch_block_norms(Ctx& c, const double* const* comps, int n_comp, double* 
 // leaf-interior transfers: staging [leaf][e^3] (x fastest) <-> field blocks
 void launch_leaves_scatter(Ctx& c, const double* stage, double* field, const int* list, int n);
 void launch_leaves_gather(Ctx& c, const double* field, double* stage, const int* list, int n);
+// whole blocks of the listed octants <-> a contiguous buffer [n][Nb^3]
+void launch_blocks_gather(Ctx& c, const double* field, double* buf, const int* list, int n);
+void launch_blocks_scatter(Ctx& c, const double* buf, double* field, const int* list, int n);
 void field_upload_leaves(Ctx& c, int f, const double* host, size_t count);
 void field_download_leaves(Ctx& c, int f, double* host, size_t count);
 void field_download_leaves_async(Ctx& c, int f, double* host, size_t count);

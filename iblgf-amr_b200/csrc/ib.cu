@@ -282,4 +282,50 @@ void launch_cg_record(Ctx& c, const int* ctl, int* rec)
     IBLGF_CUDA(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------
+// Warm start of a stage's force CG: f0 = the stage's previous force, or its
+// linear extrapolation 2 f_prev - f_prev2 once two forces are recorded
+// (count >= 2); record: f_prev2 = f_prev, f_prev = f, count + 1. The count
+// lives on the device so that a captured time step extrapolates exactly when
+// a direct one would.
+namespace
+{
+__global__ void ws_base_kernel(double* __restrict__ f0, const double* __restrict__ fp, const double* __restrict__ fp2,
+                               int n, const int* __restrict__ count, int extrapolate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f0[i] = (extrapolate && *count >= 2) ? 2.0 * fp[i] - fp2[i] : fp[i];
+}
+
+__global__ void ws_record_kernel(double* __restrict__ fp2, double* __restrict__ fp, const double* __restrict__ f, int n,
+                                 int* __restrict__ count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        fp2[i] = fp[i];
+        fp[i] = f[i];
+    }
+    if (i == 0) *count += 1;
+}
+}  // namespace
+
+void launch_ws_base(Ctx& c, double* f0, const double* fp, const double* fp2, int n, const int* count, bool extrapolate)
+{
+    if (!n) return;
+    ws_base_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(f0, fp, fp2, n, count, extrapolate ? 1 : 0);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_ws_record(Ctx& c, double* fp2, double* fp, const double* f, int n, int* count)
+{
+    if (!n) return;
+    ws_record_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(fp2, fp, f, n, count);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 }  // namespace iblgf_b200

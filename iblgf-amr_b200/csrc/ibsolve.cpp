@@ -44,17 +44,23 @@ double yang3(double x)
 // steps, then a network trained on them predicts f0 - f_prev per stage
 struct WarmStart
 {
-    int mode = 0;  // 0: previous step's force of the stage (the reference), 1: learned
+    // 0: previous step's force of the stage (the reference), 1: learned
+    // correction on top of the linear extrapolation, 2: linear extrapolation
+    // 2 f_prev - f_prev2 (both fall back to f_prev until two forces exist)
+    int mode = 0;
     int train_steps = 0, epochs = 0, steps_seen = 0, n_params = 0;
     float lr = 1e-3f;
     unsigned seed = 1;
     bool trained = false;
-    float loss_first = 0.0f, loss_last = 0.0f, sb = 1.0f, sf = 1.0f;
-    std::vector<std::vector<double>> s_duc, s_fprev, s_dfp, s_f;  // samples
-    std::vector<double> f_prev2[4];                          // force two steps back per stage
-    float sd = 1.0f, st = 1.0f;  // input / target scales
-    std::vector<double> uc_prev[4];                          // right-hand side of the previous step per stage
-    std::vector<int> order;                                  // network position -> IB point (Morton order)
+    float loss_first = 0.0f, loss_last = 0.0f;
+    // samples (stage, rhs change, previous force, its last change, target
+    // f - f_base) and per-stage input / target scales
+    std::vector<int> s_stage;
+    std::vector<std::vector<double>> s_duc, s_fprev, s_dfp, s_t;
+    float sb[4] = {1, 1, 1, 1}, sf[4] = {1, 1, 1, 1}, sd[4] = {1, 1, 1, 1}, st[4] = {1, 1, 1, 1};
+    std::vector<double> uc_prev[4];  // right-hand side of the previous step per stage
+    int count_host[4] = {0, 0, 0, 0};  // forces recorded per stage (host mirror of fcount)
+    std::vector<int> order;  // network position -> IB point (Morton order)
     DevBuf<float> params, grads, m, v, x, t, h1, h2, y, dy, dh1, dh2, partial;
 };
 
@@ -86,6 +92,8 @@ struct IbState
     DevBuf<int> cg_ctl;
     DevBuf<int> cg_rec;                 // per stage 0..3: [iterations, not converged] of its last solve
     DevBuf<double> fprev[4];            // IB::force_prev per IF-HERK stage (CG warm start), on the device
+    DevBuf<double> fprev2[4];           // the stage's force one step further back
+    DevBuf<int> fcount;                 // forces recorded per stage (extrapolation needs two)
     int* done_host = nullptr;           // pinned: the done flag, read once per iteration of a direct solve
     cudaStream_t body_stream = nullptr; // captures the loop body of a solve inside a graph
     WarmStart ws;
@@ -275,11 +283,13 @@ void ib_set_points(Ctx& c, int n, const double* X, double Re)
         s->cell_aux2 = field_create(c);
     }
     for (DevBuf<double>* b : {&s->cg_f, &s->cg_r, &s->cg_p, &s->cg_Ap, &s->cg_uc}) b->alloc(3 * (size_t)n);
-    for (auto& fp : s->fprev)
-    {
-        fp.alloc(3 * (size_t)n);
-        launch_fill_zero(c, fp.p, fp.n);
-    }
+    for (int k = 0; k < 4; ++k)
+        for (DevBuf<double>* fp : {&s->fprev[k], &s->fprev2[k]})
+        {
+            fp->alloc(3 * (size_t)n);
+            launch_fill_zero(c, fp->p, fp->n);
+        }
+    s->fcount.upload(std::vector<int>(4, 0), c.stream);
     s->cg_sc.upload(std::vector<double>(4, 0.0), c.stream);
     s->cg_ctl.upload(std::vector<int>(3, 0), c.stream);
     s->cg_rec.upload(std::vector<int>(8, 0), c.stream);
@@ -393,21 +403,25 @@ void ws_init(WarmStart& w, Ctx& c)
 
 // x [S][9][N] = ((uc - uc_prev) / sb, f_prev / sf, (f_prev - f_prev2) / sd),
 // points in network order
-std::vector<float> ws_inputs(const WarmStart& w, const std::vector<const std::vector<double>*>& duc,
+std::vector<float> ws_inputs(const WarmStart& w, const std::vector<int>& stage,
+                             const std::vector<const std::vector<double>*>& duc,
                              const std::vector<const std::vector<double>*>& fp,
                              const std::vector<const std::vector<double>*>& dfp, int N)
 {
     const int I = kWsInputs;
     std::vector<float> x(duc.size() * I * (size_t)N);
     for (size_t s_ = 0; s_ < duc.size(); ++s_)
+    {
+        const int st = stage[s_];
         for (int ch = 0; ch < 3; ++ch)
             for (int q = 0; q < N; ++q)
             {
                 const int i = w.order[q];
-                x[(s_ * I + ch) * N + q] = (float)((*duc[s_])[3 * i + ch] / w.sb);
-                x[(s_ * I + 3 + ch) * N + q] = (float)((*fp[s_])[3 * i + ch] / w.sf);
-                x[(s_ * I + 6 + ch) * N + q] = (float)((*dfp[s_])[3 * i + ch] / w.sd);
+                x[(s_ * I + ch) * N + q] = (float)((*duc[s_])[3 * i + ch] / w.sb[st]);
+                x[(s_ * I + 3 + ch) * N + q] = (float)((*fp[s_])[3 * i + ch] / w.sf[st]);
+                x[(s_ * I + 6 + ch) * N + q] = (float)((*dfp[s_])[3 * i + ch] / w.sd[st]);
             }
+    }
     return x;
 }
 
@@ -415,29 +429,30 @@ void ws_train(Ctx& c, WarmStart& w, int N)
 {
     const int S = (int)w.s_duc.size();
     if (!S) return;
-    double sb = 0, sf = 0, sd = 0;
-    for (int s_ = 0; s_ < S; ++s_)
-        for (int i = 0; i < 3 * N; ++i)
+    // per-stage rms scales of the inputs and of the target
+    for (int st = 1; st <= 3; ++st)
+    {
+        double sb = 0, sf = 0, sd = 0, stt = 0;
+        long long cnt = 0;
+        for (int s_ = 0; s_ < S; ++s_)
         {
-            sb += w.s_duc[s_][i] * w.s_duc[s_][i];
-            sf += w.s_f[s_][i] * w.s_f[s_][i];
-            sd += w.s_dfp[s_][i] * w.s_dfp[s_][i];
+            if (w.s_stage[s_] != st) continue;
+            ++cnt;
+            for (int i = 0; i < 3 * N; ++i)
+            {
+                sb += w.s_duc[s_][i] * w.s_duc[s_][i];
+                sf += w.s_fprev[s_][i] * w.s_fprev[s_][i];
+                sd += w.s_dfp[s_][i] * w.s_dfp[s_][i];
+                stt += w.s_t[s_][i] * w.s_t[s_][i];
+            }
         }
-    w.sd = (float)std::sqrt(sd / (S * 3.0 * N));
-    if (!(w.sd > 0)) w.sd = 1.0f;
-    double st = 0;
-    for (int s_ = 0; s_ < S; ++s_)
-        for (int i = 0; i < 3 * N; ++i)
-        {
-            const double d = w.s_f[s_][i] - w.s_fprev[s_][i];
-            st += d * d;
-        }
-    w.st = (float)std::sqrt(st / (S * 3.0 * N));
-    if (!(w.st > 0)) w.st = 1.0f;
-    w.sb = (float)std::sqrt(sb / (S * 3.0 * N));
-    w.sf = (float)std::sqrt(sf / (S * 3.0 * N));
-    if (!(w.sb > 0)) w.sb = 1.0f;
-    if (!(w.sf > 0)) w.sf = 1.0f;
+        const double m = cnt ? cnt * 3.0 * N : 1.0;
+        auto scale = [&](double q) { return q > 0 ? (float)std::sqrt(q / m) : 1.0f; };
+        w.sb[st] = scale(sb);
+        w.sf[st] = scale(sf);
+        w.sd[st] = scale(sd);
+        w.st[st] = scale(stt);
+    }
     std::vector<const std::vector<double>*> duc, fp, dfp;
     for (int s_ = 0; s_ < S; ++s_)
     {
@@ -445,14 +460,13 @@ void ws_train(Ctx& c, WarmStart& w, int N)
         fp.push_back(&w.s_fprev[s_]);
         dfp.push_back(&w.s_dfp[s_]);
     }
-    std::vector<float> x = ws_inputs(w, duc, fp, dfp, N), t(S * 3 * (size_t)N);
+    std::vector<float> x = ws_inputs(w, w.s_stage, duc, fp, dfp, N), t(S * 3 * (size_t)N);
     for (int s_ = 0; s_ < S; ++s_)
         for (int ch = 0; ch < 3; ++ch)
             for (int q = 0; q < N; ++q)
             {
                 const int i = w.order[q];
-                t[((size_t)s_ * 3 + ch) * N + q] =
-                    (float)((w.s_f[s_][3 * i + ch] - w.s_fprev[s_][3 * i + ch]) / w.st);
+                t[((size_t)s_ * 3 + ch) * N + q] = (float)(w.s_t[s_][3 * i + ch] / w.st[w.s_stage[s_]]);
             }
     w.x.upload(x, c.stream);
     w.t.upload(t, c.stream);
@@ -475,11 +489,13 @@ void ws_train(Ctx& c, WarmStart& w, int N)
     w.trained = true;
 }
 
-// f0 = f_prev + st * net(...), st the rms of f - f_prev in the samples
-std::vector<double> ws_predict(Ctx& c, WarmStart& w, const std::vector<double>& duc, const std::vector<double>& fp,
-                               const std::vector<double>& dfp, int N)
+// f0 = f_base + st * net(...), f_base the linear extrapolation and st the
+// stage's rms of f - f_base in the samples
+std::vector<double> ws_predict(Ctx& c, WarmStart& w, int stage, const std::vector<double>& duc,
+                               const std::vector<double>& fp, const std::vector<double>& dfp,
+                               const std::vector<double>& fbase, int N)
 {
-    std::vector<float> x = ws_inputs(w, {&duc}, {&fp}, {&dfp}, N);
+    std::vector<float> x = ws_inputs(w, {stage}, {&duc}, {&fp}, {&dfp}, N);
     DevBuf<float> dx, h1, h2, y;
     dx.upload(x, c.stream);
     h1.alloc((size_t)kWsChannels * N);
@@ -489,9 +505,9 @@ std::vector<double> ws_predict(Ctx& c, WarmStart& w, const std::vector<double>& 
     std::vector<float> hy(3 * (size_t)N);
     IBLGF_CUDA(cudaMemcpyAsync(hy.data(), y.p, hy.size() * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
-    std::vector<double> f0(fp);
+    std::vector<double> f0(fbase);
     for (int ch = 0; ch < 3; ++ch)
-        for (int q = 0; q < N; ++q) f0[3 * w.order[q] + ch] += (double)w.st * hy[(size_t)ch * N + q];
+        for (int q = 0; q < N; ++q) f0[3 * w.order[q] + ch] += (double)w.st[stage] * hy[(size_t)ch * N + q];
     return f0;
 }
 }  // namespace
@@ -499,7 +515,7 @@ std::vector<double> ws_predict(Ctx& c, WarmStart& w, const std::vector<double>& 
 void ib_warmstart(Ctx& c, int mode, int train_steps, int epochs, double lr, unsigned seed)
 {
     IbState& s = state(c);
-    if (mode != 0 && mode != 1) throw Error(IBLGF_EINVAL, "warm-start mode must be 0 or 1");
+    if (mode < 0 || mode > 2) throw Error(IBLGF_EINVAL, "warm-start mode must be 0, 1 or 2");
     if (mode == 1 && (train_steps <= 0 || epochs <= 0 || !(lr > 0)))
         throw Error(IBLGF_EINVAL, "learned warm start needs train_steps, epochs and lr > 0");
     WarmStart& w = s.ws;
@@ -679,38 +695,44 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
     if (w.mode == 1 && write_prev)
     {
         projection(c, s, s.face_aux2, s.cg_uc.p);
-        std::vector<double> uc = download(c, s.cg_uc.p, m), fp = download(c, s.fprev[stage].p, m);
+        launch_ws_base(c, s.cg_f.p, s.fprev[stage].p, s.fprev2[stage].p, (int)m, s.fcount.p + stage, true);
+        std::vector<double> uc = download(c, s.cg_uc.p, m), fp = download(c, s.fprev[stage].p, m),
+                            fp2 = download(c, s.fprev2[stage].p, m), fbase = download(c, s.cg_f.p, m);
         std::vector<double> duc(uc), dfp(fp);
         if (!w.uc_prev[stage].empty())
             for (size_t i = 0; i < duc.size(); ++i) duc[i] -= w.uc_prev[stage][i];
-        if (!w.f_prev2[stage].empty())
-            for (size_t i = 0; i < dfp.size(); ++i) dfp[i] -= w.f_prev2[stage][i];
-        std::vector<double> f = w.trained ? ws_predict(c, w, duc, fp, dfp, s.n) : fp;
-        IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, f.data(), m * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-        cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
-        f = download(c, s.cg_f.p, m);
-        // samples from steps that have a previous force (the first step's
-        // "change" is the whole force and would set the target scale)
-        if (!w.trained && !w.uc_prev[stage].empty())
+        for (size_t i = 0; i < dfp.size(); ++i) dfp[i] -= fp2[i];
+        const bool history = w.count_host[stage] >= 2 && !w.uc_prev[stage].empty();
+        if (w.trained && history)
         {
+            const std::vector<double> f0 = ws_predict(c, w, stage, duc, fp, dfp, fbase, s.n);
+            IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, f0.data(), m * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        }
+        cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
+        // samples once the extrapolation has two forces behind it
+        if (!w.trained && history)
+        {
+            std::vector<double> t = download(c, s.cg_f.p, m);
+            for (size_t i = 0; i < t.size(); ++i) t[i] -= fbase[i];
+            w.s_stage.push_back(stage);
             w.s_duc.push_back(duc);
             w.s_fprev.push_back(fp);
             w.s_dfp.push_back(dfp);
-            w.s_f.push_back(f);
+            w.s_t.push_back(t);
             if (stage == 3 && ++w.steps_seen >= w.train_steps) ws_train(c, w, s.n);
         }
         w.uc_prev[stage] = uc;
-        w.f_prev2[stage] = fp;
     }
     else
     {
-        IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, s.fprev[stage].p, m * sizeof(double), cudaMemcpyDeviceToDevice,
-                                   c.stream));
+        launch_ws_base(c, s.cg_f.p, s.fprev[stage].p, s.fprev2[stage].p, (int)m, s.fcount.p + stage, w.mode == 2);
         cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
     }
     if (write_prev)
-        IBLGF_CUDA(cudaMemcpyAsync(s.fprev[stage].p, s.cg_f.p, m * sizeof(double), cudaMemcpyDeviceToDevice,
-                                   c.stream));
+    {
+        launch_ws_record(c, s.fprev2[stage].p, s.fprev[stage].p, s.cg_f.p, (int)m, s.fcount.p + stage);
+        ++w.count_host[stage];
+    }
     // LinSysSolver::pressure_correction (linsys.hpp:131-145)
     OpLists& ol = op_lists(c);
     const int l = c.tree.depth - 1;
@@ -777,14 +799,26 @@ void ib_on_adapt(Ctx& c)
 {
     IbState* old = c.ext_get<IbState>(Ctx::kExtIb);
     if (!old) return;
-    std::vector<double> fp[4];
-    for (int k = 0; k < 4; ++k) fp[k] = download(c, old->fprev[k].p, old->fprev[k].n);
+    std::vector<double> fp[4], fp2[4];
+    for (int k = 0; k < 4; ++k)
+    {
+        fp[k] = download(c, old->fprev[k].p, old->fprev[k].n);
+        fp2[k] = download(c, old->fprev2[k].p, old->fprev2[k].n);
+    }
+    std::vector<int> cnt(4);
+    IBLGF_CUDA(cudaMemcpyAsync(cnt.data(), old->fcount.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     WarmStart ws = std::move(old->ws);
     const std::vector<double> X = old->X;
     const double Re = old->Re;
     ib_set_points(c, (int)(X.size() / 3), X.data(), Re);
     IbState& s = state(c);
-    for (int k = 0; k < 4; ++k) s.fprev[k].upload(fp[k], c.stream);
+    for (int k = 0; k < 4; ++k)
+    {
+        s.fprev[k].upload(fp[k], c.stream);
+        s.fprev2[k].upload(fp2[k], c.stream);
+    }
+    s.fcount.upload(cnt, c.stream);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     s.ws = std::move(ws);
 }

@@ -178,6 +178,31 @@ void launch_lgf_table(Ctx& c)
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+namespace
+{
+// LGF_GE::get (lgf_ge.hpp:95-110): E(n; alpha) = f[|n1|] f[|n2|] f[|n3|],
+// f[k] = e^{-2 alpha} I_k(2 alpha) from the context's table of this alpha;
+// offsets past the table (|n_i| >= stride, f below 1e-300 there for the
+// alphas of a time step) give 0
+__global__ void lgf_ge_eval_kernel(const int* __restrict__ xyz, size_t n, const double* __restrict__ f, int stride,
+                                   double* __restrict__ out)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a = abs(xyz[3 * i]), b = abs(xyz[3 * i + 1]), d = abs(xyz[3 * i + 2]);
+    out[i] = (a < stride && b < stride && d < stride) ? f[a] * f[b] * f[d] : 0.0;
+}
+}  // namespace
+
+void launch_lgf_ge_eval(Ctx& c, int ge, const int* d_coords, size_t n, double* d_out)
+{
+    if (!n) return;
+    lgf_ge_eval_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(
+        d_coords, n, c.d_ge.p + (size_t)ge * c.ge_stride, c.ge_stride, d_out);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out)
 {
     if (!n) return;

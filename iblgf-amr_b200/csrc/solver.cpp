@@ -153,14 +153,112 @@ void ctx_init(Ctx& c)
     launch_lgf_table(c);
 }
 
-bool inverse_fp32_passes(const Ctx& c)
+// The FP32 path runs the prime-factor z and y inverse passes in FP32 (the
+// c2r stage, the sum over the two kx halves and the add into the target stay
+// FP64). Measured on the 3-level Gaussian workload: 4.8e-6 relative L-inf
+// against the FP64 oracle (FP64 passes: 1.4e-7; the direct 35-term FP32 sums
+// gave 1.16e-5), inverse phase 1.89 ms instead of 2.53 ms per solve.
+// Server::compute_distribution (decomposition/server.hpp:245-330) for this
+// process's octree: loads as FmmMaskBuilder::fmm_dry accumulates them
+// (fmm.hpp:597-626: neighbour + influence count per AMR2AMR sweep in which
+// the octant is a target), then per level from the finest the leaf and
+// correction octants in Morton order split into n contiguous runs by
+// cumulative load (zero loads count 1), each other octant to the rank of its
+// least-loaded child.
+std::vector<int> domain_partition(const Ctx& c, int n)
 {
-    static const bool on = [] {
-        const char* e = std::getenv("IBLGF_INV_FP32");
-        return e && e[0] == '1';
-    }();
-    return c.cfg.precision == IBLGF_FP32 && on;
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (n < 1) throw Error(IBLGF_EINVAL, "need at least one rank");
+    std::vector<double> load(c.n_oct, 0.0);
+    const int depth = c.tree.depth, bl = c.tree.base_level;
+    for (int rl = 0; rl < depth - bl; ++rl)
+        for (int nlas = 0; nlas < 2; ++nlas)
+        {
+            const int idx = mask_idx_gen(IBLGF_AMR2AMR, rl, nlas);
+            if (idx >= (int)c.masks.size() || c.masks[idx].empty()) continue;
+            for (int o = 0; o < c.n_oct; ++o)
+            {
+                if (!c.masks[idx][2 * o + 1]) continue;
+                int nn = 0;
+                for (int i = 0; i < 27; ++i) nn += c.nbr[27 * o + i] >= 0 ? 1 : 0;
+                load[o] += nn + c.n_infl[o];
+            }
+        }
+    std::vector<int> owner(c.n_oct, -1);
+    std::vector<double> total(n, 0.0);
+    for (int l = (int)c.level_octs.size() - 1; l >= 0; --l)
+    {
+        const std::vector<int>& lo = c.level_octs[l];
+        auto candidate = [&](int o) { return (c.flags[o] & 3) != 0; };
+        double tl = 0.0;
+        for (int o : lo)
+            if (candidate(o))
+            {
+                if (load[o] == 0.0) load[o] = 1.0;
+                tl += load[o];
+            }
+        size_t it = 0;
+        double cur = 0.0;
+        for (int r = 0; r < n && it < lo.size(); ++r)
+        {
+            const double target = std::min((double)(r + 1) / n * tl, tl);
+            int count = 0;
+            while (it < lo.size() && (cur <= target || count == 0))
+            {
+                const int o = lo[it++];
+                if (!candidate(o)) continue;
+                owner[o] = r;
+                total[r] += load[o];
+                cur += load[o];
+                ++count;
+            }
+        }
+        for (int o : lo)
+        {
+            if (candidate(o) && owner[o] >= 0) continue;
+            int best = -1;
+            double bl_load = 0.0;
+            for (int k = 0; k < 8; ++k)
+            {
+                const int ch = c.child[8 * o + k];
+                if (ch < 0 || owner[ch] < 0) continue;
+                if (best < 0 || total[owner[ch]] < bl_load)
+                {
+                    best = owner[ch];
+                    bl_load = total[owner[ch]];
+                }
+            }
+            if (best >= 0)
+            {
+                if (owner[o] >= 0) total[owner[o]] -= load[o];
+                owner[o] = best;
+                total[best] += load[o];
+            }
+        }
+    }
+    for (int& w : owner)
+        if (w < 0) w = 0;  // octants with neither a leaf role nor children (none in a valid octree)
+    return owner;
 }
+
+void domain_set_owner(Ctx& c, const int* owner, int rank, iblgf_exchange_fn fn, void* user)
+{
+    need_single(c);
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    if (owner)
+    {
+        if (!fn) throw Error(IBLGF_EINVAL, "a sharded context needs an exchange callback");
+        c.owner.assign(owner, owner + c.n_oct);
+        c.rank = rank;
+    }
+    else
+        c.owner.clear();
+    c.exchange_fn = fn;
+    c.exchange_user = user;
+    c.plans.clear();
+}
+
+bool inverse_fp32_passes(const Ctx& c) { return c.cfg.precision == IBLGF_FP32; }
 
 void check_status(Ctx& c)
 {
@@ -484,6 +582,15 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
     auto S = [&](int o) { return m[2 * o] != 0; };
     auto T = [&](int o) { return m[2 * o + 1] != 0; };
     const bool neighbor_only = ge >= 0;
+    // sharded: the targets this rank owns at the sweep level and their
+    // ancestors (coarser targets interpolated into them)
+    std::vector<char> needed;
+    if (!c.owner.empty())
+    {
+        needed.assign(c.n_oct, 0);
+        for (int o : c.level_octs[level])
+            for (int a = o; a >= 0 && (a == o ? c.owner[o] == c.rank : !needed[a]); a = c.parent[a]) needed[a] = 1;
+    }
     std::vector<int> tgts;
     for (int lv = level; lv >= 0; --lv)
         for (int o : c.level_octs[lv])
@@ -492,7 +599,7 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
             if (T(o)) p.zt.push_back(o);
             if (neighbor_only && lv != level) continue;
             if (S(o)) p.srcs.push_back(o);
-            if (T(o)) tgts.push_back(o);
+            if (T(o) && (needed.empty() || needed[o])) tgts.push_back(o);
         }
     for (int o : c.level_octs[level])
     {
@@ -529,7 +636,7 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
             for (int k = 0; k < 8; ++k)
             {
                 const int ch = c.child[8 * o + k];
-                if (ch >= 0 && T(ch))
+                if (ch >= 0 && T(ch) && (needed.empty() || needed[ch]))
                 {
                     dst.push_back(ch);
                     tasks.push_back({{o, k}});
@@ -1032,6 +1139,17 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
         launch_inverse_add(c, p, c.d_acc.p, ft, scale);
     }
     for (auto& t : p.intrp) launch_tp(c, t, ft, ft, 0, 1);
+    if (!c.owner.empty() && p.add_t.n)
+    {
+        // sharded: sum the level targets' results over the ranks
+        const size_t count = p.add_t.n * c.block_elems();
+        if (c.exchange_buf.n < count) c.exchange_buf.alloc(count, c.cfg.device, c.stream);
+        launch_blocks_gather(c, ft, c.exchange_buf.p, p.add_t.p, (int)p.add_t.n);
+        if (!c.exchange_fn) throw Error(IBLGF_EINVAL, "sharded sweep without an exchange callback");
+        if (c.exchange_fn(c.exchange_user, c.exchange_buf.p, count, (void*)c.stream) != 0)
+            throw Error(IBLGF_EINTERNAL, "the exchange callback failed");
+        launch_blocks_scatter(c, c.exchange_buf.p, ft, p.add_t.p, (int)p.add_t.n);
+    }
     launch_axpy_blocks(c, ft, c.field(tgt), p.add_t.p, (int)p.add_t.n, add_with_scale, false);
     tm.mark(4);
 }
@@ -1153,6 +1271,40 @@ void apply_op(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out
             if (out[i] == in[j]) throw Error(IBLGF_EINVAL, "operator output aliases an input");
     }
     launch_op(c, op, pin, n_in, pout, n_out, ol.list[li].p, ol.dx[li].p, (int)ol.list[li].n, scale);
+}
+
+// The block operators on a list of octants (Operator::laplace ... applied to
+// it->data() with the octant's dx_level, operators.hpp:1386-1513, 2416-2531)
+void apply_op_octants(Ctx& c, int op, const int* in, int n_in, const int* out, int n_out, const int* octants, int n,
+                      double scale)
+{
+    need_single(c);
+    static const int need_in[6] = {1, 1, 3, 3, 3, 6}, need_out[6] = {1, 3, 1, 3, 3, 3};
+    if (op < 0 || op > 5) throw Error(IBLGF_EINVAL, "unknown operator");
+    if (n_in != need_in[op] || n_out != need_out[op]) throw Error(IBLGF_EINVAL, "wrong number of component fields");
+    if (n <= 0) return;
+    std::vector<int> list(octants, octants + n);
+    std::vector<double> dx(n);
+    for (int i = 0; i < n; ++i)
+    {
+        if (list[i] < 0 || list[i] >= c.n_oct) throw Error(IBLGF_EINVAL, "octant out of range");
+        dx[i] = c.cfg.dx_base / std::pow(2.0, c.levels[list[i]] - c.tree.base_level);
+    }
+    const double* pin[6] = {};
+    double* pout[3] = {};
+    for (int i = 0; i < n_in; ++i) pin[i] = c.field(in[i]);
+    for (int i = 0; i < n_out; ++i)
+    {
+        pout[i] = c.field(out[i]);
+        for (int j = 0; j < n_in; ++j)
+            if (out[i] == in[j]) throw Error(IBLGF_EINVAL, "operator output aliases an input");
+    }
+    DevBuf<int> d_list;
+    DevBuf<double> d_dx;
+    d_list.upload(list, c.stream);
+    d_dx.upload(dx, c.stream);
+    launch_op(c, op, pin, n_in, pout, n_out, d_list.p, d_dx.p, n, scale);
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // the lists are freed on return
 }
 
 // e^{-2 alpha} I_n(2 alpha), n = 0..stride-1, by Miller's backward recurrence

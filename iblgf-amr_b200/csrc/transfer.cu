@@ -418,6 +418,37 @@ void launch_leaves_scatter(Ctx& c, const double* stage, double* field, const int
     IBLGF_CUDA(cudaGetLastError());
 }
 
+namespace
+{
+// one CTA per listed block: field block <-> buf[i]
+__global__ void blocks_copy_kernel(const double* __restrict__ from, double* __restrict__ to,
+                                   const int* __restrict__ list, int b3, int gather)
+{
+    const size_t o = (size_t)list[blockIdx.x] * b3, i0 = (size_t)blockIdx.x * b3;
+    for (int i = threadIdx.x; i < b3; i += blockDim.x)
+    {
+        if (gather) to[i0 + i] = from[o + i];
+        else to[o + i] = from[i0 + i];
+    }
+}
+}  // namespace
+
+void launch_blocks_gather(Ctx& c, const double* field, double* buf, const int* list, int n)
+{
+    if (!n) return;
+    blocks_copy_kernel<<<n, 256, 0, c.stream>>>(field, buf, list, (int)c.block_elems(), 1);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_blocks_scatter(Ctx& c, const double* buf, double* field, const int* list, int n)
+{
+    if (!n) return;
+    blocks_copy_kernel<<<n, 256, 0, c.stream>>>(buf, field, list, (int)c.block_elems(), 0);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
 void launch_leaves_gather(Ctx& c, const double* field, double* stage, const int* list, int n)
 {
     if (!n) return;

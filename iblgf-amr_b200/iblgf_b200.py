@@ -18,6 +18,8 @@ FP64, FP32 = 0, 1
 STREAM, AMR2AMR = 0, 1
 
 REFINE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+# exchange(user, device_buffer, count, stream) -> 0: sum the buffer over the ranks
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
                              ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
 
 
@@ -43,7 +45,9 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_mac_variant", "iblgf_mac_tuning",
+    "iblgf_fma_peak", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
+    "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
+    "iblgf_field_download_octants",
 ]
 
 _lib = None
@@ -102,6 +106,8 @@ def lib():
     L.iblgf_ib_force.argtypes = [vp, ci, vp, vp]
     L.iblgf_ib_stage_status.argtypes = [vp, ci, vp, vp]
     L.iblgf_mac_variant.argtypes = [vp, ci]
+    L.iblgf_domain_partition.argtypes = [vp, ci, vp]
+    L.iblgf_domain_set_owner.argtypes = [vp, vp, ci, EXCHANGE_FN, vp]
     L.iblgf_mac_tuning.argtypes = [vp, vp, ci, vp]
     L.iblgf_ib_warmstart.argtypes = [vp, ci, ci, ci, cd, ctypes.c_uint]
     L.iblgf_ib_warmstart_info.argtypes = [vp, vp]
@@ -552,6 +558,35 @@ class Solver:
             self._check(lib().iblgf_ib_force(self.h, st, None, ctypes.byref(it)))
             out.append(it.value)
         return out
+
+    def partition(self, n_ranks):
+        """Owner rank per octant: the reference server's load-balanced split
+        (decomposition/server.hpp:245-330)."""
+        out = np.zeros(self.n, np.int32)
+        self._check(lib().iblgf_domain_partition(self.h, int(n_ranks), _p(out)))
+        return out
+
+    def set_owner(self, owner, rank, exchange):
+        """Shard the sweeps: this context computes the targets owned by
+        `rank`; exchange(device_ptr, count, stream) must replace the count
+        doubles at device_ptr (ordered on the cudaStream_t `stream`) by their
+        sum over the ranks. owner None ends the sharding."""
+        if owner is None:
+            self._check(lib().iblgf_domain_set_owner(self.h, None, 0, EXCHANGE_FN(), None))
+            self._exchange = None
+            return
+        own = np.ascontiguousarray(owner, dtype=np.int32)
+
+        def cb(user, ptr, count, stream):
+            try:
+                exchange(ptr, count, stream)
+                return 0
+            except Exception as e:  # reported as a failed exchange by the library
+                self._exchange_error = e
+                return 1
+
+        self._exchange = EXCHANGE_FN(cb)  # kept alive while the context uses it
+        self._check(lib().iblgf_domain_set_owner(self.h, _p(own), int(rank), self._exchange, None))
 
     def mac_variant(self, variant):
         """Pin the sibling-group MAC variant (0, 1 direct tile shapes, 2

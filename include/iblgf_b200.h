@@ -119,10 +119,47 @@ int iblgf_field_download_leaves(iblgf_ctx* ctx, int field, double* host, size_t 
  * and solve; `host` should be pinned). iblgf_synchronize waits for it. */
 int iblgf_field_download_leaves_async(iblgf_ctx* ctx, int field, double* host, size_t count);
 int iblgf_field_device_ptr(iblgf_ctx* ctx, int field, double** dptr);
+/* Whole Nb^3 blocks of the listed octants (canonical indices) from / to
+ * host memory, n blocks back to back: the reference's per-octant
+ * DataField::update_device / update_host (datafield.hpp:211-226). */
+int iblgf_field_upload_octants(iblgf_ctx* ctx, int field, const int* octants, int n, const double* host);
+int iblgf_field_download_octants(iblgf_ctx* ctx, int field, const int* octants, int n, double* host);
 
 /* ---- solver ----------------------------------------------------------- */
 /* Fmm<Setup>::apply<Source,Target>(domain, LGF_GL, level, non_leaf_as_source,
  * add_with_scale, fmm_type)  — include/iblgf/fmm/fmm.hpp:729-870 */
+/* kernel objects of Fmm::apply: LGF_GL (lgf_gl.hpp:73-105) and LGF_GE
+ * (lgf_ge.hpp:33-190, neighbour-only, lgf.hpp:209) */
+enum { IBLGF_KERNEL_GL = 0, IBLGF_KERNEL_GE = 1 };
+/* ---- sharded sweeps (several processes / GPUs on one octree) -----------
+ * iblgf_domain_partition: the reference server's load-balanced split
+ * (Server::compute_distribution, decomposition/server.hpp:245-330): per
+ * level from the finest, the leaf and correction octants in Morton order are
+ * cut into n_ranks contiguous runs of equal load (load = the octant's
+ * neighbour + influence count over the AMR2AMR sweeps it is a target of,
+ * the load FmmMaskBuilder::fmm_dry accumulates, fmm.hpp:597-626); every
+ * other octant goes to the rank of its least-loaded child. owner receives
+ * n_octants ranks.
+ * iblgf_domain_set_owner: from now on every FMM sweep of this context
+ * computes only the targets with owner == rank (and the coarser targets
+ * whose values are interpolated into them); before the sweep's result is
+ * added into its target field, exchange(user, buf, count, stream) is called
+ * with the sweep's level targets gathered into a device buffer (count
+ * doubles, ordered on `stream`, a cudaStream_t), and must replace buf by its
+ * sum over all ranks (an all-reduce; a non-owned block is zero in every rank
+ * but its owner's), returning 0 on success. Sources are transformed on every
+ * rank. owner = NULL returns to unsharded sweeps. Plans are rebuilt. */
+typedef int (*iblgf_exchange_fn)(void* user, double* device_buffer, size_t count, void* stream);
+int iblgf_domain_partition(iblgf_ctx* ctx, int n_ranks, int* owner);
+int iblgf_domain_set_owner(iblgf_ctx* ctx, const int* owner, int rank, iblgf_exchange_fn exchange, void* user);
+
+/* Fmm::apply<Source,Target>(domain, kernel, level, non_leaf_as_source,
+ * add_with_scale, fmm_type) with the kernel named explicitly: IBLGF_KERNEL_GL
+ * (as iblgf_fmm_apply) or IBLGF_KERNEL_GE at the given alpha (the kernel's
+ * alpha after change_level; the neighbour-only branch, fmm.hpp:754-770,
+ * scale 1 instead of dx^2, fmm.hpp:1024-1026). */
+int iblgf_fmm_apply_kernel(iblgf_ctx* ctx, int source, int target, int level, int non_leaf_as_source,
+                           double add_with_scale, int fmm_type, int kernel, double alpha);
 int iblgf_fmm_apply(iblgf_ctx* ctx, int source, int target, int level,
                     int non_leaf_as_source, double add_with_scale, int fmm_type);
 /* PoissonSolver::apply_lgf<Source,Target>(fmm_type) for one scalar field —
@@ -147,6 +184,11 @@ int iblgf_poisson_options(iblgf_ctx* ctx, int use_correction, int subtract_non_l
  * 3 curl (:1479, face->edge, 3/3), 4 curl_transpose (:2416, edge->face, 3/3,
  * times scale), 5 nonlinear (:2455, face u + edge omega -> face, 6/3).
  * Outputs must not alias inputs. */
+/* The same operators on the listed octants only (canonical indices), each
+ * with its own dx_level: Operator::laplace<Src,Dst>(it->data(), dx_level) and
+ * the others called per block (operators.hpp:1386-1513, 2416-2531). */
+int iblgf_op_apply_octants(iblgf_ctx* ctx, int op, const int* in, int n_in, const int* out, int n_out,
+                           const int* octants, int n, double scale);
 int iblgf_op_apply(iblgf_ctx* ctx, int op, const int* in, int n_in, const int* out, int n_out,
                    int level, double scale);
 /* client::buffer_exchange<Field>(level) (domain/decomposition/client.hpp:1120):
@@ -160,6 +202,10 @@ int iblgf_buffer_exchange(iblgf_ctx* ctx, int field, int level);
 int iblgf_lgf_table(iblgf_ctx* ctx, double* host_out, size_t count);
 /* G(n) for n host coordinate triples (x,y,z), evaluated on the device. */
 int iblgf_lgf_get(iblgf_ctx* ctx, const int* coords, size_t n, double* host_out);
+/* LGF_GE::get (lgf_ge.hpp:95-110): E(n; alpha) = f|n1| f|n2| f|n3| with
+ * f_k = e^{-2 alpha} I_k(2 alpha), for n host coordinate triples, evaluated on
+ * the device from the context's table of this alpha. */
+int iblgf_lgf_ge_get(iblgf_ctx* ctx, double alpha, const int* coords, size_t n, double* host_out);
 
 /* ---- IF-HERK time step (Ifherk::time_step, ifherk.hpp:1078-1200, with the
  * time_march loop's T += dt) -------------------------------------------------
@@ -248,16 +294,19 @@ int iblgf_ib_solve(iblgf_ctx* ctx, const int* u_fields, double alpha, double thr
 
 /* ---- learned warm start of the IB force CG (no reference counterpart: the
  * reference warm-starts from IB::force_prev, ifherk.hpp:1476) -------------
- * mode 0: previous step's force of the stage (the reference). mode 1: the
- * first IF-HERK step and the next train_steps steps run with mode 0; those
- * train_steps steps record (change of the
- * CG right-hand side since the previous step, previous force, its last
- * change, solution) per stage; a 1-D convolutional network over the IB points
- * in Morton order of their coordinates (9 -> 64 -> 64 -> 3 channels, kernel 5,
- * 24 451 FP32 parameters,
- * seeded initialisation) is then trained on them (full-batch Adam, `epochs`
+ * mode 0: previous step's force of the stage (the reference). mode 2: its
+ * linear extrapolation 2 f_prev - f_prev2 once the stage has two forces.
+ * mode 1 (learned): until trained, mode 2; from the third step on, the next
+ * train_steps steps record per stage (change of the CG right-hand side since
+ * the previous step, previous force, its last change; target: the converged
+ * force minus the extrapolation); a 1-D convolutional network over the IB
+ * points in Morton order of their coordinates (9 -> 64 -> 64 -> 3 channels,
+ * kernel 5, 24 451 FP32 parameters, seeded initialisation; inputs and target
+ * scaled per stage) is then trained on them (full-batch Adam, `epochs`
  * steps, learning rate lr, on the device) and from then on predicts the
- * initial guess f_prev + correction; CG runs to the unchanged tolerance.
+ * initial guess extrapolation + correction; CG runs to the unchanged
+ * tolerance. Modes 0 and 2 stay on the device (time steps can be captured
+ * as CUDA graphs); mode 1 assembles the network's inputs on the host.
  * iblgf_ib_warmstart_info: [mode, trained, samples, first loss, last loss,
  * parameters]. iblgf_ws_check: one forward + backward pass of the network
  * for given parameters (layout W1 b1 W2 b2 W3 b3), inputs [S][9][N] and

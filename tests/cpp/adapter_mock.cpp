@@ -1,17 +1,28 @@
 // Drives include/iblgf_b200/adapter.hpp through a minimal stand-in for the
 // reference's Domain / Octant / DataField / Setup types (only the members the
-// adapter uses), the way a reference setup (tests/poisson/vortexrings.hpp)
-// would call PoissonSolver<Setup>::solve<source, phi>().
+// adapter uses), the way reference setups (tests/poisson/vortexrings.hpp,
+// ifherk.hpp) call PoissonSolver, Fmm, the LGF kernel objects and Operator.
 //
-//   adapter_mock <in.bin> <out.bin>
+//   adapter_mock <in.bin> <out.bin> [mode alpha level]
 // in.bin: int e, bd_base[3], bd_extent[3]; double dx; int n; uint64 keys[n];
 //         int flags[n]; double source[n][Nb^3]  (octants in any order)
-// out.bin: double target[n][Nb^3] in the same order.
+// modes (out.bin in the input's octant order):
+//   poisson  PoissonSolver::solve<source, phi>()                 -> phi
+//   if       PoissonSolver::apply_lgf_IF<source, phi>(alpha)      -> phi
+//   fmm_gl   Fmm::apply<source, phi>(LGF_GL, level, nlas 1, 0.5)  -> phi
+//   fmm_ge   Fmm::apply<source, phi>(LGF_GE alpha, level, 0, 1)   -> phi
+//   ops      Operator::levelGradient<source, face>(l) for every level, then
+//            the per-block Operator::curl<face, edge>(it->data(), dx) on
+//            every octant                                         -> face[3], edge[3]
+//   kernels  LGF_GL::get and LGF_GE(alpha)::get at 64 fixed offsets -> 2 x 64 values
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <memory>
 #include <random>
+#include <string>
 #include <vector>
 
 #include "iblgf_b200/adapter.hpp"
@@ -27,16 +38,24 @@ struct Block
     double* data() { return v.data(); }
     std::size_t size() const { return v.size(); }
 };
+struct DataBlock  // the octant's data block (it->data())
+{
+    int dummy = 0;
+};
+constexpr int kTags = 4;
 struct Octant
 {
     Key k;
     int flags = 0;
-    std::array<Block, 2> f;
+    int level = 0;
+    DataBlock db;
+    std::array<std::vector<Block>, kTags> f;  // [tag][component]
     bool has_data() const { return true; }
     Key key() const { return k; }
     bool is_leaf() const { return flags & 1; }
     bool is_correction() const { return flags & 2; }
-    Block& data_r(int tag, std::size_t) { return f[tag]; }
+    DataBlock& data() { return db; }
+    Block& data_r(int tag, std::size_t comp) { return f[tag][comp]; }
 };
 struct Box
 {
@@ -79,20 +98,23 @@ struct Setup
     using simulation_t = Simulation;
     using domain_t = Domain;
 };
-struct source_f
+template<int T, std::size_t N>
+struct field
 {
-    static int tag() { return 0; }
-    static std::size_t nFields() { return 1; }
+    static int tag() { return T; }
+    static std::size_t nFields() { return N; }
 };
-struct phi_f
-{
-    static int tag() { return 1; }
-    static std::size_t nFields() { return 1; }
-};
+using source_f = field<0, 1>;
+using phi_f = field<1, 1>;
+using face_f = field<2, 3>;
+using edge_f = field<3, 3>;
 
 int main(int argc, char** argv)
 {
-    if (argc != 3) return 2;
+    if (argc != 3 && argc != 6) return 2;
+    const std::string mode = argc == 6 ? argv[3] : "poisson";
+    const double alpha = argc == 6 ? std::atof(argv[4]) : 0.0;
+    const int level = argc == 6 ? std::atoi(argv[5]) : 0;
     FILE* fi = std::fopen(argv[1], "rb");
     if (!fi) return 2;
     int e, bb[3], be[3], n;
@@ -115,9 +137,10 @@ int main(int argc, char** argv)
         auto o = std::make_unique<Octant>();
         o->k = {keys[i]};
         o->flags = flags[i];
-        o->f[0].v.resize(B);
-        o->f[1].v.assign(B, 0.0);
-        ok = std::fread(o->f[0].v.data(), 8, B, fi) == B;
+        o->level = (int)((keys[i] >> 2) & 31);
+        const std::size_t comps[kTags] = {1, 1, 3, 3};
+        for (int t = 0; t < kTags; ++t) o->f[t].assign(comps[t], Block{std::vector<double>(B, 0.0)});
+        ok = std::fread(o->f[0][0].v.data(), 8, B, fi) == B;
         d.octs.push_back(std::move(o));
     }
     std::fclose(fi);
@@ -128,11 +151,75 @@ int main(int argc, char** argv)
     std::mt19937 rng(5);
     std::shuffle(d.octs.begin(), d.octs.end(), rng);
 
-    iblgf::b200::PoissonSolver<Setup> psolver(&sim);
-    psolver.solve<source_f, phi_f>();
-
+    std::vector<double> out;
+    auto put = [&](int tag, std::size_t ncomp) {
+        for (std::size_t k = 0; k < ncomp; ++k)
+            for (Octant* o : in_order) out.insert(out.end(), o->f[tag][k].v.begin(), o->f[tag][k].v.end());
+    };
+    try
+    {
+        if (mode == "poisson")
+        {
+            iblgf::b200::PoissonSolver<Setup> psolver(&sim);
+            psolver.solve<source_f, phi_f>();
+            put(1, 1);
+        }
+        else if (mode == "if")
+        {
+            iblgf::b200::PoissonSolver<Setup> psolver(&sim);
+            psolver.apply_lgf_IF<source_f, phi_f>(alpha);
+            put(1, 1);
+        }
+        else if (mode == "fmm_gl" || mode == "fmm_ge")
+        {
+            iblgf::b200::Fmm<Setup> fmm(&d);
+            if (mode == "fmm_gl")
+            {
+                iblgf::b200::LGF_GL k;
+                fmm.apply<source_f, phi_f>(&d, &k, level, true, 0.5);
+            }
+            else
+            {
+                iblgf::b200::LGF_GE k;
+                k.alpha_base_level() = alpha;
+                fmm.apply<source_f, phi_f>(&d, &k, level, false, 1.0);
+            }
+            put(1, 1);
+        }
+        else if (mode == "ops")
+        {
+            using Op = iblgf::b200::Operator<Domain>;
+            Op::bound_domain() = &d;
+            int bl = 0, depth = 0, no = 0;
+            iblgf_ctx* c = iblgf::b200::device_domain(&d).ctx();
+            iblgf::b200::check(c, iblgf_domain_info(c, &bl, &depth, &no));
+            for (int l = bl; l < depth; ++l) Op::levelGradient<source_f, face_f>(&d, l);
+            for (auto& o : d.octs)
+                Op::curl<face_f, edge_f>(o->data(), dx / std::pow(2.0, o->level - bl));
+            put(2, 3);
+            put(3, 3);
+        }
+        else if (mode == "kernels")
+        {
+            iblgf::b200::LGF_GL gl;
+            iblgf::b200::LGF_GE ge;
+            ge.alpha_base_level() = alpha;
+            ge.change_level(0);
+            std::vector<std::array<int, 3>> pts;
+            for (int i = 0; i < 64; ++i) pts.push_back({i % 7 - 3, (i / 7) % 5 - 2, i / 35 * 37 - 5});
+            for (auto& p : pts) out.push_back(gl.get(p));
+            for (auto& p : pts) out.push_back(ge.get(p));
+        }
+        else
+            return 2;
+    }
+    catch (const std::exception& ex)
+    {
+        std::fprintf(stderr, "adapter_mock: %s\n", ex.what());
+        return 1;
+    }
     FILE* fo = std::fopen(argv[2], "wb");
-    for (Octant* o : in_order) std::fwrite(o->f[1].v.data(), 8, B, fo);
+    std::fwrite(out.data(), 8, out.size(), fo);
     std::fclose(fo);
     return 0;
 }

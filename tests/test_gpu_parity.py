@@ -200,16 +200,9 @@ def test_domain_import_matches(name):
         assert np.array_equal(o.masks(idx), gi.masks(idx)), idx
 
 
-def test_cpp_adapter_poisson_solve(tmp_path):
-    """The reference-style C++ adapter (PoissonSolver<Setup>::solve<Src,Tgt>)
-    over a stand-in domain in shuffled iteration order reproduces the oracle."""
+def _run_adapter(tmp_path, case, o, src, mode="poisson", alpha=0.0, level=0):
     import struct
     import subprocess
-    case = S.GaussianPoisson("amr_small")
-    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
-                 n_levels=case.n_levels, predicate=case.predicate)
-    src = case.fields(o)
-    ref = o.apply_lgf(src)
     fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
     with open(fin, "wb") as f:
         f.write(struct.pack("7i", case.block_extent, *case.bd_base, *case.bd_extent))
@@ -220,10 +213,74 @@ def test_cpp_adapter_poisson_solve(tmp_path):
         f.write(np.ascontiguousarray(src).tobytes())
     root = os.path.dirname(HERE)
     subprocess.run(["make", "-s", "-C", os.path.join(root, "tests", "cpp")], check=True)
-    subprocess.run([os.path.join(root, "tests", "cpp", "adapter_mock"), str(fin), str(fout)], check=True)
-    out = np.fromfile(fout, dtype=np.float64).reshape(ref.shape)
+    subprocess.run([os.path.join(root, "tests", "cpp", "adapter_mock"), str(fin), str(fout), mode, repr(alpha),
+                    str(level)], check=True)
+    return np.fromfile(fout, dtype=np.float64)
+
+
+def test_cpp_adapter_poisson_solve(tmp_path):
+    """The reference-style C++ adapter (PoissonSolver<Setup>::solve<Src,Tgt>)
+    over a stand-in domain in shuffled iteration order reproduces the oracle."""
+    case = S.GaussianPoisson("amr_small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(o)
+    ref = o.apply_lgf(src)
+    out = _run_adapter(tmp_path, case, o, src).reshape(ref.shape)
     # leaves carry the solution (poisson.hpp:761-781); non-leaf targets stay 0
     assert rel_linf(out, ref) < 1e-12
+
+
+def test_cpp_adapter_integrating_factor_and_kernel_dispatch(tmp_path):
+    """Through the C++ adapter: PoissonSolver::apply_lgf_IF (poisson.hpp:428-494),
+    Fmm::apply with an LGF_GL kernel (full sweep, non-leaf sources, scale 0.5)
+    and with an LGF_GE kernel (neighbour-only branch at alpha_base 4^(level -
+    base)), each against the oracle (FP64)."""
+    case = S.GaussianPoisson("amr_small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(o)
+    alpha = 0.05
+    out = _run_adapter(tmp_path, case, o, src, "if", alpha).reshape(src.shape)
+    assert rel_linf(out, o.apply_if(src, alpha)) < 1e-12
+    for level in range(o.base_level, o.depth):
+        out = _run_adapter(tmp_path, case, o, src, "fmm_gl", 0.0, level).reshape(src.shape)
+        assert rel_linf(out, o.fmm_apply(src, o.zeros(), level, 1, 0.5, 1)) < 1e-12
+        a = alpha * 4.0 ** (level - o.base_level)
+        out = _run_adapter(tmp_path, case, o, src, "fmm_ge", alpha, level).reshape(src.shape)
+        ref = o.fmm_apply_ge(src, o.zeros(), level, 0, 1.0, a)
+        assert rel_linf(out, ref) < 1e-12, level
+
+
+def test_cpp_adapter_operators_and_kernel_objects(tmp_path):
+    """Operator::levelGradient (gradient, then the target's buffer exchange,
+    operators.hpp:588-606) on every level and the per-block
+    Operator::curl<face, edge>(it->data(), dx_level) on every octant through
+    the adapter, against the oracle; LGF_GL::get and LGF_GE::get at fixed
+    offsets against the oracle's kernels."""
+    case = S.GaussianPoisson("amr_small")
+    o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
+                 n_levels=case.n_levels, predicate=case.predicate)
+    src = case.fields(o)
+    out = _run_adapter(tmp_path, case, o, src, "ops").reshape((6,) + src.shape)
+    face = [o.zeros() for _ in range(3)]
+    for lv in range(o.base_level, o.depth):
+        g = o.op(1, [src], [o.zeros() for _ in range(3)], lv, 1.0)
+        for k in range(3):
+            on_level = o.levels == lv
+            face[k][on_level] = o.buffer_exchange(g[k], lv)[on_level]
+    for k in range(3):
+        assert rel_linf(out[k], face[k]) < 1e-13, k
+    edge = o.op(3, face, [o.zeros() for _ in range(3)], -1, 1.0)
+    for k in range(3):
+        assert rel_linf(out[3 + k], edge[k]) < 1e-13, k
+    alpha = 0.3
+    vals = _run_adapter(tmp_path, case, o, src, "kernels", alpha)
+    pts = [(i % 7 - 3, (i // 7) % 5 - 2, i // 35 * 37 - 5) for i in range(64)]
+    gl = np.array([O.lgf_get(*p) for p in pts])
+    ge = np.array([o.lgf_ge_get(*p, alpha) for p in pts])
+    assert np.abs(vals[:64] - gl).max() < 1e-13 * np.abs(gl).max()
+    assert np.abs(vals[64:] - ge).max() < 1e-13 * np.abs(ge).max()
 
 
 @pytest.mark.parametrize("op,n_in,n_out", [(0, 1, 1), (1, 1, 3), (2, 3, 1), (3, 3, 3), (4, 3, 3), (5, 6, 3)])
