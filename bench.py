@@ -121,6 +121,9 @@ def main():
     ap.add_argument("--workload", default="amr_3level")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="with --gpus N > 1: one octree sharded over the ranks (the reference server's partition, "
+                         "an NCCL all-reduce of each sweep's level targets) instead of N independent replicas")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
     ap.add_argument("--no-ns", action="store_true", help="skip the IF-HERK step measurement")
     ap.add_argument("--ns-only", action="store_true", help="only the IF-HERK step measurement (profiling)")
@@ -188,6 +191,10 @@ def main():
                  stream=stream.cuda_stream)
     src_host = case.fields(g)
     cells = case.n_cells(g)
+    sharded = args.shard and world > 1
+    if sharded:
+        import sharding
+        g.set_owner(g.partition(world), rank, sharding.torch_allreduce_exchange())
     fs, ft = g.field(src_host), g.field()
     for _ in range(args.warmup):
         g.apply_lgf(fs, ft)
@@ -220,7 +227,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_step = ms / args.steps
-    value = world * cells / (ms_step * 1e-3)
+    # replicas: every rank solves the whole problem; sharded: one problem
+    value = (1 if sharded else world) * cells / (ms_step * 1e-3)
 
     # ---- end to end through the C ABI with pinned host buffers: the leaf
     # interiors (the cells the metric counts) in, the solution on them out
@@ -333,15 +341,17 @@ def main():
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "strong" if sharded else "weak",
                 "vs_baseline": None, "dtype": "f32" if prec == B.FP32 else "f64", "data": "synthetic",
                 "config": {"workload": wl, "cells_per_step": cells, "octants": g.n,
                            "precision": args.precision + " FFT/MAC, f64 fields and LGF table",
                            "l2": "inputs larger than L2 (fields %.0f MB, spectra cache > 126 MB)" % (g.n * g.Nb ** 3 * 8 / 1e6),
-                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "parallelism": ("sharded octree (NCCL all-reduce per sweep)" if sharded else "replicas")
+                           if world > 1 else "single GPU",
                            "sweeps_per_step": sweeps, "pairs_per_step": npairs,
                            "targets_per_step": ntgt, "group_mac_targets_per_step": int(stats[7]) / args.steps},
-                "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s",
+                "e2e": {"value": (1 if sharded else world) * cells / (e2e_ms * 1e-3), "unit": "cells/s",
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
                 "gpu_launches": int(launches),
                 "mac_autotune": {"variants": "0, 1: direct sibling-group kernel (64 x 768, 32 x 512 FP32); "
@@ -443,7 +453,7 @@ def ib_bench(B, stream, device, steps, warmup):
     out = {"workload": "sphere D=1, Re=300, uniform stream, dx_finest=D/40, 16^3 blocks, 3 mesh levels, "
                        "2009 IB points, CG threshold 1e-3, max 40; warm start: previous force per stage "
                        "(reference), its linear extrapolation (fp32_extrapolated) and the learned 1-D conv net "
-                       "correcting the extrapolation (fp32_learned, trained on 8 steps x 3 stages)"}
+                       "correcting the previous force (fp32_learned, trained on 8 steps x 3 stages)"}
     dt = 0.35 * case.dx_base / 4 / 1.0
     res = {}
     train_steps = 8
@@ -457,8 +467,8 @@ def ib_bench(B, stream, device, steps, warmup):
         g.ib_set_points(X, case.Re)
         g.ns_options((-1.0, 0.0, 0.0))
         if mode == 1:
-            # steps 3 .. train_steps + 2 record samples (the extrapolation
-            # needs two forces); the network is trained before the timed steps
+            # steps 2 .. train_steps + 1 record samples; the network is
+            # trained before the timed steps
             g.ib_warmstart(1, train_steps=train_steps, epochs=1000, lr=2e-3, seed=7)
         elif mode == 2:
             g.ib_warmstart(2)

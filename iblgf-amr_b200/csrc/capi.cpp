@@ -88,6 +88,7 @@ int iblgf_destroy(iblgf_ctx* x)
     iblgf_b200::copy_stream_release(x->c);
     x->c.fields.clear();  // stream-ordered frees on the context stream
     x->c.leaf_stage.release();
+    x->c.exchange_buf.release();  // stream-ordered: before the stream goes
     cudaStreamSynchronize(x->c.stream);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;

@@ -45,8 +45,8 @@ double yang3(double x)
 struct WarmStart
 {
     // 0: previous step's force of the stage (the reference), 1: learned
-    // correction on top of the linear extrapolation, 2: linear extrapolation
-    // 2 f_prev - f_prev2 (both fall back to f_prev until two forces exist)
+    // correction on top of the previous force, 2: linear extrapolation
+    // 2 f_prev - f_prev2 (f_prev until two forces exist)
     int mode = 0;
     int train_steps = 0, epochs = 0, steps_seen = 0, n_params = 0;
     float lr = 1e-3f;
@@ -54,7 +54,7 @@ struct WarmStart
     bool trained = false;
     float loss_first = 0.0f, loss_last = 0.0f;
     // samples (stage, rhs change, previous force, its last change, target
-    // f - f_base) and per-stage input / target scales
+    // f - f_prev) and per-stage input / target scales
     std::vector<int> s_stage;
     std::vector<std::vector<double>> s_duc, s_fprev, s_dfp, s_t;
     float sb[4] = {1, 1, 1, 1}, sf[4] = {1, 1, 1, 1}, sd[4] = {1, 1, 1, 1}, st[4] = {1, 1, 1, 1};
@@ -489,8 +489,8 @@ void ws_train(Ctx& c, WarmStart& w, int N)
     w.trained = true;
 }
 
-// f0 = f_base + st * net(...), f_base the linear extrapolation and st the
-// stage's rms of f - f_base in the samples
+// f0 = f_base + st * net(...), f_base the previous force and st the stage's
+// rms of f - f_base in the samples
 std::vector<double> ws_predict(Ctx& c, WarmStart& w, int stage, const std::vector<double>& duc,
                                const std::vector<double>& fp, const std::vector<double>& dfp,
                                const std::vector<double>& fbase, int N)
@@ -695,21 +695,21 @@ void ns_ib_stage(Ctx& c, int stage, double alpha, double threshold, int max_iter
     if (w.mode == 1 && write_prev)
     {
         projection(c, s, s.face_aux2, s.cg_uc.p);
-        launch_ws_base(c, s.cg_f.p, s.fprev[stage].p, s.fprev2[stage].p, (int)m, s.fcount.p + stage, true);
+        launch_ws_base(c, s.cg_f.p, s.fprev[stage].p, s.fprev2[stage].p, (int)m, s.fcount.p + stage, false);
         std::vector<double> uc = download(c, s.cg_uc.p, m), fp = download(c, s.fprev[stage].p, m),
                             fp2 = download(c, s.fprev2[stage].p, m), fbase = download(c, s.cg_f.p, m);
         std::vector<double> duc(uc), dfp(fp);
         if (!w.uc_prev[stage].empty())
             for (size_t i = 0; i < duc.size(); ++i) duc[i] -= w.uc_prev[stage][i];
         for (size_t i = 0; i < dfp.size(); ++i) dfp[i] -= fp2[i];
-        const bool history = w.count_host[stage] >= 2 && !w.uc_prev[stage].empty();
+        const bool history = w.count_host[stage] >= 1 && !w.uc_prev[stage].empty();
         if (w.trained && history)
         {
             const std::vector<double> f0 = ws_predict(c, w, stage, duc, fp, dfp, fbase, s.n);
             IBLGF_CUDA(cudaMemcpyAsync(s.cg_f.p, f0.data(), m * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         }
         cg_solve(c, s, s.face_aux2, alpha, threshold, max_iter, rec);
-        // samples once the extrapolation has two forces behind it
+        // samples from steps that have a previous force and right-hand side
         if (!w.trained && history)
         {
             std::vector<double> t = download(c, s.cg_f.p, m);

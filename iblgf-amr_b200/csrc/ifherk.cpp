@@ -556,7 +556,9 @@ void ns_step(Ctx& c, const int* u, int p, double dt, double Re, double* T, int n
         // steps with the immersed boundary are captured too: their force CG
         // is a conditional while-node of the graph (not with the learned
         // warm start, which assembles its inputs on the host)
-        const bool graphable = (!ib_active(c) || ib_graphable(c)) && !c.profile && !s.graph_failed;
+        // (a sharded context's sweeps call its host-side exchange: direct launches)
+        const bool graphable =
+            (!ib_active(c) || ib_graphable(c)) && !c.profile && !s.graph_failed && c.owner.empty();
         StepKey key;
         for (int k = 0; k < 3; ++k) key.u[k] = u[k];
         key.p = p;

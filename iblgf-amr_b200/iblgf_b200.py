@@ -18,9 +18,9 @@ FP64, FP32 = 0, 1
 STREAM, AMR2AMR = 0, 1
 
 REFINE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
 # exchange(user, device_buffer, count, stream) -> 0: sum the buffer over the ranks
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
-                             ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
 
 
 class Config(ctypes.Structure):

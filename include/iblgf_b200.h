@@ -296,15 +296,15 @@ int iblgf_ib_solve(iblgf_ctx* ctx, const int* u_fields, double alpha, double thr
  * reference warm-starts from IB::force_prev, ifherk.hpp:1476) -------------
  * mode 0: previous step's force of the stage (the reference). mode 2: its
  * linear extrapolation 2 f_prev - f_prev2 once the stage has two forces.
- * mode 1 (learned): until trained, mode 2; from the third step on, the next
+ * mode 1 (learned): until trained, mode 0; from the second step on, the next
  * train_steps steps record per stage (change of the CG right-hand side since
  * the previous step, previous force, its last change; target: the converged
- * force minus the extrapolation); a 1-D convolutional network over the IB
+ * force minus the previous force); a 1-D convolutional network over the IB
  * points in Morton order of their coordinates (9 -> 64 -> 64 -> 3 channels,
  * kernel 5, 24 451 FP32 parameters, seeded initialisation; inputs and target
  * scaled per stage) is then trained on them (full-batch Adam, `epochs`
  * steps, learning rate lr, on the device) and from then on predicts the
- * initial guess extrapolation + correction; CG runs to the unchanged
+ * initial guess previous force + correction; CG runs to the unchanged
  * tolerance. Modes 0 and 2 stay on the device (time steps can be captured
  * as CUDA graphs); mode 1 assembles the network's inputs on the host.
  * iblgf_ib_warmstart_info: [mode, trained, samples, first loss, last loss,
