@@ -331,6 +331,8 @@ def main():
         extra["rel_linf_vs_oracle"] = float(np.abs(g.download(ft) - ref).max() / scale)
         if out64 is not None:
             extra["fp64_plain"]["rel_linf_vs_oracle"] = float(np.abs(out64 - ref).max() / scale)
+    if rank == 0 and not args.no_cpu_baseline:
+        extra["reference_gpu"] = reference_gpu_baseline(g.Nb, ntgt, npairs, cells, extra.get("fp64_plain"))
     if rank == 0 and not args.no_ns:
         extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
         extra["ns_step_adaptive"] = ns_adapt_bench(B, stream, local, args.steps, args.warmup)
@@ -573,6 +575,39 @@ def batch_bench(B, stream, device, steps, warmup):
     out["speedup_batched_vs_sequential"] = ms_seq / out["ms_per_solve_fp32"]
     for s, _, _ in solvers:
         s.close()
+    return out
+
+
+def reference_gpu_baseline(Nb, targets, pairs, cells, fp64_ours):
+    """The reference's own GPU path for the block convolutions (its cuFFT
+    Convolution_GPU, FP64, built from the reference tree into
+    oracle/_ref/ref_conv_gpu) driven through its stock per-pair calls on
+    synthetic pairs: wall time per target for 64 and 160 pairs per target
+    (100 targets, after one pass that caches the LGF spectra) fitted as
+    a + b pairs, then evaluated for the workload's targets and pairs per
+    solve. Only the convolutions: the reference's anterpolation,
+    interpolation and bookkeeping would add to it, so the result is an upper
+    bound of the reference's cells/s."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_conv_gpu")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_conv_gpu not built (needs the reference tree at build time)"}
+    pts = []
+    for q in (64, 160):
+        r = subprocess.run([exe, "time", str(Nb), "100", str(q), "2"], capture_output=True, text=True, timeout=600)
+        if r.returncode != 0:
+            return {"unavailable": "ref_conv_gpu exited %d" % r.returncode}
+        pts.append((q, json.loads(r.stdout.strip().splitlines()[-1])["ms_per_target"]))
+    (q0, t0), (q1, t1) = pts
+    b = (t1 - t0) / (q1 - q0)
+    a = t0 - b * q0
+    ms = targets * a + pairs * b
+    out = {"kind": "reference fft::Convolution_GPU<3> (cuFFT D2Z/Z2D FP64, batches of 10), stock "
+                   "apply_forward_add / apply_backward per pair / target, synthetic pairs",
+           "ms_per_target_measured": {str(q): t for q, t in pts},
+           "ms_per_target_fit": {"per_target": a, "per_pair": b},
+           "ms_per_solve_convolutions_only": ms, "cells_per_s_upper_bound": cells / (ms * 1e-3)}
+    if fp64_ours:
+        out["fp64_ours_speedup"] = ms / fp64_ours["ms_per_step"]
     return out
 
 
