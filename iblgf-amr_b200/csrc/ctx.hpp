@@ -537,10 +537,12 @@ void copy_stream_release(Ctx& c);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
 void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
                         bool assign);
+// fp32: the three passes in FP32, the sum into the FP64 receiving block in FP64
 void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base,
-               int mode /*0 antrp add, 1 intrp add, 2 intrp assign*/);
+               int mode /*0 antrp add, 1 intrp add, 2 intrp assign*/, bool fp32 = false);
 // per-axis matrix pairs (mat_base[3]): face / edge components of the cell-centred transfers
-void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode);
+void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode,
+                    bool fp32 = false);
 void launch_halo(Ctx& c, double* f, const int* list, int n);
 void launch_source_correction(Ctx& c, const double* target_tmp, double* corr, const int* list, int n,
                               double inv_dx2);

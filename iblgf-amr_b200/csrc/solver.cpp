@@ -1117,7 +1117,11 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     launch_zero_blocks(c, fs, p.zero_s.p, (int)p.zero_s.n);
     launch_zero_blocks(c, ft, p.zero_t.p, (int)p.zero_t.n);
     launch_copy_interior(c, c.field(src), fs, p.copy_s.p, (int)p.copy_s.n);
-    for (auto& t : p.antrp) launch_tp(c, t, fs, fs, 0, 0);
+    // the FMM's Lagrange anterpolation of the sources (fmm_nli.hpp) runs its
+    // passes in FP32 on the FP32 path (the coarse sources feed FP32
+    // transforms); the interpolation of the targets stays FP64
+    const bool fp32 = c.cfg.precision == IBLGF_FP32;
+    for (auto& t : p.antrp) launch_tp(c, t, fs, fs, 0, 0, fp32);
     tm.mark(1);
     const size_t cb = c.cplx_bytes();
     if (!p.empty())

@@ -29,10 +29,10 @@ namespace
 // loads). Face and edge components use different matrices per axis.
 // lo: for the banded passes (W > 0), first column of row m's band of width W
 // in summation order (the row's nonzeros all lie in [lo, lo + W))
-template<int NB>
+template<int NB, class T>
 struct TpMats
 {
-    double m[3][2][NB * NB];
+    T m[3][2][NB * NB];
     unsigned char lo[3][2][NB];
 };
 
@@ -52,19 +52,21 @@ constexpr int tp_threads()
 // W > 0: only the W entries of row m's band [lo, lo + W) are summed, in
 // the same order; the skipped entries are zeros, whose FMAs leave the running
 // sum unchanged, so the result equals the full row's
-template<int NB, int A, int K, bool TR, bool LAST, int W>
-__device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* __restrict__ out,
-                                        const TpMats<NB>& mt, int p, double* acc)
+// T: arithmetic and shared-memory type of the passes (the accumulators acc,
+// which start from and end in the FP64 target block, stay FP64)
+template<int NB, int A, int K, bool TR, bool LAST, int W, class T>
+__device__ __forceinline__ void tp_pass(const T* __restrict__ in, T* __restrict__ out,
+                                        const TpMats<NB, T>& mt, int p, double* acc)
 {
     if constexpr (W == 0)
     {
-        double v[NB];
+        T v[NB];
 #pragma unroll
         for (int n = 0; n < NB; ++n) v[n] = in[p * NB + n];
 #pragma unroll
         for (int m = 0; m < NB; ++m)
         {
-            double s = 0.0;
+            T s = 0;
 #pragma unroll
             for (int n = 0; n < NB; ++n) s = fma(TR ? mt.m[A][K][n * NB + m] : mt.m[A][K][m * NB + n], v[n], s);
             if (LAST) acc[m] += s;
@@ -73,12 +75,12 @@ __device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* _
     }
     else
     {
-        const double* row = in + p * NB;
+        const T* row = in + p * NB;
 #pragma unroll
         for (int m = 0; m < NB; ++m)
         {
             const int lo = mt.lo[A][K][m];
-            double s = 0.0;
+            T s = 0;
 #pragma unroll
             for (int j = 0; j < W; ++j)
             {
@@ -91,12 +93,11 @@ __device__ __forceinline__ void tp_pass(const double* __restrict__ in, double* _
     }
 }
 
-template<int NB, int A, bool TR, bool LAST, int W>
-__device__ __forceinline__ void tp_pass_bit(int bit, const double* in, double* out, const TpMats<NB>& mt, int p,
-                                            double* acc)
+template<int NB, int A, bool TR, bool LAST, int W, class T>
+__device__ __forceinline__ void tp_pass_bit(int bit, const T* in, T* out, const TpMats<NB, T>& mt, int p, double* acc)
 {
-    if (bit) tp_pass<NB, A, 1, TR, LAST, W>(in, out, mt, p, acc);
-    else tp_pass<NB, A, 0, TR, LAST, W>(in, out, mt, p, acc);
+    if (bit) tp_pass<NB, A, 1, TR, LAST, W, T>(in, out, mt, p, acc);
+    else tp_pass<NB, A, 0, TR, LAST, W, T>(in, out, mt, p, acc);
 }
 
 // mode 0: dst[group] += sum_tasks A(src)        (anterpolation / coarsify)
@@ -104,16 +105,16 @@ __device__ __forceinline__ void tp_pass_bit(int bit, const double* in, double* o
 // mode 2: dst[group]  = I(src)                  (cell-centred interpolation)
 // One CTA per receiving block, one thread per pencil; the sending blocks of
 // a group are applied in child order into per-thread accumulators.
-template<int NB, bool TR, int W>
+template<int NB, bool TR, int W, class T>
 __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
     const int* __restrict__ gptr, const int* __restrict__ gdst, const int* __restrict__ tsrc,
     const int* __restrict__ tcid, const double* __restrict__ src, double* __restrict__ dst,
-    const __grid_constant__ TpMats<NB> mt, int mode)
+    const __grid_constant__ TpMats<NB, T> mt, int mode)
 {
     constexpr int N3 = NB * NB * NB;
-    extern __shared__ __align__(16) double sm[];
-    double* a = sm;
-    double* b = a + N3;
+    extern __shared__ __align__(16) unsigned char tp_smem[];
+    T* a = reinterpret_cast<T*>(tp_smem);
+    T* b = a + N3;
     const int g = blockIdx.x;
     const int p = threadIdx.x;
     const bool active = p < NB * NB;
@@ -126,13 +127,18 @@ __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
     {
         const double2* s2 = reinterpret_cast<const double2*>(src + (size_t)tsrc[t] * N3);
         const int cid = tcid[t];
-        for (int i = threadIdx.x; i < N3 / 2; i += blockDim.x) reinterpret_cast<double2*>(a)[i] = s2[i];
+        for (int i = threadIdx.x; i < N3 / 2; i += blockDim.x)
+        {
+            const double2 v = s2[i];
+            a[2 * i] = (T)v.x;
+            a[2 * i + 1] = (T)v.y;
+        }
         __syncthreads();
-        if (active) tp_pass_bit<NB, 0, TR, false, W>(cid & 1, a, b, mt, p, acc);
+        if (active) tp_pass_bit<NB, 0, TR, false, W, T>(cid & 1, a, b, mt, p, acc);
         __syncthreads();
-        if (active) tp_pass_bit<NB, 1, TR, false, W>((cid >> 1) & 1, b, a, mt, p, acc);
+        if (active) tp_pass_bit<NB, 1, TR, false, W, T>((cid >> 1) & 1, b, a, mt, p, acc);
         __syncthreads();
-        if (active) tp_pass_bit<NB, 2, TR, true, W>((cid >> 2) & 1, a, nullptr, mt, p, acc);
+        if (active) tp_pass_bit<NB, 2, TR, true, W, T>((cid >> 2) & 1, a, (T*)nullptr, mt, p, acc);
         __syncthreads();
     }
     if (!active) return;
@@ -260,63 +266,76 @@ void nb_dispatch(int Nb, F&& f)
 }
 }  // namespace
 
-void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base, int mode)
+void launch_tp(Ctx& c, const TpTasks& t, const double* src, double* dst, int mat_base, int mode, bool fp32)
 {
     const int bases[3] = {mat_base, mat_base, mat_base};
-    launch_tp_axes(c, t, src, dst, bases, mode);
+    launch_tp_axes(c, t, src, dst, bases, mode, fp32);
 }
 
-void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode)
+namespace
+{
+template<int NB, class T>
+void launch_tp_typed(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode)
+{
+    static_assert((NB * NB * NB) % 2 == 0, "blocks are copied as double2");
+    TpMats<NB, T> mt;
+    const bool tr = mode != 0;
+    int width = 0;  // widest band of any row, in summation order
+    for (int a = 0; a < 3; ++a)
+    {
+        const size_t off = (size_t)mat_base[a] * NB * NB;
+        if (c.h_mats.size() < off + 2 * NB * NB) throw Error(IBLGF_EINTERNAL, "transfer matrices missing");
+        for (int k = 0; k < 2; ++k)
+            for (int i = 0; i < NB * NB; ++i) mt.m[a][k][i] = (T)c.h_mats[off + (size_t)k * NB * NB + i];
+        for (int k = 0; k < 2; ++k)
+            for (int m = 0; m < NB; ++m)
+            {
+                int lo = NB, hi = 0;
+                for (int n = 0; n < NB; ++n)
+                    if ((tr ? mt.m[a][k][n * NB + m] : mt.m[a][k][m * NB + n]) != (T)0)
+                    {
+                        lo = std::min(lo, n);
+                        hi = n + 1;
+                    }
+                mt.lo[a][k][m] = (unsigned char)(lo < hi ? lo : 0);
+                width = std::max(width, lo < hi ? hi - lo : 0);
+            }
+    }
+    const int W = width <= 2 ? 2 : (width <= 5 ? 5 : 0);
+    if (W)
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < 2; ++k)
+                for (int m = 0; m < NB; ++m) mt.lo[a][k][m] = (unsigned char)std::min<int>(mt.lo[a][k][m], NB - W);
+    const size_t smem = 2 * (size_t)NB * NB * NB * sizeof(T);
+    auto launch = [&](auto kfn) {
+        IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kfn<<<t.n_groups, tp_threads<NB>(), smem, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
+                                                              t.task_cid.p, src, dst, mt, mode);
+    };
+    if (mode == 0)
+    {
+        if (W == 2) launch(tp_kernel<NB, false, 2, T>);
+        else if (W == 5) launch(tp_kernel<NB, false, 5, T>);
+        else launch(tp_kernel<NB, false, 0, T>);
+    }
+    else
+    {
+        if (W == 2) launch(tp_kernel<NB, true, 2, T>);
+        else if (W == 5) launch(tp_kernel<NB, true, 5, T>);
+        else launch(tp_kernel<NB, true, 0, T>);
+    }
+}
+}  // namespace
+
+// fp32: the passes in FP32 (matrices rounded to FP32), the sums into the
+// FP64 receiving blocks in FP64
+void launch_tp_axes(Ctx& c, const TpTasks& t, const double* src, double* dst, const int* mat_base, int mode, bool fp32)
 {
     if (!t.n_groups) return;
     nb_dispatch(c.Nb, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
-        static_assert((NB * NB * NB) % 2 == 0, "blocks are copied as double2");
-        TpMats<NB> mt;
-        const bool tr = mode != 0;
-        int width = 0;  // widest band of any row, in summation order
-        for (int a = 0; a < 3; ++a)
-        {
-            const size_t off = (size_t)mat_base[a] * NB * NB;
-            if (c.h_mats.size() < off + 2 * NB * NB) throw Error(IBLGF_EINTERNAL, "transfer matrices missing");
-            std::memcpy(mt.m[a], c.h_mats.data() + off, sizeof(mt.m[a]));
-            for (int k = 0; k < 2; ++k)
-                for (int m = 0; m < NB; ++m)
-                {
-                    int lo = NB, hi = 0;
-                    for (int n = 0; n < NB; ++n)
-                        if ((tr ? mt.m[a][k][n * NB + m] : mt.m[a][k][m * NB + n]) != 0.0)
-                        {
-                            lo = std::min(lo, n);
-                            hi = n + 1;
-                        }
-                    mt.lo[a][k][m] = (unsigned char)(lo < hi ? lo : 0);
-                    width = std::max(width, lo < hi ? hi - lo : 0);
-                }
-        }
-        const int W = width <= 2 ? 2 : (width <= 5 ? 5 : 0);
-        if (W)
-            for (int a = 0; a < 3; ++a)
-                for (int k = 0; k < 2; ++k)
-                    for (int m = 0; m < NB; ++m) mt.lo[a][k][m] = (unsigned char)std::min<int>(mt.lo[a][k][m], NB - W);
-        const size_t smem = 2 * (size_t)NB * NB * NB * sizeof(double);
-        auto launch = [&](auto kfn) {
-            IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            kfn<<<t.n_groups, tp_threads<NB>(), smem, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
-                                                                  t.task_cid.p, src, dst, mt, mode);
-        };
-        if (mode == 0)
-        {
-            if (W == 2) launch(tp_kernel<NB, false, 2>);
-            else if (W == 5) launch(tp_kernel<NB, false, 5>);
-            else launch(tp_kernel<NB, false, 0>);
-        }
-        else
-        {
-            if (W == 2) launch(tp_kernel<NB, true, 2>);
-            else if (W == 5) launch(tp_kernel<NB, true, 5>);
-            else launch(tp_kernel<NB, true, 0>);
-        }
+        if (fp32) launch_tp_typed<NB, float>(c, t, src, dst, mat_base, mode);
+        else launch_tp_typed<NB, double>(c, t, src, dst, mat_base, mode);
     });
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
