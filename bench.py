@@ -130,6 +130,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
     ap.add_argument("--no-ib", action="store_true", help="skip the immersed-boundary NS step measurement")
+    ap.add_argument("--mac-variant", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
+                    help="pin the sibling-group MAC variant (-1: autotune per plan)")
     ap.add_argument("--ib-only", action="store_true", help="only the immersed-boundary NS step measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
@@ -189,6 +191,7 @@ def main():
     g = B.Solver(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                  n_levels=case.n_levels, predicate=case.predicate, precision=prec, device=local,
                  stream=stream.cuda_stream)
+    g.mac_variant(args.mac_variant)
     src_host = case.fields(g)
     cells = case.n_cells(g)
     sharded = args.shard and world > 1
@@ -283,6 +286,8 @@ def main():
     # ---- roofline of the dominant phase (phase times from CUDA events on the stream)
     hbm, peak_kind = peaks()
     fma = g.fma_peak(prec)
+    # the tensor cores' issue rate at the MAC's product shape and at full width
+    tc_rate = {str(n): g.tc_mma_rate(n) for n in (16, 64, 256)} if rank == 0 else None
     names = ["forward transforms", "spectral MAC", "inverse transforms+interp+add", "zero/copy/anterp"]
     k = int(np.argmax(phases))
     per_step = phases / args.steps
@@ -357,9 +362,15 @@ def main():
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
                 "gpu_launches": int(launches),
                 "mac_autotune": {"variants": "0, 1: direct sibling-group kernel (64 x 768, 32 x 512 FP32); "
-                                             "2: block-Toeplitz kernel (TMA-staged coefficients)",
+                                             "2: block-Toeplitz kernel (TMA-staged coefficients); "
+                                             "3: tensor-core kernel (tcgen05 TF32, 3-product split, "
+                                             "M = 128 groups, N = 16, K = 8 per MMA)",
+                                 "pinned": args.mac_variant,
                                  "plans": tuning},
                 "roofline": roof,
+                "tensor_core_mma_clocks": {"per_instruction_by_N": tc_rate,
+                                           "shape": "tcgen05.mma kind::tf32, M = 128, K = 8, one issuing "
+                                                    "thread per SM"},
                 "clocks": ck.summary(),
                 "cpu_baseline": cpu}
         line.update(extra)

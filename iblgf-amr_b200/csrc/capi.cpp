@@ -54,6 +54,7 @@ namespace iblgf_b200
 void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
 void poisson_release(Ctx& c);
 double measure_fma_peak(Ctx& c, int precision);
+double measure_tc_rate(Ctx& c, int n);
 }  // namespace iblgf_b200
 
 extern "C" {
@@ -619,7 +620,8 @@ int iblgf_domain_set_owner(iblgf_ctx* x, const int* owner, int rank, iblgf_excha
 int iblgf_mac_variant(iblgf_ctx* x, int variant)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
-        if (variant < -1 || variant > 2) throw iblgf_b200::Error(IBLGF_EINVAL, "MAC variant must be -1, 0, 1 or 2");
+        if (variant < -1 || variant > 3)
+            throw iblgf_b200::Error(IBLGF_EINVAL, "MAC variant must be -1, 0, 1, 2 or 3");
         c.mac_variant_forced = variant;
     });
 }
@@ -631,7 +633,7 @@ int iblgf_mac_tuning(iblgf_ctx* x, double* out, int max_rows, int* n_rows)
         const int n = (int)c.mac_tuning.size();
         *n_rows = n;
         for (int i = 0; i < n && i < max_rows; ++i)
-            for (int j = 0; j < 7; ++j) out[7 * i + j] = c.mac_tuning[i][j];
+            for (int j = 0; j < 8; ++j) out[8 * i + j] = c.mac_tuning[i][j];
     });
 }
 
@@ -697,6 +699,15 @@ int iblgf_stats_n(iblgf_ctx* x, long long* out, int n)
 int iblgf_fma_peak(iblgf_ctx* x, int precision, double* tflops)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { *tflops = iblgf_b200::measure_fma_peak(c, precision); });
+}
+
+int iblgf_tc_mma_rate(iblgf_ctx* x, int n, double* clocks)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (!clocks) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        *clocks = iblgf_b200::measure_tc_rate(c, n);
+        iblgf_b200::check_status(c);
+    });
 }
 
 }  // extern "C"

@@ -165,6 +165,12 @@ struct FmmPlan
     DevBuf<int> tile_combo;      // per tile: coefficient table of the block-Toeplitz MAC (its level difference)
     DevBuf<int> tile_parts;      // block-Toeplitz work: tile << 2 | part for the non-empty parts of 14 groups
     int n_parts = 0;
+    // tensor-core MAC: tiles of up to 128 consecutive groups of one LGF table
+    // and pair mode (tc_gptr, tc_tab, tc_mode, tc_pm = union of the groups'
+    // parent masks), and per group its 216 candidate source rows (grp_jr)
+    int n_tc = 0;
+    DevBuf<int> tc_gptr, tc_tab, tc_mode, grp_jr;
+    DevBuf<unsigned> tc_pm;
     long long n_exec = 0;        // (target, source) products the MAC kernels execute
     long long mac_flops = 0;     // floating-point operations of the MAC kernels per frequency
     bool adj_only = false;       // every tile takes adjacent pairs only (integrating factor)
@@ -319,9 +325,9 @@ struct Ctx
     long long launches = 0;
     // group-MAC autotuning: a variant pinned by the caller (-1: tune per
     // plan) and one record per tuned plan: level, mask index, targets, ms of
-    // variants 0, 1, 2 (-1: not applicable), chosen variant
+    // variants 0, 1, 2, 3 (-1: not applicable), chosen variant
     int mac_variant_forced = -1;
-    std::vector<std::array<double, 7>> mac_tuning;
+    std::vector<std::array<double, 8>> mac_tuning;
     // device status word: bounded waits in kernels that run out set bits
     // (kStatusTimeout); read and cleared by check_status()
     DevBuf<int> d_status;
@@ -505,6 +511,14 @@ bool toeplitz_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
 // the coefficient table of level difference ld from the 343 spectrum slots
 // of its offsets (created once per context)
 int combo_table(Ctx& c, int ld, const std::vector<int>& slots);
+// tensor-core sibling-group MAC (FP32 path); false if not applicable
+bool tc_mac_ok(const Ctx& c, const FmmPlan& p);
+bool tc_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
+// tensor-core tiles from the CUDA-core tiles (tile group ranges, tables and
+// modes) and the groups' parent masks
+void build_tc_tiles(const std::vector<int>& tgptr, const std::vector<int>& ttab, const std::vector<int>& tmode,
+                    const std::vector<unsigned>& gpm, std::vector<int>& gptr, std::vector<int>& tab,
+                    std::vector<int>& mode, std::vector<unsigned>& pm);
 // waits for the context stream and throws IBLGF_ETIMEOUT if a kernel's
 // bounded wait ran out since the last check
 void check_status(Ctx& c);

@@ -757,10 +757,12 @@ void launch_forward_sources(Ctx& c, const double* fmm_s, const int* d_src_oct, i
 }
 
 // one run of the sibling-group MAC in the given variant: 0, 1 the direct
-// kernel in its two tile shapes, 2 the block-Toeplitz kernel
+// kernel in its two tile shapes, 2 the block-Toeplitz kernel, 3 the
+// tensor-core kernel
 void group_mac_variant(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc, int variant)
 {
     if (variant == 2 && toeplitz_mac(c, p, src_spec, acc)) return;
+    if (variant == 3 && tc_mac(c, p, src_spec, acc)) return;
     dispatch(c, [&](auto cv) {
         using CV = decltype(cv);
         CV::group_mac(c, p, src_spec, acc, variant);
@@ -771,7 +773,8 @@ void group_mac_variant(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc
 // applicable group-MAC variant runs twice on the sweep's real data, the
 // second run timed with CUDA events on the context stream; the fastest one
 // is kept for the plan (and run last, so that the accumulators hold its
-// result). iblgf_mac_variant() can pin a variant instead.
+// result). iblgf_mac_variant() can pin a variant instead; a pinned variant
+// that does not apply to a plan runs variant 0.
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
 {
     dispatch(c, [&](auto cv) {
@@ -781,22 +784,24 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
     });
     if (p.n_tiles)
     {
-        const bool toep_ok = !p.adj_only && p.tile_combo.p && c.cfg.precision == IBLGF_FP32;
+        const bool ok[4] = {true, true, !p.adj_only && p.tile_combo.p && c.cfg.precision == IBLGF_FP32,
+                            tc_mac_ok(c, p)};
         int v = c.mac_variant_forced;
-        if (v == 2 && !toep_ok) v = 0;
+        if (v >= 0 && !ok[v]) v = 0;
         if (v < 0) v = p.mac_variant;
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         IBLGF_CUDA(cudaStreamIsCapturing(c.stream, &cs));
         if (v < 0 && cs != cudaStreamCaptureStatusNone) v = 0;
         if (v < 0)
         {
-            const int nv = toep_ok ? 3 : 2;
-            double ms[3] = {-1.0, -1.0, -1.0};
+            constexpr int nv = 4;
+            double ms[nv] = {-1.0, -1.0, -1.0, -1.0};
             cudaEvent_t e0, e1;
             IBLGF_CUDA(cudaEventCreate(&e0));
             IBLGF_CUDA(cudaEventCreate(&e1));
             for (int k = 0; k < nv; ++k)
             {
+                if (!ok[k]) continue;
                 group_mac_variant(c, p, src_spec, acc, k);
                 IBLGF_CUDA(cudaEventRecord(e0, c.stream));
                 group_mac_variant(c, p, src_spec, acc, k);
@@ -810,9 +815,9 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
             cudaEventDestroy(e1);
             int best = 0;
             for (int k = 1; k < nv; ++k)
-                if (ms[k] < ms[best]) best = k;
+                if (ok[k] && ms[k] < ms[best]) best = k;
             p.mac_variant = best;
-            c.mac_tuning.push_back({(double)p.level, (double)p.mask_idx, (double)p.n_tgt, ms[0], ms[1], ms[2],
+            c.mac_tuning.push_back({(double)p.level, (double)p.mask_idx, (double)p.n_tgt, ms[0], ms[1], ms[2], ms[3],
                                     (double)best});
             v = best;
         }

@@ -1,7 +1,17 @@
-// FMA-throughput probe: the FP64 / FP32 CUDA-core roofline denominator that
-// the driver-measured peaks (HBM copy, bf16 GEMM) do not cover. Each thread
-// runs 8 independent register-resident FMA chains; grid = 8 CTAs per SM.
+// Throughput probes for roofline denominators the driver-measured peaks (HBM
+// copy, bf16 GEMM) do not cover:
+//  * FMA chains: the FP64 / FP32 CUDA-core peak. Each thread runs 8
+//    independent register-resident FMA chains; grid = 8 CTAs per SM.
+//  * tensor-core issue rate: SM clocks per tcgen05.mma kind::tf32 of shape
+//    M = 128, K = 8 and a given N (A in tensor memory, B in shared memory),
+//    issued back to back by one thread per CTA, one CTA per SM, into a few
+//    independent accumulators. The tensor-core spectral MAC issues N = 16
+//    products; this rate bounds it.
+#include <algorithm>
+#include <vector>
+
 #include "ctx.hpp"
+#include "tcgen05.cuh"
 
 namespace iblgf_b200
 {
@@ -52,7 +62,85 @@ double run(Ctx& c)
     const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
     return flops / (best * 1e-3) / 1e12;
 }
+template<int N, int NACC>
+__global__ void __launch_bounds__(128) tc_rate_kernel(int reps, long long* out, int* status)
+{
+    static_assert(NACC * N <= 448, "accumulator columns below the A columns");
+    __shared__ __align__(1024) float bs[N * 8];
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ unsigned tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int i = tid; i < N * 8; i += blockDim.x) bs[i] = 0.0f;
+    if (warp == 0) tc::alloc(&tmem, 512);
+    if (tid == 0) mbar_init(&bar, 1);
+    fence_proxy_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const unsigned tb = tmem;
+    long long t0 = 0;
+    if (tid == 0)
+    {
+        constexpr unsigned idesc = tc::idesc_tf32(128, N);
+        const unsigned long long bd = tc::smem_desc(bs);
+        t0 = clock64();
+        for (int r = 0; r < reps; ++r)
+            tc::mma_tf32(tb + (unsigned)((r % NACC) * N), tb + 448u, bd, idesc, r >= NACC);
+        tc::commit(&bar);
+    }
+    const bool ok = mbar_wait(&bar, 0);
+    if (tid == 0)
+    {
+        if (!ok) atomicOr(status, kStatusTimeout);
+        out[blockIdx.x] = clock64() - t0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::fence_after();
+        tc::dealloc(tb, 512);
+    }
+}
+
+template<int N, int NACC>
+double tc_rate(Ctx& c)
+{
+    int dev = 0, sms = 0;
+    IBLGF_CUDA(cudaGetDevice(&dev));
+    IBLGF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DevBuf<long long> out;
+    out.alloc(sms);
+    const int reps = 4096;
+    double best = 1e30;
+    for (int rep = 0; rep < 2; ++rep)  // the first run warms up
+    {
+        tc_rate_kernel<N, NACC><<<sms, 128, 0, c.stream>>>(reps, out.p, c.d_status.p);
+        IBLGF_CUDA(cudaGetLastError());
+        std::vector<long long> h(sms);
+        IBLGF_CUDA(cudaMemcpyAsync(h.data(), out.p, sms * sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+        double sum = 0;
+        for (long long v : h) sum += (double)v;
+        best = std::min(best, sum / sms / reps);
+    }
+    c.launches += 2;
+    return best;
+}
 }  // namespace
+
+double measure_tc_rate(Ctx& c, int n)
+{
+    switch (n)
+    {
+        case 16: return tc_rate<16, 4>(c);
+        case 32: return tc_rate<32, 4>(c);
+        case 64: return tc_rate<64, 4>(c);
+        case 128: return tc_rate<128, 2>(c);
+        case 256: return tc_rate<256, 1>(c);
+        default: throw Error(IBLGF_EINVAL, "N must be 16, 32, 64, 128 or 256");
+    }
+}
 
 double measure_fma_peak(Ctx& c, int precision)
 {

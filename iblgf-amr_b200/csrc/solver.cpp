@@ -948,6 +948,25 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
                         jr[((size_t)t * kGroupTileCap + (g - h.tgptr[t])) * 216 + kk] = h.tsrc[h.tsptr[t] + j];
                 }
         p.tile_jr.upload(jr, c.stream);
+        // the same rows per group for the tensor-core MAC, whose tiles span
+        // up to 128 consecutive groups
+        std::vector<int> gjr((size_t)std::max(h.n_groups, 1) * 216, p.n_src);
+        for (int t = 0; t < p.n_tiles; ++t)
+            for (int g = h.tgptr[t]; g < h.tgptr[t + 1]; ++g)
+                std::copy_n(jr.begin() + ((size_t)t * kGroupTileCap + (g - h.tgptr[t])) * 216, 216,
+                            gjr.begin() + (size_t)g * 216);
+        if (p.n_tiles) p.grp_jr.upload(gjr, c.stream);
+        std::vector<int> tg, tt, tm;
+        std::vector<unsigned> tp;
+        build_tc_tiles(h.tgptr, h.ttab, h.tcoarse, h.gpm, tg, tt, tm, tp);
+        p.n_tc = (int)tt.size();
+        if (p.n_tc)
+        {
+            p.tc_gptr.upload(tg, c.stream);
+            p.tc_tab.upload(tt, c.stream);
+            p.tc_mode.upload(tm, c.stream);
+            p.tc_pm.upload(tp, c.stream);
+        }
     }
     p.tile_tab.upload(h.ttab, c.stream);
     p.tile_coarse.upload(h.tcoarse, c.stream);

@@ -31,6 +31,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, u
                  : "memory");
 }
 
+// one plain arrival
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
 {
     unsigned ok;

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
 ]
@@ -124,6 +124,7 @@ def lib():
     L.iblgf_ns_clean_leaf_correction_boundary.argtypes = [vp, vp, ci, ci, ci]
     L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+    L.iblgf_tc_mma_rate.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     _lib = L
     return L
 
@@ -590,7 +591,7 @@ class Solver:
 
     def mac_variant(self, variant):
         """Pin the sibling-group MAC variant (0, 1 direct tile shapes, 2
-        block-Toeplitz; -1 autotunes per plan)."""
+        block-Toeplitz, 3 tensor cores; -1 autotunes per plan)."""
         self._check(lib().iblgf_mac_variant(self.h, int(variant)))
 
     def mac_tuning(self):
@@ -598,10 +599,10 @@ class Solver:
         (None if not applicable) and the chosen variant."""
         n = ctypes.c_int()
         self._check(lib().iblgf_mac_tuning(self.h, None, 0, ctypes.byref(n)))
-        out = np.zeros((max(n.value, 1), 7))
+        out = np.zeros((max(n.value, 1), 8))
         self._check(lib().iblgf_mac_tuning(self.h, _p(out), n.value, ctypes.byref(n)))
         return [{"level": int(r[0]), "mask": int(r[1]), "targets": int(r[2]),
-                 "ms": [None if v < 0 else float(v) for v in r[3:6]], "choice": int(r[6])} for r in out[:n.value]]
+                 "ms": [None if v < 0 else float(v) for v in r[3:7]], "choice": int(r[7])} for r in out[:n.value]]
 
     def ib_converged(self):
         """Whether each of stages 1..3 of the last step converged before
@@ -681,6 +682,12 @@ class Solver:
     def fma_peak(self, precision):
         v = ctypes.c_double()
         self._check(lib().iblgf_fma_peak(self.h, int(precision), ctypes.byref(v)))
+        return v.value
+
+    def tc_mma_rate(self, n):
+        """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""
+        v = ctypes.c_double()
+        self._check(lib().iblgf_tc_mma_rate(self.h, int(n), ctypes.byref(v)))
         return v.value
 
     def profile_read(self):

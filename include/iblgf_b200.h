@@ -389,17 +389,25 @@ int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
  * sweep of each plan the library times every applicable variant of the
  * group MAC on that sweep's data (0: direct kernel, 64 frequencies x 768
  * threads in FP32 / 32 x 512 in FP64; 1: direct kernel, 32 x 512 / 32 x 256;
- * 2: block-Toeplitz kernel with TMA-staged coefficients, FP32 only) and keeps
- * the fastest. iblgf_mac_variant pins a variant for later plans and sweeps
- * (-1: autotune). iblgf_mac_tuning returns one row of 7 doubles per tuned
- * plan: level, mask index, targets, ms of variants 0, 1, 2 (-1: not
- * applicable), chosen variant; n_rows receives the number of rows. */
+ * 2: block-Toeplitz kernel with TMA-staged coefficients, FP32 only; 3:
+ * tensor-core kernel, tcgen05 TF32 MMAs with a 3-product split and FP32
+ * accumulation in tensor memory, FP32 only) and keeps the fastest.
+ * iblgf_mac_variant pins a variant for later plans and sweeps (-1:
+ * autotune; a pinned variant that does not apply to a plan runs variant 0).
+ * iblgf_mac_tuning returns one row of 8 doubles per tuned plan: level, mask
+ * index, targets, ms of variants 0, 1, 2, 3 (-1: not applicable), chosen
+ * variant; n_rows receives the number of rows. */
 int iblgf_mac_variant(iblgf_ctx* ctx, int variant);
 int iblgf_mac_tuning(iblgf_ctx* ctx, double* out, int max_rows, int* n_rows);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the
  * roofline denominator of the CUDA-core kernels. */
 int iblgf_fma_peak(iblgf_ctx* ctx, int precision, double* tflops);
+/* Measures SM clocks per tensor-core MMA (tcgen05.mma kind::tf32, M = 128,
+ * K = 8, the given N in {16, 32, 64, 128, 256}), issued back to back by one
+ * thread per SM: the issue-rate bound of the tensor-core MAC (variant 3),
+ * whose products have N = 16. IBLGF_EINVAL for another N. */
+int iblgf_tc_mma_rate(iblgf_ctx* ctx, int n, double* clocks);
 
 #ifdef __cplusplus
 }

@@ -118,13 +118,13 @@ def test_fmm_impulse(precision, tol):
         assert np.abs(out[blk, 1:-1, 1:-1, 1:-1] - ex).max() < 5e-8 + tol
 
 
-@pytest.mark.parametrize("variant", [-1, 0, 1, 2])
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3])
 @pytest.mark.parametrize("nlas", [0, 1])
 @pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
 def test_fmm_apply_random_amr(nlas, precision, tol, variant):
     """Every sibling-group MAC variant (0, 1: direct kernel tile shapes; 2:
-    block-Toeplitz, FP32 only, the FP64 path runs variant 0 instead; -1: the
-    autotuner's choice) against the oracle."""
+    block-Toeplitz; 3: tensor cores; 2 and 3 are FP32 only, the FP64 path
+    runs variant 0 instead; -1: the autotuner's choice) against the oracle."""
     case = S.GaussianPoisson("amr_small")
     o, g = pair(case, precision)
     g.mac_variant(variant)
@@ -140,8 +140,9 @@ def test_fmm_apply_random_amr(nlas, precision, tol, variant):
         assert rel_linf(out - tgt0, ref - tgt0) < tol, (level, rel_linf(out - tgt0, ref - tgt0))
     if variant < 0:
         rec = g.mac_tuning()
-        assert rec and all(r["choice"] in (0, 1, 2) for r in rec)
+        assert rec and all(r["choice"] in (0, 1, 2, 3) for r in rec)
         assert all((r["ms"][2] is None) == (precision == B.FP64) for r in rec)
+        assert all((r["ms"][3] is None) == (precision == B.FP64) for r in rec)
 
 
 @pytest.mark.parametrize("n_levels", [0, 1])
