@@ -32,6 +32,10 @@ sys.path.insert(0, os.path.join(ROOT, "iblgf-amr_b200"))
 import iblgf_setups as S  # noqa: E402
 
 METRIC = "LGF-FMM cells/s, NS step ms: FP32-batched vs FP64 plain, 1 B200, rel err\u22641e-5"
+# DRAM bytes (read + written) of the spectral MAC per solve, from one ncu capture of the five
+# MAC launches of an amr_3level solve on the FP32 path (dram__bytes_read.sum +
+# dram__bytes_write.sum, profiles/group_mac_dram_amr_3level.md); per solve like `achieved`
+MAC_DRAM_BYTES = {("amr_3level", "fp32", 0): 4232.1e6}
 
 
 def peaks():
@@ -318,7 +322,13 @@ def main():
     else:
         roof = {"bound": "hbm", "achieved": bytes_alg / t_k / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": bytes_alg / t_k / 1e9 / hbm, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
-    roof.update({"kernel": names[k], "traffic": None, "phase_ms_per_step": dict(zip(names, per_step.tolist())),
+    chosen = {r["choice"] for r in tuning} if args.mac_variant < 0 else {args.mac_variant}
+    traffic = MAC_DRAM_BYTES.get((args.workload, args.precision, min(chosen) if len(chosen) == 1 else -1)) \
+        if k == 1 else None
+    roof.update({"kernel": names[k], "traffic": traffic,
+                 "traffic_source": "ncu capture of the MAC launches of one solve (profiles/group_mac_dram_amr_3level.md)"
+                 if traffic else None,
+                 "phase_ms_per_step": dict(zip(names, per_step.tolist())),
                  "algorithmic_flops": flops, "algorithmic_bytes": bytes_alg})
     if k == 1:
         # the pair list's work (8 Nc flops per (target, source) pair) per
