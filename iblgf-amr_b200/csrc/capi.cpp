@@ -55,6 +55,8 @@ void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
 void poisson_release(Ctx& c);
 double measure_fma_peak(Ctx& c, int precision);
 double measure_tc_rate(Ctx& c, int n);
+void wait_selftest(Ctx& c, long long polls);
+long long first_nonfinite(Ctx& c, const double* p, size_t n);
 }  // namespace iblgf_b200
 
 extern "C" {
@@ -699,6 +701,30 @@ int iblgf_stats_n(iblgf_ctx* x, long long* out, int n)
 int iblgf_fma_peak(iblgf_ctx* x, int precision, double* tflops)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { *tflops = iblgf_b200::measure_fma_peak(c, precision); });
+}
+
+int iblgf_wait_selftest(iblgf_ctx* x, long long polls)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        iblgf_b200::wait_selftest(c, polls);
+        iblgf_b200::check_status(c);  // synchronises; IBLGF_ETIMEOUT when the wait ran out
+    });
+}
+
+int iblgf_field_first_nonfinite(iblgf_ctx* x, int f, long long* index)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        if (!index) throw iblgf_b200::Error(IBLGF_EINVAL, "null argument");
+        *index = iblgf_b200::first_nonfinite(c, c.field(f), c.field_elems());
+    });
+}
+
+int iblgf_debug_fail_alloc(long long after)
+{
+    if (after < -1) return IBLGF_EINVAL;
+    iblgf_b200::alloc_fail_countdown().store(after);
+    return IBLGF_OK;
 }
 
 int iblgf_tc_mma_rate(iblgf_ctx* x, int n, double* clocks)

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <atomic>
 #include <cstdint>
 #include <functional>
 #include <map>
@@ -37,6 +38,27 @@ struct Error : std::runtime_error
                                       std::string(#call) + ": " + cudaGetErrorString(e_));   \
     } while (0)
 
+// Fault injection on the host: when armed (>= 0) the countdown is decremented
+// by every device allocation of the library, and the allocation that finds it
+// at 0 fails with IBLGF_ENOMEM instead of calling the allocator (then the
+// countdown disarms itself). Set through iblgf_debug_fail_alloc().
+inline std::atomic<long long>& alloc_fail_countdown()
+{
+    static std::atomic<long long> v{-1};
+    return v;
+}
+inline void simulated_alloc_failure()
+{
+    auto& v = alloc_fail_countdown();
+    long long cur = v.load();
+    while (cur >= 0)
+        if (v.compare_exchange_weak(cur, cur - 1))
+        {
+            if (cur == 0) throw Error(IBLGF_ENOMEM, "simulated device allocation failure (iblgf_debug_fail_alloc)");
+            return;
+        }
+}
+
 // Owning device buffer.
 template<class T>
 struct DevBuf
@@ -64,6 +86,7 @@ struct DevBuf
     {
         release();
         if (count == 0) return;
+        simulated_alloc_failure();
         IBLGF_CUDA(cudaMalloc(&p, count * sizeof(T)));
         n = count;
     }
@@ -236,6 +259,7 @@ struct PoolBuf
         release();
         s = stream;
         if (count == 0) return;
+        simulated_alloc_failure();
         IBLGF_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(double),
                                            field_pool(device), stream));
         n = count;

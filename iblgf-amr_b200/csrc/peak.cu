@@ -62,6 +62,18 @@ double run(Ctx& c)
     const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
     return flops / (best * 1e-3) / 1e12;
 }
+// The bounded-wait path of the kernels that wait on mbarriers, run on
+// purpose: one CTA waits on a barrier that nothing arrives on, `polls`
+// try_wait polls, then records the timeout in the status word and returns.
+__global__ void wait_selftest_kernel(long long polls, int* status)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    const bool ok = mbar_wait(&bar, 0, polls);
+    if (!ok && threadIdx.x == 0) atomicOr(status, kStatusTimeout);
+}
+
 template<int N, int NACC>
 __global__ void __launch_bounds__(128) tc_rate_kernel(int reps, long long* out, int* status)
 {
@@ -128,6 +140,14 @@ double tc_rate(Ctx& c)
     return best;
 }
 }  // namespace
+
+void wait_selftest(Ctx& c, long long polls)
+{
+    if (polls < 1 || polls > kWaitLimit) throw Error(IBLGF_EINVAL, "polls must be in [1, 2^22]");
+    wait_selftest_kernel<<<1, 32, 0, c.stream>>>(polls, c.d_status.p);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
 
 double measure_tc_rate(Ctx& c, int n)
 {

@@ -51,9 +51,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 }
 
 // Bounded wait for the phase of the given parity; false if it ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit = kWaitLimit)
 {
-    for (long long i = 0; i < kWaitLimit; ++i)
+    for (long long i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

@@ -381,7 +381,36 @@ __global__ void fill_zero_kernel(double* __restrict__ p, size_t n)
     else
         for (size_t j = i; j < n; j += stride) p[j] = 0.0;
 }
+// smallest index of a non-finite value (NaN or +-inf); *first starts at ~0
+__global__ void nonfinite_kernel(const double* __restrict__ p, size_t n, unsigned long long* first)
+{
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        if (!isfinite(p[j]))
+        {
+            atomicMin(first, (unsigned long long)j);
+            return;  // later indices of this thread are larger
+        }
+}
 }  // namespace
+
+long long first_nonfinite(Ctx& c, const double* p, size_t n)
+{
+    DevBuf<unsigned long long> d;
+    d.alloc(1);
+    IBLGF_CUDA(cudaMemsetAsync(d.p, 0xFF, sizeof(unsigned long long), c.stream));
+    if (n)
+    {
+        const size_t blocks = std::min<size_t>((n + 255) / 256, 148 * 8);
+        nonfinite_kernel<<<(unsigned)blocks, 256, 0, c.stream>>>(p, n, d.p);
+        c.launches += 1;
+        IBLGF_CUDA(cudaGetLastError());
+    }
+    unsigned long long h = 0;
+    IBLGF_CUDA(cudaMemcpyAsync(&h, d.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
+    return h == ~0ull ? -1 : (long long)h;
+}
 
 // a plain kernel (not cudaMemsetAsync), so that the zeroing can sit in the
 // body of a conditional graph node

@@ -45,7 +45,8 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
 ]
@@ -125,6 +126,9 @@ def lib():
     L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_tc_mma_rate.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+    L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
+    L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
+    L.iblgf_debug_fail_alloc.argtypes = [ctypes.c_longlong]
     _lib = L
     return L
 
@@ -133,11 +137,24 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-ENOTCONVERGED = 6
+# status codes (include/iblgf_b200.h)
+EINVAL, ECUDA, ENOMEM, ETIMEOUT, EINTERNAL, ENOTCONVERGED = 1, 2, 3, 4, 5, 6
+
+
+def debug_fail_alloc(after):
+    """Arm the library's fault injector: the (after + 1)-th device
+    allocation from now fails with ENOMEM (-1 disarms)."""
+    rc = lib().iblgf_debug_fail_alloc(int(after))
+    if rc != 0:
+        raise IblgfError("iblgf_debug_fail_alloc: bad argument", rc)
 
 
 class IblgfError(RuntimeError):
-    pass
+    """A library call failed; `code` is its status (IBLGF_E*)."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 class IblgfNotConverged(IblgfError):
@@ -198,7 +215,7 @@ class Solver:
         h = ctypes.c_void_p()
         rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
-            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()), rc)
         self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
         self._async_out = []  # host buffers of asynchronous downloads in flight
@@ -396,7 +413,7 @@ class Solver:
     # ------------------------------------------------------------ basics
     def _check(self, rc):
         if rc != 0:
-            raise IblgfError("iblgf error %d: %s" % (rc, lib().iblgf_last_error(self.h).decode()))
+            raise IblgfError("iblgf error %d: %s" % (rc, lib().iblgf_last_error(self.h).decode()), rc)
 
     def close(self):
         if getattr(self, "h", None):
@@ -684,6 +701,17 @@ class Solver:
         self._check(lib().iblgf_fma_peak(self.h, int(precision), ctypes.byref(v)))
         return v.value
 
+    def wait_selftest(self, polls):
+        """Run the bounded device wait on a barrier nothing arrives on;
+        raises IblgfError with code ETIMEOUT (the expected outcome)."""
+        self._check(lib().iblgf_wait_selftest(self.h, int(polls)))
+
+    def first_nonfinite(self, fid):
+        """Smallest element index of a NaN / inf in the field, or -1."""
+        v = ctypes.c_longlong()
+        self._check(lib().iblgf_field_first_nonfinite(self.h, fid, ctypes.byref(v)))
+        return v.value
+
     def tc_mma_rate(self, n):
         """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""
         v = ctypes.c_double()
@@ -734,7 +762,7 @@ class BatchSolver(Solver):
         h = ctypes.c_void_p()
         rc = L.iblgf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
-            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()))
+            raise IblgfError("iblgf_create failed (%d): %s" % (rc, L.iblgf_last_error(None).decode()), rc)
         self._destroy = L.iblgf_destroy  # kept so that close() works during interpreter shutdown
         self.h = h
         self._async_out = []  # host buffers of asynchronous downloads in flight

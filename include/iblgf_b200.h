@@ -409,6 +409,22 @@ int iblgf_fma_peak(iblgf_ctx* ctx, int precision, double* tflops);
  * whose products have N = 16. IBLGF_EINVAL for another N. */
 int iblgf_tc_mma_rate(iblgf_ctx* ctx, int n, double* clocks);
 
+/* Failure detection (no reference counterpart: the reference ignores most
+ * CUDA return codes and stops CG silently).
+ * iblgf_wait_selftest runs the library's bounded mbarrier wait on a barrier
+ * nothing arrives on, for `polls` polls (1 .. 2^22), and returns what a
+ * kernel whose wait ran out returns: IBLGF_ETIMEOUT, the status word read
+ * and cleared; the context stays usable.
+ * iblgf_field_first_nonfinite sets *index to the smallest element index
+ * (octant-major, x fastest) of a NaN or infinite value in field f, or -1.
+ * iblgf_debug_fail_alloc arms a process-wide fault injector: the
+ * (after + 1)-th device allocation of the library from now on fails with
+ * IBLGF_ENOMEM without calling the allocator (then it disarms); -1 disarms.
+ * The failing call returns IBLGF_ENOMEM and its context stays destroyable. */
+int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
+int iblgf_field_first_nonfinite(iblgf_ctx* ctx, int f, long long* index);
+int iblgf_debug_fail_alloc(long long after);
+
 #ifdef __cplusplus
 }
 #endif
