@@ -352,6 +352,9 @@ struct Ctx
     // variants 0, 1, 2, 3 (-1: not applicable), chosen variant
     int mac_variant_forced = -1;
     std::vector<std::array<double, 8>> mac_tuning;
+    // the autotuner's choice per (tree level, mask index), reused by plans
+    // rebuilt for the same sweep after an adaptation instead of re-timing
+    std::map<std::pair<int, int>, int> mac_choice;
     // device status word: bounded waits in kernels that run out set bits
     // (kStatusTimeout); read and cleared by check_status()
     DevBuf<int> d_status;

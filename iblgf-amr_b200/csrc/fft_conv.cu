@@ -773,8 +773,10 @@ void group_mac_variant(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc
 // applicable group-MAC variant runs twice on the sweep's real data, the
 // second run timed with CUDA events on the context stream; the fastest one
 // is kept for the plan (and run last, so that the accumulators hold its
-// result). iblgf_mac_variant() can pin a variant instead; a pinned variant
-// that does not apply to a plan runs variant 0.
+// result). A plan rebuilt for the same (level, mask index) sweep, after an
+// adaptation, takes the choice made for its predecessor without re-timing.
+// iblgf_mac_variant() can pin a variant instead; a pinned variant that does
+// not apply to a plan runs variant 0.
 void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
 {
     dispatch(c, [&](auto cv) {
@@ -789,6 +791,11 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
         int v = c.mac_variant_forced;
         if (v >= 0 && !ok[v]) v = 0;
         if (v < 0) v = p.mac_variant;
+        if (v < 0)
+        {
+            auto it = c.mac_choice.find({p.level, p.mask_idx});
+            if (it != c.mac_choice.end() && ok[it->second]) v = p.mac_variant = it->second;
+        }
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         IBLGF_CUDA(cudaStreamIsCapturing(c.stream, &cs));
         if (v < 0 && cs != cudaStreamCaptureStatusNone) v = 0;
@@ -817,6 +824,7 @@ void launch_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc)
             for (int k = 1; k < nv; ++k)
                 if (ok[k] && ms[k] < ms[best]) best = k;
             p.mac_variant = best;
+            c.mac_choice[{p.level, p.mask_idx}] = best;
             c.mac_tuning.push_back({(double)p.level, (double)p.mask_idx, (double)p.n_tgt, ms[0], ms[1], ms[2], ms[3],
                                     (double)best});
             v = best;
