@@ -260,6 +260,14 @@ int iblgf_field_download_leaves(iblgf_ctx* x, int f, double* host, size_t count)
     });
 }
 
+int iblgf_field_upload_leaves_async(iblgf_ctx* x, int f, const double* host, size_t count)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        need_field(c, f);
+        iblgf_b200::field_upload_leaves_async(c, f, host, count);
+    });
+}
+
 int iblgf_field_download_leaves_async(iblgf_ctx* x, int f, double* host, size_t count)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {

@@ -308,6 +308,11 @@ struct Ctx
     PoolBuf leaf_out;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_gathered = nullptr, ev_copied = nullptr;
+    // asynchronous leaf uploads: host -> leaf_in on copy_stream, scattered
+    // into the field on `stream` (which waits for the copy); the next copy
+    // into leaf_in waits for the scatter
+    PoolBuf leaf_in;
+    cudaEvent_t ev_in_copied = nullptr, ev_scattered = nullptr;
 
     // fields
     std::vector<std::unique_ptr<Field>> fields;
@@ -575,6 +580,7 @@ void field_upload_leaves(Ctx& c, int f, const double* host, size_t count);
 void field_download_leaves(Ctx& c, int f, double* host, size_t count);
 void field_download_leaves_async(Ctx& c, int f, double* host, size_t count);
 void copy_stream_release(Ctx& c);
+void field_upload_leaves_async(Ctx& c, int f, const double* host, size_t count);
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n);
 void launch_axpy_blocks(Ctx& c, const double* src, double* dst, const int* list, int n, double a,
                         bool assign);

@@ -550,6 +550,21 @@ void field_download_leaves(Ctx& c, int f, double* host, size_t count)
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+namespace
+{
+void ensure_copy_stream(Ctx& c)
+{
+    if (c.copy_stream) return;
+    IBLGF_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_gathered, cudaEventDisableTiming));
+    IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_copied, cudaEventDisableTiming));
+    IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_in_copied, cudaEventDisableTiming));
+    IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_scattered, cudaEventDisableTiming));
+    IBLGF_CUDA(cudaEventRecord(c.ev_copied, c.copy_stream));
+    IBLGF_CUDA(cudaEventRecord(c.ev_scattered, c.stream));
+}
+}  // namespace
+
 // Gather on the context stream, host copy on a second stream, so that the
 // copy overlaps whatever the context stream runs next (the next upload, the
 // next solve). The gather waits for the previous asynchronous copy out of
@@ -560,13 +575,7 @@ void field_download_leaves_async(Ctx& c, int f, double* host, size_t count)
     const int n = leaf_blocks(c);
     const size_t e = (size_t)c.Nb - 2, vals = (size_t)n * e * e * e;
     if (!host || count != vals) throw Error(IBLGF_EINVAL, "leaf field size mismatch");
-    if (!c.copy_stream)
-    {
-        IBLGF_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
-        IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_gathered, cudaEventDisableTiming));
-        IBLGF_CUDA(cudaEventCreateWithFlags(&c.ev_copied, cudaEventDisableTiming));
-        IBLGF_CUDA(cudaEventRecord(c.ev_copied, c.copy_stream));
-    }
+    ensure_copy_stream(c);
     IBLGF_CUDA(cudaStreamWaitEvent(c.stream, c.ev_copied, 0));
     if (c.leaf_out.n != std::max<size_t>(1, vals)) c.leaf_out.alloc(std::max<size_t>(1, vals), c.cfg.device, c.stream);
     launch_leaves_gather(c, c.field(f), c.leaf_out.p, c.d_leaf_blocks.p, n);
@@ -576,16 +585,47 @@ void field_download_leaves_async(Ctx& c, int f, double* host, size_t count)
     IBLGF_CUDA(cudaEventRecord(c.ev_copied, c.copy_stream));
 }
 
+// Host copy on the copy stream into leaf_in, then zeroing and scatter into
+// the field on the context stream, which waits for the copy; the copy waits
+// for the previous upload's scatter out of leaf_in. Issued right after a
+// solve, the copy of the next input runs under that solve.
+void field_upload_leaves_async(Ctx& c, int f, const double* host, size_t count)
+{
+    if (!c.finalized) throw Error(IBLGF_EINVAL, "domain not finalized");
+    const int n = leaf_blocks(c);
+    const size_t e = (size_t)c.Nb - 2, vals = (size_t)n * e * e * e;
+    if (!host || count != vals) throw Error(IBLGF_EINVAL, "leaf field size mismatch");
+    ensure_copy_stream(c);
+    if (c.leaf_in.n != std::max<size_t>(1, vals))
+    {
+        // stream-ordered on the context stream; the copy stream waits for it
+        IBLGF_CUDA(cudaStreamSynchronize(c.copy_stream));
+        c.leaf_in.alloc(std::max<size_t>(1, vals), c.cfg.device, c.stream);
+        IBLGF_CUDA(cudaEventRecord(c.ev_scattered, c.stream));
+    }
+    IBLGF_CUDA(cudaStreamWaitEvent(c.copy_stream, c.ev_scattered, 0));
+    IBLGF_CUDA(cudaMemcpyAsync(c.leaf_in.p, host, vals * sizeof(double), cudaMemcpyHostToDevice, c.copy_stream));
+    IBLGF_CUDA(cudaEventRecord(c.ev_in_copied, c.copy_stream));
+    IBLGF_CUDA(cudaStreamWaitEvent(c.stream, c.ev_in_copied, 0));
+    IBLGF_CUDA(cudaMemsetAsync(c.field(f), 0, c.field_elems() * sizeof(double), c.stream));
+    launch_leaves_scatter(c, c.leaf_in.p, c.field(f), c.d_leaf_blocks.p, n);
+    IBLGF_CUDA(cudaEventRecord(c.ev_scattered, c.stream));
+}
+
 void copy_stream_release(Ctx& c)
 {
     if (!c.copy_stream) return;
     cudaStreamSynchronize(c.copy_stream);
+    cudaStreamSynchronize(c.stream);
     c.leaf_out.release();
+    c.leaf_in.release();
     cudaEventDestroy(c.ev_gathered);
     cudaEventDestroy(c.ev_copied);
+    cudaEventDestroy(c.ev_in_copied);
+    cudaEventDestroy(c.ev_scattered);
     cudaStreamDestroy(c.copy_stream);
     c.copy_stream = nullptr;
-    c.ev_gathered = c.ev_copied = nullptr;
+    c.ev_gathered = c.ev_copied = c.ev_in_copied = c.ev_scattered = nullptr;
 }
 
 void launch_copy_interior(Ctx& c, const double* src, double* dst, const int* list, int n)

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -84,6 +84,7 @@ def lib():
     L.iblgf_field_upload_leaves.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_download_leaves.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_download_leaves_async.argtypes = [vp, ci, vp, sz]
+    L.iblgf_field_upload_leaves_async.argtypes = [vp, ci, vp, sz]
     L.iblgf_field_device_ptr.argtypes = [vp, ci, pp]
     L.iblgf_fmm_apply.argtypes = [vp, ci, ci, ci, ci, cd, ci]
     L.iblgf_poisson_apply_lgf.argtypes = [vp, ci, ci, ci]
@@ -482,27 +483,42 @@ class Solver:
         self._check(lib().iblgf_field_download_leaves(self.h, fid, _p(a), a.size))
         return a
 
+    def _leaf_host(self, what, buf):
+        """(pointer, count) of a C-contiguous float64 host array or tensor of
+        shape (n_leaves, e, e, e); raises otherwise."""
+        e = self.block_extent
+        shape = (self.n_leaves, e, e, e)
+        if hasattr(buf, "data_ptr"):  # torch tensor
+            import torch
+            ok = (buf.dtype == torch.float64 and buf.is_contiguous() and tuple(buf.shape) == shape
+                  and buf.device.type == "cpu")
+            ptr, n = buf.data_ptr(), buf.numel()
+        else:
+            ok = (isinstance(buf, np.ndarray) and buf.dtype == np.float64 and buf.flags.c_contiguous
+                  and buf.shape == shape)
+            ptr, n = (buf.ctypes.data, buf.size) if ok else (0, 0)
+        if not ok:
+            raise IblgfError("%s: the host buffer must be a C-contiguous float64 array of shape %s" % (what, shape))
+        return ptr, n
+
     def download_leaves_async(self, fid, out):
         """Starts the copy of the leaf interiors into `out` and returns; the
         copy is complete after synchronize(). `out` is a C-contiguous float64
         array or tensor of shape (n_leaves, e, e, e), pinned for the copy to
         overlap; it is kept alive here until synchronize() or close()."""
-        e = self.block_extent
-        shape = (self.n_leaves, e, e, e)
-        if hasattr(out, "data_ptr"):  # torch tensor
-            import torch
-            ok = (out.dtype == torch.float64 and out.is_contiguous() and tuple(out.shape) == shape
-                  and out.device.type == "cpu")
-            ptr, n = out.data_ptr(), out.numel()
-        else:
-            ok = (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
-                  and out.shape == shape)
-            ptr, n = (out.ctypes.data, out.size) if ok else (0, 0)
-        if not ok:
-            raise IblgfError("download_leaves_async: out must be a C-contiguous float64 host array of shape %s"
-                             % (shape,))
+        ptr, n = self._leaf_host("download_leaves_async", out)
         self._check(lib().iblgf_field_download_leaves_async(self.h, fid, ctypes.c_void_p(ptr), n))
         self._async_out.append(out)
+
+    def upload_leaves_async(self, fid, vals):
+        """Starts the copy of leaf interiors from `vals` (pinned, shape
+        (n_leaves, e, e, e)) into the field and returns: the copy runs on the
+        library's copy stream, the scatter is ordered on the solver stream
+        after it. `vals` is kept alive until synchronize() or close() and must
+        not change before then."""
+        ptr, n = self._leaf_host("upload_leaves_async", vals)
+        self._check(lib().iblgf_field_upload_leaves_async(self.h, fid, ctypes.c_void_p(ptr), n))
+        self._async_out.append(vals)
 
     def zero(self, fid):
         self._check(lib().iblgf_field_zero(self.h, fid))

@@ -118,6 +118,13 @@ int iblgf_field_download_leaves(iblgf_ctx* ctx, int field, double* host, size_t 
  * context (overlapping the context stream's next work, e.g. the next upload
  * and solve; `host` should be pinned). iblgf_synchronize waits for it. */
 int iblgf_field_download_leaves_async(iblgf_ctx* ctx, int field, double* host, size_t count);
+/* As iblgf_field_upload_leaves, but returns at once: the copy from `host`
+ * (pinned) runs on the context's second stream, the zeroing and scatter are
+ * ordered on the context stream after it. Issued right after a solve, the
+ * next input's copy runs under that solve. `host` must stay unchanged until
+ * the next synchronising call; a later asynchronous upload waits for this
+ * one's scatter. */
+int iblgf_field_upload_leaves_async(iblgf_ctx* ctx, int field, const double* host, size_t count);
 int iblgf_field_device_ptr(iblgf_ctx* ctx, int field, double** dptr);
 /* Whole Nb^3 blocks of the listed octants (canonical indices) from / to
  * host memory, n blocks back to back: the reference's per-octant

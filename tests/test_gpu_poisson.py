@@ -78,6 +78,37 @@ def test_async_leaf_download_pipeline():
         np.testing.assert_array_equal(o.numpy(), r)
 
 
+def test_async_leaf_upload_download_pipeline():
+    """Three solves with every input uploaded asynchronously (the next input
+    issued right after the current solve, so its copy runs under it) and
+    every solution downloaded asynchronously: each equals the synchronous
+    solve of that input, bit for bit."""
+    import torch
+    case = S.GaussianPoisson("amr_small")
+    g = solver(case, B.FP32)
+    e = g.block_extent
+    rng = np.random.default_rng(9)
+    srcs = [torch.from_numpy(rng.standard_normal((g.n_leaves, e, e, e))).pin_memory() for _ in range(3)]
+    fs, ft = g.field(), g.field()
+    ref = []
+    for x in srcs:
+        g.upload_leaves(fs, x.numpy())
+        g.apply_lgf(fs, ft)
+        ref.append(g.download_leaves(ft))
+    outs = [torch.empty((g.n_leaves, e, e, e), dtype=torch.float64).pin_memory() for _ in srcs]
+    g.upload_leaves_async(fs, srcs[0])
+    for k in range(len(srcs)):
+        g.apply_lgf(fs, ft)
+        if k + 1 < len(srcs):
+            g.upload_leaves_async(fs, srcs[k + 1])
+        g.download_leaves_async(ft, outs[k])
+    g.synchronize()
+    for r, o in zip(ref, outs):
+        np.testing.assert_array_equal(o.numpy(), r)
+    with pytest.raises(B.IblgfError):
+        g.upload_leaves_async(fs, np.zeros((g.n_leaves, e, e, e), np.float32))
+
+
 def test_async_leaf_download_checks_its_buffer():
     """The asynchronous download takes only a C-contiguous float64 host
     buffer of the leaf shape (the copy writes n_leaves e^3 doubles)."""

@@ -56,3 +56,46 @@ def test_conv_block_noalloc_rejects_null():
     g = _solver(8, B.FP64)
     L = B.lib()
     assert L.iblgf_conv_block_noalloc(g.h, None, None, None, 1.0) == 1  # IBLGF_EINVAL
+
+
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
+def test_conv_block_noalloc_is_capturable_without_allocation(precision, tol):
+    """After its one-time set-up call, the entry point allocates, frees and
+    synchronises nothing: a second call recorded under global-mode stream
+    capture (where cudaMalloc, cudaFree and synchronisation from any thread
+    fail the capture) succeeds, and the replayed graph gives the allocating
+    entry point's block."""
+    torch = pytest.importorskip("torch")
+    N = 18
+    P = 2 * N - 1
+    s = torch.cuda.Stream()
+    g = B.Solver((-4 * N,) * 3, (8 * N,) * 3, N - 2, 1.0, [((-2 * N + 4,) * 3, ((N - 2) * 2,) * 3)],
+                 precision=precision, stream=s.cuda_stream)
+    L = B.lib()
+    rng = np.random.default_rng(11)
+    src = torch.tensor(rng.standard_normal(N ** 3), device="cuda", dtype=torch.float64)
+    ker = torch.tensor(rng.standard_normal(P ** 3), device="cuda", dtype=torch.float64)
+    base = rng.standard_normal(N ** 3)
+    out = torch.tensor(base, device="cuda", dtype=torch.float64)
+    ref = torch.tensor(base, device="cuda", dtype=torch.float64)
+
+    def call(o):
+        return L.iblgf_conv_block_noalloc(g.h, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(ker.data_ptr()),
+                                          ctypes.c_void_p(o.data_ptr()), 0.5)
+
+    warm = torch.zeros(N ** 3, device="cuda", dtype=torch.float64)
+    assert call(warm) == 0  # one-time set-up, outside any capture
+    assert L.iblgf_synchronize(g.h) == 0
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s, capture_error_mode="global"):
+        rc = call(out)
+    assert rc == 0, L.iblgf_last_error(g.h)
+    graph.replay()
+    torch.cuda.synchronize()
+    g.conv_block(src.data_ptr(), ker.data_ptr(), ref.data_ptr(), 0.5)
+    assert L.iblgf_synchronize(g.h) == 0
+    a = out.cpu().numpy() - base
+    b = ref.cpu().numpy() - base
+    assert float(np.abs(a - b).max() / np.abs(b).max()) < tol
+    del graph
+    g.close()
