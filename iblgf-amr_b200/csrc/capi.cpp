@@ -636,6 +636,13 @@ int iblgf_mac_variant(iblgf_ctx* x, int variant)
     });
 }
 
+int iblgf_ge_direct(iblgf_ctx* x, int enable)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        c.ge_direct_enabled = enable != 0;
+    });
+}
+
 int iblgf_mac_tuning(iblgf_ctx* x, double* out, int max_rows, int* n_rows)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {

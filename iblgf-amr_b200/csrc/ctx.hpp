@@ -194,6 +194,10 @@ struct FmmPlan
     int n_tc = 0;
     DevBuf<int> tc_gptr, tc_tab, tc_mode, grp_jr;
     DevBuf<unsigned> tc_pm;
+    // neighbour-only plans: the direct separable sweep's targets and their
+    // 27 neighbour sources (octants, -1: none)
+    int n_ge = 0;
+    DevBuf<int> ge_tgt, ge_src;
     long long n_exec = 0;        // (target, source) products the MAC kernels execute
     long long mac_flops = 0;     // floating-point operations of the MAC kernels per frequency
     bool adj_only = false;       // every tile takes adjacent pairs only (integrating factor)
@@ -222,6 +226,9 @@ struct HostPlan
     std::vector<int> tgptr{0}, tsptr{0}, tsrc, ttab, tcoarse, gtgt;
     std::vector<unsigned short> gsrc;
     std::vector<unsigned> gpm;
+    // neighbour-only (integrating factor) plans: per target octant its
+    // source octants by neighbour offset, (ox+1) + 3 (oy+1) + 9 (oz+1), -1: none
+    std::vector<int> ge_tgt, ge_src;
     std::vector<std::array<int, 4>> tab_keys;  // 343 per table
     int n_groups = 0, max_tile_src = 0, n_spec_unique = 0;
     long long n_pairs = 0, n_exec = 0;
@@ -356,6 +363,8 @@ struct Ctx
     // plan) and one record per tuned plan: level, mask index, targets, ms of
     // variants 0, 1, 2, 3 (-1: not applicable), chosen variant
     int mac_variant_forced = -1;
+    // integrating-factor sweeps by direct separable sums when the kernel allows
+    bool ge_direct_enabled = true;
     std::vector<std::array<double, 8>> mac_tuning;
     // the autotuner's choice per (tree level, mask index), reused by plans
     // rebuilt for the same sweep after an adaptation instead of re-timing
@@ -543,6 +552,10 @@ bool toeplitz_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);
 // the coefficient table of level difference ld from the 343 spectrum slots
 // of its offsets (created once per context)
 int combo_table(Ctx& c, int ld, const std::vector<int>& slots);
+// direct separable sweep of a neighbour-only plan with integrating-factor
+// table ge (adds into ft); false if the plan or the table does not allow it
+bool ge_direct_ok(const Ctx& c, int ge);
+bool launch_ge_direct(Ctx& c, const FmmPlan& p, const double* fs, double* ft, int ge, double scale);
 // tensor-core sibling-group MAC (FP32 path); false if not applicable
 bool tc_mac_ok(const Ctx& c, const FmmPlan& p);
 bool tc_mac(Ctx& c, const FmmPlan& p, const void* src_spec, void* acc);

@@ -681,6 +681,26 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
         }
         if (!x.src.empty()) tp.push_back(std::move(x));
     }
+    if (neighbor_only)
+        for (auto& x : tp)
+        {
+            p.ge_tgt.push_back(x.t);
+            const size_t b = p.ge_src.size();
+            p.ge_src.resize(b + 27, -1);
+            for (int s : x.src)
+            {
+                const int o = p.srcs[s];
+                int n = 0, ok = 1;
+                for (int a = 0, w = 1; a < 3; ++a, w *= 3)
+                {
+                    const int d = c.bbase[3 * o + a] - c.bbase[3 * x.t + a];
+                    if (d != 0 && d != e && d != -e) ok = 0;
+                    n += (d / e + 1) * w;
+                }
+                if (!ok || p.ge_src[b + n] != -1) throw Error(IBLGF_EINTERNAL, "neighbour-only source is not an adjacent block");
+                p.ge_src[b + n] = o;
+            }
+        }
     // sibling groups: a target joins its parent's group when the structured
     // candidate set (children of the parent's 27 neighbours; non-adjacent ones
     // only below the sweep level) reproduces its pair list exactly
@@ -928,6 +948,12 @@ std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h)
     }
     p.n_csr_tgt = h.n_csr_tgt;
     p.n_groups = h.n_groups;
+    p.n_ge = (int)h.ge_tgt.size();
+    if (p.n_ge)
+    {
+        p.ge_tgt.upload(h.ge_tgt, c.stream);
+        p.ge_src.upload(h.ge_src, c.stream);
+    }
     p.n_tiles = (int)h.ttab.size();
     p.max_tile_src = h.max_tile_src;
     p.tile_gptr.upload(h.tgptr, c.stream);
@@ -1143,7 +1169,10 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
     for (auto& t : p.antrp) launch_tp(c, t, fs, fs, 0, 0, fp32);
     tm.mark(1);
     const size_t cb = c.cplx_bytes();
-    if (!p.empty())
+    // integrating-factor sweeps whose kernel is negligible beyond 8 cells:
+    // direct separable sums instead of transforms (same result to FP64 rounding)
+    const bool direct = ge >= 0 && c.ge_direct_enabled && p.n_ge && ge_direct_ok(c, ge);
+    if (!p.empty() && !direct)
     {
         // the source spectra and one zero row after them (absent MAC candidates read it)
         ensure_bytes(c.d_src_spec, (size_t)(p.n_src + 1) * c.NC * cb);
@@ -1153,9 +1182,10 @@ void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add
         launch_forward_sources(c, fs, p.src_oct.p, p.n_src, c.d_src_spec.p);
     }
     tm.mark(2);
-    if (!p.empty()) launch_mac(c, p, c.d_src_spec.p, c.d_acc.p);
+    if (!p.empty() && !direct) launch_mac(c, p, c.d_src_spec.p, c.d_acc.p);
     tm.mark(3);
-    if (!p.empty())
+    if (!p.empty() && direct) launch_ge_direct(c, p, fs, ft, ge, 1.0);
+    else if (!p.empty())
     {
         // compute_influence_field (fmm.hpp:1021-1026): dx^2 for LGF_GL, 1 for LGF_GE
         const double scale = (ge >= 0 ? 1.0 : dx_level * dx_level) / ((double)c.P * c.P * c.P);

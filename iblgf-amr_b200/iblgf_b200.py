@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -127,6 +127,7 @@ def lib():
     L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_tc_mma_rate.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+    L.iblgf_ge_direct.argtypes = [vp, ci]
     L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
     L.iblgf_debug_fail_alloc.argtypes = [ctypes.c_longlong]
@@ -621,6 +622,11 @@ class Solver:
 
         self._exchange = EXCHANGE_FN(cb)  # kept alive while the context uses it
         self._check(lib().iblgf_domain_set_owner(self.h, _p(own), int(rank), self._exchange, None))
+
+    def ge_direct(self, enable):
+        """Integrating-factor sweeps by direct separable sums (True, default,
+        where the kernel allows) or by block FFT convolutions (False)."""
+        self._check(lib().iblgf_ge_direct(self.h, 1 if enable else 0))
 
     def mac_variant(self, variant):
         """Pin the sibling-group MAC variant (0, 1 direct tile shapes, 2

@@ -405,6 +405,13 @@ int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
  * index, targets, ms of variants 0, 1, 2, 3 (-1: not applicable), chosen
  * variant; n_rows receives the number of rows. */
 int iblgf_mac_variant(iblgf_ctx* ctx, int variant);
+/* Integrating-factor sweeps (neighbour-only, LGF_GE; fmm.hpp:754-770) whose
+ * 1-D factor e^{-2a} I_m(2a) is below 2^-56 of its centre value for every
+ * m > 8 run as direct separable sums over the 27 neighbour blocks instead of
+ * block FFT convolutions: the same sums up to terms below FP64 rounding
+ * (default on). iblgf_ge_direct(ctx, 0) selects the transform path for all
+ * of them. */
+int iblgf_ge_direct(iblgf_ctx* ctx, int enable);
 int iblgf_mac_tuning(iblgf_ctx* ctx, double* out, int max_rows, int* n_rows);
 /* Measures the device's FMA throughput (TFLOP/s, 2 flops per FMA) for
  * IBLGF_FP64 or IBLGF_FP32 with a register-resident FMA chain kernel; the

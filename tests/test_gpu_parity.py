@@ -324,6 +324,31 @@ def test_integrating_factor_apply_if(precision, tol, alpha):
     assert rel_linf(g.download(ft), ref) < tol
 
 
+@pytest.mark.parametrize("precision", [B.FP64, B.FP32])
+@pytest.mark.parametrize("alpha", [0.002, 0.05])
+def test_integrating_factor_direct_sums_match_transforms(precision, alpha):
+    """The integrating factor's neighbour sweeps as direct separable sums
+    (taken when e^{-2a} I_m(2a) is negligible beyond 8 cells, here on the
+    coarser levels at least) against the same sweeps by block FFT
+    convolution, and against the oracle."""
+    case = S.GaussianPoisson("amr_small")
+    o, g = pair(case, precision)
+    src = case.fields(o)
+    ref = o.apply_if(src, alpha)
+    fs, ft = g.field(src), g.field()
+    out = {}
+    for direct in (False, True):
+        g.ge_direct(direct)
+        g.zero(ft)
+        n0 = g.launches()
+        g.apply_if(fs, ft, alpha)
+        out[direct] = (g.download(ft), g.launches() - n0)
+    assert out[True][1] < out[False][1]  # fewer launches: the direct path ran
+    tol = 1e-13 if precision == B.FP64 else 1e-5
+    assert rel_linf(out[True][0], out[False][0]) < tol
+    assert rel_linf(out[True][0], ref) < (1e-12 if precision == B.FP64 else 1e-5)
+
+
 @pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-12), (B.FP32, 1e-5)])
 def test_poisson_stream_mask(precision, tol):
     """apply_lgf with MASK_TYPE::STREAM (base level only, stream mask: sources
