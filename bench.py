@@ -130,6 +130,7 @@ def main():
                          "an NCCL all-reduce of each sweep's level targets) instead of N independent replicas")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison run")
     ap.add_argument("--no-ns", action="store_true", help="skip the IF-HERK step measurement")
+    ap.add_argument("--no-adapt", action="store_true", help="skip the adaptive IF-HERK march measurement")
     ap.add_argument("--ns-only", action="store_true", help="only the IF-HERK step measurement (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
@@ -179,9 +180,10 @@ def main():
     stream = torch.cuda.Stream()
     if args.ns_only:
         if rank == 0:
-            print(json.dumps({"ns_step": ns_bench(B, stream, local, args.steps, args.warmup),
-                              "ns_step_adaptive": ns_adapt_bench(B, stream, local, args.steps, args.warmup)}),
-                  flush=True)
+            out = {"ns_step": ns_bench(B, stream, local, args.steps, args.warmup)}
+            if not args.no_adapt:
+                out["ns_step_adaptive"] = ns_adapt_bench(B, stream, local, args.steps, args.warmup)
+            print(json.dumps(out), flush=True)
         return
     if args.ib_only:
         if rank == 0:
@@ -359,7 +361,8 @@ def main():
         extra["reference_gpu"] = reference_gpu_baseline(g.Nb, ntgt, npairs, cells, extra.get("fp64_plain"))
     if rank == 0 and not args.no_ns:
         extra["ns_step"] = ns_bench(B, stream, local, args.steps, args.warmup)
-        extra["ns_step_adaptive"] = ns_adapt_bench(B, stream, local, args.steps, args.warmup)
+        if not args.no_adapt:
+            extra["ns_step_adaptive"] = ns_adapt_bench(B, stream, local, args.steps, args.warmup)
     if rank == 0 and not args.no_ib:
         extra["ns_step_ib"] = ib_bench(B, stream, local, args.steps, args.warmup)
     if rank == 0 and not args.no_batch:

@@ -7,10 +7,11 @@
 // E(n) = e^{-6a} I_n1(2a) I_n2(2a) I_n3(2a) = g(n1) g(n2) g(n3) with
 // g(m) = e^{-2a} I_m(2a) (lgf_ge.hpp:158-175). The reference forms it with
 // block FFT convolutions; here it is summed directly, which is exact up to
-// the terms with some |n_k| > R = 8: the host takes this path only when
-// g(m) <= 2^-56 g(0) for every m > R, i.e. when every dropped term lies
-// below FP64 rounding of the result (g(9) / g(0) ~ a^9 / 9!: the IF-HERK
-// steps' integrating factors, a ~ 1e-3 .. 2e-2, give < 1e-21).
+// the terms with some |n_k| > R: the host takes the smallest R in {4, 6, 8}
+// with g(m) <= 2^-56 g(0) for every m > R, i.e. every dropped term lies
+// below FP64 rounding of the result (g(m) / g(0) ~ a^m / m!: the IF-HERK
+// steps' integrating factors, a ~ 5e-4 .. 2e-2, take R = 4 .. 8), and the
+// transform path when none qualifies.
 //
 // Per target block two CTAs (halves of the output x range). Source nodes
 // are indexed by their position s relative to the target block, s in
@@ -30,7 +31,7 @@ namespace iblgf_b200
 {
 namespace
 {
-constexpr int kGeR = 8;
+constexpr int kGeRs[3] = {4, 6, 8};
 
 template<int NB, int R>
 __global__ void __launch_bounds__(256) ge_direct_kernel(const double* __restrict__ fs, double* __restrict__ ft,
@@ -137,36 +138,55 @@ __global__ void __launch_bounds__(256) ge_direct_kernel(const double* __restrict
     }
 }
 
-template<int NB>
+template<int NB, int R>
 void launch_ge_direct_nb(Ctx& c, const FmmPlan& p, const double* fs, double* ft, const double* gtab, double scale)
 {
-    constexpr int Q = NB + 2 * kGeR, H = (NB + 1) / 2;
+    constexpr int Q = NB + 2 * R, H = (NB + 1) / 2;
     const size_t smem = (size_t)H * Q * Q * sizeof(double);
-    auto kfn = ge_direct_kernel<NB, kGeR>;
+    auto kfn = ge_direct_kernel<NB, R>;
     IBLGF_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kfn<<<dim3((unsigned)p.n_ge, 2), 256, smem, c.stream>>>(fs, ft, p.ge_tgt.p, p.ge_src.p, gtab, scale);
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
 }
+
+// the truncation radius of table ge: the smallest R in kGeRs beyond which
+// the 1-D factor is negligible, 0 if none
+int ge_direct_radius(const Ctx& c, int ge)
+{
+    if (ge < 0) return 0;
+    if (c.Nb != 6 && c.Nb != 8 && c.Nb != 10 && c.Nb != 12 && c.Nb != 16 && c.Nb != 18) return 0;
+    const double* f = c.ge_host.data() + (size_t)ge * c.ge_stride;
+    for (int R : kGeRs)
+    {
+        if (c.ge_stride <= R + 1) return 0;
+        bool ok = true;
+        for (int m = R + 1; m < c.ge_stride && ok; ++m) ok = std::fabs(f[m]) <= std::ldexp(std::fabs(f[0]), -56);
+        if (ok) return R;
+    }
+    return 0;
+}
+
+template<int NB>
+void launch_ge_direct_r(Ctx& c, const FmmPlan& p, const double* fs, double* ft, const double* gtab, double scale,
+                        int R)
+{
+    if (R == 4) launch_ge_direct_nb<NB, 4>(c, p, fs, ft, gtab, scale);
+    else if (R == 6) launch_ge_direct_nb<NB, 6>(c, p, fs, ft, gtab, scale);
+    else launch_ge_direct_nb<NB, 8>(c, p, fs, ft, gtab, scale);
+}
 }  // namespace
 
-bool ge_direct_ok(const Ctx& c, int ge)
-{
-    if (ge < 0 || c.ge_stride <= kGeR + 1) return false;
-    if (c.Nb != 6 && c.Nb != 8 && c.Nb != 10 && c.Nb != 12 && c.Nb != 16 && c.Nb != 18) return false;
-    const double* f = c.ge_host.data() + (size_t)ge * c.ge_stride;
-    for (int m = kGeR + 1; m < c.ge_stride; ++m)
-        if (!(std::fabs(f[m]) <= std::ldexp(std::fabs(f[0]), -56))) return false;
-    return true;
-}
+bool ge_direct_ok(const Ctx& c, int ge) { return ge_direct_radius(c, ge) > 0; }
 
 bool launch_ge_direct(Ctx& c, const FmmPlan& p, const double* fs, double* ft, int ge, double scale)
 {
-    if (!p.n_ge || !ge_direct_ok(c, ge)) return false;
+    const int R = ge_direct_radius(c, ge);
+    if (!p.n_ge || !R) return false;
     const double* gtab = c.d_ge.p + (size_t)ge * c.ge_stride;
 #define IBLGF_GE(NBV)                                                \
     case NBV:                                                        \
-        launch_ge_direct_nb<NBV>(c, p, fs, ft, gtab, scale);         \
+        launch_ge_direct_r<NBV>(c, p, fs, ft, gtab, scale, R);       \
         return true;
     switch (c.Nb)
     {

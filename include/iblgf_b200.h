@@ -407,9 +407,9 @@ int iblgf_stats_n(iblgf_ctx* ctx, long long* out, int n);
 int iblgf_mac_variant(iblgf_ctx* ctx, int variant);
 /* Integrating-factor sweeps (neighbour-only, LGF_GE; fmm.hpp:754-770) whose
  * 1-D factor e^{-2a} I_m(2a) is below 2^-56 of its centre value for every
- * m > 8 run as direct separable sums over the 27 neighbour blocks instead of
- * block FFT convolutions: the same sums up to terms below FP64 rounding
- * (default on). iblgf_ge_direct(ctx, 0) selects the transform path for all
+ * m > R, R in {4, 6, 8} (the smallest that holds), run as direct separable
+ * sums over the 27 neighbour blocks instead of block FFT convolutions: the
+ * same sums up to terms below FP64 rounding (default on). iblgf_ge_direct(ctx, 0) selects the transform path for all
  * of them. */
 int iblgf_ge_direct(iblgf_ctx* ctx, int enable);
 int iblgf_mac_tuning(iblgf_ctx* ctx, double* out, int max_rows, int* n_rows);

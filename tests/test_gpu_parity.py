@@ -325,12 +325,13 @@ def test_integrating_factor_apply_if(precision, tol, alpha):
 
 
 @pytest.mark.parametrize("precision", [B.FP64, B.FP32])
-@pytest.mark.parametrize("alpha", [0.002, 0.05])
+@pytest.mark.parametrize("alpha", [0.0004, 0.002, 0.05])
 def test_integrating_factor_direct_sums_match_transforms(precision, alpha):
     """The integrating factor's neighbour sweeps as direct separable sums
-    (taken when e^{-2a} I_m(2a) is negligible beyond 8 cells, here on the
-    coarser levels at least) against the same sweeps by block FFT
-    convolution, and against the oracle."""
+    (taken when e^{-2a} I_m(2a) is negligible beyond R = 4, 6 or 8 cells; the
+    three alphas cover the three radii on the base level, alpha x 4^level on
+    the finer ones) against the same sweeps by block FFT convolution, and
+    against the oracle."""
     case = S.GaussianPoisson("amr_small")
     o, g = pair(case, precision)
     src = case.fields(o)
