@@ -273,6 +273,32 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
+    # ---- launch overhead: the same solve replayed from a CUDA graph (every
+    # launch of one apply_lgf recorded once); equal times mean the step is not
+    # launch-bound, the premise a persistent work-queue sweep would need
+    graph_rec = None
+    if rank == 0 and not sharded:
+        try:
+            g.synchronize()
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg, stream=stream, capture_error_mode="relaxed"):
+                g.apply_lgf(fs, ft)
+            for _ in range(2):
+                cg.replay()
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            with torch.cuda.stream(stream):
+                for _ in range(args.steps):
+                    cg.replay()
+            q1.record(stream)
+            torch.cuda.synchronize()
+            graph_rec = {"ms_per_step_graph_replay": q0.elapsed_time(q1) / args.steps,
+                         "ms_per_step_direct_launches": ms_step, "launches_per_step": launches / args.steps}
+            del cg
+        except Exception as ex:  # a capture the runtime refuses is reported, not fatal
+            graph_rec = {"unavailable": str(ex)[:200]}
+
     # ---- FP64 plain path on the same input, and accuracy of this run against it
     extra = {}
     out64 = None
@@ -389,6 +415,7 @@ def main():
                                              "M = 128 groups, N = 16, K = 8 per MMA)",
                                  "pinned": args.mac_variant,
                                  "plans": tuning},
+                "launch_overhead": graph_rec,
                 "roofline": roof,
                 "tensor_core_mma_clocks": {"per_instruction_by_N": tc_rate,
                                            "shape": "tcgen05.mma kind::tf32, M = 128, K = 8, one issuing "
