@@ -146,6 +146,68 @@ __global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_kernel(
     for (int m = 0; m < NB; ++m) d[m * NB * NB] = acc[m];
 }
 
+// Width-2 band, sending-side form (mode 0, coarsening): thread p = (x', y')
+// owns the receiving z-pencil, as in the last pass of tp_kernel, and forms
+// the three passes' values it needs straight from the sending block in
+// registers, in the passes' order (x band, then y band, then z band, the
+// band entries in summation order): the same FMAs as tp_kernel<NB, false, 2>
+// without the shared-memory staging and its barriers. Sending blocks whose x
+// or y band is zero for the thread (they feed other octants of the
+// receiving block) are skipped: their sums would add exact zeros.
+template<int NB, class T>
+__global__ void __launch_bounds__(tp_threads<NB>(), 2) tp_band2_kernel(
+    const int* __restrict__ gptr, const int* __restrict__ gdst, const int* __restrict__ tsrc,
+    const int* __restrict__ tcid, const double* __restrict__ src, double* __restrict__ dst,
+    const __grid_constant__ TpMats<NB, T> mt)
+{
+    constexpr int N3 = NB * NB * NB;
+    const int g = blockIdx.x;
+    const int p = threadIdx.x;
+    if (p >= NB * NB) return;
+    const int xo = p % NB, yo = p / NB;
+    double* d = dst + (size_t)gdst[g] * N3 + p;
+    double acc[NB];
+#pragma unroll
+    for (int m = 0; m < NB; ++m) acc[m] = d[m * NB * NB];
+    for (int t = gptr[g]; t < gptr[g + 1]; ++t)
+    {
+        const int cid = tcid[t];
+        const int kx = cid & 1, ky = (cid >> 1) & 1, kz = (cid >> 2) & 1;
+        const int lx = mt.lo[0][kx][xo], ly = mt.lo[1][ky][yo];
+        const T wx0 = mt.m[0][kx][xo * NB + lx], wx1 = mt.m[0][kx][xo * NB + lx + 1];
+        const T wy0 = mt.m[1][ky][yo * NB + ly], wy1 = mt.m[1][ky][yo * NB + ly + 1];
+        if ((wx0 == (T)0 && wx1 == (T)0) || (wy0 == (T)0 && wy1 == (T)0)) continue;
+        const double* blk = src + (size_t)tsrc[t] * N3;
+        T cz[NB];
+#pragma unroll
+        for (int nz = 0; nz < NB; ++nz)
+        {
+            const double* r0 = blk + (size_t)(nz * NB + ly) * NB + lx;
+            const double* r1 = r0 + NB;
+            T b0 = 0, b1 = 0;
+            b0 = fma(wx0, (T)__ldg(r0), b0);
+            b0 = fma(wx1, (T)__ldg(r0 + 1), b0);
+            b1 = fma(wx0, (T)__ldg(r1), b1);
+            b1 = fma(wx1, (T)__ldg(r1 + 1), b1);
+            T c = 0;
+            c = fma(wy0, b0, c);
+            c = fma(wy1, b1, c);
+            cz[nz] = c;
+        }
+#pragma unroll
+        for (int m = 0; m < NB; ++m)
+        {
+            const int lz = mt.lo[2][kz][m];
+            T s = 0;
+            s = fma(mt.m[2][kz][m * NB + lz], cz[lz], s);
+            s = fma(mt.m[2][kz][m * NB + lz + 1], cz[lz + 1], s);
+            acc[m] += s;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NB; ++m) d[m * NB * NB] = acc[m];
+}
+
 // threads walk the buffer shell only: the two z = 0, NB-1 planes, then per
 // inner z plane its ring (rows y = 0, NB-1, columns x = 0, NB-1)
 template<int NB>
@@ -314,7 +376,12 @@ void launch_tp_typed(Ctx& c, const TpTasks& t, const double* src, double* dst, c
     };
     if (mode == 0)
     {
-        if (W == 2) launch(tp_kernel<NB, false, 2, T>);
+        if (W == 2)
+        {
+            auto kfn = tp_band2_kernel<NB, T>;
+            kfn<<<t.n_groups, tp_threads<NB>(), 0, c.stream>>>(t.group_ptr.p, t.group_dst.p, t.task_src.p,
+                                                              t.task_cid.p, src, dst, mt);
+        }
         else if (W == 5) launch(tp_kernel<NB, false, 5, T>);
         else launch(tp_kernel<NB, false, 0, T>);
     }
