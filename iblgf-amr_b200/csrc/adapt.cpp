@@ -71,6 +71,8 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
     std::vector<int> old_idx(t.o.size(), -1);
     for (size_t i = 0; i < t.o.size(); ++i)
         if (t.o[i].has_data) old_idx[i] = t.o[i].idx;
+    std::vector<std::tuple<int, int, int>> plan_keys;
+    for (const auto& kv : c.plans) plan_keys.push_back(kv.first);
     c.plans.clear();
     poisson_release(c);
     domain_rebuild(c);
@@ -133,6 +135,8 @@ void domain_adapt(Ctx& c, int n_att, const u64* keys, const int* lchange, int n_
     for (int o = 0; o < c.n_oct; ++o) old_corr[o] = c.levels[o] == t.base_level && old_corr_keys.count(c.keys[o]);
     ns_on_adapt(c, bmu, old_corr);
     ib_on_adapt(c);
+    // the sweeps of the next steps: their plans built now, in parallel
+    prebuild_plans(c, plan_keys);
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
     if (base_mesh_update) *base_mesh_update = bmu ? 1 : 0;
 }

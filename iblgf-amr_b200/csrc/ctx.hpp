@@ -365,6 +365,7 @@ struct Ctx
     int mac_variant_forced = -1;
     // integrating-factor sweeps by direct separable sums when the kernel allows
     bool ge_direct_enabled = true;
+    bool trace = false;  // IBLGF_TRACE: plan-build trace lines on stderr
     std::vector<std::array<double, 8>> mac_tuning;
     // the autotuner's choice per (tree level, mask index), reused by plans
     // rebuilt for the same sweep after an adaptation instead of re-timing
@@ -423,7 +424,10 @@ void fmm_apply(Ctx& c, int src, int tgt, int level, bool nlas, double scale, int
 // one FMM sweep of a ready plan: zero / copy / anterpolate, forward transforms,
 // MAC, inverse transforms + add, interpolate, add into tgt (fmm.hpp:729-870)
 void run_sweep(Ctx& c, FmmPlan& p, int src, int tgt, double dx_level, double add_with_scale, int ge);
-HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge);
+// direct_only: a neighbour-only plan for the direct separable sweep (target
+// and neighbour lists only; no pair lists, groups or spectra)
+HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge, bool direct_only = false);
+void prebuild_plans(Ctx& c, const std::vector<std::tuple<int, int, int>>& keys);
 std::unique_ptr<FmmPlan> upload_plan(Ctx& c, const HostPlan& h);
 void host_tasks(HostTasks& ht, const std::vector<int>& dst, const std::vector<std::vector<std::pair<int, int>>>& tasks);
 void upload_host_tasks(Ctx& c, TpTasks& tt, const HostTasks& ht);

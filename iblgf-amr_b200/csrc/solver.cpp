@@ -12,9 +12,15 @@
 // All device work is ordered on the context stream; a sweep issues no host
 // synchronisation once its plan exists.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <thread>
 
 #include "ctx.hpp"
 
@@ -90,6 +96,10 @@ void append_halves(std::vector<double>& out, const std::vector<double>& full, in
 
 void ctx_init(Ctx& c)
 {
+    // IBLGF_TRACE=1: one stderr line per FMM plan build (host build and
+    // upload times) for tracing set-up and adaptation costs
+    const char* tr = std::getenv("IBLGF_TRACE");
+    c.trace = tr && tr[0] && tr[0] != '0';
     const int e = c.cfg.block_extent;
     c.Nb = e + 2;
     c.P = 2 * c.Nb - 1;
@@ -572,7 +582,7 @@ void upload_host_tasks(Ctx& c, TpTasks& tt, const HostTasks& ht)
     tt.task_cid.upload(ht.cid, c.stream);
 }
 
-HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
+HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge, bool direct_only)
 {
     HostPlan p;
     p.level = level;
@@ -701,6 +711,12 @@ HostPlan build_host_plan(const Ctx& c, int level, int idx, int ge)
                 p.ge_src[b + n] = o;
             }
         }
+    if (neighbor_only && direct_only)
+    {
+        // the direct sweep needs the targets and their neighbour sources only
+        p.tgt_list = p.ge_tgt;
+        return p;
+    }
     // sibling groups: a target joins its parent's group when the structured
     // candidate set (children of the parent's 27 neighbours; non-adjacent ones
     // only below the sweep level) reproduces its pair list exactly
@@ -1062,15 +1078,78 @@ namespace
 {
 FmmPlan& get_plan(Ctx& c, int level, int idx, int ge)
 {
-    auto key = std::make_tuple(idx, level, ge);
+    // neighbour-only plans for the direct sweep are built without the
+    // transform path's pair lists, groups and spectra (keyed apart)
+    const bool direct = ge >= 0 && c.ge_direct_enabled && ge_direct_ok(c, ge);
+    auto key = std::make_tuple(idx, level, ge < 0 ? -1 : 2 * ge + (direct ? 1 : 0));
     auto it = c.plans.find(key);
     if (it != c.plans.end()) return *it->second;
-    auto plan = upload_plan(c, build_host_plan(c, level, idx, ge));
+    const auto t0 = std::chrono::steady_clock::now();
+    HostPlan h = build_host_plan(c, level, idx, ge, direct);
+    const auto t1 = std::chrono::steady_clock::now();
+    auto plan = upload_plan(c, h);
+    if (c.trace)
+    {
+        const auto t2 = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "iblgf plan level %d mask %d ge %d%s: %zu targets, %lld pairs; build %.2f ms, upload %.2f ms\n",
+                     level, idx, ge, direct ? " (direct)" : "", h.tgt_list.size(), h.n_pairs,
+                     std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                     std::chrono::duration<double, std::milli>(t2 - t1).count());
+    }
     auto& ref = *plan;
     c.plans.emplace(key, std::move(plan));
     return ref;
 }
 
+}  // namespace
+
+// Rebuilds the plans of the given keys (the sweeps that existed before an
+// adaptation) for the current octree: the host plans are built on parallel
+// host threads (build_host_plan only reads the context), then uploaded in
+// key order on the context stream. Keys whose level or mask no longer exists
+// are skipped; the first sweep that needs one builds it as before.
+void prebuild_plans(Ctx& c, const std::vector<std::tuple<int, int, int>>& keys)
+{
+    if (!c.owner.empty()) return;
+    std::vector<std::tuple<int, int, int>> todo;
+    for (const auto& k : keys)
+    {
+        const int idx = std::get<0>(k), level = std::get<1>(k);
+        if (idx < 0 || idx >= (int)c.masks.size() || level < c.tree.base_level || level >= c.tree.depth) continue;
+        if (!c.plans.count(k)) todo.push_back(k);
+    }
+    if (todo.empty()) return;
+    std::vector<HostPlan> hp(todo.size());
+    std::vector<std::string> err(todo.size());
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i = next++; i < todo.size(); i = next++)
+        {
+            const int idx = std::get<0>(todo[i]), level = std::get<1>(todo[i]), gk = std::get<2>(todo[i]);
+            try
+            {
+                hp[i] = build_host_plan(c, level, idx, gk < 0 ? -1 : gk / 2, gk >= 0 && (gk & 1));
+            }
+            catch (const std::exception& e)
+            {
+                err[i] = e.what();
+            }
+        }
+    };
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned k = 1; k < std::min<unsigned>(hw, (unsigned)todo.size()); ++k) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (size_t i = 0; i < todo.size(); ++i)
+    {
+        if (!err[i].empty()) continue;  // rebuilt on first use instead
+        c.plans.emplace(todo[i], upload_plan(c, hp[i]));
+    }
+}
+
+namespace
+{
 void ensure_bytes(DevBuf<char>& b, size_t bytes)
 {
     if (b.n < bytes) b.alloc(bytes);
