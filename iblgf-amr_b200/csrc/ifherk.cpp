@@ -25,6 +25,8 @@ namespace iblgf_b200
 {
 void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only, int width = 1);
 void launch_axpby(Ctx& c, double* to, const double* from, double a, int mode);
+void launch_clean_vf(Ctx& c, double* const* f, int n, const int* d_leaf, bool non_leaf_only, int width = 1);
+void launch_axpby_vf(Ctx& c, double* const* to, const double* const* from, int n, double a, int mode);
 void launch_smooth(Ctx& c, double* f, const int* list, const int* ptr, const int* dirs, int n, int reps);
 
 namespace
@@ -365,21 +367,31 @@ class Step
     double coeff_a(int i, int j) const { return a[i * (i - 1) / 2 + j - 1]; }
     double* F(int id) { return c.field(id); }
 
+    // the components of a vector field in one launch each
     void clean(const VF& f, bool non_leaf_only)
     {
-        for (int k = 0; k < f.n; ++k) launch_clean(c, F(f.id[k]), s.leaf.p, non_leaf_only);
+        double* p[3] = {F(f.id[0]), f.n > 1 ? F(f.id[1]) : nullptr, f.n > 2 ? F(f.id[2]) : nullptr};
+        launch_clean_vf(c, p, f.n, s.leaf.p, non_leaf_only);
     }
     void copy(const VF& from, const VF& to, double a_)
     {
-        for (int k = 0; k < from.n; ++k) launch_axpby(c, F(to.id[k]), F(from.id[k]), a_, 0);
+        double* t[3];
+        const double* fr[3];
+        for (int k = 0; k < from.n; ++k) t[k] = F(to.id[k]), fr[k] = F(from.id[k]);
+        launch_axpby_vf(c, t, fr, from.n, a_, 0);
     }
     void add(const VF& from, const VF& to, double a_)
     {
-        for (int k = 0; k < from.n; ++k) launch_axpby(c, F(to.id[k]), F(from.id[k]), a_, 1);
+        double* t[3];
+        const double* fr[3];
+        for (int k = 0; k < from.n; ++k) t[k] = F(to.id[k]), fr[k] = F(from.id[k]);
+        launch_axpby_vf(c, t, fr, from.n, a_, 1);
     }
     void scale(const VF& f, double a_)
     {
-        for (int k = 0; k < f.n; ++k) launch_axpby(c, F(f.id[k]), nullptr, a_, 2);
+        double* t[3];
+        for (int k = 0; k < f.n; ++k) t[k] = F(f.id[k]);
+        launch_axpby_vf(c, t, nullptr, f.n, a_, 2);
     }
     void exchange(const VF& f, int l)
     {

@@ -35,6 +35,44 @@ __global__ void clean_kernel(double* __restrict__ f, const int* __restrict__ lea
     }
 }
 
+// up to three component fields per launch (blockIdx.y = component)
+struct Fields3
+{
+    double* to[3];
+    const double* from[3];
+};
+
+template<int NB>
+__global__ void clean3_kernel(Fields3 f, const int* __restrict__ leaf, int non_leaf_only, int w)
+{
+    constexpr int N3 = NB * NB * NB;
+    const int o = blockIdx.x;
+    double* b = f.to[blockIdx.y] + (size_t)o * N3;
+    const bool shell = non_leaf_only && leaf[o];
+    for (int i = threadIdx.x; i < N3; i += blockDim.x)
+    {
+        if (shell)
+        {
+            const int x = i % NB, y = (i / NB) % NB, z = i / (NB * NB);
+            if (x >= w && y >= w && z >= w && x < NB - w && y < NB - w && z < NB - w) continue;
+        }
+        b[i] = 0.0;
+    }
+}
+
+// mode 0: to = a * from; 1: to += a * from; 2: to *= a (per component)
+__global__ void axpby3_kernel(Fields3 f, double a, size_t n, int mode)
+{
+    double* __restrict__ to = f.to[blockIdx.y];
+    const double* __restrict__ from = f.from[blockIdx.y];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    {
+        if (mode == 0) to[i] = from[i] * a;
+        else if (mode == 1) to[i] += from[i] * a;
+        else to[i] *= a;
+    }
+}
+
 // mode 0: to = a * from; 1: to += a * from; 2: to *= a; 3: to += a
 __global__ void axpby_kernel(double* __restrict__ to, const double* __restrict__ from, double a, size_t n, int mode)
 {
@@ -118,6 +156,36 @@ void launch_clean(Ctx& c, double* f, const int* d_leaf, bool non_leaf_only, int 
         constexpr int NB = decltype(nbc)::value;
         clean_kernel<NB><<<c.n_oct, 256, 0, c.stream>>>(f, d_leaf, non_leaf_only ? 1 : 0, width);
     });
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+// the component fields of one vector field in one launch
+void launch_clean_vf(Ctx& c, double* const* f, int n, const int* d_leaf, bool non_leaf_only, int width)
+{
+    if (!c.n_oct || n < 1 || n > 3) return;
+    Fields3 p{};
+    for (int k = 0; k < n; ++k) p.to[k] = f[k];
+    nb_switch(c.Nb, [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        clean3_kernel<NB><<<dim3(c.n_oct, n), 256, 0, c.stream>>>(p, d_leaf, non_leaf_only ? 1 : 0, width);
+    });
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void launch_axpby_vf(Ctx& c, double* const* to, const double* const* from, int n, double a, int mode)
+{
+    const size_t elems = c.field_elems();
+    if (!elems || n < 1 || n > 3) return;
+    Fields3 p{};
+    for (int k = 0; k < n; ++k)
+    {
+        p.to[k] = to[k];
+        p.from[k] = from ? from[k] : nullptr;
+    }
+    const unsigned grid = (unsigned)std::min<size_t>((elems + 255) / 256, 148 * 16 / n);
+    axpby3_kernel<<<dim3(grid, n), 256, 0, c.stream>>>(p, a, elems, mode);
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
 }
