@@ -55,6 +55,9 @@ void launch_lgf_eval(Ctx& c, const int* d_coords, size_t n, double* d_out);
 void poisson_release(Ctx& c);
 double measure_fma_peak(Ctx& c, int precision);
 double measure_tc_rate(Ctx& c, int n);
+double helm2d_origin(double c);
+void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out);
+void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale);
 void wait_selftest(Ctx& c, long long polls);
 long long first_nonfinite(Ctx& c, const double* p, size_t n);
 }  // namespace iblgf_b200
@@ -716,6 +719,41 @@ int iblgf_stats_n(iblgf_ctx* x, long long* out, int n)
 int iblgf_fma_peak(iblgf_ctx* x, int precision, double* tflops)
 {
     return guard(x, [&](iblgf_b200::Ctx& c) { *tflops = iblgf_b200::measure_fma_peak(c, precision); });
+}
+
+int iblgf_helm2d_origin(double c, double* out)
+{
+    if (!out || !(c > 0.0)) return IBLGF_EINVAL;
+    *out = iblgf_b200::helm2d_origin(c);
+    return IBLGF_OK;
+}
+
+int iblgf_helm2d_lgf(iblgf_ctx* x, double c, int nx, int ny, double* host_out)
+{
+    return guard(x, [&](iblgf_b200::Ctx& cx) {
+        if (!host_out || nx < 1 || ny < 1) throw iblgf_b200::Error(IBLGF_EINVAL, "bad table arguments");
+        iblgf_b200::DevBuf<double> d;
+        d.alloc((size_t)nx * ny);
+        iblgf_b200::helm2d_table(cx, c, nx, ny, d.p);
+        IBLGF_CUDA(cudaMemcpyAsync(host_out, d.p, (size_t)nx * ny * sizeof(double), cudaMemcpyDeviceToHost, cx.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(cx.stream));
+    });
+}
+
+int iblgf_helm2d_apply(iblgf_ctx* x, double c, int nx, int ny, const double* host_f, double* host_u, double scale)
+{
+    return guard(x, [&](iblgf_b200::Ctx& cx) {
+        if (!host_f || !host_u || nx < 1 || ny < 1) throw iblgf_b200::Error(IBLGF_EINVAL, "bad arguments");
+        const size_t n = (size_t)nx * ny;
+        iblgf_b200::DevBuf<double> f, u;
+        f.alloc(n);
+        u.alloc(n);
+        IBLGF_CUDA(cudaMemcpyAsync(f.p, host_f, n * sizeof(double), cudaMemcpyHostToDevice, cx.stream));
+        IBLGF_CUDA(cudaMemcpyAsync(u.p, host_u, n * sizeof(double), cudaMemcpyHostToDevice, cx.stream));
+        iblgf_b200::helm2d_apply(cx, c, nx, ny, f.p, u.p, scale);
+        IBLGF_CUDA(cudaMemcpyAsync(host_u, u.p, n * sizeof(double), cudaMemcpyDeviceToHost, cx.stream));
+        IBLGF_CUDA(cudaStreamSynchronize(cx.stream));
+    });
 }
 
 int iblgf_wait_selftest(iblgf_ctx* x, long long polls)

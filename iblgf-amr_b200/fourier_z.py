@@ -1,0 +1,43 @@
+"""Fourier-in-z solves on a uniform 2-D cell grid through the 2-D Helmholtz
+lattice Green's function (Solver.helm2d_apply, lgf::Helmholtz<2>).
+
+The reference's z-periodic setups (PoissonSolver::apply_lgf_and_helm,
+include/iblgf/solver/poisson/poisson.hpp:173-219) transform the fields along
+z, solve one 2-D problem per z mode with the Helmholtz kernel of that mode's
+wave number (c = k 2 pi dx / L_z, poisson.hpp:107-112) and the 2-D Laplace
+kernel for mode 0, and transform back. Here the 2-D problems are solved
+exactly on a uniform grid (every source cell with every target cell, on the
+device); the reference's 2-D quadtree FMM, which approximates the same sums
+on an adaptive mesh, is not part of this library, nor is mode 0's 2-D Laplace
+kernel (its lookup table is not in the reference tree), so the source must
+have zero mean along z.
+"""
+import numpy as np
+
+
+def mode_wave_numbers(nz, z_operator="second_order"):
+    """c_k per z mode k = 0 .. nz-1 for unit spacing: 'second_order' for the
+    three-point z Laplacian (c_k^2 = 2 - 2 cos(2 pi k / nz)), 'spectral' for
+    the exact z derivative (c_k = 2 pi min(k, nz - k) / nz)."""
+    k = np.arange(nz)
+    if z_operator == "second_order":
+        return 2.0 * np.abs(np.sin(np.pi * k / nz))
+    if z_operator == "spectral":
+        return 2.0 * np.pi * np.minimum(k, nz - k) / nz
+    raise ValueError("z_operator must be 'second_order' or 'spectral'")
+
+
+def solve(solver, f, z_operator="second_order"):
+    """u with (Delta_xy + D_zz) u = f on the unbounded x-y plane (u decaying),
+    periodic in z, unit spacing; f has shape (nz, ny, nx) and zero mean along
+    z at every (y, x)."""
+    f = np.asarray(f, dtype=np.float64)
+    nz = f.shape[0]
+    fh = np.fft.fft(f, axis=0)
+    if np.abs(fh[0]).max() > 1e-12 * max(np.abs(fh).max(), 1e-300):
+        raise ValueError("the source needs zero mean along z (mode 0 would need the 2-D Laplace kernel)")
+    ck = mode_wave_numbers(nz, z_operator)
+    uh = np.zeros_like(fh)
+    for k in range(1, nz):
+        uh[k] = solver.helm2d_apply(ck[k], fh[k].real) + 1j * solver.helm2d_apply(ck[k], fh[k].imag)
+    return np.fft.ifft(uh, axis=0).real

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -127,6 +127,9 @@ def lib():
     L.iblgf_block_norms.argtypes = [vp, vp, ci, vp, vp]
     L.iblgf_fma_peak.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_tc_mma_rate.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+    L.iblgf_helm2d_origin.argtypes = [cd, ctypes.POINTER(ctypes.c_double)]
+    L.iblgf_helm2d_lgf.argtypes = [vp, cd, ci, ci, vp]
+    L.iblgf_helm2d_apply.argtypes = [vp, cd, ci, ci, vp, vp, cd]
     L.iblgf_ge_direct.argtypes = [vp, ci]
     L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
@@ -733,6 +736,20 @@ class Solver:
         v = ctypes.c_longlong()
         self._check(lib().iblgf_field_first_nonfinite(self.h, fid, ctypes.byref(v)))
         return v.value
+
+    def helm2d_lgf(self, c, nx, ny):
+        """2-D Helmholtz LGF get(n, m) (lgf::Helmholtz<2>) for 0 <= n < nx,
+        0 <= m < ny, as an (ny, nx) array."""
+        out = np.zeros((ny, nx))
+        self._check(lib().iblgf_helm2d_lgf(self.h, float(c), int(nx), int(ny), _p(out)))
+        return out
+
+    def helm2d_apply(self, c, f, u=None, scale=1.0):
+        """u + scale * (get * f) over the uniform grid of f (shape (ny, nx))."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        u = np.zeros_like(f) if u is None else np.ascontiguousarray(u, dtype=np.float64).copy()
+        self._check(lib().iblgf_helm2d_apply(self.h, float(c), f.shape[1], f.shape[0], _p(f), _p(u), float(scale)))
+        return u
 
     def tc_mma_rate(self, n):
         """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""

@@ -436,6 +436,22 @@ int iblgf_tc_mma_rate(iblgf_ctx* ctx, int n, double* clocks);
  * IBLGF_ENOMEM without calling the allocator (then it disarms); -1 disarms.
  * The failing call returns IBLGF_ENOMEM and its context stays destroyable. */
 int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
+
+/* Two-dimensional Helmholtz lattice Green's function, the kernel of the
+ * Fourier-in-z solvers (one per z mode; lgf::Helmholtz<2>::get,
+ * include/iblgf/lgf/helmholtz.hpp:152-163, Helmholtz_Lookup
+ * helmholtz_lookup.hpp:45-176): get(n, m) = G_c(n, m) - origin(c), the
+ * decaying solution of the five-point equation (Delta_h - c^2) g = delta.
+ * iblgf_helm2d_origin: origin_val(c) (c > 0).
+ * iblgf_helm2d_lgf: host_out[m * nx + n] = get(n, m), 0 <= n < nx, 0 <= m < ny.
+ * iblgf_helm2d_apply: host_u += scale * sum_j get(i - j) host_f[j] over a
+ * uniform nx x ny cell grid (x fastest; every pair, the exact unbounded
+ * solution of (Delta_h - c^2) u = f on that support); nx <= 6144.
+ * The 2-D quadtree FMM that applies the kernel on an adaptive mesh is not
+ * part of this library. */
+int iblgf_helm2d_origin(double c, double* out);
+int iblgf_helm2d_lgf(iblgf_ctx* ctx, double c, int nx, int ny, double* host_out);
+int iblgf_helm2d_apply(iblgf_ctx* ctx, double c, int nx, int ny, const double* host_f, double* host_u, double scale);
 int iblgf_field_first_nonfinite(iblgf_ctx* ctx, int f, long long* index);
 int iblgf_debug_fail_alloc(long long after);
 

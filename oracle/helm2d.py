@@ -1,0 +1,91 @@
+"""Test infrastructure: the oracle of the 2-D Helmholtz lattice Green's function
+(numpy). Only tests import it; it is never part of the product path.
+
+Restates include/iblgf/lgf/helmholtz_lookup.hpp:
+  * integrandFcn / integralHelmholtzTrap (:134-150): the trapezoidal rule on
+    [-pi, pi] of (1 - cos(m x) / K^n) / (K - 1/K) / (2 pi), a = 4 - 2 cos x + c^2,
+    K = (a + sqrt(a^2 - 4)) / 2, refined (point count doubled) until the
+    relative change falls below the tolerance (boost::math::quadrature::
+    trapezoidal, tolerance 1e-20 in the reference; here until it stops
+    changing in FP64);
+  * origin_val / hypergeometric (:94-119): 0.5 / (2 + c^2/2) times the Gauss
+    series 2F1(1/2, 1/2; 1; z), z = (2 / (2 + c^2/2))^2, summed until a term
+    falls below 1e-20;
+and include/iblgf/lgf/helmholtz.hpp:152-163, Helmholtz<2>::get = the integral
+at (max(|n|, |m|), min(|n|, |m|)) minus origin_val.
+"""
+import math
+
+import numpy as np
+
+
+def origin_val(c):
+    z = (2.0 / (2.0 + c * c / 2.0)) ** 2
+    a, b, cc = 0.5, 0.5, 1.0
+    term = a * b * z / cc
+    value = 1.0 + term
+    n = 1
+    while abs(term) > 1e-20:
+        a, b, cc, n = a + 1.0, b + 1.0, cc + 1.0, n + 1
+        term *= a * b * z / cc / n
+        value += term
+    return 0.5 / (2.0 + c * c / 2.0) * value
+
+
+def integral(n, m, c, tol=1e-16, max_points=1 << 22):
+    """integralHelmholtzTrap(n, m, c): trapezoidal rule refined by doubling."""
+    def trap(npts):
+        x = -math.pi + 2.0 * math.pi * np.arange(npts) / npts
+        a = 4.0 - 2.0 * np.cos(x) + c * c
+        K = 0.5 * (a + np.sqrt(a * a - 4.0))
+        f = (1.0 - np.cos(x * m) / K ** n) * (1.0 / (K - 1.0 / K)) / (2.0 * math.pi)
+        return float(f.sum() * (2.0 * math.pi / npts))
+    npts = 16
+    prev = trap(npts)
+    while npts < max_points:
+        npts *= 2
+        cur = trap(npts)
+        if abs(cur - prev) <= tol * abs(cur):
+            return cur
+        prev = cur
+    return prev
+
+
+def lgf(n, m, c):
+    """Helmholtz<2>::get at the offset (n, m)."""
+    x, y = abs(int(n)), abs(int(m))
+    if x < y:
+        x, y = y, x
+    return integral(x, y, c) - origin_val(c)
+
+
+def table(c, nx, ny):
+    """get(n, m) for 0 <= n < nx, 0 <= m < ny as an (ny, nx) array."""
+    cache = {}
+    out = np.zeros((ny, nx))
+    for m in range(ny):
+        for n in range(nx):
+            key = (max(n, m), min(n, m))
+            if key not in cache:
+                cache[key] = lgf(key[0], key[1], c)
+            out[m, n] = cache[key]
+    return out
+
+
+def apply(c, f):
+    """u = sum_j get(i - j) f(j) over the uniform grid of f (shape (ny, nx))."""
+    ny, nx = f.shape
+    t = table(c, nx, ny)
+    u = np.zeros_like(f, dtype=np.float64)
+    for sy in range(ny):
+        for sx in range(nx):
+            v = f[sy, sx]
+            if v == 0.0:
+                continue
+            u += v * t[np.abs(np.arange(ny) - sy)][:, np.abs(np.arange(nx) - sx)]
+    return u
+
+
+def residual(g, c):
+    """(Delta_h - c^2) applied to g at the interior nodes (five-point)."""
+    return (g[1:-1, 2:] + g[1:-1, :-2] + g[2:, 1:-1] + g[:-2, 1:-1] - (4.0 + c * c) * g[1:-1, 1:-1])

@@ -1,0 +1,68 @@
+"""The 2-D Helmholtz lattice Green's function on the device (the kernel of the
+reference's Fourier-in-z solvers, lgf::Helmholtz<2>) against the oracle
+restating helmholtz_lookup.hpp, and the uniform-grid and Fourier-in-z solves
+built on it against the discrete equations they solve."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import fourier_z
+import iblgf_b200 as B
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+import helm2d as H  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def g():
+    s = B.Solver((-32, -32, -32), (64, 64, 64), 16, 1.0, [((-16, -16, -16), (32, 32, 32))])
+    yield s
+    s.close()
+
+
+@pytest.mark.parametrize("c", [0.05, 0.3, 1.5])
+def test_lgf_table_matches_oracle(g, c):
+    t = g.helm2d_lgf(c, 12, 9)
+    ref = H.table(c, 12, 9)
+    # get(n, m) = G - origin: the reference form cancels digits where G ~ origin
+    assert np.abs(t - ref).max() < 1e-13 * abs(ref[0, 0])
+    o = np.zeros(1)
+    assert abs(B.lib().iblgf_helm2d_origin(c, o.ctypes.data_as(B.ctypes.POINTER(B.ctypes.c_double)))) == 0
+    assert abs(o[0] - H.origin_val(c)) < 1e-15 * o[0]
+
+
+def test_apply_matches_oracle_and_solves_the_equation(g):
+    c = 0.7
+    rng = np.random.default_rng(11)
+    f = rng.standard_normal((10, 12))
+    u0 = rng.standard_normal((10, 12))
+    u = g.helm2d_apply(c, f, u0, 0.5)
+    ref = u0 + 0.5 * H.apply(c, f)
+    assert np.abs(u - ref).max() < 1e-12 * np.abs(ref).max()
+    w = g.helm2d_apply(c, f)
+    assert np.abs(H.residual(w, c) - f[1:-1, 1:-1]).max() < 1e-11 * np.abs(f).max()
+
+
+@pytest.mark.parametrize("z_operator", ["second_order", "spectral"])
+def test_fourier_z_solve(g, z_operator):
+    """A z-periodic 3-D problem through one 2-D Helmholtz solve per z mode:
+    the result satisfies the 3-D equation at every interior x-y cell."""
+    rng = np.random.default_rng(5)
+    nz, ny, nx = 8, 20, 24
+    f = rng.standard_normal((nz, ny, nx))
+    f -= f.mean(axis=0, keepdims=True)
+    u = fourier_z.solve(g, f, z_operator)
+    lap_xy = u[:, 1:-1, 2:] + u[:, 1:-1, :-2] + u[:, 2:, 1:-1] + u[:, :-2, 1:-1] - 4 * u[:, 1:-1, 1:-1]
+    if z_operator == "second_order":
+        dzz = np.roll(u, 1, axis=0) + np.roll(u, -1, axis=0) - 2 * u
+    else:
+        k = fourier_z.mode_wave_numbers(nz, "spectral")
+        dzz = np.fft.ifft(-(k ** 2)[:, None, None] * np.fft.fft(u, axis=0), axis=0).real
+    r = lap_xy + dzz[:, 1:-1, 1:-1] - f[:, 1:-1, 1:-1]
+    assert np.abs(r).max() < 1e-10 * np.abs(f).max()
+    with pytest.raises(ValueError):
+        fourier_z.solve(g, f + 1.0, z_operator)

@@ -1,0 +1,49 @@
+"""The 2-D Helmholtz LGF oracle (restating helmholtz_lookup.hpp /
+helmholtz.hpp) pinned to the mathematics, since the reference stores no
+values of it: get(n, m) = G_c(n, m) - origin_val(c) is the decaying solution
+of the five-point screened Poisson equation (Delta_h - c^2) g = delta, and
+origin_val(c) (the hypergeometric series) equals the quadrature of
+1 / (K - 1/K) / (2 pi). No GPU."""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+import helm2d as H  # noqa: E402
+
+
+@pytest.mark.parametrize("c", [0.1, 0.5, 2.0])
+def test_origin_is_the_centre_integral(c):
+    npts = 1 << 14
+    x = -math.pi + 2 * math.pi * np.arange(npts) / npts
+    a = 4 - 2 * np.cos(x) + c * c
+    K = 0.5 * (a + np.sqrt(a * a - 4))
+    c0 = float((1 / (K - 1 / K)).sum() / npts)
+    # the series sums thousands of terms when z is close to 1 (small c)
+    assert abs(H.origin_val(c) - c0) < 1e-13 * c0
+
+
+@pytest.mark.parametrize("c", [0.1, 0.5, 2.0])
+def test_lgf_solves_the_screened_poisson_equation(c):
+    n = 9
+    g = np.zeros((2 * n + 1, 2 * n + 1))
+    for i in range(-n, n + 1):
+        for j in range(-n, n + 1):
+            g[j + n, i + n] = H.lgf(i, j, c)
+    r = H.residual(g, c)
+    delta = np.zeros_like(r)
+    delta[n - 1, n - 1] = 1.0
+    assert np.abs(r - delta).max() < 1e-12
+    assert np.allclose(g, g.T) and np.allclose(g, g[::-1, :])
+
+
+def test_apply_solves_the_equation_on_its_support():
+    c = 0.7
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((10, 12))
+    u = H.apply(c, f)
+    # the unbounded solution: (Delta_h - c^2) u = f at every interior cell
+    assert np.abs(H.residual(u, c) - f[1:-1, 1:-1]).max() < 1e-11 * np.abs(f).max()
