@@ -19,10 +19,23 @@
 // fixed per c (a power of two with c N >= 48, at least 64): relative error
 // below 1e-16 for c >= ~0.01.
 //
+// Mode 0 (c = 0) is the 2-D lattice Green's function of the five-point
+// Laplacian, LGF_GL<2> (lgf_gl.hpp:93-99, lgf_gl_lookup.hpp:46-60, 121-131):
+// the reference reads it from a table for small offsets (not in the reference
+// tree) and uses -asym(n, m) = log(r) / (2 pi) - Cfund - Integral_val -
+// cos(4 theta) / (24 pi r^2) beyond; both are the regularised LGF
+//     G0(n, m) = 1/pi int_0^pi (1 - e^{-|n| s} cos(m x)) / (2 sinh s) dx,
+//     cosh s = 2 - cos x,
+// with G0(0, 0) = 0 and Delta_h G0 = delta. Its integrand is smooth on
+// [0, pi] but has a |x| kink when continued to [-pi, pi], so G0 uses
+// Gauss-Legendre nodes on [0, pi] (Newton iteration on the Legendre
+// recurrence, computed on the host) instead of the periodic trapezoidal rule.
+//
 // helm2d_table_kernel  get(n, m) for 0 <= n < nx, 0 <= m < ny (one thread each)
 // helm2d_apply_kernel  u(i) = sum_j get(i - j) f(j) over a uniform nx x ny
 //                      cell grid, one thread per target cell, the source row
 //                      staged through shared memory
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -55,6 +68,31 @@ __global__ void helm2d_table_kernel(int nx, int ny, double c, int npts, double* 
     out[i] = -s * h / (2.0 * M_PI);
 }
 
+__global__ void lap2d_table_kernel(int nx, int ny, const double* __restrict__ gx, const double* __restrict__ gw,
+                                   int npts, double* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return;
+    int n = i % nx, m = i / nx;
+    if (n < m)
+    {
+        const int t = n;
+        n = m;
+        m = t;
+    }
+    double s = 0.0;
+    for (int k = 0; k < npts; ++k)
+    {
+        const double x = gx[k];
+        const double hs = sin(0.5 * x);
+        const double t = 2.0 * hs * hs;           // 1 - cos x without cancellation
+        const double r = sqrt(t * (2.0 + t));     // sinh s
+        const double sg = log1p(t + r);           // s = acosh(2 - cos x)
+        s += gw[k] * (1.0 - exp(-n * sg) * cos(m * x)) / (2.0 * r);
+    }
+    out[i] = s / M_PI;
+}
+
 // u[y][x] += scale * sum over sources of table[|dy|][|dx|] f[sy][sx]
 __global__ void helm2d_apply_kernel(int nx, int ny, const double* __restrict__ table, const double* __restrict__ f,
                                     double* __restrict__ u, double scale)
@@ -82,6 +120,38 @@ int trapezoid_points(double c)
     while (n < (1 << 20) && c * n < 48.0) n *= 2;
     return n;
 }
+
+// Gauss-Legendre nodes and weights on [0, pi]: the roots of P_N by Newton's
+// method from the Chebyshev-like first guesses cos(pi (i + 3/4) / (N + 1/2)),
+// P_N and P_N' from the three-term recurrence; weights 2 / ((1 - t^2) P_N'^2)
+void gauss_legendre_0_pi(int N, std::vector<double>& x, std::vector<double>& w)
+{
+    x.assign(N, 0.0);
+    w.assign(N, 0.0);
+    for (int i = 0; i < (N + 1) / 2; ++i)
+    {
+        double t = std::cos(M_PI * (i + 0.75) / (N + 0.5)), dp = 0.0;
+        for (int it = 0; it < 100; ++it)
+        {
+            double p0 = 1.0, p1 = t;
+            for (int k = 2; k <= N; ++k)
+            {
+                const double p2 = ((2.0 * k - 1.0) * t * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = N * (t * p1 - p0) / (t * t - 1.0);
+            const double dt = p1 / dp;
+            t -= dt;
+            if (std::fabs(dt) < 1e-16) break;
+        }
+        const double wt = 2.0 / ((1.0 - t * t) * dp * dp);
+        // t and -t, mapped from [-1, 1] to [0, pi]
+        x[i] = 0.5 * M_PI * (1.0 - t);
+        x[N - 1 - i] = 0.5 * M_PI * (1.0 + t);
+        w[i] = w[N - 1 - i] = 0.5 * M_PI * wt;
+    }
+}
 }  // namespace
 
 // origin_val (helmholtz_lookup.hpp:94-119): the Gauss hypergeometric series
@@ -101,9 +171,22 @@ double helm2d_origin(double c)
 
 void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
 {
-    if (!(cz > 0.0) || nx < 1 || ny < 1) throw Error(IBLGF_EINVAL, "need c > 0 and a non-empty table");
+    if (!(cz >= 0.0) || nx < 1 || ny < 1) throw Error(IBLGF_EINVAL, "need c >= 0 and a non-empty table");
     const int total = nx * ny;
-    helm2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, cz, trapezoid_points(cz), dev_out);
+    if (cz > 0.0)
+        helm2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, cz, trapezoid_points(cz), dev_out);
+    else
+    {
+        // node count grows with the offsets (the integrand varies on a scale 1 / |n| near 0)
+        const int npts = std::min(8192, 96 + 6 * std::max(nx, ny));
+        std::vector<double> x, w;
+        gauss_legendre_0_pi(npts, x, w);
+        x.insert(x.end(), w.begin(), w.end());
+        DevBuf<double> d;
+        d.upload(x, c.stream);
+        lap2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, d.p, d.p + npts, npts, dev_out);
+        IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // the nodes are freed on return
+    }
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
 }

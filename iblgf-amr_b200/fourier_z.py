@@ -7,10 +7,10 @@ z, solve one 2-D problem per z mode with the Helmholtz kernel of that mode's
 wave number (c = k 2 pi dx / L_z, poisson.hpp:107-112) and the 2-D Laplace
 kernel for mode 0, and transform back. Here the 2-D problems are solved
 exactly on a uniform grid (every source cell with every target cell, on the
-device); the reference's 2-D quadtree FMM, which approximates the same sums
-on an adaptive mesh, is not part of this library, nor is mode 0's 2-D Laplace
-kernel (its lookup table is not in the reference tree), so the source must
-have zero mean along z.
+device; mode 0 with the 2-D Laplace LGF, c = 0); the reference's 2-D quadtree
+FMM, which approximates the same sums on an adaptive mesh, is not part of
+this library. Mode 0's solution is the unbounded one (it grows like the log
+of the distance when the source's total is not zero).
 """
 import numpy as np
 
@@ -28,16 +28,13 @@ def mode_wave_numbers(nz, z_operator="second_order"):
 
 
 def solve(solver, f, z_operator="second_order"):
-    """u with (Delta_xy + D_zz) u = f on the unbounded x-y plane (u decaying),
-    periodic in z, unit spacing; f has shape (nz, ny, nx) and zero mean along
-    z at every (y, x)."""
+    """u with (Delta_xy + D_zz) u = f on the unbounded x-y plane, periodic
+    in z, unit spacing; f has shape (nz, ny, nx)."""
     f = np.asarray(f, dtype=np.float64)
     nz = f.shape[0]
     fh = np.fft.fft(f, axis=0)
-    if np.abs(fh[0]).max() > 1e-12 * max(np.abs(fh).max(), 1e-300):
-        raise ValueError("the source needs zero mean along z (mode 0 would need the 2-D Laplace kernel)")
     ck = mode_wave_numbers(nz, z_operator)
     uh = np.zeros_like(fh)
-    for k in range(1, nz):
+    for k in range(nz):
         uh[k] = solver.helm2d_apply(ck[k], fh[k].real) + 1j * solver.helm2d_apply(ck[k], fh[k].imag)
     return np.fft.ifft(uh, axis=0).real

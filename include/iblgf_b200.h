@@ -441,7 +441,10 @@ int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
  * Fourier-in-z solvers (one per z mode; lgf::Helmholtz<2>::get,
  * include/iblgf/lgf/helmholtz.hpp:152-163, Helmholtz_Lookup
  * helmholtz_lookup.hpp:45-176): get(n, m) = G_c(n, m) - origin(c), the
- * decaying solution of the five-point equation (Delta_h - c^2) g = delta.
+ * decaying solution of the five-point equation (Delta_h - c^2) g = delta;
+ * c = 0 gives mode 0's kernel, the 2-D LGF of the five-point Laplacian
+ * (LGF_GL<2>::get at level difference 0, lgf_gl.hpp:93-99: the regularised
+ * G0 with G0(0, 0) = 0, log r / (2 pi) + 0.2573... far away).
  * iblgf_helm2d_origin: origin_val(c) (c > 0).
  * iblgf_helm2d_lgf: host_out[m * nx + n] = get(n, m), 0 <= n < nx, 0 <= m < ny.
  * iblgf_helm2d_apply: host_u += scale * sum_j get(i - j) host_f[j] over a

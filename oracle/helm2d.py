@@ -12,8 +12,13 @@ Restates include/iblgf/lgf/helmholtz_lookup.hpp:
     series 2F1(1/2, 1/2; 1; z), z = (2 / (2 + c^2/2))^2, summed until a term
     falls below 1e-20;
 and include/iblgf/lgf/helmholtz.hpp:152-163, Helmholtz<2>::get = the integral
-at (max(|n|, |m|), min(|n|, |m|)) minus origin_val.
+at (max(|n|, |m|), min(|n|, |m|)) minus origin_val. For c = 0 (mode 0, LGF_GL<2>,
+include/iblgf/lgf/lgf_gl.hpp:93-99, lgf_gl_lookup.hpp:46-60, 121-131) the
+regularised 2-D LGF G0(n, m) = 1/pi int_0^pi (1 - e^{-|n| s} cos(m x)) /
+(2 sinh s) dx, cosh s = 2 - cos x, by Gauss-Legendre quadrature (numpy), and
+the reference's far-field expansion asym() restated for comparison.
 """
+import functools
 import math
 
 import numpy as np
@@ -51,8 +56,39 @@ def integral(n, m, c, tol=1e-16, max_points=1 << 22):
     return prev
 
 
+@functools.lru_cache(maxsize=64)
+def _gauss_legendre_0_pi(npts):
+    x, w = np.polynomial.legendre.leggauss(npts)
+    x = (x + 1.0) * math.pi / 2.0
+    t = 2.0 * np.sin(x / 2.0) ** 2      # 1 - cos x, without cancellation
+    r = np.sqrt(t * (2.0 + t))          # sinh s
+    return x, w * math.pi / 2.0, np.log1p(t + r), r
+
+
+def lap_lgf(n, m, npts=None):
+    """G0(n, m), the 2-D LGF of the five-point Laplacian with G0(0, 0) = 0
+    (node count growing with the offset; numpy's nodes lose accuracy for
+    counts in the thousands)."""
+    n, m = abs(int(n)), abs(int(m))
+    if n < m:
+        n, m = m, n
+    x, w, s, r = _gauss_legendre_0_pi(npts or 256 + 8 * n)
+    return float((w * (1.0 - np.exp(-n * s) * np.cos(m * x)) / (2.0 * r)).sum() / math.pi)
+
+
+def lap_asym(n1, n2):
+    """-LGF_GL_Lookup::asym(n1, n2) (lgf_gl_lookup.hpp:121-131): the
+    reference's mode-0 kernel beyond its table."""
+    c_fund, integral_val = -0.18124942796, -0.076093998454228
+    r = math.sqrt(n1 * n1 + n2 * n2)
+    theta = math.atan2(n2, n1)
+    return -(-0.5 / math.pi * math.log(r) + c_fund + integral_val + 1.0 / 24.0 / math.pi * math.cos(4 * theta) / r / r)
+
+
 def lgf(n, m, c):
-    """Helmholtz<2>::get at the offset (n, m)."""
+    """Helmholtz<2>::get at the offset (n, m); c = 0: G0."""
+    if c == 0.0:
+        return lap_lgf(n, m)
     x, y = abs(int(n)), abs(int(m))
     if x < y:
         x, y = y, x

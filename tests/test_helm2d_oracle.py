@@ -40,6 +40,22 @@ def test_lgf_solves_the_screened_poisson_equation(c):
     assert np.allclose(g, g.T) and np.allclose(g, g[::-1, :])
 
 
+def test_mode0_kernel_is_the_laplace_lgf():
+    """c = 0: the regularised 2-D LGF (G0(0, 0) = 0, Delta_h G0 = delta),
+    equal to the reference's far-field expansion (its table is not in the
+    reference tree) to the expansion's own error, O(r^-4)."""
+    n = 6
+    g = np.array([[H.lap_lgf(i, j) for i in range(-n, n + 1)] for j in range(-n, n + 1)])
+    r = H.residual(g, 0.0)
+    delta = np.zeros_like(r)
+    delta[n - 1, n - 1] = 1.0
+    assert abs(g[n, n]) == 0.0 and np.abs(r - delta).max() < 1e-13
+    assert abs(H.lap_lgf(1, 0) - 0.25) < 1e-13  # G0(1, 0) = 1/4 exactly
+    for (a, b) in [(30, 0), (40, 17), (60, 60), (100, 3)]:
+        # the expansion stops at r^-2: its remainder is O(r^-4)
+        assert abs(H.lap_lgf(a, b) - H.lap_asym(a, b)) < 0.05 / (a * a + b * b) ** 2
+
+
 def test_apply_solves_the_equation_on_its_support():
     c = 0.7
     rng = np.random.default_rng(3)
