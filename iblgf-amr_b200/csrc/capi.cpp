@@ -58,6 +58,8 @@ double measure_tc_rate(Ctx& c, int n);
 double helm2d_origin(double c);
 void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out);
 void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale);
+void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
+               const double* dev_src, double* dev_dst);
 void wait_selftest(Ctx& c, long long polls);
 long long first_nonfinite(Ctx& c, const double* p, size_t n);
 }  // namespace iblgf_b200
@@ -753,6 +755,15 @@ int iblgf_helm2d_apply(iblgf_ctx* x, double c, int nx, int ny, const double* hos
         iblgf_b200::helm2d_apply(cx, c, nx, ny, f.p, u.p, scale);
         IBLGF_CUDA(cudaMemcpyAsync(host_u, u.p, n * sizeof(double), cudaMemcpyDeviceToHost, cx.stream));
         IBLGF_CUDA(cudaStreamSynchronize(cx.stream));
+    });
+}
+
+int iblgf_helm2d_op(iblgf_ctx* x, int op, int nb, int n_blocks, int n_modes, double dx_level, double lz,
+                    double scale, const double* dev_src, double* dev_dst)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (n_blocks && (!dev_src || !dev_dst)) throw iblgf_b200::Error(IBLGF_EINVAL, "null field");
+        iblgf_b200::helm2d_op(c, op, nb, n_blocks, n_modes, dx_level, lz, scale, dev_src, dev_dst);
     });
 }
 

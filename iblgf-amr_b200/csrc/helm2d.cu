@@ -114,6 +114,87 @@ __global__ void helm2d_apply_kernel(int nx, int ny, const double* __restrict__ t
     if (x < nx) u[(size_t)y * nx + x] += scale * acc;
 }
 
+// Complex Helmholtz (Fourier-in-z) block operators on 2-D blocks
+// (include/iblgf/operators/operators.hpp:1516-1545 laplace, :1585-1614
+// gradient, :1763-1795 divergence, :1972-2008 curl, :2178-2217
+// curl_transpose, the all-modes forms): a block holds [component][NB][NB],
+// x fastest; a scalar field has sep = 2 N_modes components (mode i: real 2i,
+// imaginary 2i+1), a vector field three groups of sep (x, y, z); the z
+// derivative of mode i is multiplication by i omega_i, omega_i = 2 pi i / lz.
+// One CTA per block, threads over the interior nodes (1 .. NB-2 per axis);
+// buffers are read, not written.
+// op: 0 laplace (cell -> cell), 1 gradient (cell -> face), 2 divergence
+// (face -> cell), 3 curl (face -> edge), 4 curl_transpose (edge -> face, x scale)
+template<int OP>
+__global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, double dx, double lz, double scale,
+                               const double* __restrict__ src, double* __restrict__ dst)
+{
+    const int sep = 2 * n_modes, N2 = nb * nb;
+    const double* s = src + (size_t)blockIdx.x * in_comp * N2;
+    double* d = dst + (size_t)blockIdx.x * out_comp * N2;
+    const double fac = 1.0 / dx;
+    for (int p = threadIdx.x; p < N2; p += blockDim.x)
+    {
+        const int x = p % nb, y = p / nb;
+        if (x == 0 || y == 0 || x == nb - 1 || y == nb - 1) continue;
+        auto at = [&](int c, int ox, int oy) { return s[(size_t)c * N2 + p + ox + oy * nb]; };
+        auto out = [&](int c) -> double& { return d[(size_t)c * N2 + p]; };
+        for (int i = 0; i < sep; ++i)
+        {
+            if (OP == 0)
+                out(i) = fac * fac * (-4.0 * at(i, 0, 0) + at(i, 0, -1) + at(i, 0, 1) + at(i, -1, 0) + at(i, 1, 0));
+            else if (OP == 1)
+            {
+                out(i) = fac * (at(i, 0, 0) - at(i, -1, 0));
+                out(sep + i) = fac * (at(i, 0, 0) - at(i, 0, -1));
+            }
+            else if (OP == 2)
+                out(i) = fac * (-at(i, 0, 0) - at(sep + i, 0, 0) + at(i, 1, 0) + at(sep + i, 0, 1));
+            else if (OP == 3)
+            {
+                out(i) = fac * (at(2 * sep + i, 0, 0) - at(2 * sep + i, 0, -1));
+                out(sep + i) = fac * (-at(2 * sep + i, 0, 0) + at(2 * sep + i, -1, 0));
+                out(2 * sep + i) = fac * (at(sep + i, 0, 0) - at(sep + i, -1, 0) - at(i, 0, 0) + at(i, 0, -1));
+            }
+            else
+            {
+                const double f = fac * scale;
+                out(i) = f * (-at(2 * sep + i, 0, 0) + at(2 * sep + i, 0, 1));
+                out(sep + i) = f * (at(2 * sep + i, 0, 0) - at(2 * sep + i, 1, 0));
+                out(2 * sep + i) = f * (-at(sep + i, 0, 0) + at(sep + i, 1, 0) + at(i, 0, 0) - at(i, 0, 1));
+            }
+        }
+        for (int i = 0; i < n_modes; ++i)
+        {
+            const double om = 2.0 * M_PI * i / lz;
+            const int re = 2 * i, im = 2 * i + 1;
+            if (OP == 0)
+            {
+                out(re) -= at(re, 0, 0) * om * om;
+                out(im) -= at(im, 0, 0) * om * om;
+            }
+            else if (OP == 1)
+            {
+                out(2 * sep + re) = -at(im, 0, 0) * om;
+                out(2 * sep + im) = at(re, 0, 0) * om;
+            }
+            else if (OP == 2)
+            {
+                out(re) -= at(2 * sep + im, 0, 0) * om;
+                out(im) += at(2 * sep + re, 0, 0) * om;
+            }
+            else
+            {
+                const double w = OP == 3 ? om : om * scale;
+                out(re) += at(sep + im, 0, 0) * w;
+                out(im) -= at(sep + re, 0, 0) * w;
+                out(sep + re) -= at(im, 0, 0) * w;
+                out(sep + im) += at(re, 0, 0) * w;
+            }
+        }
+    }
+}
+
 int trapezoid_points(double c)
 {
     int n = 64;
@@ -186,6 +267,30 @@ void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
         d.upload(x, c.stream);
         lap2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, d.p, d.p + npts, npts, dev_out);
         IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // the nodes are freed on return
+    }
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
+               const double* dev_src, double* dev_dst)
+{
+    if (op < 0 || op > 4 || nb < 3 || n_blocks < 0 || n_modes < 1 || !(dx > 0.0) || !(lz > 0.0))
+        throw Error(IBLGF_EINVAL, "bad Helmholtz operator arguments");
+    if (!n_blocks) return;
+    const int sep = 2 * n_modes;
+    const int in_comp = (op == 0 || op == 1) ? sep : 3 * sep;
+    const int out_comp = (op == 0 || op == 2) ? sep : 3 * sep;
+    auto go = [&](auto kfn) {
+        kfn<<<n_blocks, 256, 0, c.stream>>>(nb, n_modes, in_comp, out_comp, dx, lz, scale, dev_src, dev_dst);
+    };
+    switch (op)
+    {
+        case 0: go(helm_op_kernel<0>); break;
+        case 1: go(helm_op_kernel<1>); break;
+        case 2: go(helm_op_kernel<2>); break;
+        case 3: go(helm_op_kernel<3>); break;
+        default: go(helm_op_kernel<4>); break;
     }
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -130,6 +130,7 @@ def lib():
     L.iblgf_helm2d_origin.argtypes = [cd, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_helm2d_lgf.argtypes = [vp, cd, ci, ci, vp]
     L.iblgf_helm2d_apply.argtypes = [vp, cd, ci, ci, vp, vp, cd]
+    L.iblgf_helm2d_op.argtypes = [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp]
     L.iblgf_ge_direct.argtypes = [vp, ci]
     L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
@@ -750,6 +751,19 @@ class Solver:
         u = np.zeros_like(f) if u is None else np.ascontiguousarray(u, dtype=np.float64).copy()
         self._check(lib().iblgf_helm2d_apply(self.h, float(c), f.shape[1], f.shape[0], _p(f), _p(u), float(scale)))
         return u
+
+    HELM_OPS = {"laplace": 0, "gradient": 1, "divergence": 2, "curl": 3, "curl_transpose": 4}
+
+    def helm2d_op(self, op, src, dst, n_modes, dx_level, lz, scale=1.0):
+        """A complex Helmholtz block operator on 2-D blocks (torch CUDA
+        tensors [n_blocks][ncomp][nb][nb], float64); dst updated in place."""
+        import torch
+        for t in (src, dst):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise IblgfError("helm2d_op takes contiguous float64 CUDA tensors")
+        self._check(lib().iblgf_helm2d_op(self.h, self.HELM_OPS[op], src.shape[-1], src.shape[0], int(n_modes),
+                                          float(dx_level), float(lz), float(scale),
+                                          ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
 
     def tc_mma_rate(self, n):
         """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""

@@ -455,6 +455,18 @@ int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
 int iblgf_helm2d_origin(double c, double* out);
 int iblgf_helm2d_lgf(iblgf_ctx* ctx, double c, int nx, int ny, double* host_out);
 int iblgf_helm2d_apply(iblgf_ctx* ctx, double c, int nx, int ny, const double* host_f, double* host_u, double scale);
+/* Complex Helmholtz (Fourier-in-z) block operators on 2-D blocks
+ * (domain::Operator::laplace_helmholtz_complex, gradient_, divergence_,
+ * curl_, curl_transpose_helmholtz_complex; operators.hpp:1516-1545,
+ * 1585-1614, 1763-1795, 1972-2008, 2178-2217). op: 0 laplace (cell ->
+ * cell), 1 gradient (cell -> face), 2 divergence (face -> cell), 3 curl
+ * (face -> edge), 4 curl_transpose (edge -> face, times scale). Device
+ * arrays of n_blocks blocks, each [component][nb][nb] (x fastest): scalar
+ * fields 2 n_modes components (mode i: real 2i, imaginary 2i+1), vector
+ * fields three groups of those (x, y, z); the z derivative of mode i is
+ * i omega_i, omega_i = 2 pi i / lz. Interior nodes are written, buffers read. */
+int iblgf_helm2d_op(iblgf_ctx* ctx, int op, int nb, int n_blocks, int n_modes, double dx_level, double lz,
+                    double scale, const double* dev_src, double* dev_dst);
 int iblgf_field_first_nonfinite(iblgf_ctx* ctx, int f, long long* index);
 int iblgf_debug_fail_alloc(long long after);
 

@@ -125,3 +125,69 @@ def apply(c, f):
 def residual(g, c):
     """(Delta_h - c^2) applied to g at the interior nodes (five-point)."""
     return (g[1:-1, 2:] + g[1:-1, :-2] + g[2:, 1:-1] + g[:-2, 1:-1] - (4.0 + c * c) * g[1:-1, 1:-1])
+
+
+# -- complex Helmholtz (Fourier-in-z) block operators on 2-D blocks --------
+# include/iblgf/operators/operators.hpp:1516-1545 laplace_helmholtz_complex,
+# :1585-1614 gradient_helmholtz_complex, :1763-1795 divergence_helmholtz_complex,
+# :1972-2008 curl_helmholtz_complex, :2178-2217 curl_transpose_helmholtz_complex.
+# A block holds [component][NB][NB] (x fastest); a scalar field has
+# sep = 2 N_modes components (mode i: real 2i, imaginary 2i+1), a vector field
+# three groups of sep (x, y, z). Each operator writes the interior nodes
+# (1 .. NB-2 on both axes) and reads their one-cell neighbours;
+# omega_i = 2 pi i / lz.
+def helm_op(op, src, dst, n_modes, dx, lz, scale=1.0):
+    """op: 'laplace', 'gradient', 'divergence', 'curl', 'curl_transpose';
+    src, dst: arrays [n_blocks][ncomp][NB][NB]; dst is updated in place."""
+    sep = 2 * n_modes
+    nb = src.shape[-1]
+    I = slice(1, nb - 1)
+
+    def at(c, ox, oy):
+        return src[:, c, 1 + oy:nb - 1 + oy, 1 + ox:nb - 1 + ox]
+
+    fac = 1.0 / dx
+    om = [2.0 * math.pi * i / lz for i in range(n_modes)]
+    if op == "laplace":
+        for i in range(sep):
+            dst[:, i, I, I] = fac * fac * (-4.0 * at(i, 0, 0) + at(i, 0, -1) + at(i, 0, 1) + at(i, -1, 0) + at(i, 1, 0))
+        for i in range(n_modes):
+            dst[:, 2 * i, I, I] -= at(2 * i, 0, 0) * om[i] * om[i]
+            dst[:, 2 * i + 1, I, I] -= at(2 * i + 1, 0, 0) * om[i] * om[i]
+    elif op == "gradient":
+        for i in range(sep):
+            dst[:, i, I, I] = fac * (at(i, 0, 0) - at(i, -1, 0))
+            dst[:, sep + i, I, I] = fac * (at(i, 0, 0) - at(i, 0, -1))
+        for i in range(n_modes):
+            dst[:, 2 * sep + 2 * i, I, I] = -at(2 * i + 1, 0, 0) * om[i]
+            dst[:, 2 * sep + 2 * i + 1, I, I] = at(2 * i, 0, 0) * om[i]
+    elif op == "divergence":
+        for i in range(sep):
+            dst[:, i, I, I] = fac * (-at(i, 0, 0) - at(sep + i, 0, 0) + at(i, 1, 0) + at(sep + i, 0, 1))
+        for i in range(n_modes):
+            dst[:, 2 * i, I, I] -= at(2 * sep + 2 * i + 1, 0, 0) * om[i]
+            dst[:, 2 * i + 1, I, I] += at(2 * sep + 2 * i, 0, 0) * om[i]
+    elif op == "curl":
+        for i in range(sep):
+            dst[:, i, I, I] = fac * (at(2 * sep + i, 0, 0) - at(2 * sep + i, 0, -1))
+            dst[:, sep + i, I, I] = fac * (-at(2 * sep + i, 0, 0) + at(2 * sep + i, -1, 0))
+            dst[:, 2 * sep + i, I, I] = fac * (at(sep + i, 0, 0) - at(sep + i, -1, 0) - at(i, 0, 0) + at(i, 0, -1))
+        for i in range(n_modes):
+            dst[:, 2 * i, I, I] += at(sep + 2 * i + 1, 0, 0) * om[i]
+            dst[:, 2 * i + 1, I, I] -= at(sep + 2 * i, 0, 0) * om[i]
+            dst[:, sep + 2 * i, I, I] -= at(2 * i + 1, 0, 0) * om[i]
+            dst[:, sep + 2 * i + 1, I, I] += at(2 * i, 0, 0) * om[i]
+    elif op == "curl_transpose":
+        f = fac * scale
+        for i in range(sep):
+            dst[:, i, I, I] = f * (-at(2 * sep + i, 0, 0) + at(2 * sep + i, 0, 1))
+            dst[:, sep + i, I, I] = f * (at(2 * sep + i, 0, 0) - at(2 * sep + i, 1, 0))
+            dst[:, 2 * sep + i, I, I] = f * (-at(sep + i, 0, 0) + at(sep + i, 1, 0) + at(i, 0, 0) - at(i, 0, 1))
+        for i in range(n_modes):
+            dst[:, 2 * i, I, I] += at(sep + 2 * i + 1, 0, 0) * om[i] * scale
+            dst[:, 2 * i + 1, I, I] -= at(sep + 2 * i, 0, 0) * om[i] * scale
+            dst[:, sep + 2 * i, I, I] -= at(2 * i + 1, 0, 0) * om[i] * scale
+            dst[:, sep + 2 * i + 1, I, I] += at(2 * i, 0, 0) * om[i] * scale
+    else:
+        raise ValueError(op)
+    return dst

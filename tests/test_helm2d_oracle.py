@@ -63,3 +63,24 @@ def test_apply_solves_the_equation_on_its_support():
     u = H.apply(c, f)
     # the unbounded solution: (Delta_h - c^2) u = f at every interior cell
     assert np.abs(H.residual(u, c) - f[1:-1, 1:-1]).max() < 1e-11 * np.abs(f).max()
+
+
+def test_complex_helmholtz_operators_are_mimetic():
+    """The restated complex (Fourier-in-z) operators keep the staggered
+    identities: div grad = laplace, curl grad = 0, div curl^T = 0, per mode
+    (the z derivative of mode i is i omega_i)."""
+    rng = np.random.default_rng(1)
+    nm, nb, dx, lz = 3, 12, 0.3, 2.0
+    sep = 2 * nm
+    u = rng.standard_normal((2, sep, nb, nb))
+    g = H.helm_op("gradient", u, np.zeros((2, 3 * sep, nb, nb)), nm, dx, lz)
+    d = H.helm_op("divergence", g, np.zeros((2, sep, nb, nb)), nm, dx, lz)
+    lap = H.helm_op("laplace", u, np.zeros((2, sep, nb, nb)), nm, dx, lz)
+    tol = 1e-12 * np.abs(lap).max()
+    assert np.abs(d - lap)[:, :, 1:nb - 2, 1:nb - 2].max() < tol
+    c = H.helm_op("curl", g, np.zeros((2, 3 * sep, nb, nb)), nm, dx, lz)
+    assert np.abs(c)[:, :, 2:nb - 1, 2:nb - 1].max() < tol
+    e = rng.standard_normal((2, 3 * sep, nb, nb))
+    ct = H.helm_op("curl_transpose", e, np.zeros((2, 3 * sep, nb, nb)), nm, dx, lz, 0.7)
+    dd = H.helm_op("divergence", ct, np.zeros((2, sep, nb, nb)), nm, dx, lz)
+    assert np.abs(dd)[:, :, 1:nb - 2, 1:nb - 2].max() < tol
