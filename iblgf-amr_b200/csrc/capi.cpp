@@ -59,7 +59,9 @@ double helm2d_origin(double c);
 void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out);
 void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale);
 void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
-               const double* dev_src, double* dev_dst);
+               const unsigned char* host_mode_mask, const double* dev_src, double* dev_dst);
+void helm2d_nonlinear(Ctx& c, int nb, int n_blocks, int n_planes, const unsigned char* host_plane_mask,
+                      const double* dev_face, const double* dev_edge, double* dev_dst);
 void wait_selftest(Ctx& c, long long polls);
 long long first_nonfinite(Ctx& c, const double* p, size_t n);
 }  // namespace iblgf_b200
@@ -763,7 +765,25 @@ int iblgf_helm2d_op(iblgf_ctx* x, int op, int nb, int n_blocks, int n_modes, dou
 {
     return guard(x, [&](iblgf_b200::Ctx& c) {
         if (n_blocks && (!dev_src || !dev_dst)) throw iblgf_b200::Error(IBLGF_EINVAL, "null field");
-        iblgf_b200::helm2d_op(c, op, nb, n_blocks, n_modes, dx_level, lz, scale, dev_src, dev_dst);
+        iblgf_b200::helm2d_op(c, op, nb, n_blocks, n_modes, dx_level, lz, scale, nullptr, dev_src, dev_dst);
+    });
+}
+
+int iblgf_helm2d_op_modes(iblgf_ctx* x, int op, int nb, int n_blocks, int n_modes, const unsigned char* mode_mask,
+                          double dx_level, double lz, double scale, const double* dev_src, double* dev_dst)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (n_blocks && (!dev_src || !dev_dst)) throw iblgf_b200::Error(IBLGF_EINVAL, "null field");
+        iblgf_b200::helm2d_op(c, op, nb, n_blocks, n_modes, dx_level, lz, scale, mode_mask, dev_src, dev_dst);
+    });
+}
+
+int iblgf_helm2d_nonlinear(iblgf_ctx* x, int nb, int n_blocks, int n_planes, const unsigned char* plane_mask,
+                           const double* dev_face, const double* dev_edge, double* dev_dst)
+{
+    return guard(x, [&](iblgf_b200::Ctx& c) {
+        if (n_blocks && (!dev_face || !dev_edge || !dev_dst)) throw iblgf_b200::Error(IBLGF_EINVAL, "null field");
+        iblgf_b200::helm2d_nonlinear(c, nb, n_blocks, n_planes, plane_mask, dev_face, dev_edge, dev_dst);
     });
 }
 

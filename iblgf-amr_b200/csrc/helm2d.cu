@@ -45,6 +45,14 @@ namespace iblgf_b200
 {
 namespace
 {
+// A set of up to 2048 units (z modes or z planes), passed by value.
+struct UnitMask
+{
+    static constexpr int kMax = 2048;
+    unsigned w[kMax / 32];
+    __device__ bool on(int i) const { return (w[i >> 5] >> (i & 31)) & 1u; }
+};
+
 __global__ void helm2d_table_kernel(int nx, int ny, double c, int npts, double* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,12 +130,16 @@ __global__ void helm2d_apply_kernel(int nx, int ny, const double* __restrict__ t
 // imaginary 2i+1), a vector field three groups of sep (x, y, z); the z
 // derivative of mode i is multiplication by i omega_i, omega_i = 2 pi i / lz.
 // One CTA per block, threads over the interior nodes (1 .. NB-2 per axis);
-// buffers are read, not written.
+// buffers are read, not written. The mask selects the modes written: all of
+// them for the forms above, one for the _oneMode forms (:1548, :1620, :1801,
+// :2017, :2224), the first N_modes / 2^r for the _refined forms (:1653,
+// :1839, :2125), any set for the ModesBool forms (:1889, :1931); the
+// components of unselected modes are left as they were.
 // op: 0 laplace (cell -> cell), 1 gradient (cell -> face), 2 divergence
 // (face -> cell), 3 curl (face -> edge), 4 curl_transpose (edge -> face, x scale)
 template<int OP>
 __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, double dx, double lz, double scale,
-                               const double* __restrict__ src, double* __restrict__ dst)
+                               UnitMask mask, const double* __restrict__ src, double* __restrict__ dst)
 {
     const int sep = 2 * n_modes, N2 = nb * nb;
     const double* s = src + (size_t)blockIdx.x * in_comp * N2;
@@ -141,6 +153,7 @@ __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, d
         auto out = [&](int c) -> double& { return d[(size_t)c * N2 + p]; };
         for (int i = 0; i < sep; ++i)
         {
+            if (!mask.on(i >> 1)) continue;
             if (OP == 0)
                 out(i) = fac * fac * (-4.0 * at(i, 0, 0) + at(i, 0, -1) + at(i, 0, 1) + at(i, -1, 0) + at(i, 1, 0));
             else if (OP == 1)
@@ -166,6 +179,7 @@ __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, d
         }
         for (int i = 0; i < n_modes; ++i)
         {
+            if (!mask.on(i)) continue;
             const double om = 2.0 * M_PI * i / lz;
             const int re = 2 * i, im = 2 * i + 1;
             if (OP == 0)
@@ -192,6 +206,43 @@ __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, d
                 out(sep + im) += at(re, 0, 0) * w;
             }
         }
+    }
+}
+
+// nonlinear_helmholtz (operators.hpp:2627-2766; _oneMode :2776-2831,
+// _refined :2840-2895): the convective term on the z collocation planes of
+// the Fourier-in-z solver. face (velocity), edge (vorticity) and dst are
+// [block][3 n_planes][NB][NB] (x fastest; component group x, y, z, one
+// component per z plane); per selected plane, at the interior nodes,
+//   dst_x = 1/2 w_y (u_z + u_z[-x]) - 1/4 (w_z (u_y + u_y[-x]) + w_z[+y] (u_y[+y] + u_y[-x+y]))
+//   dst_y = 1/4 (w_z (u_x + u_x[-y]) + w_z[+x] (u_x[+x] + u_x[+x-y])) - 1/2 w_x (u_z + u_z[-y])
+//   dst_z = 1/2 (w_x u_y + w_x[+y] u_y[+y] - w_y u_x - w_y[+x] u_x[+x]).
+// The mask selects planes: every plane; planes mode P .. mode P + P - 1 for
+// the _oneMode form (P planes per mode); every 2^r-th for the _refined form.
+__global__ void helm_nonlinear_kernel(int nb, int n_planes, UnitMask mask, const double* __restrict__ face,
+                                      const double* __restrict__ edge, double* __restrict__ dst)
+{
+    const int N2 = nb * nb;
+    const size_t blk = (size_t)blockIdx.x * 3 * n_planes * N2;
+    const double* u = face + blk;
+    const double* w = edge + blk;
+    double* d = dst + blk;
+    for (int q = threadIdx.x; q < n_planes * N2; q += blockDim.x)
+    {
+        const int i = q / N2, p = q - i * N2;
+        const int x = p % nb, y = p / nb;
+        if (x == 0 || y == 0 || x == nb - 1 || y == nb - 1 || !mask.on(i)) continue;
+        const int cx = i, cy = n_planes + i, cz = 2 * n_planes + i;
+        auto U = [&](int c, int ox, int oy) { return u[(size_t)c * N2 + p + ox + oy * nb]; };
+        auto W = [&](int c, int ox, int oy) { return w[(size_t)c * N2 + p + ox + oy * nb]; };
+        d[(size_t)cx * N2 + p] = 0.5 * W(cy, 0, 0) * (U(cz, 0, 0) + U(cz, -1, 0)) -
+                                 0.25 * (W(cz, 0, 0) * (U(cy, 0, 0) + U(cy, -1, 0)) +
+                                         W(cz, 0, 1) * (U(cy, 0, 1) + U(cy, -1, 1)));
+        d[(size_t)cy * N2 + p] = 0.25 * (W(cz, 0, 0) * (U(cx, 0, 0) + U(cx, 0, -1)) +
+                                         W(cz, 1, 0) * (U(cx, 1, 0) + U(cx, 1, -1))) -
+                                 0.5 * W(cx, 0, 0) * (U(cz, 0, 0) + U(cz, 0, -1));
+        d[(size_t)cz * N2 + p] = 0.5 * (W(cx, 0, 0) * U(cy, 0, 0) + W(cx, 0, 1) * U(cy, 0, 1) -
+                                        W(cy, 0, 0) * U(cx, 0, 0) - W(cy, 1, 0) * U(cx, 1, 0));
     }
 }
 
@@ -272,17 +323,28 @@ void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
     IBLGF_CUDA(cudaGetLastError());
 }
 
+UnitMask unit_mask(int n_units, const unsigned char* host_mask)
+{
+    if (n_units < 1 || n_units > UnitMask::kMax)
+        throw Error(IBLGF_EINVAL, "the mode (or plane) count is outside 1 .. 2048");
+    UnitMask m{};
+    for (int i = 0; i < n_units; ++i)
+        if (!host_mask || host_mask[i]) m.w[i >> 5] |= 1u << (i & 31);
+    return m;
+}
+
 void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
-               const double* dev_src, double* dev_dst)
+               const unsigned char* host_mode_mask, const double* dev_src, double* dev_dst)
 {
     if (op < 0 || op > 4 || nb < 3 || n_blocks < 0 || n_modes < 1 || !(dx > 0.0) || !(lz > 0.0))
         throw Error(IBLGF_EINVAL, "bad Helmholtz operator arguments");
+    const UnitMask mask = unit_mask(n_modes, host_mode_mask);
     if (!n_blocks) return;
     const int sep = 2 * n_modes;
     const int in_comp = (op == 0 || op == 1) ? sep : 3 * sep;
     const int out_comp = (op == 0 || op == 2) ? sep : 3 * sep;
     auto go = [&](auto kfn) {
-        kfn<<<n_blocks, 256, 0, c.stream>>>(nb, n_modes, in_comp, out_comp, dx, lz, scale, dev_src, dev_dst);
+        kfn<<<n_blocks, 256, 0, c.stream>>>(nb, n_modes, in_comp, out_comp, dx, lz, scale, mask, dev_src, dev_dst);
     };
     switch (op)
     {
@@ -292,6 +354,17 @@ void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, dou
         case 3: go(helm_op_kernel<3>); break;
         default: go(helm_op_kernel<4>); break;
     }
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void helm2d_nonlinear(Ctx& c, int nb, int n_blocks, int n_planes, const unsigned char* host_plane_mask,
+                      const double* dev_face, const double* dev_edge, double* dev_dst)
+{
+    if (nb < 3 || n_blocks < 0) throw Error(IBLGF_EINVAL, "bad nonlinear term arguments");
+    const UnitMask mask = unit_mask(n_planes, host_plane_mask);
+    if (!n_blocks) return;
+    helm_nonlinear_kernel<<<n_blocks, 256, 0, c.stream>>>(nb, n_planes, mask, dev_face, dev_edge, dev_dst);
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
 }

@@ -38,3 +38,24 @@ def solve(solver, f, z_operator="second_order"):
     for k in range(nz):
         uh[k] = solver.helm2d_apply(ck[k], fh[k].real) + 1j * solver.helm2d_apply(ck[k], fh[k].imag)
     return np.fft.ifft(uh, axis=0).real
+
+
+def refined_modes(n_modes, ref_level_up):
+    """The modes the _refined operator forms compute (operators.hpp:1653-1722,
+    1839-1887, 2125-2176): the first n_modes / 2^r; like the reference, an
+    n_modes that 2^r does not divide is an error."""
+    d = 1 << int(ref_level_up)
+    if n_modes % d:
+        raise ValueError("number of modes not divisible by 2^ref_level_up")
+    return range(n_modes // d)
+
+
+def one_mode_planes(mode, planes_per_mode=3):
+    """The z planes nonlinear_helmholtz_oneMode computes (operators.hpp:2776-2831)."""
+    return range(mode * planes_per_mode, (mode + 1) * planes_per_mode)
+
+
+def refined_planes(n_planes, ref_level_up):
+    """The z planes nonlinear_helmholtz_refined computes (operators.hpp:2840-2895):
+    every 2^r-th."""
+    return range(0, n_planes, 1 << int(ref_level_up))

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_helm2d_op_modes", "iblgf_helm2d_nonlinear", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -131,6 +131,8 @@ def lib():
     L.iblgf_helm2d_lgf.argtypes = [vp, cd, ci, ci, vp]
     L.iblgf_helm2d_apply.argtypes = [vp, cd, ci, ci, vp, vp, cd]
     L.iblgf_helm2d_op.argtypes = [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp]
+    L.iblgf_helm2d_op_modes.argtypes = [vp, ci, ci, ci, ci, vp, cd, cd, cd, vp, vp]
+    L.iblgf_helm2d_nonlinear.argtypes = [vp, ci, ci, ci, vp, vp, vp, vp]
     L.iblgf_ge_direct.argtypes = [vp, ci]
     L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
@@ -754,16 +756,70 @@ class Solver:
 
     HELM_OPS = {"laplace": 0, "gradient": 1, "divergence": 2, "curl": 3, "curl_transpose": 4}
 
-    def helm2d_op(self, op, src, dst, n_modes, dx_level, lz, scale=1.0):
-        """A complex Helmholtz block operator on 2-D blocks (torch CUDA
-        tensors [n_blocks][ncomp][nb][nb], float64); dst updated in place."""
+    @staticmethod
+    def _cuda_f64(*ts):
         import torch
-        for t in (src, dst):
+        for t in ts:
             if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
-                raise IblgfError("helm2d_op takes contiguous float64 CUDA tensors")
-        self._check(lib().iblgf_helm2d_op(self.h, self.HELM_OPS[op], src.shape[-1], src.shape[0], int(n_modes),
-                                          float(dx_level), float(lz), float(scale),
-                                          ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
+                raise IblgfError("the Helmholtz block operators take contiguous float64 CUDA tensors")
+
+    @staticmethod
+    def _unit_mask(n, units):
+        """A byte per unit (mode or plane): None selects all, else the
+        selected indices or a boolean sequence of length n."""
+        if units is None:
+            return None
+        m = np.asarray(units)
+        if m.dtype == bool:
+            if m.shape != (n,):
+                raise IblgfError("a boolean mask has one entry per unit")
+            out = m.astype(np.uint8)
+        else:
+            out = np.zeros(n, np.uint8)
+            idx = m.astype(np.int64).ravel()
+            if idx.size and (idx.min() < 0 or idx.max() >= n):
+                raise IblgfError("unit index out of range")
+            out[idx] = 1
+        return out
+
+    def helm2d_op(self, op, src, dst, n_modes, dx_level, lz, scale=1.0, modes=None):
+        """A complex Helmholtz block operator on 2-D blocks (torch CUDA
+        tensors [n_blocks][ncomp][nb][nb], float64); dst updated in place.
+        modes: None (all modes, the plain forms), the selected mode indices
+        (a single one: the _oneMode forms; range(n_modes >> r): the _refined
+        forms) or a boolean sequence (the ModesBool forms)."""
+        self._cuda_f64(src, dst)
+        k = self.HELM_OPS[op]
+        sep = 2 * int(n_modes)
+        cin, cout = (sep if k in (0, 1) else 3 * sep), (sep if k in (0, 2) else 3 * sep)
+        nb = src.shape[-1]
+        if (src.dim() != 4 or dst.dim() != 4 or tuple(src.shape[1:]) != (cin, nb, nb)
+                or tuple(dst.shape) != (src.shape[0], cout, nb, nb)):
+            raise IblgfError("%s takes [n_blocks][%d][nb][nb] into [n_blocks][%d][nb][nb]" % (op, cin, cout))
+        mask = self._unit_mask(int(n_modes), modes)
+        if mask is None:
+            self._check(lib().iblgf_helm2d_op(self.h, k, nb, src.shape[0], int(n_modes),
+                                              float(dx_level), float(lz), float(scale),
+                                              ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
+        else:
+            self._check(lib().iblgf_helm2d_op_modes(self.h, k, nb, src.shape[0],
+                                                    int(n_modes), _p(mask), float(dx_level), float(lz), float(scale),
+                                                    ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
+
+    def helm2d_nonlinear(self, face, edge, dst, n_planes, planes=None):
+        """The convective term on the z collocation planes
+        (nonlinear_helmholtz): face, edge, dst are torch CUDA tensors
+        [n_blocks][3 n_planes][nb][nb], float64; planes as helm2d_op's modes."""
+        self._cuda_f64(face, edge, dst)
+        nb = face.shape[-1]
+        shape = (face.shape[0], 3 * int(n_planes), nb, nb)
+        if face.dim() != 4 or any(tuple(t.shape) != shape for t in (face, edge, dst)):
+            raise IblgfError("the nonlinear term takes three [n_blocks][3 n_planes][nb][nb] tensors")
+        mask = self._unit_mask(int(n_planes), planes)
+        self._check(lib().iblgf_helm2d_nonlinear(self.h, nb, face.shape[0], int(n_planes),
+                                                 None if mask is None else _p(mask),
+                                                 ctypes.c_void_p(face.data_ptr()), ctypes.c_void_p(edge.data_ptr()),
+                                                 ctypes.c_void_p(dst.data_ptr())))
 
     def tc_mma_rate(self, n):
         """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""

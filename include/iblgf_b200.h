@@ -467,6 +467,28 @@ int iblgf_helm2d_apply(iblgf_ctx* ctx, double c, int nx, int ny, const double* h
  * i omega_i, omega_i = 2 pi i / lz. Interior nodes are written, buffers read. */
 int iblgf_helm2d_op(iblgf_ctx* ctx, int op, int nb, int n_blocks, int n_modes, double dx_level, double lz,
                     double scale, const double* dev_src, double* dev_dst);
+/* The same operators restricted to a set of z modes: mode_mask[i] != 0
+ * selects mode i (n_modes bytes; NULL selects all); the components of the
+ * other modes are left as they were. Replaces the single-mode forms
+ * (laplace_/gradient_/divergence_/curl_/curl_transpose_helmholtz_complex_oneMode,
+ * operators.hpp:1548, 1620, 1801, 2017, 2224: one mode selected), the
+ * refined forms (gradient_/divergence_/curl_helmholtz_complex_refined,
+ * :1653, 1839, 2125: the first n_modes / 2^r modes) and the ModesBool forms
+ * (divergence_helmholtz_complex(..., ModesBool), _Modes, :1889, 1931).
+ * n_modes <= 2048. */
+int iblgf_helm2d_op_modes(iblgf_ctx* ctx, int op, int nb, int n_blocks, int n_modes, const unsigned char* mode_mask,
+                          double dx_level, double lz, double scale, const double* dev_src, double* dev_dst);
+/* The convective term on the z collocation planes of the Fourier-in-z
+ * solver (domain::Operator::nonlinear_helmholtz, operators.hpp:2627-2766;
+ * _oneMode :2776-2831 and _refined :2840-2895 through plane_mask). dev_face
+ * (velocity, faces), dev_edge (vorticity, edges), dev_dst (faces): n_blocks
+ * blocks of [3 n_planes][nb][nb] (x fastest; groups x, y, z, one component
+ * per z plane). plane_mask[i] != 0 selects plane i (NULL: all; the single-mode
+ * form selects planes mode P .. mode P + P - 1 for P planes per mode, the
+ * refined form every 2^r-th plane); interior nodes of the selected planes are
+ * written. n_planes <= 2048. */
+int iblgf_helm2d_nonlinear(iblgf_ctx* ctx, int nb, int n_blocks, int n_planes, const unsigned char* plane_mask,
+                           const double* dev_face, const double* dev_edge, double* dev_dst);
 int iblgf_field_first_nonfinite(iblgf_ctx* ctx, int f, long long* index);
 int iblgf_debug_fail_alloc(long long after);
 

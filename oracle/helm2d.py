@@ -136,9 +136,25 @@ def residual(g, c):
 # three groups of sep (x, y, z). Each operator writes the interior nodes
 # (1 .. NB-2 on both axes) and reads their one-cell neighbours;
 # omega_i = 2 pi i / lz.
-def helm_op(op, src, dst, n_modes, dx, lz, scale=1.0):
+def helm_op(op, src, dst, n_modes, dx, lz, scale=1.0, modes=None):
     """op: 'laplace', 'gradient', 'divergence', 'curl', 'curl_transpose';
-    src, dst: arrays [n_blocks][ncomp][NB][NB]; dst is updated in place."""
+    src, dst: arrays [n_blocks][ncomp][NB][NB]; dst is updated in place.
+    modes: the modes computed (None: all; the _oneMode forms, :1548-1583,
+    1620-1652, 1801-1837, 2017-2057, 2224-2270, compute one; the _refined
+    forms, :1653-1722, 1839-1887, 2125-2176, the first n_modes / 2^r).
+    A mode's components depend on that mode's inputs alone, so a restricted
+    form equals the full one on the selected modes' components."""
+    if modes is not None:
+        out = dst.copy()
+        full = helm_op(op, src, dst.copy(), n_modes, dx, lz, scale)
+        sep = 2 * n_modes
+        groups = 1 if op in ("laplace", "divergence") else 3
+        for m in modes:
+            for g in range(groups):
+                for c in (2 * m, 2 * m + 1):
+                    out[:, g * sep + c] = full[:, g * sep + c]
+        dst[...] = out
+        return dst
     sep = 2 * n_modes
     nb = src.shape[-1]
     I = slice(1, nb - 1)
@@ -190,4 +206,29 @@ def helm_op(op, src, dst, n_modes, dx, lz, scale=1.0):
             dst[:, sep + 2 * i + 1, I, I] += at(2 * i, 0, 0) * om[i] * scale
     else:
         raise ValueError(op)
+    return dst
+
+
+def nonlinear(face, edge, dst, n_planes, planes=None):
+    """nonlinear_helmholtz (operators.hpp:2627-2766; _oneMode :2776-2831 and
+    _refined :2840-2895 with planes = the planes they compute): face, edge,
+    dst are [n_blocks][3 n_planes][NB][NB]; dst's interior nodes of the
+    selected planes are overwritten."""
+    nb = face.shape[-1]
+    I = slice(1, nb - 1)
+
+    def U(c, ox, oy):
+        return face[:, c, 1 + oy:nb - 1 + oy, 1 + ox:nb - 1 + ox]
+
+    def W(c, ox, oy):
+        return edge[:, c, 1 + oy:nb - 1 + oy, 1 + ox:nb - 1 + ox]
+
+    for i in (range(n_planes) if planes is None else planes):
+        x, y, z = i, n_planes + i, 2 * n_planes + i
+        dst[:, x, I, I] = (0.5 * W(y, 0, 0) * (U(z, 0, 0) + U(z, -1, 0))
+                           - 0.25 * (W(z, 0, 0) * (U(y, 0, 0) + U(y, -1, 0)) + W(z, 0, 1) * (U(y, 0, 1) + U(y, -1, 1))))
+        dst[:, y, I, I] = (0.25 * (W(z, 0, 0) * (U(x, 0, 0) + U(x, 0, -1)) + W(z, 1, 0) * (U(x, 1, 0) + U(x, 1, -1)))
+                           - 0.5 * W(x, 0, 0) * (U(z, 0, 0) + U(z, 0, -1)))
+        dst[:, z, I, I] = 0.5 * (W(x, 0, 0) * U(y, 0, 0) + W(x, 0, 1) * U(y, 0, 1)
+                                 - W(y, 0, 0) * U(x, 0, 0) - W(y, 1, 0) * U(x, 1, 0))
     return dst

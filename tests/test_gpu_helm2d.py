@@ -97,3 +97,54 @@ def test_complex_helmholtz_operators_match_oracle(g, op):
     g.synchronize()
     out = d.cpu().numpy()
     assert np.abs(out - ref).max() < 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("sel", ["one_mode", "refined", "bool"])
+@pytest.mark.parametrize("op", ["laplace", "gradient", "divergence", "curl", "curl_transpose"])
+def test_mode_restricted_operators_match_oracle(g, op, sel):
+    """The _oneMode, _refined and ModesBool forms: only the selected modes'
+    components change."""
+    import torch
+    rng = np.random.default_rng(3)
+    nm, nb, nblk, dx, lz = 4, 12, 3, 0.5, 2.0
+    modes = {"one_mode": [2], "refined": list(fourier_z.refined_modes(nm, 1)),
+             "bool": np.array([True, False, False, True])}[sel]
+    sep = 2 * nm
+    cin = sep if op in ("laplace", "gradient") else 3 * sep
+    cout = sep if op in ("laplace", "divergence") else 3 * sep
+    src = rng.standard_normal((nblk, cin, nb, nb))
+    dst0 = rng.standard_normal((nblk, cout, nb, nb))
+    sel_idx = np.flatnonzero(modes) if sel == "bool" else modes
+    ref = H.helm_op(op, src, dst0.copy(), nm, dx, lz, 0.4, modes=sel_idx)
+    d = torch.tensor(dst0, device="cuda")
+    g.helm2d_op(op, torch.tensor(src, device="cuda"), d, nm, dx, lz, 0.4, modes=modes)
+    g.synchronize()
+    assert np.abs(d.cpu().numpy() - ref).max() < 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("sel", ["all", "one_mode", "refined"])
+def test_nonlinear_term_matches_oracle(g, sel):
+    import torch
+    rng = np.random.default_rng(6)
+    npl, nb, nblk = 12, 18, 4
+    planes = {"all": None, "one_mode": fourier_z.one_mode_planes(1, 3),
+              "refined": fourier_z.refined_planes(npl, 1)}[sel]
+    face = rng.standard_normal((nblk, 3 * npl, nb, nb))
+    edge = rng.standard_normal((nblk, 3 * npl, nb, nb))
+    dst0 = rng.standard_normal((nblk, 3 * npl, nb, nb))
+    ref = H.nonlinear(face, edge, dst0.copy(), npl, planes)
+    d = torch.tensor(dst0, device="cuda")
+    g.helm2d_nonlinear(torch.tensor(face, device="cuda"), torch.tensor(edge, device="cuda"), d, npl,
+                       None if planes is None else list(planes))
+    g.synchronize()
+    assert np.abs(d.cpu().numpy() - ref).max() < 1e-14 * np.abs(ref).max()
+
+
+def test_unit_masks_are_checked(g):
+    import torch
+    t = torch.zeros((1, 6, 8, 8), dtype=torch.float64, device="cuda")
+    with pytest.raises(B.IblgfError):
+        g.helm2d_op("laplace", t, t.clone(), 3, 1.0, 1.0, modes=[3])  # mode index out of range
+    with pytest.raises(B.IblgfError):
+        big = torch.zeros((1, 3 * 4096, 4, 4), dtype=torch.float64, device="cuda")
+        g.helm2d_nonlinear(big, big, big.clone(), 4096)  # more planes than a mask holds

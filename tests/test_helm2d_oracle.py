@@ -84,3 +84,34 @@ def test_complex_helmholtz_operators_are_mimetic():
     ct = H.helm_op("curl_transpose", e, np.zeros((2, 3 * sep, nb, nb)), nm, dx, lz, 0.7)
     dd = H.helm_op("divergence", ct, np.zeros((2, sep, nb, nb)), nm, dx, lz)
     assert np.abs(dd)[:, :, 1:nb - 2, 1:nb - 2].max() < tol
+
+
+def test_nonlinear_term_is_the_cross_product_for_uniform_fields():
+    """nonlinear_helmholtz's staggered averages reduce to w x u when the
+    fields are uniform on each plane; only the selected planes are written."""
+    rng = np.random.default_rng(4)
+    npl, nb = 5, 8
+    uv = rng.standard_normal((3, npl))
+    wv = rng.standard_normal((3, npl))
+    face = np.repeat(np.repeat(uv.reshape(1, 3 * npl, 1, 1), nb, 2), nb, 3)
+    edge = np.repeat(np.repeat(wv.reshape(1, 3 * npl, 1, 1), nb, 2), nb, 3)
+    dst = np.full((1, 3 * npl, nb, nb), 7.0)
+    H.nonlinear(face, edge, dst, npl, planes=[1, 3])
+    cross = np.cross(wv.T, uv.T).T  # (w x u) per plane
+    for i in range(npl):
+        for g in range(3):
+            block = dst[0, g * npl + i, 1:-1, 1:-1]
+            if i in (1, 3):
+                assert np.abs(block - cross[g, i]).max() < 1e-14
+            else:
+                assert (block == 7.0).all()
+    assert (dst[0, :, 0, :] == 7.0).all()
+
+
+def test_mode_selections_follow_the_reference_forms():
+    import fourier_z
+    assert list(fourier_z.refined_modes(8, 2)) == [0, 1]
+    with pytest.raises(ValueError):
+        fourier_z.refined_modes(6, 2)  # the reference throws when 2^r does not divide N_modes
+    assert list(fourier_z.one_mode_planes(2, 3)) == [6, 7, 8]
+    assert list(fourier_z.refined_planes(12, 2)) == [0, 4, 8]
