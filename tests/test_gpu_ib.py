@@ -47,15 +47,16 @@ def test_ib_solve_needs_points():
         g.ib_solve(uf, 0.0)
 
 
-@pytest.mark.parametrize("precision,tol,ptol", [(B.FP64, 1e-9, 1e-9), (B.FP32, 1e-4, 5e-4)])
-def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
+@pytest.mark.parametrize("precision,tol", [(B.FP64, 1e-9), (B.FP32, 1e-4)])
+def test_ns_step_with_ib_matches_oracle(precision, tol):
     """Three IF-HERK steps past the sphere in a uniform stream (frame velocity
     (-1, 0, 0): the body at rest, the fluid moving at +1): velocity, pressure
     and the three stage forces of the last step against the oracle. The first
     step runs direct, the second is captured as a CUDA graph (its force CG a
     conditional while-node) and the third replays that graph. In FP32 the
     pressure (d_i / (a33 dt), a factor 400 here) carries the FP32
-    perturbation of the IB CG iterates: 5e-4 for it, 1e-4 for velocity."""
+    perturbation of the IB CG iterates (about 1.5e-6 of the force, so 6e-4
+    for it), 1e-4 for velocity."""
     case = S.SphereIB("small")
     o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                  n_levels=case.n_levels, predicate=case.predicate)
@@ -64,6 +65,7 @@ def test_ns_step_with_ib_matches_oracle(precision, tol, ptol):
     X = O.sphere_points(case.dx_base, o.depth - 1 - o.base_level, case.ibph)
     u0 = case.velocity(o)
     dt, fv = 0.01, (-1.0, 0.0, 0.0)
+    ptol = 1e-9 if precision == B.FP64 else 1.5e-6 / (0.25 * dt)
     ur, pr, fr = o.ns_step_ib(u0, dt, case.Re, X, fv, 0.0, 3)
     g.ib_set_points(X, case.Re)
     g.ns_options(fv)
