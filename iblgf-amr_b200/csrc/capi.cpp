@@ -57,6 +57,7 @@ double measure_fma_peak(Ctx& c, int precision);
 double measure_tc_rate(Ctx& c, int n);
 double helm2d_origin(double c);
 void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out);
+void helm2d_points(Ctx& c, double cz, int count, const int* host_nm, double* host_out);
 void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale);
 void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
                const unsigned char* host_mode_mask, const double* dev_src, double* dev_dst);
@@ -742,6 +743,11 @@ int iblgf_helm2d_lgf(iblgf_ctx* x, double c, int nx, int ny, double* host_out)
         IBLGF_CUDA(cudaMemcpyAsync(host_out, d.p, (size_t)nx * ny * sizeof(double), cudaMemcpyDeviceToHost, cx.stream));
         IBLGF_CUDA(cudaStreamSynchronize(cx.stream));
     });
+}
+
+int iblgf_helm2d_get(iblgf_ctx* x, double c, int n, const int* host_nm, double* host_out)
+{
+    return guard(x, [&](iblgf_b200::Ctx& cx) { iblgf_b200::helm2d_points(cx, c, n, host_nm, host_out); });
 }
 
 int iblgf_helm2d_apply(iblgf_ctx* x, double c, int nx, int ny, const double* host_f, double* host_u, double scale)

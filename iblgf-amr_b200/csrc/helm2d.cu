@@ -36,6 +36,7 @@
 //                      cell grid, one thread per target cell, the source row
 //                      staged through shared memory
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
 
@@ -53,11 +54,29 @@ struct UnitMask
     __device__ bool on(int i) const { return (w[i >> 5] >> (i & 31)) & 1u; }
 };
 
-__global__ void helm2d_table_kernel(int nx, int ny, double c, int npts, double* __restrict__ out)
+// Offset of element i: (i % nx, i / nx) of a table, or the i-th pair of nm
+// (absolute values) when a list of offsets is given.
+__device__ inline void offset_of(int i, int nx, const int* nm, int& n, int& m)
+{
+    if (nm)
+    {
+        n = abs(nm[2 * i]);
+        m = abs(nm[2 * i + 1]);
+    }
+    else
+    {
+        n = i % nx;
+        m = i / nx;
+    }
+}
+
+__global__ void helm2d_table_kernel(int nx, int ny, const int* __restrict__ nm, double c, int npts,
+                                    double* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nx * ny) return;
-    int n = i % nx, m = i / nx;
+    int n, m;
+    offset_of(i, nx, nm, n, m);
     if (n < m)
     {
         const int t = n;
@@ -76,12 +95,13 @@ __global__ void helm2d_table_kernel(int nx, int ny, double c, int npts, double* 
     out[i] = -s * h / (2.0 * M_PI);
 }
 
-__global__ void lap2d_table_kernel(int nx, int ny, const double* __restrict__ gx, const double* __restrict__ gw,
-                                   int npts, double* __restrict__ out)
+__global__ void lap2d_table_kernel(int nx, int ny, const int* __restrict__ nm, const double* __restrict__ gx,
+                                   const double* __restrict__ gw, int npts, double* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nx * ny) return;
-    int n = i % nx, m = i / nx;
+    int n, m;
+    offset_of(i, nx, nm, n, m);
     if (n < m)
     {
         const int t = n;
@@ -301,26 +321,57 @@ double helm2d_origin(double c)
     return 0.5 / (2.0 + c * c / 2.0) * value;
 }
 
-void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
+namespace
 {
-    if (!(cz >= 0.0) || nx < 1 || ny < 1) throw Error(IBLGF_EINVAL, "need c >= 0 and a non-empty table");
+// get(n, m) for a table (nm null: 0 <= n < nx, 0 <= m < ny) or for the nx
+// offsets of nm (ny = 1); extent = the largest |offset| + 1 on either axis
+void launch_lgf(Ctx& c, double cz, int nx, int ny, const int* dev_nm, int extent, double* dev_out)
+{
     const int total = nx * ny;
     if (cz > 0.0)
-        helm2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, cz, trapezoid_points(cz), dev_out);
+        helm2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, dev_nm, cz, trapezoid_points(cz),
+                                                                       dev_out);
     else
     {
         // node count grows with the offsets (the integrand varies on a scale 1 / |n| near 0)
-        const int npts = std::min(8192, 96 + 6 * std::max(nx, ny));
+        const int npts = std::min(8192, 96 + 6 * extent);
         std::vector<double> x, w;
         gauss_legendre_0_pi(npts, x, w);
         x.insert(x.end(), w.begin(), w.end());
         DevBuf<double> d;
         d.upload(x, c.stream);
-        lap2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, d.p, d.p + npts, npts, dev_out);
+        lap2d_table_kernel<<<(total + 127) / 128, 128, 0, c.stream>>>(nx, ny, dev_nm, d.p, d.p + npts, npts, dev_out);
         IBLGF_CUDA(cudaStreamSynchronize(c.stream));  // the nodes are freed on return
     }
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
+{
+    if (!(cz >= 0.0) || nx < 1 || ny < 1) throw Error(IBLGF_EINVAL, "need c >= 0 and a non-empty table");
+    launch_lgf(c, cz, nx, ny, nullptr, std::max(nx, ny), dev_out);
+}
+
+void helm2d_points(Ctx& c, double cz, int count, const int* host_nm, double* host_out)
+{
+    if (!(cz >= 0.0) || count < 0 || (count && (!host_nm || !host_out)))
+        throw Error(IBLGF_EINVAL, "need c >= 0 and offset / output arrays");
+    if (!count) return;
+    int extent = 1;
+    for (int i = 0; i < 2 * count; ++i)
+    {
+        if (host_nm[i] == INT_MIN) throw Error(IBLGF_EINVAL, "offset out of range");
+        extent = std::max(extent, std::abs(host_nm[i]) + 1);
+    }
+    DevBuf<int> nm;
+    nm.upload(std::vector<int>(host_nm, host_nm + 2 * count), c.stream);
+    DevBuf<double> out;
+    out.alloc((size_t)count);
+    launch_lgf(c, cz, count, 1, nm.p, extent, out.p);
+    IBLGF_CUDA(cudaMemcpyAsync(host_out, out.p, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 UnitMask unit_mask(int n_units, const unsigned char* host_mask)

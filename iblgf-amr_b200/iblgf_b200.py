@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_helm2d_op_modes", "iblgf_helm2d_nonlinear", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_get", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_helm2d_op_modes", "iblgf_helm2d_nonlinear", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -129,6 +129,7 @@ def lib():
     L.iblgf_tc_mma_rate.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_helm2d_origin.argtypes = [cd, ctypes.POINTER(ctypes.c_double)]
     L.iblgf_helm2d_lgf.argtypes = [vp, cd, ci, ci, vp]
+    L.iblgf_helm2d_get.argtypes = [vp, cd, ci, vp, vp]
     L.iblgf_helm2d_apply.argtypes = [vp, cd, ci, ci, vp, vp, cd]
     L.iblgf_helm2d_op.argtypes = [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp]
     L.iblgf_helm2d_op_modes.argtypes = [vp, ci, ci, ci, ci, vp, cd, cd, cd, vp, vp]
@@ -745,6 +746,14 @@ class Solver:
         0 <= m < ny, as an (ny, nx) array."""
         out = np.zeros((ny, nx))
         self._check(lib().iblgf_helm2d_lgf(self.h, float(c), int(nx), int(ny), _p(out)))
+        return out
+
+    def helm2d_get(self, c, offsets):
+        """get(n, m) of the 2-D Helmholtz LGF (c = 0: the 2-D Laplace LGF)
+        at each offset of an (k, 2) integer array."""
+        nm = np.ascontiguousarray(np.asarray(offsets, dtype=np.int32).reshape(-1, 2))
+        out = np.zeros(nm.shape[0])
+        self._check(lib().iblgf_helm2d_get(self.h, float(c), nm.shape[0], _p(nm), _p(out)))
         return out
 
     def helm2d_apply(self, c, f, u=None, scale=1.0):

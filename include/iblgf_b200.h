@@ -447,6 +447,9 @@ int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
  * G0 with G0(0, 0) = 0, log r / (2 pi) + 0.2573... far away).
  * iblgf_helm2d_origin: origin_val(c) (c > 0).
  * iblgf_helm2d_lgf: host_out[m * nx + n] = get(n, m), 0 <= n < nx, 0 <= m < ny.
+ * iblgf_helm2d_get: host_out[i] = get(host_nm[2i], host_nm[2i + 1]) for n
+ * offsets (Helmholtz<2>::get(coordinate) and get(N, M), helmholtz.hpp:161-176,
+ * with c the level's c_level).
  * iblgf_helm2d_apply: host_u += scale * sum_j get(i - j) host_f[j] over a
  * uniform nx x ny cell grid (x fastest; every pair, the exact unbounded
  * solution of (Delta_h - c^2) u = f on that support); nx <= 6144.
@@ -454,6 +457,7 @@ int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
  * part of this library. */
 int iblgf_helm2d_origin(double c, double* out);
 int iblgf_helm2d_lgf(iblgf_ctx* ctx, double c, int nx, int ny, double* host_out);
+int iblgf_helm2d_get(iblgf_ctx* ctx, double c, int n, const int* host_nm, double* host_out);
 int iblgf_helm2d_apply(iblgf_ctx* ctx, double c, int nx, int ny, const double* host_f, double* host_u, double scale);
 /* Complex Helmholtz (Fourier-in-z) block operators on 2-D blocks
  * (domain::Operator::laplace_helmholtz_complex, gradient_, divergence_,

@@ -328,6 +328,63 @@ class LGF_GE
     double alpha_base_ = 0.0, alpha_ = 0.0;
 };
 
+// lgf::Helmholtz<2> (lgf/helmholtz.hpp:37-193): the 2-D screened kernel of
+// one z mode of the Fourier-in-z solvers. c is the coarse level's value;
+// change_level(ld) sets c_level = c / 2^ld and origin = origin_val(c_level)
+// (:127-158); get() returns the trapezoidal integral of helmholtz_lookup.hpp
+// minus the origin the object holds (:161-176), evaluated on the device. As in
+// the reference, the default constructor holds c = 0.1 with origin 0 until a
+// change_c / change_level sets it. c must be > 0 (mode 0 uses the Laplace
+// kernel, whose origin series diverges).
+class Helmholtz
+{
+  public:
+    Helmholtz() : c_(0.1), c_level_(0.1), origin_(0.0) {}
+    explicit Helmholtz(double C) : c_(C), c_level_(C) { origin_ = origin_val(C); }
+    bool neighbor_only() const noexcept { return false; }
+    bool LaplaceLGF() const noexcept { return false; }
+    bool HelmholtzLGF() const noexcept { return true; }
+    double return_c() const noexcept { return c_level_; }
+    double origin() const noexcept { return origin_; }
+    void change_c(double C)
+    {
+        c_ = c_level_ = C;
+        origin_ = origin_val(C);
+    }
+    void change_level(int level_diff)
+    {
+        c_level_ = c_ * std::pow(0.5, level_diff);
+        origin_ = origin_val(c_level_);
+    }
+    template<class Coord>
+    double get(const Coord& c) const
+    {
+        return get((int)c[0], (int)c[1]);
+    }
+    double get(int N, int M) const
+    {
+        const int nm[2] = {N, M};
+        double v = 0.0;  // the device value is the integral minus origin_val(c_level)
+        check(detail::kernel_ctx(), iblgf_helm2d_get(detail::kernel_ctx(), c_level_, 1, nm, &v));
+        return v + origin_val(c_level_) - origin_;
+    }
+    template<class BlockDescriptor>
+    std::tuple<bool, double, int, int> get_key(const BlockDescriptor& b, int /*level_diff*/) const
+    {
+        const auto base = b.base();
+        return std::tuple<bool, double, int, int>(true, c_level_, base[0], base[1]);
+    }
+
+  private:
+    static double origin_val(double C)
+    {
+        double o = 0.0;
+        if (iblgf_helm2d_origin(C, &o) != IBLGF_OK) throw std::runtime_error("iblgf_b200: Helmholtz needs c > 0");
+        return o;
+    }
+    double c_, c_level_, origin_;
+};
+
 // ----------------------------------------------------------------- solvers
 // PoissonSolver<Setup> (solver/poisson/poisson.hpp:46): apply_lgf / solve /
 // apply_lgf_IF for every component of the source field.

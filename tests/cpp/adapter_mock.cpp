@@ -14,7 +14,10 @@
 //   ops      Operator::levelGradient<source, face>(l) for every level, then
 //            the per-block Operator::curl<face, edge>(it->data(), dx) on
 //            every octant                                         -> face[3], edge[3]
-//   kernels  LGF_GL::get and LGF_GE(alpha)::get at 64 fixed offsets -> 2 x 64 values
+//   kernels  LGF_GL::get and LGF_GE(alpha)::get at 64 fixed offsets -> 2 x 64 values,
+//            then Helmholtz(c = alpha)::get at 16 fixed 2-D offsets, the same
+//            after change_level(1), and a default-constructed Helmholtz's
+//            get(3, 1)                                          -> 2 x 16 + 1 values
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -209,6 +212,14 @@ int main(int argc, char** argv)
             for (int i = 0; i < 64; ++i) pts.push_back({i % 7 - 3, (i / 7) % 5 - 2, i / 35 * 37 - 5});
             for (auto& p : pts) out.push_back(gl.get(p));
             for (auto& p : pts) out.push_back(ge.get(p));
+            iblgf::b200::Helmholtz h(alpha);
+            std::vector<std::array<int, 2>> p2;
+            for (int i = 0; i < 16; ++i) p2.push_back({i % 5 - 2, i / 5 * 3 - 4});
+            for (auto& p : p2) out.push_back(h.get(p));
+            h.change_level(1);
+            for (auto& p : p2) out.push_back(h.get(p[0], p[1]));
+            iblgf::b200::Helmholtz h0;
+            out.push_back(h0.get(3, 1));
         }
         else
             return 2;

@@ -148,3 +148,17 @@ def test_unit_masks_are_checked(g):
     with pytest.raises(B.IblgfError):
         big = torch.zeros((1, 3 * 4096, 4, 4), dtype=torch.float64, device="cuda")
         g.helm2d_nonlinear(big, big, big.clone(), 4096)  # more planes than a mask holds
+
+
+@pytest.mark.parametrize("c", [0.0, 0.3])
+def test_point_evaluation_matches_the_table(g, c):
+    """iblgf_helm2d_get at scattered signed offsets equals the table entries
+    of their absolute values (the kernel is even in both offsets)."""
+    rng = np.random.default_rng(8)
+    nm = rng.integers(-15, 16, size=(40, 2))
+    nm[0] = (15, 0)  # the extent the node count follows, as the table's
+    vals = g.helm2d_get(c, nm)
+    t = g.helm2d_lgf(c, 16, 16)
+    ref = t[np.abs(nm[:, 1]), np.abs(nm[:, 0])]
+    assert np.abs(vals - ref).max() < 1e-14 * np.abs(ref).max()
+    assert g.helm2d_get(c, np.zeros((0, 2), np.int32)).size == 0

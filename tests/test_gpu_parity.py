@@ -6,6 +6,7 @@ bit-exact.
 """
 import json
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -257,8 +258,8 @@ def test_cpp_adapter_operators_and_kernel_objects(tmp_path):
     """Operator::levelGradient (gradient, then the target's buffer exchange,
     operators.hpp:588-606) on every level and the per-block
     Operator::curl<face, edge>(it->data(), dx_level) on every octant through
-    the adapter, against the oracle; LGF_GL::get and LGF_GE::get at fixed
-    offsets against the oracle's kernels."""
+    the adapter, against the oracle; LGF_GL::get, LGF_GE::get and
+    Helmholtz<2>::get at fixed offsets against the oracle's kernels."""
     case = S.GaussianPoisson("amr_small")
     o = O.Domain(case.bd_base, case.bd_extent, case.block_extent, case.dx_base, case.blocks,
                  n_levels=case.n_levels, predicate=case.predicate)
@@ -281,7 +282,17 @@ def test_cpp_adapter_operators_and_kernel_objects(tmp_path):
     gl = np.array([O.lgf_get(*p) for p in pts])
     ge = np.array([o.lgf_ge_get(*p, alpha) for p in pts])
     assert np.abs(vals[:64] - gl).max() < 1e-13 * np.abs(gl).max()
-    assert np.abs(vals[64:] - ge).max() < 1e-13 * np.abs(ge).max()
+    assert np.abs(vals[64:128] - ge).max() < 1e-13 * np.abs(ge).max()
+    # Helmholtz<2> (c = alpha): get, get after change_level(1) (c / 2), and the
+    # default object (c = 0.1, origin 0 until a level or c is set)
+    sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
+    import helm2d as H
+    p2 = [(i % 5 - 2, i // 5 * 3 - 4) for i in range(16)]
+    for j, c in enumerate((alpha, alpha / 2)):
+        ref = np.array([H.lgf(n, m, c) for n, m in p2])
+        assert np.abs(vals[128 + 16 * j:144 + 16 * j] - ref).max() < 1e-13 * np.abs(ref).max()
+    h0 = H.lgf(3, 1, 0.1) + H.origin_val(0.1)
+    assert abs(vals[160] - h0) < 1e-13 * abs(h0) and vals.size == 161
 
 
 @pytest.mark.parametrize("op,n_in,n_out", [(0, 1, 1), (1, 1, 3), (2, 3, 1), (3, 3, 3), (4, 3, 3), (5, 6, 3)])
