@@ -63,6 +63,8 @@ void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, dou
                const unsigned char* host_mode_mask, const double* dev_src, double* dev_dst);
 void helm2d_nonlinear(Ctx& c, int nb, int n_blocks, int n_planes, const unsigned char* host_plane_mask,
                       const double* dev_face, const double* dev_edge, double* dev_dst);
+void helm2d_real_op(Ctx& c, int op, int nb, int n_blocks, int np, double dx, double dx_fine, double cz, double scale,
+                    const double* a, int a_comp, const double* b, int b_comp, double* d, int d_comp, double* e);
 void wait_selftest(Ctx& c, long long polls);
 long long first_nonfinite(Ctx& c, const double* p, size_t n);
 }  // namespace iblgf_b200
@@ -781,6 +783,16 @@ int iblgf_helm2d_op_modes(iblgf_ctx* x, int op, int nb, int n_blocks, int n_mode
     return guard(x, [&](iblgf_b200::Ctx& c) {
         if (n_blocks && (!dev_src || !dev_dst)) throw iblgf_b200::Error(IBLGF_EINVAL, "null field");
         iblgf_b200::helm2d_op(c, op, nb, n_blocks, n_modes, dx_level, lz, scale, mode_mask, dev_src, dev_dst);
+    });
+}
+
+int iblgf_helm2d_real_op(iblgf_ctx* x, int op, int nb, int n_blocks, int n_planes, double dx_level, double dx_fine,
+                         double c, double scale, const double* dev_a, int a_comp, const double* dev_b, int b_comp,
+                         double* dev_d, int d_comp, double* dev_e)
+{
+    return guard(x, [&](iblgf_b200::Ctx& cx) {
+        iblgf_b200::helm2d_real_op(cx, op, nb, n_blocks, n_planes, dx_level, dx_fine, c, scale, dev_a, a_comp, dev_b,
+                                   b_comp, dev_d, d_comp, dev_e);
     });
 }
 

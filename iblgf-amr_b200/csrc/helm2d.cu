@@ -266,6 +266,92 @@ __global__ void helm_nonlinear_kernel(int nb, int n_planes, UnitMask mask, const
     }
 }
 
+// Real-valued 2-D block operators of the Fourier-in-z family (fields in
+// physical z, or one real mode; a, b inputs, d and e outputs, each
+// [block][components][NB][NB], x fastest, with a_comp / b_comp / d_comp
+// components; interior nodes written):
+//  0 curl_helmholtz (operators.hpp:2305-2414): face -> edge on np z planes
+//    (3 np components each); in-plane differences / dx_level, the z
+//    difference between plane i and i - 1 (periodic) / dx_fine
+//  1 curl_helmholtz_real (:2059-2081): face -> edge, edge x and y zero
+//  2 curl_helmholtz_real with Uz (:2083-2119): edge x, y from the scalar b
+//  3 curl_transpose_helmholtz_complex_linear (:2272-2303): edge -> face x, y
+//    (d) and face z (e), scaled, plus the c scale cross terms
+//  4 nonlinear_linear_helm (:2534-2572): face a, edge b -> face x, y (d) and
+//    the z component (e) of the linearised convective term
+//  5 curl_transpose, two-dimensional branch (:2416-2453): edge scalar ->
+//    face x, y, scaled
+template<int OP>
+__global__ void helm_real_op_kernel(int nb, int np, double dx, double dx_fine, double c, double scale,
+                                    const double* __restrict__ a, int a_comp, const double* __restrict__ b,
+                                    int b_comp, double* __restrict__ d, int d_comp, double* __restrict__ e)
+{
+    const int N2 = nb * nb;
+    const size_t blk = blockIdx.x;
+    const double* A = a + blk * a_comp * N2;
+    const double* Bf = b ? b + blk * b_comp * N2 : nullptr;
+    double* D = d + blk * d_comp * N2;
+    double* Ef = e ? e + blk * N2 : nullptr;
+    const double fac = 1.0 / dx;
+    const int units = OP == 0 ? np : 1;
+    for (int q = threadIdx.x; q < units * N2; q += blockDim.x)
+    {
+        const int i = q / N2, p = q - i * N2;
+        const int x = p % nb, y = p / nb;
+        if (x == 0 || y == 0 || x == nb - 1 || y == nb - 1) continue;
+        auto at = [&](int k, int ox, int oy) { return A[(size_t)k * N2 + p + ox + oy * nb]; };
+        auto bt = [&](int k, int ox, int oy) { return Bf[(size_t)k * N2 + p + ox + oy * nb]; };
+        auto out = [&](int k) -> double& { return D[(size_t)k * N2 + p]; };
+        if (OP == 0)
+        {
+            // plane 0's z difference wraps to plane np - 1; its z component is
+            // written as two differences (the reference's i = 0 branch)
+            const int sep = np, im = i == 0 ? np - 1 : i - 1;
+            const int X = i, Y = sep + i, Z = 2 * sep + i;
+            out(X) = (at(Z, 0, 0) - at(Z, 0, -1)) / dx - (at(Y, 0, 0) - at(sep + im, 0, 0)) / dx_fine;
+            out(Y) = (at(X, 0, 0) - at(im, 0, 0)) / dx_fine - (at(Z, 0, 0) - at(Z, -1, 0)) / dx;
+            if (i > 0) out(Z) = (at(Y, 0, 0) - at(Y, -1, 0) - at(X, 0, 0) + at(X, 0, -1)) * fac;
+            else out(Z) = (at(Y, 0, 0) - at(Y, -1, 0)) / dx - (at(X, 0, 0) - at(X, 0, -1)) / dx;
+        }
+        else if (OP == 1 || OP == 2)
+        {
+            if (OP == 1)
+            {
+                out(0) = 0.0;
+                out(1) = 0.0;
+            }
+            else
+            {
+                out(0) = (bt(0, 0, 0) - bt(0, 0, -1)) * fac;
+                out(1) = (-bt(0, 0, 0) + bt(0, -1, 0)) * fac;
+            }
+            out(2) = (at(1, 0, 0) - at(1, -1, 0) - at(0, 0, 0) + at(0, 0, -1)) * fac;
+        }
+        else if (OP == 3)
+        {
+            const double f = fac * scale;
+            out(0) = (-at(2, 0, 0) + at(2, 0, 1)) * f;
+            out(1) = (at(2, 0, 0) - at(2, 1, 0)) * f;
+            Ef[p] = (-at(1, 0, 0) + at(1, 1, 0) + at(0, 0, 0) - at(0, 0, 1)) * f;
+            out(0) += at(1, 0, 0) * c * scale;
+            out(1) -= at(0, 0, 0) * c * scale;
+        }
+        else if (OP == 4)
+        {
+            out(0) = 0.25 * (-bt(2, 0, 0) * (at(1, 0, 0) + at(1, -1, 0)) - bt(2, 0, 1) * (at(1, 0, 1) + at(1, -1, 1)));
+            out(1) = 0.25 * (bt(2, 0, 0) * (at(0, 0, 0) + at(0, 0, -1)) + bt(2, 1, 0) * (at(0, 1, 0) + at(0, 1, -1)));
+            Ef[p] = 0.5 * (bt(0, 0, 0) * at(1, 0, 0) + bt(0, 0, 1) * at(1, 0, 1) - bt(1, 0, 0) * at(0, 0, 0) -
+                           bt(1, 1, 0) * at(0, 1, 0));
+        }
+        else
+        {
+            const double f = fac * scale;
+            out(0) = (-at(0, 0, 0) + at(0, 0, 1)) * f;
+            out(1) = (-at(0, 1, 0) + at(0, 0, 0)) * f;
+        }
+    }
+}
+
 int trapezoid_points(double c)
 {
     int n = 64;
@@ -416,6 +502,37 @@ void helm2d_nonlinear(Ctx& c, int nb, int n_blocks, int n_planes, const unsigned
     const UnitMask mask = unit_mask(n_planes, host_plane_mask);
     if (!n_blocks) return;
     helm_nonlinear_kernel<<<n_blocks, 256, 0, c.stream>>>(nb, n_planes, mask, dev_face, dev_edge, dev_dst);
+    c.launches += 1;
+    IBLGF_CUDA(cudaGetLastError());
+}
+
+void helm2d_real_op(Ctx& c, int op, int nb, int n_blocks, int np, double dx, double dx_fine, double cz, double scale,
+                    const double* a, int a_comp, const double* b, int b_comp, double* d, int d_comp, double* e)
+{
+    // components each operator reads or writes: a, b (0: unused), d, e (0/1)
+    static const int need[6][4] = {{3, 0, 3, 0}, {2, 0, 3, 0}, {2, 1, 3, 0}, {3, 0, 2, 1}, {2, 3, 2, 1}, {1, 0, 2, 0}};
+    if (op < 0 || op > 5 || nb < 3 || n_blocks < 0 || !(dx > 0.0) || (op == 0 && !(dx_fine > 0.0)))
+        throw Error(IBLGF_EINVAL, "bad Helmholtz real operator arguments");
+    if (op == 0 && (np < 1 || np > (1 << 20))) throw Error(IBLGF_EINVAL, "bad z plane count");
+    const int m = op == 0 ? np : 1;
+    const int* k = need[op];
+    if (a_comp < k[0] * m || d_comp < k[2] * m || (k[1] && b_comp < k[1]))
+        throw Error(IBLGF_EINVAL, "too few components for the operator");
+    if (!n_blocks) return;
+    if (!a || !d || (k[1] && !b) || (k[3] && !e)) throw Error(IBLGF_EINVAL, "null field");
+    auto go = [&](auto kfn) {
+        kfn<<<n_blocks, 256, 0, c.stream>>>(nb, np, dx, dx_fine, cz, scale, a, a_comp, k[1] ? b : nullptr,
+                                            k[1] ? b_comp : 0, d, d_comp, k[3] ? e : nullptr);
+    };
+    switch (op)
+    {
+        case 0: go(helm_real_op_kernel<0>); break;
+        case 1: go(helm_real_op_kernel<1>); break;
+        case 2: go(helm_real_op_kernel<2>); break;
+        case 3: go(helm_real_op_kernel<3>); break;
+        case 4: go(helm_real_op_kernel<4>); break;
+        default: go(helm_real_op_kernel<5>); break;
+    }
     c.launches += 1;
     IBLGF_CUDA(cudaGetLastError());
 }

@@ -45,7 +45,7 @@ EXPORTS = [
     "iblgf_ws_check", "iblgf_conv_block", "iblgf_conv_block_noalloc",
     "iblgf_kernel_launches", "iblgf_profile", "iblgf_profile_read", "iblgf_stats", "iblgf_stats_n", "iblgf_adapt", "iblgf_block_norms", "iblgf_ns_fields", "iblgf_ns_clean",
     "iblgf_ns_clean_leaf_correction_boundary",
-    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_get", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_helm2d_op_modes", "iblgf_helm2d_nonlinear", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
+    "iblgf_fma_peak", "iblgf_tc_mma_rate", "iblgf_helm2d_origin", "iblgf_helm2d_lgf", "iblgf_helm2d_get", "iblgf_helm2d_apply", "iblgf_helm2d_op", "iblgf_helm2d_op_modes", "iblgf_helm2d_nonlinear", "iblgf_helm2d_real_op", "iblgf_ge_direct", "iblgf_field_upload_leaves_async", "iblgf_wait_selftest", "iblgf_field_first_nonfinite",
     "iblgf_debug_fail_alloc", "iblgf_mac_variant", "iblgf_mac_tuning", "iblgf_domain_partition", "iblgf_domain_set_owner",
     "iblgf_fmm_apply_kernel", "iblgf_lgf_ge_get", "iblgf_op_apply_octants", "iblgf_field_upload_octants",
     "iblgf_field_download_octants",
@@ -134,6 +134,7 @@ def lib():
     L.iblgf_helm2d_op.argtypes = [vp, ci, ci, ci, ci, cd, cd, cd, vp, vp]
     L.iblgf_helm2d_op_modes.argtypes = [vp, ci, ci, ci, ci, vp, cd, cd, cd, vp, vp]
     L.iblgf_helm2d_nonlinear.argtypes = [vp, ci, ci, ci, vp, vp, vp, vp]
+    L.iblgf_helm2d_real_op.argtypes = [vp, ci, ci, ci, ci, cd, cd, cd, cd, vp, ci, vp, ci, vp, ci, vp]
     L.iblgf_ge_direct.argtypes = [vp, ci]
     L.iblgf_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.iblgf_field_first_nonfinite.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_longlong)]
@@ -829,6 +830,30 @@ class Solver:
                                                  None if mask is None else _p(mask),
                                                  ctypes.c_void_p(face.data_ptr()), ctypes.c_void_p(edge.data_ptr()),
                                                  ctypes.c_void_p(dst.data_ptr())))
+
+    HELM_REAL_OPS = {"curl_planes": 0, "curl_real": 1, "curl_real_uz": 2, "curl_transpose_linear": 3,
+                     "nonlinear_linear": 4, "curl_transpose_2d": 5}
+
+    def helm2d_real_op(self, op, a, d, b=None, e=None, n_planes=1, dx_level=1.0, dx_fine=1.0, c=0.0, scale=1.0):
+        """A real-valued Fourier-in-z family block operator on 2-D blocks
+        (torch CUDA float64 tensors [n_blocks][components][nb][nb]; the
+        operator reads a (and b) and writes d (and e, one component)):
+        curl_planes (curl_helmholtz on n_planes z planes), curl_real,
+        curl_real_uz (b: Uz), curl_transpose_linear (e: face z),
+        nonlinear_linear (a face, b edge; e: z), curl_transpose_2d."""
+        k = self.HELM_REAL_OPS[op]
+        ts = [t for t in (a, b, d, e) if t is not None]
+        self._cuda_f64(*ts)
+        nb = a.shape[-1]
+        for t in ts:
+            if t.dim() != 4 or t.shape[0] != a.shape[0] or tuple(t.shape[2:]) != (nb, nb):
+                raise IblgfError("the real operators take [n_blocks][components][nb][nb] tensors")
+        if e is not None and e.shape[1] != 1:
+            raise IblgfError("e holds one component")
+        ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+        self._check(lib().iblgf_helm2d_real_op(self.h, k, nb, a.shape[0], int(n_planes), float(dx_level),
+                                               float(dx_fine), float(c), float(scale), ptr(a), a.shape[1], ptr(b),
+                                               0 if b is None else b.shape[1], ptr(d), d.shape[1], ptr(e)))
 
     def tc_mma_rate(self, n):
         """SM clocks per tensor-core MMA (TF32, M = 128, K = 8, N = n)."""

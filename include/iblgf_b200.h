@@ -493,6 +493,27 @@ int iblgf_helm2d_op_modes(iblgf_ctx* ctx, int op, int nb, int n_blocks, int n_mo
  * written. n_planes <= 2048. */
 int iblgf_helm2d_nonlinear(iblgf_ctx* ctx, int nb, int n_blocks, int n_planes, const unsigned char* plane_mask,
                            const double* dev_face, const double* dev_edge, double* dev_dst);
+/* Real-valued block operators of the same family on 2-D blocks. Device
+ * fields of n_blocks blocks, [components][nb][nb] (x fastest), with the
+ * component counts given (an operator reads or writes the leading ones);
+ * interior nodes written. op:
+ *  0 curl_helmholtz (operators.hpp:2305-2414): dev_a face, dev_d edge, each
+ *    3 n_planes components (groups x, y, z, a component per z plane); the
+ *    in-plane differences over dx_level, the z difference of plane i with
+ *    plane i - 1 (plane 0 with n_planes - 1) over dx_fine;
+ *  1 curl_helmholtz_real (:2059-2081): face (2) -> edge (3), edge x, y zero;
+ *  2 curl_helmholtz_real with Uz (:2083-2119): face (2) and the scalar dev_b
+ *    (1) -> edge (3);
+ *  3 curl_transpose_helmholtz_complex_linear (:2272-2303): edge (3) -> face
+ *    x, y (dev_d, 2) and face z (dev_e, 1), times scale, with the c terms;
+ *  4 nonlinear_linear_helm (:2534-2572): face dev_a (2), edge dev_b (3) ->
+ *    dev_d (2) and dev_e (1);
+ *  5 curl_transpose, 2-D branch (:2416-2453): edge scalar (1) -> face (2),
+ *    times scale.
+ * dx_fine is read by op 0 only, c by op 3 only, scale by ops 3 and 5. */
+int iblgf_helm2d_real_op(iblgf_ctx* ctx, int op, int nb, int n_blocks, int n_planes, double dx_level, double dx_fine,
+                         double c, double scale, const double* dev_a, int a_comp, const double* dev_b, int b_comp,
+                         double* dev_d, int d_comp, double* dev_e);
 int iblgf_field_first_nonfinite(iblgf_ctx* ctx, int f, long long* index);
 int iblgf_debug_fail_alloc(long long after);
 

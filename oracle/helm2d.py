@@ -232,3 +232,60 @@ def nonlinear(face, edge, dst, n_planes, planes=None):
         dst[:, z, I, I] = 0.5 * (W(x, 0, 0) * U(y, 0, 0) + W(x, 0, 1) * U(y, 0, 1)
                                  - W(y, 0, 0) * U(x, 0, 0) - W(y, 1, 0) * U(x, 1, 0))
     return dst
+
+
+def real_op(op, a, d, b=None, e=None, n_planes=1, dx=1.0, dx_fine=1.0, c=0.0, scale=1.0):
+    """The real-valued family on 2-D blocks ([n_blocks][comp][NB][NB]; d, e
+    updated in place at the interior nodes):
+    curl_planes        curl_helmholtz, operators.hpp:2305-2414
+    curl_real          curl_helmholtz_real, :2059-2081
+    curl_real_uz       curl_helmholtz_real with Uz, :2083-2119
+    curl_transpose_linear  curl_transpose_helmholtz_complex_linear, :2272-2303
+    nonlinear_linear   nonlinear_linear_helm, :2534-2572
+    curl_transpose_2d  curl_transpose, two-dimensional branch, :2416-2453"""
+    nb = a.shape[-1]
+    I = slice(1, nb - 1)
+
+    def A(k, ox, oy):
+        return a[:, k, 1 + oy:nb - 1 + oy, 1 + ox:nb - 1 + ox]
+
+    def Bv(k, ox, oy):
+        return b[:, k, 1 + oy:nb - 1 + oy, 1 + ox:nb - 1 + ox]
+
+    fac = 1.0 / dx
+    if op == "curl_planes":
+        sep = n_planes
+        for i in range(sep):
+            im = sep - 1 if i == 0 else i - 1
+            X, Y, Z = i, sep + i, 2 * sep + i
+            d[:, X, I, I] = (A(Z, 0, 0) - A(Z, 0, -1)) / dx - (A(Y, 0, 0) - A(sep + im, 0, 0)) / dx_fine
+            d[:, Y, I, I] = (A(X, 0, 0) - A(im, 0, 0)) / dx_fine - (A(Z, 0, 0) - A(Z, -1, 0)) / dx
+            if i > 0:
+                d[:, Z, I, I] = (A(Y, 0, 0) - A(Y, -1, 0) - A(X, 0, 0) + A(X, 0, -1)) * fac
+            else:
+                d[:, Z, I, I] = (A(Y, 0, 0) - A(Y, -1, 0)) / dx - (A(X, 0, 0) - A(X, 0, -1)) / dx
+    elif op in ("curl_real", "curl_real_uz"):
+        if op == "curl_real":
+            d[:, 0, I, I] = 0.0
+            d[:, 1, I, I] = 0.0
+        else:
+            d[:, 0, I, I] = (Bv(0, 0, 0) - Bv(0, 0, -1)) * fac
+            d[:, 1, I, I] = (-Bv(0, 0, 0) + Bv(0, -1, 0)) * fac
+        d[:, 2, I, I] = (A(1, 0, 0) - A(1, -1, 0) - A(0, 0, 0) + A(0, 0, -1)) * fac
+    elif op == "curl_transpose_linear":
+        f = fac * scale
+        d[:, 0, I, I] = (-A(2, 0, 0) + A(2, 0, 1)) * f + A(1, 0, 0) * c * scale
+        d[:, 1, I, I] = (A(2, 0, 0) - A(2, 1, 0)) * f - A(0, 0, 0) * c * scale
+        e[:, 0, I, I] = (-A(1, 0, 0) + A(1, 1, 0) + A(0, 0, 0) - A(0, 0, 1)) * f
+    elif op == "nonlinear_linear":
+        d[:, 0, I, I] = 0.25 * (-Bv(2, 0, 0) * (A(1, 0, 0) + A(1, -1, 0)) - Bv(2, 0, 1) * (A(1, 0, 1) + A(1, -1, 1)))
+        d[:, 1, I, I] = 0.25 * (Bv(2, 0, 0) * (A(0, 0, 0) + A(0, 0, -1)) + Bv(2, 1, 0) * (A(0, 1, 0) + A(0, 1, -1)))
+        e[:, 0, I, I] = 0.5 * (Bv(0, 0, 0) * A(1, 0, 0) + Bv(0, 0, 1) * A(1, 0, 1)
+                               - Bv(1, 0, 0) * A(0, 0, 0) - Bv(1, 1, 0) * A(0, 1, 0))
+    elif op == "curl_transpose_2d":
+        f = fac * scale
+        d[:, 0, I, I] = (-A(0, 0, 0) + A(0, 0, 1)) * f
+        d[:, 1, I, I] = (-A(0, 1, 0) + A(0, 0, 0)) * f
+    else:
+        raise ValueError(op)
+    return d

@@ -162,3 +162,48 @@ def test_point_evaluation_matches_the_table(g, c):
     ref = t[np.abs(nm[:, 1]), np.abs(nm[:, 0])]
     assert np.abs(vals - ref).max() < 1e-14 * np.abs(ref).max()
     assert g.helm2d_get(c, np.zeros((0, 2), np.int32)).size == 0
+
+
+# (a components, b components or 0, d components, e used) per real operator
+REAL_SHAPES = {"curl_planes": (15, 0, 15, False), "curl_real": (3, 0, 3, False), "curl_real_uz": (2, 1, 3, False),
+               "curl_transpose_linear": (3, 0, 2, True), "nonlinear_linear": (2, 3, 2, True),
+               "curl_transpose_2d": (1, 0, 2, False)}
+
+
+@pytest.mark.parametrize("op", sorted(REAL_SHAPES))
+def test_real_operators_match_oracle(g, op):
+    """The real-valued family (curl_helmholtz on z planes, curl_helmholtz_real,
+    curl_transpose_helmholtz_complex_linear, nonlinear_linear_helm, the 2-D
+    curl_transpose) against their restatement; components the operator does
+    not write keep their values."""
+    import torch
+    rng = np.random.default_rng(12)
+    na, nbc, nd, use_e = REAL_SHAPES[op]
+    nb, nblk, dx, dxf, npl = 12, 3, 0.3, 0.05, 5
+    a = rng.standard_normal((nblk, na, nb, nb))
+    b = rng.standard_normal((nblk, nbc, nb, nb)) if nbc else None
+    d0 = rng.standard_normal((nblk, nd, nb, nb))
+    e0 = rng.standard_normal((nblk, 1, nb, nb)) if use_e else None
+    kw = dict(n_planes=npl, dx=dx, dx_fine=dxf, c=0.7, scale=1.3)
+    d_ref = H.real_op(op, a, d0.copy(), b=b, e=None if e0 is None else e0.copy(), **kw)
+    cu = lambda x: None if x is None else torch.tensor(x, device="cuda")
+    d, e = cu(d0), cu(e0)
+    g.helm2d_real_op(op, cu(a), d, b=cu(b), e=e, n_planes=npl, dx_level=dx, dx_fine=dxf, c=0.7, scale=1.3)
+    g.synchronize()
+    assert np.abs(d.cpu().numpy() - d_ref).max() < 1e-13 * np.abs(d_ref).max()
+    if use_e:
+        e_ref = e0.copy()
+        H.real_op(op, a, d0.copy(), b=b, e=e_ref, **kw)
+        assert np.abs(e.cpu().numpy() - e_ref).max() < 1e-13 * np.abs(e_ref).max()
+
+
+def test_real_operators_check_their_arguments(g):
+    import torch
+    t = torch.zeros((2, 2, 8, 8), dtype=torch.float64, device="cuda")
+    with pytest.raises(B.IblgfError):
+        g.helm2d_real_op("curl_real", t, t.clone())  # the edge output needs 3 components
+    with pytest.raises(B.IblgfError):
+        g.helm2d_real_op("curl_real_uz", t, torch.zeros((2, 3, 8, 8), dtype=torch.float64, device="cuda"))  # no Uz
+    with pytest.raises(B.IblgfError):
+        g.helm2d_real_op("curl_planes", torch.zeros((2, 6, 8, 8), dtype=torch.float64, device="cuda"),
+                         torch.zeros((2, 6, 8, 8), dtype=torch.float64, device="cuda"), n_planes=3)  # 9 needed

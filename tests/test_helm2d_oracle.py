@@ -115,3 +115,51 @@ def test_mode_selections_follow_the_reference_forms():
         fourier_z.refined_modes(6, 2)  # the reference throws when 2^r does not divide N_modes
     assert list(fourier_z.one_mode_planes(2, 3)) == [6, 7, 8]
     assert list(fourier_z.refined_planes(12, 2)) == [0, 4, 8]
+
+
+def test_real_operators_agree_with_the_complex_and_plane_forms():
+    """The real-valued restatements against the ones pinned above:
+    curl_helmholtz_real with Uz is the complex curl of mode 0 (real parts);
+    curl_transpose_helmholtz_complex_linear at c = 0 is mode 0's complex
+    curl_transpose; curl_helmholtz on fields constant along z is the in-plane
+    curl of every plane; nonlinear_linear_helm is the plane convective term
+    with u_z = 0; the 2-D curl_transpose is divergence-free."""
+    rng = np.random.default_rng(9)
+    nb, nblk, dx = 10, 2, 0.4
+    I = slice(1, nb - 1)
+    # complex layout, one mode: x_re, x_im, y_re, y_im, z_re, z_im
+    fc = rng.standard_normal((nblk, 6, nb, nb))
+    cc = H.helm_op("curl", fc, np.zeros((nblk, 6, nb, nb)), 1, dx, 1.0)
+    r = H.real_op("curl_real_uz", fc[:, [0, 2]], np.zeros((nblk, 3, nb, nb)), b=fc[:, [4]], dx=dx)
+    assert np.abs(r[:, :, I, I] - cc[:, [0, 2, 4]][:, :, I, I]).max() < 1e-12
+    r0 = H.real_op("curl_real", fc[:, [0, 2]], np.ones((nblk, 3, nb, nb)), dx=dx)
+    assert (r0[:, :2, I, I] == 0).all() and np.array_equal(r0[:, 2, I, I], r[:, 2, I, I])
+    ct = H.helm_op("curl_transpose", fc, np.zeros((nblk, 6, nb, nb)), 1, dx, 1.0, 0.6)
+    d = np.zeros((nblk, 2, nb, nb))
+    e = np.zeros((nblk, 1, nb, nb))
+    H.real_op("curl_transpose_linear", fc[:, [0, 2, 4]], d, e=e, dx=dx, c=0.0, scale=0.6)
+    assert np.abs(d[:, :, I, I] - ct[:, [0, 2]][:, :, I, I]).max() < 1e-12
+    assert np.abs(e[:, 0, I, I] - ct[:, 4, I, I]).max() < 1e-12
+    # planes: the same 2-D field on every plane -> no z differences
+    npl = 4
+    f2 = rng.standard_normal((nblk, 3, nb, nb))
+    planes = np.repeat(f2, npl, axis=1)  # groups x, y, z of npl planes each
+    cp = H.real_op("curl_planes", planes, np.zeros((nblk, 3 * npl, nb, nb)), n_planes=npl, dx=dx, dx_fine=0.1)
+    ref = H.real_op("curl_real_uz", f2[:, :2], np.zeros((nblk, 3, nb, nb)), b=f2[:, [2]], dx=dx)
+    for i in range(npl):
+        got = cp[:, [i, npl + i, 2 * npl + i]]
+        assert np.abs(got[:, :, I, I] - ref[:, :, I, I]).max() < 1e-12
+    # linearised convective term = the plane form with u_z = 0
+    u = rng.standard_normal((nblk, 3, nb, nb))
+    u[:, 2] = 0.0
+    w = rng.standard_normal((nblk, 3, nb, nb))
+    full = H.nonlinear(u, w, np.zeros((nblk, 3, nb, nb)), 1)
+    d = np.zeros((nblk, 2, nb, nb))
+    e = np.zeros((nblk, 1, nb, nb))
+    H.real_op("nonlinear_linear", u[:, :2], d, b=w, e=e)
+    assert np.abs(d[:, :, I, I] - full[:, :2, I, I]).max() < 1e-13
+    assert np.abs(e[:, 0, I, I] - full[:, 2, I, I]).max() < 1e-13
+    s = rng.standard_normal((nblk, 1, nb, nb))
+    f = H.real_op("curl_transpose_2d", s, np.zeros((nblk, 2, nb, nb)), dx=dx, scale=0.5)
+    div = f[:, 0, 1:-2, 2:-1] - f[:, 0, 1:-2, 1:-2] + f[:, 1, 2:-1, 1:-2] - f[:, 1, 1:-2, 1:-2]
+    assert np.abs(div[:, 1:, 1:]).max() < 1e-12
