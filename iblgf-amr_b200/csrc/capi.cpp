@@ -57,6 +57,7 @@ double measure_fma_peak(Ctx& c, int precision);
 double measure_tc_rate(Ctx& c, int n);
 double helm2d_origin(double c);
 void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out);
+void helm2d_check_table(double cz, int nx, int ny);
 void helm2d_points(Ctx& c, double cz, int count, const int* host_nm, double* host_out);
 void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale);
 void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, double lz, double scale,
@@ -738,7 +739,8 @@ int iblgf_helm2d_origin(double c, double* out)
 int iblgf_helm2d_lgf(iblgf_ctx* x, double c, int nx, int ny, double* host_out)
 {
     return guard(x, [&](iblgf_b200::Ctx& cx) {
-        if (!host_out || nx < 1 || ny < 1) throw iblgf_b200::Error(IBLGF_EINVAL, "bad table arguments");
+        if (!host_out) throw iblgf_b200::Error(IBLGF_EINVAL, "bad table arguments");
+        iblgf_b200::helm2d_check_table(c, nx, ny);
         iblgf_b200::DevBuf<double> d;
         d.alloc((size_t)nx * ny);
         iblgf_b200::helm2d_table(cx, c, nx, ny, d.p);
@@ -755,7 +757,8 @@ int iblgf_helm2d_get(iblgf_ctx* x, double c, int n, const int* host_nm, double* 
 int iblgf_helm2d_apply(iblgf_ctx* x, double c, int nx, int ny, const double* host_f, double* host_u, double scale)
 {
     return guard(x, [&](iblgf_b200::Ctx& cx) {
-        if (!host_f || !host_u || nx < 1 || ny < 1) throw iblgf_b200::Error(IBLGF_EINVAL, "bad arguments");
+        if (!host_f || !host_u || nx < 1 || ny < 1 || nx > 6144 || ny > 65535)
+            throw iblgf_b200::Error(IBLGF_EINVAL, "bad arguments (1 <= nx <= 6144, 1 <= ny <= 65535)");
         const size_t n = (size_t)nx * ny;
         iblgf_b200::DevBuf<double> f, u;
         f.alloc(n);

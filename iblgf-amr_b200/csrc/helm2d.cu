@@ -434,9 +434,15 @@ void launch_lgf(Ctx& c, double cz, int nx, int ny, const int* dev_nm, int extent
 }
 }  // namespace
 
-void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
+void helm2d_check_table(double cz, int nx, int ny)
 {
     if (!(cz >= 0.0) || nx < 1 || ny < 1) throw Error(IBLGF_EINVAL, "need c >= 0 and a non-empty table");
+    if ((long long)nx * ny > (1ll << 28)) throw Error(IBLGF_EINVAL, "the table holds at most 2^28 entries");
+}
+
+void helm2d_table(Ctx& c, double cz, int nx, int ny, double* dev_out)
+{
+    helm2d_check_table(cz, nx, ny);
     launch_lgf(c, cz, nx, ny, nullptr, std::max(nx, ny), dev_out);
 }
 
@@ -540,6 +546,8 @@ void helm2d_real_op(Ctx& c, int op, int nb, int n_blocks, int np, double dx, dou
 void helm2d_apply(Ctx& c, double cz, int nx, int ny, const double* dev_f, double* dev_u, double scale)
 {
     if (nx > 6144) throw Error(IBLGF_EINVAL, "the uniform 2-D solve takes at most 6144 cells along x");
+    if (ny > 65535) throw Error(IBLGF_EINVAL, "the uniform 2-D solve takes at most 65535 cells along y");
+    helm2d_check_table(cz, nx, ny);
     DevBuf<double> table;
     table.alloc((size_t)nx * ny);
     helm2d_table(c, cz, nx, ny, table.p);

@@ -744,7 +744,9 @@ class Solver:
 
     def helm2d_lgf(self, c, nx, ny):
         """2-D Helmholtz LGF get(n, m) (lgf::Helmholtz<2>) for 0 <= n < nx,
-        0 <= m < ny, as an (ny, nx) array."""
+        0 <= m < ny, as an (ny, nx) array (at most 2^28 entries)."""
+        if not (0 < int(nx) and 0 < int(ny) and int(nx) * int(ny) <= 1 << 28):
+            raise IblgfError("the table holds 1 .. 2^28 entries")
         out = np.zeros((ny, nx))
         self._check(lib().iblgf_helm2d_lgf(self.h, float(c), int(nx), int(ny), _p(out)))
         return out

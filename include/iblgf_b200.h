@@ -452,7 +452,8 @@ int iblgf_wait_selftest(iblgf_ctx* ctx, long long polls);
  * with c the level's c_level).
  * iblgf_helm2d_apply: host_u += scale * sum_j get(i - j) host_f[j] over a
  * uniform nx x ny cell grid (x fastest; every pair, the exact unbounded
- * solution of (Delta_h - c^2) u = f on that support); nx <= 6144.
+ * solution of (Delta_h - c^2) u = f on that support); nx <= 6144, ny <= 65535.
+ * Tables hold at most 2^28 entries.
  * The 2-D quadtree FMM that applies the kernel on an adaptive mesh is not
  * part of this library. */
 int iblgf_helm2d_origin(double c, double* out);

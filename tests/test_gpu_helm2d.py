@@ -207,3 +207,16 @@ def test_real_operators_check_their_arguments(g):
     with pytest.raises(B.IblgfError):
         g.helm2d_real_op("curl_planes", torch.zeros((2, 6, 8, 8), dtype=torch.float64, device="cuda"),
                          torch.zeros((2, 6, 8, 8), dtype=torch.float64, device="cuda"), n_planes=3)  # 9 needed
+
+
+def test_table_and_solve_extents_are_checked(g):
+    """Oversized requests are refused before anything is allocated or launched."""
+    one = np.zeros(1)
+    # 2^29 entries: refused by the library before it allocates or writes
+    assert B.lib().iblgf_helm2d_lgf(g.h, 0.5, 1 << 15, 1 << 14, one.ctypes.data_as(B.ctypes.c_void_p)) == B.EINVAL
+    with pytest.raises(B.IblgfError):
+        g.helm2d_lgf(0.5, 1 << 15, 1 << 14)
+    with pytest.raises(B.IblgfError):
+        g.helm2d_lgf(-1.0, 4, 4)
+    with pytest.raises(B.IblgfError):
+        g.helm2d_apply(0.5, np.zeros((4, 6145)))
