@@ -466,6 +466,14 @@ void helm2d_points(Ctx& c, double cz, int count, const int* host_nm, double* hos
     IBLGF_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+// Blocks are nb x nb with nb <= 4096, and one launch indexes at most
+// 2^31 - 1 (unit, node) pairs.
+void check_block_extent(int nb, long long units)
+{
+    if (nb < 3 || nb > 4096) throw Error(IBLGF_EINVAL, "block extent outside 3 .. 4096");
+    if (units * nb * nb > 0x7fffffffll) throw Error(IBLGF_EINVAL, "too many (plane, node) pairs per block");
+}
+
 UnitMask unit_mask(int n_units, const unsigned char* host_mask)
 {
     if (n_units < 1 || n_units > UnitMask::kMax)
@@ -481,6 +489,7 @@ void helm2d_op(Ctx& c, int op, int nb, int n_blocks, int n_modes, double dx, dou
 {
     if (op < 0 || op > 4 || nb < 3 || n_blocks < 0 || n_modes < 1 || !(dx > 0.0) || !(lz > 0.0))
         throw Error(IBLGF_EINVAL, "bad Helmholtz operator arguments");
+    check_block_extent(nb, 6ll * n_modes);  // components per block of the widest field
     const UnitMask mask = unit_mask(n_modes, host_mode_mask);
     if (!n_blocks) return;
     const int sep = 2 * n_modes;
@@ -505,6 +514,7 @@ void helm2d_nonlinear(Ctx& c, int nb, int n_blocks, int n_planes, const unsigned
                       const double* dev_face, const double* dev_edge, double* dev_dst)
 {
     if (nb < 3 || n_blocks < 0) throw Error(IBLGF_EINVAL, "bad nonlinear term arguments");
+    check_block_extent(nb, 3ll * n_planes);
     const UnitMask mask = unit_mask(n_planes, host_plane_mask);
     if (!n_blocks) return;
     helm_nonlinear_kernel<<<n_blocks, 256, 0, c.stream>>>(nb, n_planes, mask, dev_face, dev_edge, dev_dst);
@@ -520,6 +530,7 @@ void helm2d_real_op(Ctx& c, int op, int nb, int n_blocks, int np, double dx, dou
     if (op < 0 || op > 5 || nb < 3 || n_blocks < 0 || !(dx > 0.0) || (op == 0 && !(dx_fine > 0.0)))
         throw Error(IBLGF_EINVAL, "bad Helmholtz real operator arguments");
     if (op == 0 && (np < 1 || np > (1 << 20))) throw Error(IBLGF_EINVAL, "bad z plane count");
+    check_block_extent(nb, op == 0 ? 3ll * np : 3ll);
     const int m = op == 0 ? np : 1;
     const int* k = need[op];
     if (a_comp < k[0] * m || d_comp < k[2] * m || (k[1] && b_comp < k[1]))
