@@ -163,3 +163,18 @@ def test_real_operators_agree_with_the_complex_and_plane_forms():
     f = H.real_op("curl_transpose_2d", s, np.zeros((nblk, 2, nb, nb)), dx=dx, scale=0.5)
     div = f[:, 0, 1:-2, 2:-1] - f[:, 0, 1:-2, 1:-2] + f[:, 1, 2:-1, 1:-2] - f[:, 1, 1:-2, 1:-2]
     assert np.abs(div[:, 1:, 1:]).max() < 1e-12
+
+
+def test_mode_and_plane_masks_are_bytes_per_unit():
+    """The host side of the mode / plane selections: indices or a boolean
+    sequence become one byte per unit; out-of-range indices and wrong-length
+    boolean masks are refused before the library is called."""
+    import iblgf_b200 as B
+    assert B.Solver._unit_mask(4, None) is None
+    assert B.Solver._unit_mask(4, [2]).tolist() == [0, 0, 1, 0]
+    assert B.Solver._unit_mask(4, range(2)).tolist() == [1, 1, 0, 0]
+    assert B.Solver._unit_mask(4, np.array([True, False, False, True])).tolist() == [1, 0, 0, 1]
+    assert B.Solver._unit_mask(3, []).tolist() == [0, 0, 0]
+    for bad in ([4], [-1], np.array([True, False])):
+        with pytest.raises(B.IblgfError):
+            B.Solver._unit_mask(4, bad)
