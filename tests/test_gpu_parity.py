@@ -1,6 +1,6 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
 
-Tolerances: FP64 plain path <= 1e-12 relative L-inf (north-star parity bar);
+Tolerances: FP64 plain path <= 1e-12 relative L-inf (the FP64 parity bar);
 FP32 FFT/MAC path <= 1e-5 relative L-inf; integer data (keys, lists, masks)
 bit-exact.
 """
