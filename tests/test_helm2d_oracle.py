@@ -178,3 +178,23 @@ def test_mode_and_plane_masks_are_bytes_per_unit():
     for bad in ([4], [-1], np.array([True, False])):
         with pytest.raises(B.IblgfError):
             B.Solver._unit_mask(4, bad)
+
+
+@pytest.mark.parametrize("c", [0.5, 1.2])
+def test_lgf_matches_a_direct_solve_of_the_lattice_equation(c):
+    """Independent of the quadrature: (Delta_h - c^2) g = delta solved as a
+    sparse linear system on [-L, L]^2 with g = 0 outside (the kernel decays
+    like e^{-c r}, so L = 90 leaves < 1e-15 of the kernel at the edge)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    L = 90
+    n = 2 * L + 1
+    one = np.ones(n)
+    d2 = sp.diags([one[:-1], -2 * one, one[:-1]], [-1, 0, 1])
+    eye = sp.identity(n)
+    A = (sp.kron(eye, d2) + sp.kron(d2, eye) - c * c * sp.identity(n * n)).tocsc()
+    rhs = np.zeros(n * n)
+    rhs[L * n + L] = 1.0
+    g = spl.spsolve(A, rhs).reshape(n, n)
+    for (a, b) in [(0, 0), (1, 0), (3, 2), (7, 1), (12, 9)]:
+        assert abs(g[L + b, L + a] - H.lgf(a, b, c)) < 1e-13 * abs(g[L, L])
