@@ -138,6 +138,8 @@ def main():
     ap.add_argument("--mac-variant", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
                     help="pin the sibling-group MAC variant (-1: autotune per plan)")
     ap.add_argument("--ib-only", action="store_true", help="only the immersed-boundary NS step measurement")
+    ap.add_argument("--helm-only", action="store_true",
+                    help="only the Fourier-in-z 2-D block operators (bandwidth of each)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -188,6 +190,10 @@ def main():
     if args.ib_only:
         if rank == 0:
             print(json.dumps({"ns_step_ib": ib_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
+        return
+    if args.helm_only:
+        if rank == 0:
+            print(json.dumps({"helm_ops": helm_bench(B, stream, local, args.steps, args.warmup)}), flush=True)
         return
     if args.batch_only:
         if rank == 0:
@@ -463,6 +469,53 @@ def ns_bench(B, stream, device, steps, warmup):
                 "dt": dt, "Re": case.Re, "steps": steps, "warmup": warmup,
                 "speedup_fp32_vs_fp64": out["ms_per_step_fp64"] / out["ms_per_step_fp32"],
                 "rel_linf_u_fp32_vs_fp64": float(np.abs(res["fp32"] - res["fp64"]).max() / np.abs(res["fp64"]).max())})
+    return out
+
+
+def helm_bench(B, stream, device, steps, warmup):
+    """The Fourier-in-z family of block operators on 2-D blocks, each timed
+    with CUDA events over `steps` launches after `warmup`, on fields larger
+    than L2 (2048 blocks of 18^2 nodes; 16 z modes, i.e. 32 real components
+    per scalar field, or 48 z planes). Achieved bandwidth counts every input
+    component read once and every output component written once per launch
+    (the one-cell neighbours come from cache)."""
+    import torch
+    g = B.Solver((-32, -32, -32), (64, 64, 64), 16, 1.0, [((-16, -16, -16), (32, 32, 32))], device=device,
+                 stream=stream.cuda_stream)
+    hbm, kind = peaks()
+    nblk, nb, nm, npl = 2048, 18, 16, 48
+    sep, per = 2 * nm, nblk * nb * nb * 8
+    gen = torch.Generator(device="cuda").manual_seed(7)
+
+    def rnd(c):
+        return torch.randn((nblk, c, nb, nb), dtype=torch.float64, device="cuda", generator=gen)
+
+    cases = []
+    for op, cin, cout in (("laplace", sep, sep), ("gradient", sep, 3 * sep), ("divergence", 3 * sep, sep),
+                          ("curl", 3 * sep, 3 * sep), ("curl_transpose", 3 * sep, 3 * sep)):
+        src, dst = rnd(cin), rnd(cout)
+        cases.append((op + "_helmholtz_complex", (cin + cout) * per,
+                      lambda op=op, src=src, dst=dst: g.helm2d_op(op, src, dst, nm, 0.1, 2.0, 1.0)))
+    face, edge, dnl = rnd(3 * npl), rnd(3 * npl), rnd(3 * npl)
+    cases.append(("nonlinear_helmholtz", 9 * npl * per, lambda: g.helm2d_nonlinear(face, edge, dnl, npl)))
+    cases.append(("curl_helmholtz_planes", 6 * npl * per,
+                  lambda: g.helm2d_real_op("curl_planes", face, dnl, n_planes=npl, dx_level=0.1, dx_fine=0.05)))
+    torch.cuda.synchronize()
+    out = {}
+    for name, nbytes, fn in cases:
+        for _ in range(warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / steps * 1e-3
+        out[name] = {"ms": t * 1e3, "bytes": nbytes, "GB/s": nbytes / t / 1e9, "frac_of_hbm": nbytes / t / 1e9 / hbm}
+    out.update({"workload": "2048 blocks of 18^2 nodes, 16 z modes (complex operators) or 48 z planes",
+                "hbm_gbs": hbm, "hbm_peak": kind, "steps": steps, "warmup": warmup})
+    g.close()
     return out
 
 
