@@ -149,8 +149,8 @@ __global__ void helm2d_apply_kernel(int nx, int ny, const double* __restrict__ t
 // x fastest; a scalar field has sep = 2 N_modes components (mode i: real 2i,
 // imaginary 2i+1), a vector field three groups of sep (x, y, z); the z
 // derivative of mode i is multiplication by i omega_i, omega_i = 2 pi i / lz.
-// One CTA per block, threads over the interior nodes (1 .. NB-2 per axis);
-// buffers are read, not written. The mask selects the modes written: all of
+// One CTA per block, threads over (mode, interior node) pairs (nodes
+// 1 .. NB-2 per axis); buffers are read, not written. The mask selects the modes written: all of
 // them for the forms above, one for the _oneMode forms (:1548, :1620, :1801,
 // :2017, :2224), the first N_modes / 2^r for the _refined forms (:1653,
 // :1839, :2125), any set for the ModesBool forms (:1889, :1931); the
@@ -165,15 +165,18 @@ __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, d
     const double* s = src + (size_t)blockIdx.x * in_comp * N2;
     double* d = dst + (size_t)blockIdx.x * out_comp * N2;
     const double fac = 1.0 / dx;
-    for (int p = threadIdx.x; p < N2; p += blockDim.x)
+    // one thread per (mode, node): it owns every output component of that
+    // mode at that node (consecutive threads take consecutive nodes)
+    for (int q = threadIdx.x; q < n_modes * N2; q += blockDim.x)
     {
+        const int mode = q / N2, p = q - mode * N2;
         const int x = p % nb, y = p / nb;
-        if (x == 0 || y == 0 || x == nb - 1 || y == nb - 1) continue;
+        if (x == 0 || y == 0 || x == nb - 1 || y == nb - 1 || !mask.on(mode)) continue;
         auto at = [&](int c, int ox, int oy) { return s[(size_t)c * N2 + p + ox + oy * nb]; };
         auto out = [&](int c) -> double& { return d[(size_t)c * N2 + p]; };
-        for (int i = 0; i < sep; ++i)
+        const int re = 2 * mode, im = 2 * mode + 1;
+        for (int i = re; i <= im; ++i)
         {
-            if (!mask.on(i >> 1)) continue;
             if (OP == 0)
                 out(i) = fac * fac * (-4.0 * at(i, 0, 0) + at(i, 0, -1) + at(i, 0, 1) + at(i, -1, 0) + at(i, 1, 0));
             else if (OP == 1)
@@ -197,11 +200,8 @@ __global__ void helm_op_kernel(int nb, int n_modes, int in_comp, int out_comp, d
                 out(2 * sep + i) = f * (-at(sep + i, 0, 0) + at(sep + i, 1, 0) + at(i, 0, 0) - at(i, 0, 1));
             }
         }
-        for (int i = 0; i < n_modes; ++i)
         {
-            if (!mask.on(i)) continue;
-            const double om = 2.0 * M_PI * i / lz;
-            const int re = 2 * i, im = 2 * i + 1;
+            const double om = 2.0 * M_PI * mode / lz;
             if (OP == 0)
             {
                 out(re) -= at(re, 0, 0) * om * om;
