@@ -800,6 +800,8 @@ class Solver:
         modes: None (all modes, the plain forms), the selected mode indices
         (a single one: the _oneMode forms; range(n_modes >> r): the _refined
         forms) or a boolean sequence (the ModesBool forms)."""
+        if op not in self.HELM_OPS:
+            raise IblgfError("unknown Helmholtz operator %r (one of %s)" % (op, ", ".join(self.HELM_OPS)))
         self._cuda_f64(src, dst)
         k = self.HELM_OPS[op]
         sep = 2 * int(n_modes)
@@ -843,6 +845,8 @@ class Solver:
         curl_planes (curl_helmholtz on n_planes z planes), curl_real,
         curl_real_uz (b: Uz), curl_transpose_linear (e: face z),
         nonlinear_linear (a face, b edge; e: z), curl_transpose_2d."""
+        if op not in self.HELM_REAL_OPS:
+            raise IblgfError("unknown Helmholtz operator %r (one of %s)" % (op, ", ".join(self.HELM_REAL_OPS)))
         k = self.HELM_REAL_OPS[op]
         ts = [t for t in (a, b, d, e) if t is not None]
         self._cuda_f64(*ts)

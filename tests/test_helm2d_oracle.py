@@ -198,3 +198,11 @@ def test_lgf_matches_a_direct_solve_of_the_lattice_equation(c):
     g = spl.spsolve(A, rhs).reshape(n, n)
     for (a, b) in [(0, 0), (1, 0), (3, 2), (7, 1), (12, 9)]:
         assert abs(g[L + b, L + a] - H.lgf(a, b, c)) < 1e-13 * abs(g[L, L])
+
+
+def test_unknown_operator_names_are_refused():
+    import iblgf_b200 as B
+    with pytest.raises(B.IblgfError):
+        B.Solver.helm2d_op(None, "grad", None, None, 1, 1.0, 1.0)
+    with pytest.raises(B.IblgfError):
+        B.Solver.helm2d_real_op(None, "curl_helmholtz", None, None)
