@@ -201,8 +201,13 @@ def test_lgf_matches_a_direct_solve_of_the_lattice_equation(c):
 
 
 def test_unknown_operator_names_are_refused():
+    """Checked before any tensor or device is touched (a stand-in for the
+    solver carries only the operator tables)."""
+    import types
+
     import iblgf_b200 as B
+    stub = types.SimpleNamespace(HELM_OPS=B.Solver.HELM_OPS, HELM_REAL_OPS=B.Solver.HELM_REAL_OPS)
     with pytest.raises(B.IblgfError):
-        B.Solver.helm2d_op(None, "grad", None, None, 1, 1.0, 1.0)
+        B.Solver.helm2d_op(stub, "grad", None, None, 1, 1.0, 1.0)
     with pytest.raises(B.IblgfError):
-        B.Solver.helm2d_real_op(None, "curl_helmholtz", None, None)
+        B.Solver.helm2d_real_op(stub, "curl_helmholtz", None, None)
